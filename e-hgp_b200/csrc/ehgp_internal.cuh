@@ -1,0 +1,159 @@
+// Internal declarations shared by the sm_100a translation units of the
+// MorseHGP3D product path.  Nothing here crosses the C ABI (include/ehgp.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ehgp.h"
+
+#ifndef __CUDACC__
+#error "ehgp_internal.cuh is CUDA-only"
+#endif
+
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ != 1000)
+#error "this library is built for sm_100a only"
+#endif
+
+namespace ehgp {
+
+// ---- device error word ---------------------------------------------------
+// Kernels never trap: they OR a flag into the context's error word and skip
+// the offending access; the host reads the word once per call.
+enum DeviceErrorBit : uint32_t {
+  kErrNonFinite = 1u << 0,
+  kErrDuplicate = 1u << 1,
+  kErrNumericRange = 1u << 2,
+  kErrInternal = 1u << 3,
+  kErrTimeout = 1u << 4,
+  kErrCapacity = 1u << 5,
+};
+
+constexpr uint32_t kInvalid32 = 0xffffffffu;
+constexpr int kMortonBitsPerAxis = 21;
+constexpr uint64_t kMortonGrid = uint64_t{1} << kMortonBitsPerAxis;
+
+// ---- binary64 total order -------------------------------------------------
+// Same map as exact::binary64_total_order_key (include/morsehgp3d/exact/binary64.hpp:23-29)
+// applied to canonical words (-0 already replaced by +0).
+__host__ __device__ __forceinline__ uint64_t order_key(uint64_t bits) {
+  return (bits >> 63) ? ~bits : (bits ^ (uint64_t{1} << 63));
+}
+
+// ---- radix sort of u32 indices by an indirect 64-bit key -----------------
+struct RadixScratch {
+  uint32_t* counts = nullptr;   // [256 * max_tiles]
+  uint32_t* state = nullptr;    // per pass: [cur_in, trivial] pairs, kMaxPasses + 1 entries
+  uint32_t max_tiles = 0;
+};
+constexpr int kRadixThreads = 256;
+constexpr int kRadixItems = 4;
+constexpr int kRadixTile = kRadixThreads * kRadixItems;
+constexpr int kRadixMaxPasses = 32;
+
+// Key source for one sorting stage: key(v) = order_key(words[v]) when
+// `order` is set, else words[v].
+struct IndirectKey {
+  const uint64_t* words;
+  int order;
+};
+
+// Sorts vals (length n, ping-pong buffers vals0/vals1) stably by the keys of
+// `stages` applied least-significant stage first, 8 bits per pass.  Returns
+// nothing on the host: the buffer holding the result is recorded in
+// scratch.state at index `passes` (0 -> vals0, 1 -> vals1).  The number of
+// passes issued is returned.
+int radix_sort_indirect(cudaStream_t stream, uint32_t n, uint32_t* vals0, uint32_t* vals1,
+                        const IndirectKey* stages, const int* stage_bits, int stage_count,
+                        RadixScratch& scratch, uint64_t* launches);
+
+__device__ __forceinline__ const uint32_t* radix_result(const uint32_t* state, int passes,
+                                                        const uint32_t* vals0, const uint32_t* vals1) {
+  return state[2 * passes] ? vals1 : vals0;
+}
+
+// ---- context -----------------------------------------------------------------
+struct LbvhBuffers {
+  // input staging
+  double* xyz_in = nullptr;        // [3*max_n] interleaved input (binary64)
+  float* xyz_in_f32 = nullptr;     // [3*max_n] interleaved input (binary32)
+  uint64_t* cin = nullptr;         // [3*max_n] canonical words by input index, axis-major
+  // canonical cloud (by PointId)
+  double* px = nullptr;            // [max_n]
+  double* py = nullptr;
+  double* pz = nullptr;
+  uint32_t* source_index = nullptr;// [max_n]
+  // Morton stage
+  uint64_t* code = nullptr;        // [max_n] code by PointId
+  uint32_t* vals0 = nullptr;       // [max_n]
+  uint32_t* vals1 = nullptr;       // [max_n]
+  uint32_t* leaf_pid = nullptr;    // [max_n] PointId at sorted position
+  uint64_t* leaf_code = nullptr;   // [max_n]
+  uint32_t* group_of = nullptr;    // [max_n] scan of heads
+  uint32_t* block_sums = nullptr;  // scan partials
+  uint32_t* gstart = nullptr;      // [max_n + 1]
+  uint64_t* gcode = nullptr;       // [max_n]
+  // top (unique-code) radix tree
+  uint32_t* top_left = nullptr;    // [max_n] encoded child (bit31 = group leaf)
+  uint32_t* top_right = nullptr;
+  uint32_t* top_parent_int = nullptr;   // [max_n] parent of internal node i (or invalid)
+  uint32_t* top_parent_grp = nullptr;   // [max_n] parent of group g
+  uint32_t* grp_root_idx = nullptr;     // [max_n] postorder index of group subtree root
+  uint32_t* grp_depth = nullptr;        // [max_n]
+  // nodes in strict postorder (2n-1)
+  uint32_t* n_left = nullptr;
+  uint32_t* n_right = nullptr;
+  uint32_t* n_begin = nullptr;
+  uint32_t* n_end = nullptr;
+  uint32_t* n_parent = nullptr;
+  uint32_t* n_lo = nullptr;         // [3][2n] lower witnesses
+  uint32_t* n_hi = nullptr;         // [3][2n] upper witnesses
+  uint32_t* n_flag = nullptr;       // [2n] bottom-up arrival counters
+  // frame
+  uint64_t* frame = nullptr;        // [12]: lower bits[3], upper bits[3], lower wit[3], upper wit[3]
+  unsigned long long* frame_partial = nullptr;  // per-block partials
+  uint32_t* frame_done = nullptr;
+  // results/export
+  uint32_t* stats = nullptr;        // [8]: m, max_depth, collision groups, max collision, ...
+  void* export_buf = nullptr;       // snapshot export (reference layout)
+  uint64_t export_bytes = 0;
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  uint64_t max_points = 0;
+  uint64_t device_bytes = 0;
+  bool poisoned = false;
+  std::mutex mutex;
+  std::string last_error;
+  double last_ms = 0.0;
+  uint64_t last_launches = 0;
+  uint32_t* d_err = nullptr;       // device error word
+  uint32_t* h_status = nullptr;    // pinned: [err, stats...]
+  RadixScratch radix;
+  LbvhBuffers lb;
+  uint32_t* lb_top_split = nullptr;     // [max_n] split group of top internal node
+  uint32_t* lb_top_gmin = nullptr;      // [max_n] first group of top internal node
+  uint32_t* lb_top_gmax = nullptr;      // [max_n] last group of top internal node
+  std::vector<void*> allocations;
+  uint64_t built_n = 0;            // points of the resident index (0 = none)
+};
+
+// Allocation helper: records the bytes on ctx.
+cudaError_t ctx_alloc(Ctx& ctx, void** ptr, size_t bytes);
+
+// LBVH stage (ehgp_lbvh.cu)
+cudaError_t lbvh_alloc(Ctx& ctx);
+// Runs the full device build on ctx.lb.xyz_in (input_kind 0 = f64, 1 = f32).
+// Returns the number of kernel launches issued.
+uint64_t lbvh_enqueue(Ctx& ctx, uint32_t n, int input_kind);
+// Copies the requested snapshot parts to the host (synchronises).
+cudaError_t lbvh_export(Ctx& ctx, uint32_t n, const ehgp_lbvh_out* out);
+
+}  // namespace ehgp

@@ -1,0 +1,152 @@
+// Stable LSD radix sort of 32-bit indices by indirect 64-bit keys (sm_100a).
+//
+// Used twice on the LBVH path:
+//  * the canonical PointId order: lexicographic (x, y, z) binary64 total-order
+//    keys, i.e. the std::sort of src/cpu/spatial/point_cloud.cpp:58-62;
+//  * the Morton leaf order: (code, PointId), i.e. std::sort with
+//    morton_leaf_less (src/cpu/spatial/lbvh.cpp:93-100,512) -- stability of
+//    the LSD passes over an input in PointId order gives the PointId tie-break.
+//
+// Each 8-bit pass is three kernels: a per-tile histogram (upsweep), a
+// single-CTA scan that also detects a pass in which every key has the same
+// digit, and a stable scatter (downsweep).  Trivial passes are skipped on the
+// device (the scatter returns at once and the ping-pong buffer is not
+// flipped), so the host never synchronises inside a sort and the whole
+// sequence can be captured in a CUDA graph.
+#include "ehgp_internal.cuh"
+
+namespace ehgp {
+namespace {
+
+__device__ __forceinline__ uint32_t digit_of(const IndirectKey& k, uint32_t v, int shift) {
+  uint64_t w = __ldg(k.words + v);
+  if (k.order) w = order_key(w);
+  return (uint32_t)(w >> shift) & 0xffu;
+}
+
+__global__ void __launch_bounds__(kRadixThreads)
+k_radix_upsweep(uint32_t n, const uint32_t* __restrict__ vals0, const uint32_t* __restrict__ vals1,
+                IndirectKey key, int shift, const uint32_t* __restrict__ state, int pass,
+                uint32_t* __restrict__ counts, uint32_t tiles) {
+  __shared__ uint32_t hist[256];
+  const uint32_t tile = blockIdx.x;
+  hist[threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t* in = state[2 * pass] ? vals1 : vals0;
+  const uint32_t base = tile * kRadixTile;
+#pragma unroll
+  for (int r = 0; r < kRadixItems; ++r) {
+    const uint32_t i = base + r * kRadixThreads + threadIdx.x;
+    if (i < n) atomicAdd(&hist[digit_of(key, in[i], shift)], 1u);
+  }
+  __syncthreads();
+  counts[threadIdx.x * tiles + tile] = hist[threadIdx.x];
+}
+
+// One CTA of 256 threads: thread d owns digit d.
+__global__ void __launch_bounds__(256)
+k_radix_scan(uint32_t n, uint32_t* __restrict__ counts, uint32_t tiles, uint32_t* __restrict__ state,
+             int pass) {
+  __shared__ uint32_t totals[256];
+  __shared__ uint32_t trivial;
+  const uint32_t d = threadIdx.x;
+  if (d == 0) trivial = 0;
+  uint32_t sum = 0;
+  for (uint32_t t = 0; t < tiles; ++t) sum += counts[d * tiles + t];
+  totals[d] = sum;
+  __syncthreads();
+  if (sum == n) trivial = 1;
+  // exclusive scan of the 256 digit totals (Hillis-Steele in shared memory)
+  uint32_t v = sum;
+  for (int off = 1; off < 256; off <<= 1) {
+    __syncthreads();
+    const uint32_t add = (d >= (uint32_t)off) ? totals[d - off] : 0u;
+    __syncthreads();
+    v += add;
+    totals[d] = v;
+  }
+  __syncthreads();
+  uint32_t run = v - sum;  // exclusive base of digit d
+  for (uint32_t t = 0; t < tiles; ++t) {
+    const uint32_t c = counts[d * tiles + t];
+    counts[d * tiles + t] = run;
+    run += c;
+  }
+  __syncthreads();
+  if (d == 0) {
+    const uint32_t cur = state[2 * pass];
+    state[2 * pass + 1] = trivial;
+    state[2 * (pass + 1)] = trivial ? cur : (cur ^ 1u);
+  }
+}
+
+__global__ void __launch_bounds__(kRadixThreads)
+k_radix_downsweep(uint32_t n, uint32_t* __restrict__ vals0, uint32_t* __restrict__ vals1,
+                  IndirectKey key, int shift, const uint32_t* __restrict__ state, int pass,
+                  const uint32_t* __restrict__ counts, uint32_t tiles) {
+  if (state[2 * pass + 1]) return;  // every key has the same digit: order unchanged
+  constexpr int kWarps = kRadixThreads / 32;
+  __shared__ uint32_t base[256];
+  __shared__ uint32_t warp_cnt[kWarps][256];
+  const uint32_t tile = blockIdx.x;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const uint32_t* in = state[2 * pass] ? vals1 : vals0;
+  uint32_t* out = state[2 * pass] ? vals0 : vals1;
+  base[tid] = counts[tid * tiles + tile];
+  const uint32_t lanemask_lt = (1u << lane) - 1u;
+  for (int r = 0; r < kRadixItems; ++r) {
+    const uint32_t i = tile * kRadixTile + r * kRadixThreads + tid;
+    const bool valid = i < n;
+    const uint32_t v = valid ? in[i] : 0u;
+    const uint32_t dig = valid ? digit_of(key, v, shift) : 256u;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) warp_cnt[w][tid] = 0;
+    __syncthreads();
+    const uint32_t peers = __match_any_sync(0xffffffffu, dig);
+    const uint32_t rank = __popc(peers & lanemask_lt);
+    if (valid && rank == 0) warp_cnt[warp][dig] = __popc(peers);
+    __syncthreads();
+    // exclusive prefix over warps, per digit (thread tid owns digit tid)
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t c = warp_cnt[w][tid];
+      warp_cnt[w][tid] = run;
+      run += c;
+    }
+    __syncthreads();
+    if (valid) out[base[dig] + warp_cnt[warp][dig] + rank] = v;
+    __syncthreads();
+    base[tid] += run;
+    __syncthreads();
+  }
+}
+
+__global__ void k_radix_init(uint32_t* state) {
+  if (threadIdx.x == 0) state[0] = 0;
+}
+
+}  // namespace
+
+int radix_sort_indirect(cudaStream_t stream, uint32_t n, uint32_t* vals0, uint32_t* vals1,
+                        const IndirectKey* stages, const int* stage_bits, int stage_count,
+                        RadixScratch& scratch, uint64_t* launches) {
+  const uint32_t tiles = (n + kRadixTile - 1) / kRadixTile;
+  k_radix_init<<<1, 32, 0, stream>>>(scratch.state);
+  *launches += 1;
+  int pass = 0;
+  for (int s = 0; s < stage_count; ++s) {
+    for (int shift = 0; shift < stage_bits[s]; shift += 8) {
+      k_radix_upsweep<<<tiles, kRadixThreads, 0, stream>>>(n, vals0, vals1, stages[s], shift, scratch.state,
+                                                           pass, scratch.counts, tiles);
+      k_radix_scan<<<1, 256, 0, stream>>>(n, scratch.counts, tiles, scratch.state, pass);
+      k_radix_downsweep<<<tiles, kRadixThreads, 0, stream>>>(n, vals0, vals1, stages[s], shift, scratch.state,
+                                                             pass, scratch.counts, tiles);
+      *launches += 3;
+      ++pass;
+    }
+  }
+  return pass;
+}
+
+}  // namespace ehgp

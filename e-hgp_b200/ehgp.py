@@ -1,0 +1,199 @@
+"""Host-side Python mirror of the C ABI in include/ehgp.h (ctypes).
+
+This is how tests, the smoke check and bench.py drive the sm_100a library.
+It mirrors the reference's GPU context interface for the product path
+(Ludwig-H/E-HGP, morsehgp3d/include/morsehgp3d/gpu/morton_lbvh_build.hpp:185-208):
+a context is created for a maximum point count and then builds clouds; a
+failure raises, and a CUDA failure poisons the context.
+
+Error mapping follows the reference's exceptions:
+    EHGP_ERR_INVALID_ARGUMENT -> InvalidArgument (std::invalid_argument)
+    EHGP_ERR_DUPLICATE_POINT  -> DuplicatePoint  (std::invalid_argument)
+    EHGP_ERR_CAPACITY         -> CapacityError   (std::length_error)
+    anything else             -> EhgpError
+
+The library is loaded from e-hgp_b200/lib/libehgp_b200.so; there is no
+fallback: if it is missing, `load()` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libehgp_b200.so")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "ehgp.h")
+
+STATUS = {
+    0: "EHGP_OK", 1: "EHGP_ERR_INVALID_ARGUMENT", 2: "EHGP_ERR_DUPLICATE_POINT",
+    3: "EHGP_ERR_CAPACITY", 4: "EHGP_ERR_OUT_OF_MEMORY", 5: "EHGP_ERR_TIMEOUT",
+    6: "EHGP_ERR_DEGENERATE", 7: "EHGP_ERR_NUMERIC_RANGE", 8: "EHGP_ERR_CUDA",
+    9: "EHGP_ERR_POISONED", 10: "EHGP_ERR_NOT_BUILT",
+}
+
+
+class EhgpError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+class InvalidArgument(EhgpError, ValueError):
+    pass
+
+
+class DuplicatePoint(InvalidArgument):
+    pass
+
+
+class CapacityError(EhgpError):
+    pass
+
+
+class NumericRange(EhgpError):
+    pass
+
+
+_ERRORS = {1: InvalidArgument, 2: DuplicatePoint, 3: CapacityError, 7: NumericRange}
+
+
+class Limits(C.Structure):
+    _fields_ = [("max_points", C.c_uint64), ("hbm_fraction", C.c_double)]
+
+
+class LbvhOut(C.Structure):
+    _fields_ = [
+        ("source_index", C.c_void_p), ("leaves", C.c_void_p), ("nodes", C.c_void_p),
+        ("counters", C.c_void_p), ("root_aabb_bits", C.c_void_p), ("root_node_index", C.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Loads the sm_100a library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: run `python e-hgp_b200/build.py`")
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    sigs = {
+        "ehgp_ctx_create": (C.c_int, [C.c_int, C.POINTER(Limits), C.POINTER(P)]),
+        "ehgp_ctx_destroy": (C.c_int, [P]),
+        "ehgp_last_error": (C.c_char_p, [P]),
+        "ehgp_status_string": (C.c_char_p, [C.c_int]),
+        "ehgp_ctx_device_bytes": (C.c_uint64, [P]),
+        "ehgp_lbvh_build": (C.c_int, [P, P, C.c_uint64, C.POINTER(LbvhOut)]),
+        "ehgp_lbvh_build_f32": (C.c_int, [P, P, C.c_uint64, C.POINTER(LbvhOut)]),
+        "ehgp_lbvh_build_device": (C.c_int, [P, P, C.c_uint64, C.POINTER(LbvhOut)]),
+        "ehgp_last_timing": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def declared_symbols(header: str = HEADER) -> list[str]:
+    """Names of the functions include/ehgp.h declares."""
+    import re
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ehgp_[a-z0-9_]+)\s*\(", text)))
+
+
+@dataclass
+class LbvhSnapshot:
+    """Reference-layout MortonLbvhSnapshot (include/morsehgp3d/spatial/lbvh.hpp:109-121)."""
+    source_index: np.ndarray   # (n,) u64: input index of PointId p
+    leaves: np.ndarray         # (n, 2) u64: (Morton code, PointId)
+    nodes: np.ndarray          # (2n-1, 10) u64: lower[3], upper[3], left, right, begin, end
+    counters: np.ndarray       # (5,) u64
+    root_aabb: np.ndarray      # (6,) u64 binary64 words
+    root: int
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class Context:
+    """One device context (mirrors gpu::MortonLbvhBuildContext)."""
+
+    def __init__(self, max_points: int, device: int = 0, hbm_fraction: float = 0.8):
+        self.lib = load()
+        self._h = C.c_void_p()
+        lim = Limits(max_points, hbm_fraction)
+        st = self.lib.ehgp_ctx_create(device, C.byref(lim), C.byref(self._h))
+        if st != 0:
+            raise _ERRORS.get(st, EhgpError)(st, "context creation failed")
+        self.max_points = max_points
+
+    def close(self) -> None:
+        if self._h:
+            self.lib.ehgp_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int) -> None:
+        if st != 0:
+            msg = self.lib.ehgp_last_error(self._h).decode()
+            raise _ERRORS.get(st, EhgpError)(st, msg)
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.lib.ehgp_ctx_device_bytes(self._h))
+
+    def last_timing(self) -> tuple[float, int]:
+        ms, launches = C.c_double(), C.c_uint64()
+        self._check(self.lib.ehgp_last_timing(self._h, C.byref(ms), C.byref(launches)))
+        return ms.value, launches.value
+
+    def lbvh_build(self, points: np.ndarray, outputs: bool = True) -> LbvhSnapshot | None:
+        """Canonical cloud + exact Morton LBVH (ehgp_lbvh_build / _f32).
+
+        points: (n, 3) float64 or float32 array.  With outputs=False only the
+        device-resident index is built (nothing is copied back)."""
+        pts = np.ascontiguousarray(points)
+        if pts.ndim != 2 or pts.shape[1] != 3:
+            raise InvalidArgument(1, "points must have shape (n, 3)")
+        n = pts.shape[0]
+        if outputs:
+            snap = LbvhSnapshot(
+                np.empty(n, np.uint64), np.empty((n, 2), np.uint64),
+                np.empty((max(2 * n - 1, 0), 10), np.uint64), np.empty(5, np.uint64),
+                np.empty(6, np.uint64), 0)
+            root = np.zeros(1, np.uint64)
+            out = LbvhOut(_ptr(snap.source_index), _ptr(snap.leaves), _ptr(snap.nodes),
+                          _ptr(snap.counters), _ptr(snap.root_aabb), _ptr(root))
+        else:
+            snap, out = None, LbvhOut(None, None, None, None, None, None)
+        if pts.dtype == np.float32:
+            st = self.lib.ehgp_lbvh_build_f32(self._h, _ptr(pts), n, C.byref(out))
+        else:
+            pts = pts.astype(np.float64, copy=False)
+            st = self.lib.ehgp_lbvh_build(self._h, _ptr(pts), n, C.byref(out))
+        self._check(st)
+        if snap is not None:
+            snap.root = int(root[0])
+        return snap

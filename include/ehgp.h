@@ -1,0 +1,138 @@
+/*
+ * ehgp.h — C ABI of the B200 (sm_100a) MorseHGP3D product path.
+ *
+ * Plain C: fixed-width integers, plain pointers and sizes, integer status
+ * codes.  No C++ exceptions and no torch types cross this boundary.
+ *
+ * Every entry point below replaces one interface of the reference
+ * (Ludwig-H/E-HGP, directory morsehgp3d/); the citation is given beside it.
+ * Record layouts that a reference caller reads byte-for-byte keep the
+ * reference's layout and carry a static size check in the implementation.
+ *
+ * Threading: one context owns one CUDA stream and its device buffers; calls
+ * on one context are serialised by the context.  All calls are synchronous:
+ * when an entry point returns, its host outputs are complete.
+ *
+ * Errors: a status other than EHGP_OK is returned and a message is kept in
+ * the context (ehgp_last_error).  A CUDA failure poisons the context (every
+ * later call returns EHGP_ERR_POISONED), mirroring the reference's
+ * poisoned-context rule (src/cuda/phase14_morton_lbvh_build_internal.hpp:99-132).
+ */
+#ifndef EHGP_H_
+#define EHGP_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+typedef enum ehgp_status {
+  EHGP_OK = 0,
+  EHGP_ERR_INVALID_ARGUMENT = 1, /* null pointer, n = 0, non-finite coordinate  */
+  EHGP_ERR_DUPLICATE_POINT = 2,  /* two input points are geometrically equal    */
+  EHGP_ERR_CAPACITY = 3,         /* n above the context's max_points            */
+  EHGP_ERR_OUT_OF_MEMORY = 4,    /* device allocation refused                   */
+  EHGP_ERR_TIMEOUT = 5,          /* a bounded device wait ran out               */
+  EHGP_ERR_DEGENERATE = 6,       /* relevant extra-shell diagnostic (journal refuses) */
+  EHGP_ERR_NUMERIC_RANGE = 7,    /* a fixed-width exact evaluation would overflow */
+  EHGP_ERR_CUDA = 8,             /* CUDA runtime error; context is poisoned     */
+  EHGP_ERR_POISONED = 9,         /* an earlier CUDA error poisoned the context  */
+  EHGP_ERR_NOT_BUILT = 10        /* stage needs an earlier stage's device state  */
+} ehgp_status;
+
+/* ---- limits and context -------------------------------------------------- */
+typedef struct ehgp_limits {
+  uint64_t max_points;   /* largest cloud one call accepts                    */
+  double hbm_fraction;   /* admission ceiling as a fraction of HBM (0.8)      */
+} ehgp_limits;
+
+typedef struct ehgp_ctx ehgp_ctx;
+
+/* Replaces gpu::MortonLbvhBuildContext::MortonLbvhBuildContext(max_n)
+ * (include/morsehgp3d/gpu/morton_lbvh_build.hpp:185-189): creates a context on
+ * `device` whose buffers hold clouds of up to limits->max_points points. */
+int ehgp_ctx_create(int device, const ehgp_limits* limits, ehgp_ctx** out_ctx);
+/* Replaces ~MortonLbvhBuildContext (morton_lbvh_build.hpp:190). */
+int ehgp_ctx_destroy(ehgp_ctx* ctx);
+/* Message of the last failed call on ctx (empty string when none). */
+const char* ehgp_last_error(const ehgp_ctx* ctx);
+/* Static name of a status code. */
+const char* ehgp_status_string(int status);
+/* Device bytes owned by the context (resident buffers). */
+uint64_t ehgp_ctx_device_bytes(const ehgp_ctx* ctx);
+
+/* ---- LBVH snapshot records (reference layout) ---------------------------- */
+/* Same fields, order and sizes as spatial::MortonLbvhSnapshotLeaf,
+ * MortonLbvhSnapshotNode and MortonLbvhSnapshotCounters
+ * (include/morsehgp3d/spatial/lbvh.hpp:44-50, 62-78, 80-89): 16, 80, 40 bytes. */
+typedef struct ehgp_lbvh_leaf {
+  uint64_t morton_code;
+  uint64_t point_id;
+} ehgp_lbvh_leaf;
+
+#define EHGP_INVALID_NODE_INDEX (~(uint64_t)0)
+
+typedef struct ehgp_lbvh_node {
+  uint64_t lower_point_ids[3];
+  uint64_t upper_point_ids[3];
+  uint64_t left_child;  /* EHGP_INVALID_NODE_INDEX for a leaf */
+  uint64_t right_child; /* EHGP_INVALID_NODE_INDEX for a leaf */
+  uint64_t leaf_begin;
+  uint64_t leaf_end;
+} ehgp_lbvh_node;
+
+typedef struct ehgp_lbvh_counters {
+  uint64_t point_count;
+  uint64_t node_count;
+  uint64_t maximum_depth;
+  uint64_t morton_collision_group_count;
+  uint64_t maximum_morton_collision_size;
+} ehgp_lbvh_counters;
+
+/* Host-side outputs of ehgp_lbvh_build.  Any pointer may be NULL to skip that
+ * output; the device-resident index is built either way. */
+typedef struct ehgp_lbvh_out {
+  uint64_t* source_index;        /* [n]: input position of PointId p          */
+  ehgp_lbvh_leaf* leaves;        /* [n]: (Morton code, PointId), sorted       */
+  ehgp_lbvh_node* nodes;         /* [2n-1]: strict left/right postorder        */
+  ehgp_lbvh_counters* counters;  /* [1]                                       */
+  uint64_t* root_aabb_bits;      /* [6]: lower xyz, upper xyz binary64 words  */
+  uint64_t* root_node_index;     /* [1]: always 2n-2                          */
+} ehgp_lbvh_out;
+
+/* Canonical point cloud + exact Morton LBVH, fused on the device.
+ *
+ * Replaces, as one call:
+ *   spatial::CanonicalPointCloud::rejecting_duplicates
+ *     (include/morsehgp3d/spatial/point_cloud.hpp:31, src/cpu/spatial/point_cloud.cpp:40-94),
+ *   spatial::MortonLbvhIndex::build (src/cpu/spatial/lbvh.cpp:484-549), and
+ *   gpu::MortonLbvhBuildContext::build (include/morsehgp3d/gpu/morton_lbvh_build.hpp:196)
+ *     with its launcher seam build_phase14_morton_lbvh_snapshot_on_gpu
+ *     (src/cuda/phase14_morton_lbvh_build_internal.hpp:150-156).
+ *
+ * xyz: host array of n points, interleaved x,y,z binary64 values.
+ * PointIds are the ranks of the points in lexicographic binary64 total order
+ * (-0 canonicalised to +0).  Results are bit-identical to the reference's
+ * MortonLbvhSnapshot.  Errors: EHGP_ERR_INVALID_ARGUMENT (n = 0, non-finite
+ * coordinate), EHGP_ERR_DUPLICATE_POINT, EHGP_ERR_CAPACITY. */
+int ehgp_lbvh_build(ehgp_ctx* ctx, const double* xyz, uint64_t n, const ehgp_lbvh_out* out);
+
+/* Same as ehgp_lbvh_build for binary32 input, widened exactly to binary64. */
+int ehgp_lbvh_build_f32(ehgp_ctx* ctx, const float* xyz, uint64_t n, const ehgp_lbvh_out* out);
+
+/* Same as ehgp_lbvh_build, with xyz already resident in device memory
+ * (interleaved binary64, 3n values); no host->device copy of the points. */
+int ehgp_lbvh_build_device(ehgp_ctx* ctx, const double* d_xyz, uint64_t n, const ehgp_lbvh_out* out);
+
+/* Device time (ms) of the last call's kernels, measured with CUDA events on
+ * the context's stream, and the number of kernel launches it issued. */
+int ehgp_last_timing(const ehgp_ctx* ctx, double* device_ms, uint64_t* kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EHGP_H_ */

@@ -1,0 +1,262 @@
+// ORACLE — test infrastructure only, never the product path.
+//
+// A CPU restatement, in plain C++, of the reference's algorithm for each stage
+// of the MorseHGP3D product path (Ludwig-H/E-HGP, morsehgp3d/), written for
+// clarity over speed.  Only tests/, the smoke check and bench.py's CPU
+// baseline may load it, and only as the checker.  Exact arithmetic uses the
+// arbitrary-precision integer of oracle/boost_shim.
+//
+// Pinning: tests check this restatement against the reference's own code
+// compiled here (oracle/_ref, built by oracle/Makefile) and against the
+// committed golden vectors in tests/golden/.
+#include <boost/multiprecision/cpp_int.hpp>
+
+#include <algorithm>
+#include <array>
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace {
+
+using Big = boost::multiprecision::cpp_int;
+using u64 = std::uint64_t;
+
+// exact::canonicalize_binary64_bits / binary64_total_order_key
+// (include/morsehgp3d/exact/binary64.hpp:17-29)
+u64 canonical(u64 bits) {
+  if ((bits & 0x7ff0000000000000ull) == 0x7ff0000000000000ull)
+    throw std::invalid_argument("binary64 coordinates must be finite");
+  return bits == 0x8000000000000000ull ? 0ull : bits;
+}
+u64 order_key(u64 bits) { return (bits >> 63) ? ~bits : (bits ^ (u64{1} << 63)); }
+
+u64 bits_of(double v) {
+  u64 b;
+  std::memcpy(&b, &v, 8);
+  return b;
+}
+
+struct Cloud {
+  std::vector<std::array<u64, 3>> bits;  // canonical words by PointId
+  std::vector<u64> source;               // input index by PointId
+};
+
+// CanonicalPointCloud::rejecting_duplicates (src/cpu/spatial/point_cloud.cpp:40-94):
+// PointId = rank in lexicographic order of the three total-order keys.
+Cloud canonical_cloud(const double* xyz, u64 n) {
+  if (n == 0) throw std::invalid_argument("a canonical point cloud cannot be empty");
+  std::vector<std::array<u64, 3>> keys(n);
+  std::vector<std::array<u64, 3>> words(n);
+  for (u64 i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) {
+      words[i][a] = canonical(bits_of(xyz[3 * i + a]));
+      keys[i][a] = order_key(words[i][a]);
+    }
+  std::vector<u64> order(n);
+  for (u64 i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](u64 l, u64 r) { return keys[l] < keys[r]; });
+  for (u64 i = 1; i < n; ++i)
+    if (keys[order[i - 1]] == keys[order[i]])
+      throw std::invalid_argument("a canonical point cloud cannot contain duplicate geometric points");
+  Cloud c;
+  c.bits.resize(n);
+  c.source = order;
+  for (u64 p = 0; p < n; ++p) c.bits[p] = words[order[p]];
+  return c;
+}
+
+// A finite binary64 value as significand * 2^exponent (lbvh.cpp:162-186).
+struct Dyadic {
+  long long sig;
+  int exp;
+};
+Dyadic decode(u64 bits) {
+  const u64 e = (bits >> 52) & 0x7ff, f = bits & ((u64{1} << 52) - 1);
+  Dyadic d{(long long)f, -1074};
+  if (e != 0) {
+    d.sig = (long long)(f | (u64{1} << 52));
+    d.exp = (int)e - 1075;
+  }
+  if (bits >> 63) d.sig = -d.sig;
+  return d;
+}
+
+// quantized_coordinate_from_bits (src/cpu/spatial/lbvh.cpp:237-296): the
+// exact floor(2^21 (x - l) / (u - l)) with the two boundary rules.
+u64 quantize(u64 x, u64 l, u64 u) {
+  if (l == u) return 0;
+  if (x == u) return (u64{1} << 21) - 1;
+  const Dyadic dx = decode(x), dl = decode(l), du = decode(u);
+  int emin = 0;
+  bool have = false;
+  for (const Dyadic& d : {dl, dx, du})
+    if (d.sig != 0) {
+      emin = have ? std::min(emin, d.exp) : d.exp;
+      have = true;
+    }
+  auto aligned = [&](const Dyadic& d) {
+    Big v = d.sig;
+    if (d.sig != 0) v <<= (unsigned)(d.exp - emin);
+    return v;
+  };
+  const Big L = aligned(dl), X = aligned(dx), U = aligned(du);
+  const Big q = (Big(u64{1} << 21) * (X - L)) / (U - L);
+  return q.convert_to<u64>();
+}
+
+// interleaved_morton_code (src/cpu/spatial/lbvh.cpp:78-91)
+u64 interleave(u64 qx, u64 qy, u64 qz) {
+  u64 code = 0;
+  for (int b = 0; b < 21; ++b) {
+    code |= ((qx >> b) & 1) << (3 * b + 2);
+    code |= ((qy >> b) & 1) << (3 * b + 1);
+    code |= ((qz >> b) & 1) << (3 * b);
+  }
+  return code;
+}
+
+struct Node {
+  u64 lo[3], hi[3], left, right, begin, end;
+};
+
+struct Lbvh {
+  std::vector<std::pair<u64, u64>> leaves;  // (code, PointId)
+  std::vector<Node> nodes;                   // postorder
+  u64 max_depth = 0, collision_groups = 0, max_collision = 0;
+  std::array<u64, 6> root_aabb{};
+};
+
+// MortonLbvhIndex::build (src/cpu/spatial/lbvh.cpp:484-549) with find_split
+// (:831-860), build_range (:862-906) and the witness rules (:46-76).
+Lbvh build_lbvh(const Cloud& c) {
+  const u64 n = c.bits.size();
+  auto key = [&](u64 id, int a) { return order_key(c.bits[id][a]); };
+  Lbvh t;
+  // exact frame: first extremum in PointId order wins (lbvh.cpp:107-155)
+  std::array<u64, 3> lo_id{}, hi_id{};
+  for (u64 p = 1; p < n; ++p)
+    for (int a = 0; a < 3; ++a) {
+      if (key(p, a) < key(lo_id[a], a)) lo_id[a] = p;
+      if (key(p, a) > key(hi_id[a], a)) hi_id[a] = p;
+    }
+  for (int a = 0; a < 3; ++a) {
+    t.root_aabb[a] = c.bits[lo_id[a]][a];
+    t.root_aabb[3 + a] = c.bits[hi_id[a]][a];
+  }
+  t.leaves.resize(n);
+  for (u64 p = 0; p < n; ++p) {
+    u64 q[3];
+    for (int a = 0; a < 3; ++a) q[a] = quantize(c.bits[p][a], t.root_aabb[a], t.root_aabb[3 + a]);
+    t.leaves[p] = {interleave(q[0], q[1], q[2]), p};
+  }
+  std::sort(t.leaves.begin(), t.leaves.end());
+  for (u64 b = 0; b < n;) {
+    u64 e = b + 1;
+    while (e < n && t.leaves[e].first == t.leaves[b].first) ++e;
+    if (e - b > 1) {
+      ++t.collision_groups;
+      t.max_collision = std::max(t.max_collision, e - b);
+    }
+    b = e;
+  }
+  auto split = [&](u64 b, u64 e) -> u64 {
+    const u64 f = t.leaves[b].first, l = t.leaves[e - 1].first;
+    if (f == l) return b + (e - b) / 2;
+    const int hb = 63 - __builtin_clzll(f ^ l);
+    u64 lo = b + 1, hi = e;
+    while (lo < hi) {
+      const u64 mid = lo + (hi - lo) / 2;
+      if (((t.leaves[mid].first >> hb) & 1) == 0) lo = mid + 1;
+      else hi = mid;
+    }
+    return lo;
+  };
+  std::function<u64(u64, u64, u64)> rec = [&](u64 b, u64 e, u64 depth) -> u64 {
+    t.max_depth = std::max(t.max_depth, depth);
+    Node nd{};
+    nd.begin = b;
+    nd.end = e;
+    if (e - b == 1) {
+      for (int a = 0; a < 3; ++a) nd.lo[a] = nd.hi[a] = t.leaves[b].second;
+      nd.left = nd.right = ~u64{0};
+    } else {
+      const u64 s = split(b, e);
+      nd.left = rec(b, s, depth + 1);
+      nd.right = rec(s, e, depth + 1);
+      const Node& L = t.nodes[nd.left];
+      const Node& R = t.nodes[nd.right];
+      for (int a = 0; a < 3; ++a) {
+        const u64 kl = key(L.lo[a], a), kr = key(R.lo[a], a);
+        nd.lo[a] = (kr < kl || (kr == kl && R.lo[a] < L.lo[a])) ? R.lo[a] : L.lo[a];
+        const u64 hl = key(L.hi[a], a), hr = key(R.hi[a], a);
+        nd.hi[a] = (hr > hl || (hr == hl && R.hi[a] < L.hi[a])) ? R.hi[a] : L.hi[a];
+      }
+    }
+    t.nodes.push_back(nd);
+    return t.nodes.size() - 1;
+  };
+  rec(0, n, 0);
+  return t;
+}
+
+int report(const std::exception& e, char* err, u64 errlen, int code) {
+  if (err && errlen) {
+    std::strncpy(err, e.what(), errlen - 1);
+    err[errlen - 1] = 0;
+  }
+  return code;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Same outputs and layout as ref_lbvh_build in oracle/ref_driver.cpp.
+int oracle_lbvh_build(const double* xyz, u64 n, u64* source_index, u64* leaves, u64* nodes, u64* counters,
+                      u64* root_aabb, u64* root, char* err, u64 errlen) {
+  try {
+    const Cloud c = canonical_cloud(xyz, n);
+    const Lbvh t = build_lbvh(c);
+    if (source_index)
+      for (u64 p = 0; p < n; ++p) source_index[p] = c.source[p];
+    if (leaves)
+      for (u64 i = 0; i < n; ++i) {
+        leaves[2 * i] = t.leaves[i].first;
+        leaves[2 * i + 1] = t.leaves[i].second;
+      }
+    if (nodes)
+      for (u64 i = 0; i < t.nodes.size(); ++i) {
+        const Node& nd = t.nodes[i];
+        u64* r = nodes + 10 * i;
+        for (int a = 0; a < 3; ++a) {
+          r[a] = nd.lo[a];
+          r[3 + a] = nd.hi[a];
+        }
+        r[6] = nd.left;
+        r[7] = nd.right;
+        r[8] = nd.begin;
+        r[9] = nd.end;
+      }
+    if (counters) {
+      counters[0] = n;
+      counters[1] = 2 * n - 1;
+      counters[2] = t.max_depth;
+      counters[3] = t.collision_groups;
+      counters[4] = t.max_collision;
+    }
+    if (root_aabb)
+      for (int k = 0; k < 6; ++k) root_aabb[k] = t.root_aabb[k];
+    if (root) *root = 2 * n - 2;
+    return 0;
+  } catch (const std::invalid_argument& e) {
+    return report(e, err, errlen, 1);
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 2);
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,165 @@
+// Test-oracle driver over the reference's own CPU code (Ludwig-H/E-HGP,
+// morsehgp3d/src/cpu), compiled unmodified from its source tree against the
+// project-written Boost shim in oracle/boost_shim.  Built by oracle/Makefile
+// into oracle/_ref/libehgp_ref.so.  Test infrastructure only: it is the
+// checker for the CUDA path and the timed reference CPU baseline, never part
+// of the product path.
+//
+// Entry points are extern "C" with flat arrays so that Python tests can call
+// them through ctypes.  Every function returns 0 on success, or a nonzero code
+// with the reference's exception text copied into `err` (capacity errlen).
+#include "morsehgp3d/exact/point.hpp"
+#include "morsehgp3d/spatial/lbvh.hpp"
+#include "morsehgp3d/spatial/point_cloud.hpp"
+
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <span>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace morsehgp3d::gpu {
+// MortonLbvhIndex names this class a friend (include/morsehgp3d/spatial/lbvh.hpp:421);
+// its real definition lives in the GPU sources, which are not linked here, so
+// the oracle uses the name to read the private node array for comparison.
+class SpatialLbvhContext {
+ public:
+  static void export_nodes(const spatial::MortonLbvhIndex& index, uint64_t* out) {
+    for (std::size_t i = 0; i < index.nodes_.size(); ++i) {
+      const auto& nd = index.nodes_[i];
+      uint64_t* r = out + 10 * i;
+      for (int a = 0; a < 3; ++a) {
+        r[a] = nd.lower_point_ids[a];
+        r[3 + a] = nd.upper_point_ids[a];
+      }
+      const uint64_t invalid = ~uint64_t{0};
+      r[6] = nd.left_child == static_cast<std::size_t>(-1) ? invalid : nd.left_child;
+      r[7] = nd.right_child == static_cast<std::size_t>(-1) ? invalid : nd.right_child;
+      r[8] = nd.leaf_begin;
+      r[9] = nd.leaf_end;
+    }
+  }
+  static uint64_t root(const spatial::MortonLbvhIndex& index) { return index.root_index_; }
+};
+}  // namespace morsehgp3d::gpu
+
+namespace {
+
+using morsehgp3d::exact::CertifiedPoint3;
+using morsehgp3d::spatial::CanonicalPointCloud;
+using morsehgp3d::spatial::MortonLbvhIndex;
+
+int report(const std::exception& e, char* err, uint64_t errlen, int code) {
+  if (err && errlen) {
+    std::strncpy(err, e.what(), errlen - 1);
+    err[errlen - 1] = 0;
+  }
+  return code;
+}
+
+std::vector<CertifiedPoint3> points_from(const double* xyz, uint64_t n) {
+  std::vector<CertifiedPoint3> pts;
+  pts.reserve(n);
+  for (uint64_t i = 0; i < n; ++i) pts.push_back(CertifiedPoint3::from_binary64(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
+  return pts;
+}
+
+}  // namespace
+
+extern "C" {
+
+// CanonicalPointCloud::rejecting_duplicates + MortonLbvhIndex::build.
+// Outputs (any may be null): source_index[n], leaves[2n] (code, id),
+// nodes[10(2n-1)] in the MortonLbvhSnapshotNode field order, counters[5],
+// root_aabb[6], root[1].  seconds[2]: canonicalisation and build wall time.
+int ref_lbvh_build(const double* xyz, uint64_t n, uint64_t* source_index, uint64_t* leaves, uint64_t* nodes,
+                   uint64_t* counters, uint64_t* root_aabb, uint64_t* root, double* seconds, char* err,
+                   uint64_t errlen) {
+  try {
+    const auto pts = points_from(xyz, n);
+    const auto t0 = std::chrono::steady_clock::now();
+    const CanonicalPointCloud cloud = CanonicalPointCloud::rejecting_duplicates(pts);
+    const auto t1 = std::chrono::steady_clock::now();
+    const MortonLbvhIndex index = MortonLbvhIndex::build(cloud);
+    const auto t2 = std::chrono::steady_clock::now();
+    if (seconds) {
+      seconds[0] = std::chrono::duration<double>(t1 - t0).count();
+      seconds[1] = std::chrono::duration<double>(t2 - t1).count();
+    }
+    if (source_index)
+      for (uint64_t p = 0; p < n; ++p) source_index[p] = cloud.source_index(p);
+    if (leaves) {
+      const auto lv = index.leaves();
+      for (uint64_t i = 0; i < n; ++i) {
+        leaves[2 * i] = lv[i].morton_code;
+        leaves[2 * i + 1] = lv[i].point_id;
+      }
+    }
+    if (nodes) morsehgp3d::gpu::SpatialLbvhContext::export_nodes(index, nodes);
+    if (counters) {
+      const auto& c = index.build_counters();
+      counters[0] = c.point_count;
+      counters[1] = c.node_count;
+      counters[2] = c.maximum_depth;
+      counters[3] = c.morton_collision_group_count;
+      counters[4] = c.maximum_morton_collision_size;
+    }
+    if (root_aabb) {
+      const auto& bb = index.root_aabb();
+      for (int a = 0; a < 3; ++a) {
+        root_aabb[a] = bb.lower_binary64_bits[a];
+        root_aabb[3 + a] = bb.upper_binary64_bits[a];
+      }
+    }
+    if (root) *root = morsehgp3d::gpu::SpatialLbvhContext::root(index);
+    return 0;
+  } catch (const std::invalid_argument& e) {
+    return report(e, err, errlen, 1);
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 2);
+  }
+}
+
+// MortonLbvhIndex::import_certified_snapshot (src/cpu/spatial/lbvh.cpp:551-829):
+// the reference's own exhaustive validator of a device-built snapshot.  Returns
+// 0 when the reference accepts every leaf, node, split, witness and counter.
+int ref_lbvh_certify(const double* xyz, uint64_t n, const uint64_t* leaves, const uint64_t* nodes,
+                     const uint64_t* counters, const uint64_t* root_aabb, uint64_t root, char* err,
+                     uint64_t errlen) {
+  try {
+    const auto pts = points_from(xyz, n);
+    const CanonicalPointCloud cloud = CanonicalPointCloud::rejecting_duplicates(pts);
+    morsehgp3d::spatial::MortonLbvhSnapshot snap;
+    snap.point_count = n;
+    snap.root_node_index = root;
+    for (int a = 0; a < 3; ++a) {
+      snap.root_aabb.lower_binary64_bits[a] = root_aabb[a];
+      snap.root_aabb.upper_binary64_bits[a] = root_aabb[3 + a];
+    }
+    snap.proposed_counters = {counters[0], counters[1], counters[2], counters[3], counters[4]};
+    snap.leaves.resize(n);
+    for (uint64_t i = 0; i < n; ++i) snap.leaves[i] = {leaves[2 * i], leaves[2 * i + 1]};
+    snap.nodes.resize(2 * n - 1);
+    for (uint64_t i = 0; i < 2 * n - 1; ++i) {
+      auto& nd = snap.nodes[i];
+      const uint64_t* r = nodes + 10 * i;
+      for (int a = 0; a < 3; ++a) {
+        nd.lower_point_ids[a] = r[a];
+        nd.upper_point_ids[a] = r[3 + a];
+      }
+      nd.left_child = r[6];
+      nd.right_child = r[7];
+      nd.leaf_begin = r[8];
+      nd.leaf_end = r[9];
+    }
+    const MortonLbvhIndex index = MortonLbvhIndex::import_certified_snapshot(cloud, snap);
+    return index.ready() ? 0 : 3;
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 1);
+  }
+}
+
+}  // extern "C"
