@@ -561,7 +561,9 @@ k_top_index(uint32_t n, const uint32_t* __restrict__ stats, const uint32_t* __re
     const uint32_t p = up & ~kRightBit;
     const uint32_t pe = gstart[top_gmax[p] + 1];
     pidx = 2 * pe - 2 - (right_turns - self_right);
+    if (pidx >= 2 * n - 1) { atomicOr(err, kErrInternal); return; }
   }
+  if (idx >= 2 * n - 1 || e > n || b >= e) { atomicOr(err, kErrInternal); return; }
   if (is_group) {
     const uint32_t g = t - (m - 1);
     grp_root_idx[g] = idx;
@@ -607,6 +609,7 @@ k_group_subtrees(uint32_t n, const uint32_t* __restrict__ stats, const uint32_t*
   uint32_t max_depth = 0;
   while (top > 0) {
     const Item it = stack[--top];
+    if (it.idx >= 2 * n - 1 || it.e > n || it.b >= it.e) { atomicOr(err, kErrInternal); return; }
     max_depth = max(max_depth, it.depth);
     n_begin[it.idx] = it.b;
     n_end[it.idx] = it.e;
@@ -657,10 +660,12 @@ k_bottom_up(uint32_t n, const uint32_t* __restrict__ stats, const uint32_t* __re
   for (uint32_t step = 0; step < 2 * n + 64; ++step) {
     const uint32_t p = n_parent[cur];
     if (p == kInvalid32) return;
+    if (p >= 2 * n - 1) { atomicOr(err, kErrInternal); return; }
     __threadfence();
     if (atomicAdd(&n_flag[p], 1u) == 0u) return;  // first arrival: the sibling finishes
     __threadfence();
     const uint32_t l = n_left[p], r = n_right[p];
+    if (l >= 2 * n - 1 || r >= 2 * n - 1) { atomicOr(err, kErrInternal); return; }
     for (int a = 0; a < 3; ++a) {
       const uint32_t ll = __ldcg(n_lo + (uint64_t)a * N2 + l), rl = __ldcg(n_lo + (uint64_t)a * N2 + r);
       const uint32_t lh = __ldcg(n_hi + (uint64_t)a * N2 + l), rh = __ldcg(n_hi + (uint64_t)a * N2 + r);
