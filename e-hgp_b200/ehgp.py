@@ -94,6 +94,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "ehgp_lbvh_build_f32": (C.c_int, [P, P, C.c_uint64, C.POINTER(LbvhOut)]),
         "ehgp_lbvh_build_device": (C.c_int, [P, P, C.c_uint64, C.POINTER(LbvhOut)]),
         "ehgp_last_timing": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+        "ehgp_lbvh_build_noalloc": (C.c_int, [P, C.c_uint64, C.POINTER(LbvhOut), P]),
+        "ehgp_lbvh_noalloc_max_points": (C.c_uint64, []),
+        "ehgp_lbvh_noalloc_scratch_bytes": (C.c_uint64, []),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -124,6 +127,33 @@ class LbvhSnapshot:
 
 def _ptr(a: np.ndarray) -> int:
     return a.ctypes.data
+
+
+def _empty_snapshot(n: int) -> tuple[LbvhSnapshot, np.ndarray, LbvhOut]:
+    snap = LbvhSnapshot(
+        np.empty(n, np.uint64), np.empty((n, 2), np.uint64),
+        np.empty((max(2 * n - 1, 0), 10), np.uint64), np.empty(5, np.uint64),
+        np.empty(6, np.uint64), 0)
+    root = np.zeros(1, np.uint64)
+    out = LbvhOut(_ptr(snap.source_index), _ptr(snap.leaves), _ptr(snap.nodes),
+                  _ptr(snap.counters), _ptr(snap.root_aabb), _ptr(root))
+    return snap, root, out
+
+
+def lbvh_build_noalloc(points: np.ndarray, stream: int = 0) -> LbvhSnapshot:
+    """ehgp_lbvh_build_noalloc: the LBVH build without any allocation by the
+    library, for callers that may not call cudaMalloc.  At most
+    ehgp_lbvh_noalloc_max_points() points; runs on the current device."""
+    lib = load()
+    pts = np.ascontiguousarray(points, dtype=np.float64)
+    if pts.ndim != 2 or pts.shape[1] != 3:
+        raise InvalidArgument(1, "points must have shape (n, 3)")
+    snap, root, out = _empty_snapshot(pts.shape[0])
+    st = lib.ehgp_lbvh_build_noalloc(_ptr(pts), pts.shape[0], C.byref(out), C.c_void_p(stream))
+    if st != 0:
+        raise _ERRORS.get(st, EhgpError)(st, "ehgp_lbvh_build_noalloc failed")
+    snap.root = int(root[0])
+    return snap
 
 
 class Context:

@@ -127,6 +127,23 @@ int ehgp_lbvh_build_f32(ehgp_ctx* ctx, const float* xyz, uint64_t n, const ehgp_
  * (interleaved binary64, 3n values); no host->device copy of the points. */
 int ehgp_lbvh_build_device(ehgp_ctx* ctx, const double* d_xyz, uint64_t n, const ehgp_lbvh_out* out);
 
+/* Allocation-free LBVH build.  No counterpart in the reference: it exists for
+ * callers that may not call cudaMalloc (a host framework that owns all device
+ * memory through its own pool, or a latency-critical caller that cannot
+ * accept cudaMalloc's device-wide synchronisation), and so cannot create a
+ * context.  Same inputs, outputs and results as ehgp_lbvh_build, with host
+ * `xyz` and host outputs, run on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream) of the current device.  All scratch lives in one fixed
+ * __device__ array of ehgp_lbvh_noalloc_scratch_bytes() bytes that every GPU
+ * loading this library holds until exit; n above
+ * ehgp_lbvh_noalloc_max_points() (16384) returns EHGP_ERR_CAPACITY.  The
+ * first call on a device looks the array up (cudaGetSymbolAddress) and must
+ * come before any stream capture.  Calls share the array: calls whose GPU
+ * work overlaps race and must not be issued. */
+int ehgp_lbvh_build_noalloc(const double* xyz, uint64_t n, const ehgp_lbvh_out* out, void* stream);
+uint64_t ehgp_lbvh_noalloc_max_points(void);
+uint64_t ehgp_lbvh_noalloc_scratch_bytes(void);
+
 /* Device time (ms) of the last call's kernels, measured with CUDA events on
  * the context's stream, and the number of kernel launches it issued. */
 int ehgp_last_timing(const ehgp_ctx* ctx, double* device_ms, uint64_t* kernel_launches);
