@@ -24,6 +24,20 @@ cudaError_t ctx_alloc(Ctx& ctx, void** ptr, size_t bytes) {
 
 namespace {
 
+int fail(Ctx* ctx, int status, const char* msg);
+int cuda_fail(Ctx* ctx, cudaError_t e, const char* where);
+int device_status(Ctx* ctx, uint32_t err);
+
+}  // namespace
+
+namespace ehgp {
+int abi_fail(Ctx* ctx, int status, const char* msg) { return fail(ctx, status, msg); }
+int abi_cuda_fail(Ctx* ctx, cudaError_t e, const char* where) { return cuda_fail(ctx, e, where); }
+int abi_device_status(Ctx* ctx, uint32_t err) { return device_status(ctx, err); }
+}  // namespace ehgp
+
+namespace {
+
 int fail(Ctx* ctx, int status, const char* msg) {
   if (ctx) ctx->last_error = msg;
   return status;
@@ -65,6 +79,8 @@ int lbvh_build_common(Ctx* ctx, const void* src, uint64_t n, const ehgp_lbvh_out
   ehgp::LbvhBuffers& b = ctx->lb;
   const uint32_t n32 = (uint32_t)n;
   ctx->built_n = 0;
+  ctx->geom_ready = false;
+  ctx->emst_ready = false;
   if (where == 0) {
     e = cudaMemcpyAsync(b.xyz_in, src, 3 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
   } else if (where == 1) {
@@ -96,8 +112,6 @@ int lbvh_build_common(Ctx* ctx, const void* src, uint64_t n, const ehgp_lbvh_out
 
 extern "C" {
 
-struct ehgp_ctx : ehgp::Ctx {};
-
 int ehgp_ctx_create(int device, const ehgp_limits* limits, ehgp_ctx** out_ctx) {
   if (!limits || !out_ctx || limits->max_points == 0 || limits->max_points > 0x7fffffffull)
     return EHGP_ERR_INVALID_ARGUMENT;
@@ -119,10 +133,11 @@ int ehgp_ctx_create(int device, const ehgp_limits* limits, ehgp_ctx** out_ctx) {
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     const double frac = (limits->hbm_fraction > 0.0 && limits->hbm_fraction <= 1.0) ? limits->hbm_fraction : 0.8;
-    const double estimate = 400.0 * (double)limits->max_points;  // bytes per point of the LBVH stage
+    const double estimate = 900.0 * (double)limits->max_points;  // bytes per point of the resident stages
     if (estimate > frac * (double)total_b || estimate > (double)free_b) e = cudaErrorMemoryAllocation;
   }
   if (e == cudaSuccess) e = ehgp::lbvh_alloc(*ctx);
+  if (e == cudaSuccess) e = ehgp::geom_alloc(*ctx);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) {
     const int st = (e == cudaErrorMemoryAllocation) ? EHGP_ERR_OUT_OF_MEMORY : EHGP_ERR_CUDA;

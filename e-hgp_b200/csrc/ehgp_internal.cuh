@@ -123,6 +123,47 @@ struct LbvhBuffers {
   uint64_t export_bytes = 0;
 };
 
+// Traversal node: outward-rounded binary32 box + children (32 bytes, two
+// 16-byte loads).  Leaves: left == kInvalid32, right = PointId.
+struct __align__(16) TNode {
+  float lo[3];
+  uint32_t left;
+  float hi[3];
+  uint32_t right;
+};
+
+// Buffers of the geometric stages (k-NN, Boruvka EMST, k=1 forest).
+struct GeomBuffers {
+  TNode* tnodes = nullptr;          // [2n]
+  uint32_t* leaf_node = nullptr;    // [n] postorder index of the leaf at sorted position i
+  int* scale = nullptr;             // [4]: S, max high bit, valid, spare
+  // k-NN
+  uint32_t* knn_ids = nullptr;      // [n * 11]
+  uint32_t* knn_meta = nullptr;     // [n * 2]: strict count, shell count
+  uint64_t* knn_cut = nullptr;      // [n * 4]: cutoff numerator limbs
+  // Boruvka
+  uint32_t* labels = nullptr;       // [n] frozen component label by PointId
+  uint32_t* nlabel = nullptr;       // [2n] uniform node label or kInvalid32 (mixed)
+  uint32_t* nflag = nullptr;        // [2n]
+  uint32_t* best_q = nullptr;       // [n]
+  double* best_d = nullptr;         // [n]
+  unsigned long long* comp_dbits = nullptr;  // [n]
+  uint32_t* comp_best = nullptr;    // [n]
+  uint32_t* uf = nullptr;           // [n]
+  uint32_t* counters = nullptr;     // [8]: components, minima, accepted
+  uint32_t* minima = nullptr;       // [4 * 2n]: per round log (label, source, u, v)
+  uint32_t* edge_u = nullptr;       // [n] accepted edges
+  uint32_t* edge_v = nullptr;       // [n]
+  uint64_t* key_u = nullptr;        // [n] sort keys
+  uint64_t* key_v = nullptr;
+  uint64_t* key_d = nullptr;
+  uint32_t* order0 = nullptr;       // [n]
+  uint32_t* order1 = nullptr;       // [n]
+  uint64_t* edge_D = nullptr;       // [n * 4] exact squared lengths, sorted order
+  uint32_t* sorted_u = nullptr;     // [n]
+  uint32_t* sorted_v = nullptr;     // [n]
+};
+
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -143,6 +184,13 @@ struct Ctx {
   uint32_t* lb_top_gmax = nullptr;      // [max_n] last group of top internal node
   std::vector<void*> allocations;
   uint64_t built_n = 0;            // points of the resident index (0 = none)
+  GeomBuffers gb;
+  bool geom_ready = false;         // traversal nodes + scale built for built_n
+  int scale_S = 0;                 // host copy of the cloud scale
+  bool scale_valid = false;
+  uint32_t emst_rounds = 0;
+  uint32_t emst_minima = 0;        // total per-round minima logged
+  bool emst_ready = false;
 };
 
 // Allocation helper: records the bytes on ctx.
@@ -156,4 +204,20 @@ uint64_t lbvh_enqueue(Ctx& ctx, uint32_t n, int input_kind);
 // Copies the requested snapshot parts to the host (synchronises).
 cudaError_t lbvh_export(Ctx& ctx, uint32_t n, const ehgp_lbvh_out* out);
 
+// Geometric stages (ehgp_geom.cu)
+cudaError_t geom_alloc(Ctx& ctx);
+// Traversal nodes, leaf map and cloud scale for the resident LBVH.
+uint64_t geom_prepare(Ctx& ctx, uint32_t n);
+
+}  // namespace ehgp
+
+extern "C" {
+struct ehgp_ctx : ehgp::Ctx {};
+}
+
+// Shared status helpers of the C ABI (ehgp_context.cu).
+namespace ehgp {
+int abi_fail(Ctx* ctx, int status, const char* msg);
+int abi_cuda_fail(Ctx* ctx, cudaError_t e, const char* where);
+int abi_device_status(Ctx* ctx, uint32_t err);
 }  // namespace ehgp

@@ -72,6 +72,29 @@ class LbvhOut(C.Structure):
     ]
 
 
+class KnnOut(C.Structure):
+    _fields_ = [("ids", C.c_void_p), ("meta", C.c_void_p), ("cutoff_num", C.c_void_p)]
+
+
+class EmstOut(C.Structure):
+    _fields_ = [("u", C.c_void_p), ("v", C.c_void_p), ("squared_length_num", C.c_void_p),
+                ("rounds", C.c_void_p), ("minima", C.c_void_p), ("minima_capacity", C.c_uint64),
+                ("minima_count", C.c_void_p)]
+
+
+class K1ForestOut(C.Structure):
+    _fields_ = [("level_num", C.c_void_p), ("nodes", C.c_void_p), ("child_ids", C.c_void_p),
+                ("batches", C.c_void_p), ("counts", C.c_void_p), ("root_node_id", C.c_void_p)]
+
+
+def limbs_to_int(a: np.ndarray) -> int:
+    """Little-endian 64-bit limbs -> Python int."""
+    v = 0
+    for w in reversed([int(x) for x in a]):
+        v = (v << 64) | w
+    return v
+
+
 _lib = None
 
 
@@ -94,6 +117,10 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "ehgp_lbvh_build_f32": (C.c_int, [P, P, C.c_uint64, C.POINTER(LbvhOut)]),
         "ehgp_lbvh_build_device": (C.c_int, [P, P, C.c_uint64, C.POINTER(LbvhOut)]),
         "ehgp_last_timing": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+        "ehgp_cloud_scale": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+        "ehgp_knn": (C.c_int, [P, C.c_uint32, C.POINTER(KnnOut)]),
+        "ehgp_emst": (C.c_int, [P, C.POINTER(EmstOut)]),
+        "ehgp_k1_forest": (C.c_int, [P, C.POINTER(K1ForestOut)]),
         "ehgp_lbvh_build_noalloc": (C.c_int, [P, C.c_uint64, C.POINTER(LbvhOut), P]),
         "ehgp_lbvh_noalloc_max_points": (C.c_uint64, []),
         "ehgp_lbvh_noalloc_scratch_bytes": (C.c_uint64, []),
@@ -224,6 +251,60 @@ class Context:
             pts = pts.astype(np.float64, copy=False)
             st = self.lib.ehgp_lbvh_build(self._h, _ptr(pts), n, C.byref(out))
         self._check(st)
+        self.n = n
         if snap is not None:
             snap.root = int(root[0])
         return snap
+
+    # ---- exact geometry of the resident cloud ----------------------------------
+    def scale(self) -> tuple[int, bool]:
+        s, valid = C.c_int32(), C.c_int32()
+        self._check(self.lib.ehgp_cloud_scale(self._h, C.byref(s), C.byref(valid)))
+        return s.value, bool(valid.value)
+
+    def knn(self, k: int) -> dict:
+        """ehgp_knn: per PointId, canonical top-k ids, (strict, shell) counts and
+        the exact cutoff as a Fraction."""
+        from fractions import Fraction
+        n = self.n
+        ids = np.empty((n, k), np.uint32)
+        meta = np.empty((n, 2), np.uint32)
+        cut = np.empty((n, 4), np.uint64)
+        out = KnnOut(_ptr(ids), _ptr(meta), _ptr(cut))
+        self._check(self.lib.ehgp_knn(self._h, k, C.byref(out)))
+        S, _ = self.scale()
+        den = 1 << (2 * S)
+        return {"ids": ids, "meta": meta, "cutoff_num": cut,
+                "cutoff": [Fraction(limbs_to_int(c), den) for c in cut]}
+
+    def emst(self, with_minima: bool = True) -> dict:
+        """ehgp_emst: EMST edges in (squared length, u, v) order with exact lengths."""
+        n = self.n
+        m = max(n - 1, 0)
+        u = np.empty(max(m, 1), np.uint32)
+        v = np.empty(max(m, 1), np.uint32)
+        D = np.empty((max(m, 1), 4), np.uint64)
+        rounds = np.zeros(1, np.uint32)
+        cap = 2 * n if with_minima else 0
+        minima = np.empty((max(cap, 1), 4), np.uint32)
+        mcount = np.zeros(1, np.uint64)
+        out = EmstOut(_ptr(u), _ptr(v), _ptr(D), _ptr(rounds), _ptr(minima) if cap else None, cap, _ptr(mcount))
+        self._check(self.lib.ehgp_emst(self._h, C.byref(out)))
+        mc = int(mcount[0]) if cap else 0
+        return {"u": u[:m], "v": v[:m], "D": D[:m], "rounds": int(rounds[0]), "minima": minima[:mc]}
+
+    def k1_forest(self) -> dict:
+        """ehgp_k1_forest on the last EMST: reference-layout compact forest arenas."""
+        n = self.n
+        m = max(n - 1, 1)
+        lv = np.empty((m, 4), np.uint64)
+        nodes = np.empty((m, 6), np.uint64)
+        child = np.empty(2 * m, np.uint64)
+        batches = np.empty((m, 7), np.uint64)
+        counts = np.zeros(4, np.uint64)
+        root = np.zeros(1, np.uint64)
+        out = K1ForestOut(_ptr(lv), _ptr(nodes), _ptr(child), _ptr(batches), _ptr(counts), _ptr(root))
+        self._check(self.lib.ehgp_k1_forest(self._h, C.byref(out)))
+        L, N, Ch, B = (int(x) for x in counts)
+        return {"level_num": lv[:L], "nodes": nodes[:N], "children": child[:Ch], "batches": batches[:B],
+                "root": int(root[0])}

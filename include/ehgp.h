@@ -127,6 +127,60 @@ int ehgp_lbvh_build_f32(ehgp_ctx* ctx, const float* xyz, uint64_t n, const ehgp_
  * (interleaved binary64, 3n values); no host->device copy of the points. */
 int ehgp_lbvh_build_device(ehgp_ctx* ctx, const double* d_xyz, uint64_t n, const ehgp_lbvh_out* out);
 
+/* ---- exact geometry of the resident cloud --------------------------------- */
+/* Exact fixed-point scale of the resident cloud: every coordinate x is the
+ * integer x * 2^S, and every squared distance below is an integer numerator
+ * N with value N / 2^(2S).  *valid = 0 when some |x| * 2^S >= 2^124; the exact
+ * stages then return EHGP_ERR_NUMERIC_RANGE. */
+int ehgp_cloud_scale(ehgp_ctx* ctx, int32_t* scale_exponent, int32_t* valid);
+
+typedef struct ehgp_knn_out {
+  uint32_t* ids;        /* [n*k]: per PointId p, its top-k canonical choice in (squared distance, PointId) order */
+  uint32_t* meta;       /* [n*2]: (points strictly below the cutoff, points exactly at the cutoff) */
+  uint64_t* cutoff_num; /* [n*4]: k-th squared distance numerator, 64-bit limbs, little endian, scale 2^-2S */
+} ehgp_knn_out;
+
+/* Exact k nearest other points (k <= 11) of every point of the resident cloud.
+ * Replaces spatial::lbvh_top_k(index, cloud, query = point p, k, exclusions = {p})
+ * (include/morsehgp3d/spatial/lbvh.hpp:424-430) for all p at once: the cutoff is
+ * the k-th smallest exact squared distance, `meta` gives the strict count and
+ * the COMPLETE equality-shell size, `ids` the canonical choice (strict points,
+ * then the least shell PointIds; TopKPartition, src/cpu/spatial/brute_force.cpp:319-384). */
+int ehgp_knn(ehgp_ctx* ctx, uint32_t k, const ehgp_knn_out* out);
+
+typedef struct ehgp_emst_out {
+  uint32_t* u;                  /* [n-1]: u < v, ordered by (squared length, u, v) */
+  uint32_t* v;                  /* [n-1] */
+  uint64_t* squared_length_num; /* [(n-1)*4]: exact numerators at scale 2^-2S (merge level = 1/4 of it) */
+  uint32_t* rounds;             /* [1]: Boruvka rounds */
+  uint32_t* minima;             /* [minima_capacity*4]: (round, component label, source PointId, target PointId) */
+  uint64_t minima_capacity;
+  uint64_t* minima_count;       /* [1] */
+} ehgp_emst_out;
+
+/* Exact Euclidean minimum spanning tree by LBVH Boruvka with frozen
+ * least-PointId labels and kappa = (squared length, u, v) minima.  Replaces
+ * hierarchy::build_exact_lbvh_boruvka (include/morsehgp3d/hierarchy/boruvka.hpp:130)
+ * and gpu::build_gpu_proposed_cpu_exact_k1_boruvka
+ * (include/morsehgp3d/gpu/k1_boruvka.hpp:1004): decisions are exact on the
+ * device, no CPU replay. */
+int ehgp_emst(ehgp_ctx* ctx, const ehgp_emst_out* out);
+
+typedef struct ehgp_k1_forest_out {
+  uint64_t* level_num;    /* [(n-1)*4]: batch squared lengths (numerators, scale 2^-2S); level = length / 4 */
+  uint64_t* nodes;        /* [(n-1)*6]: id, level_index, child_offset, child_count, minimum_point_id, coverage_size */
+  uint64_t* child_ids;    /* [2(n-1)]: child arena (leaves are PointIds, merge nodes n, n+1, ...) */
+  uint64_t* batches;      /* [(n-1)*7]: level_index, edge_offset, edge_count, node_offset, node_count, pre, post */
+  uint64_t* counts;       /* [4]: levels, merge nodes, child references, batches */
+  uint64_t* root_node_id; /* [1] */
+} ehgp_k1_forest_out;
+
+/* Compact k=1 merge forest of the last ehgp_emst result: equal-length batches
+ * frozen before each batch, one (multi)fusion node per connected group.
+ * Replaces hierarchy::build_compact_k1_forest(point_count, edges)
+ * (include/morsehgp3d/hierarchy/k1_forest.hpp:108) with the same arenas. */
+int ehgp_k1_forest(ehgp_ctx* ctx, const ehgp_k1_forest_out* out);
+
 /* Allocation-free LBVH build.  No counterpart in the reference: it exists for
  * callers that may not call cudaMalloc (a host framework that owns all device
  * memory through its own pool, or a latency-critical caller that cannot

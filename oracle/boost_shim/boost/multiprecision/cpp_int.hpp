@@ -381,6 +381,16 @@ class cpp_int {
       q = cpp_int(); r = std::move(ra);
       return;
     }
+    if (a.size_ <= 2) {  // both magnitudes fit 128 bits
+      const limb* ad = a.data(); const limb* bd = b.data();
+      const dlimb x = (dlimb)ad[0] | (a.size_ > 1 ? (dlimb)ad[1] << 64 : 0);
+      const dlimb y = (dlimb)bd[0] | (b.size_ > 1 ? (dlimb)bd[1] << 64 : 0);
+      cpp_int qq, rr;
+      qq.set_u128(x / y, false);
+      rr.set_u128(x % y, false);
+      q = std::move(qq); r = std::move(rr);
+      return;
+    }
     if (b.size_ == 1) {
       cpp_int qa = a; qa.neg_ = false;
       limb rem = qa.div_small_inplace(b.data()[0]);
@@ -390,9 +400,12 @@ class cpp_int {
     }
     const unsigned n = b.size_, m = a.size_ - b.size_;
     const unsigned s = (unsigned)__builtin_clzll(b.data()[n - 1]);
-    // normalised copies
-    limb* vn = new limb[n];
-    limb* un = new limb[a.size_ + 1];
+    // normalised copies (on the stack for operands up to 32 limbs)
+    constexpr unsigned kStackLimbs = 32;
+    limb vbuf[kStackLimbs], ubuf[kStackLimbs + 1];
+    const bool heap = n > kStackLimbs || a.size_ + 1 > kStackLimbs + 1;
+    limb* vn = heap ? new limb[n] : vbuf;
+    limb* un = heap ? new limb[a.size_ + 1] : ubuf;
     const limb* vb = b.data(); const limb* ua = a.data();
     for (unsigned i = n - 1; i > 0; --i)
       vn[i] = s ? (vb[i] << s) | (vb[i - 1] >> (64 - s)) : vb[i];
@@ -441,7 +454,7 @@ class cpp_int {
     for (unsigned i = 0; i < n; ++i)
       rd[i] = s ? (un[i] >> s) | (un[i + 1] << (64 - s)) : un[i];
     rr.neg_ = false; rr.trim();
-    delete[] vn; delete[] un;
+    if (heap) { delete[] vn; delete[] un; }
     q = std::move(qq); r = std::move(rr);
   }
   void shl(unsigned long long s) {

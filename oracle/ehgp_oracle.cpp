@@ -203,6 +203,230 @@ Lbvh build_lbvh(const Cloud& c) {
   return t;
 }
 
+// ---- exact geometry at one dyadic scale ------------------------------------------
+// Every canonical coordinate as an integer numerator over 2^S (S = the largest
+// fractional bit count); squared distances are then integers over 2^(2S).
+struct FixedCloud {
+  std::vector<std::array<Big, 3>> X;
+  int S = 0;
+};
+
+FixedCloud fixed_cloud(const Cloud& c) {
+  FixedCloud f;
+  int S = 0;
+  for (const auto& p : c.bits)
+    for (int a = 0; a < 3; ++a) {
+      const Dyadic d = decode(p[a]);
+      if (d.sig == 0) continue;
+      const long long m = d.sig < 0 ? -d.sig : d.sig;
+      S = std::max(S, -(d.exp + __builtin_ctzll((u64)m)));
+    }
+  f.S = S;
+  f.X.resize(c.bits.size());
+  for (size_t i = 0; i < c.bits.size(); ++i)
+    for (int a = 0; a < 3; ++a) {
+      const Dyadic d = decode(c.bits[i][a]);
+      Big v = d.sig;
+      const int sh = d.exp + S;
+      if (d.sig != 0) {
+        if (sh >= 0) v <<= (unsigned)sh;
+        else v /= (Big(1) << (unsigned)(-sh));  // exact: S bounds the fractional bits
+      }
+      f.X[i][a] = v;
+    }
+  return f;
+}
+
+Big dist2(const FixedCloud& f, u64 a, u64 b) {
+  Big s = 0;
+  for (int k = 0; k < 3; ++k) {
+    const Big d = f.X[a][k] - f.X[b][k];
+    s += d * d;
+  }
+  return s;
+}
+
+// reduced "num den" of N / 2^e
+std::string reduced(Big N, int e) {
+  while (e > 0 && N != 0 && (N % 2) == 0) {
+    N /= 2;
+    --e;
+  }
+  if (N == 0) e = 0;
+  return N.str() + " " + (Big(1) << (unsigned)e).str();
+}
+
+// Brute-force exact top-k with exclusions {p}: the partition of
+// TopKPartition::from_evaluated_neighbors (src/cpu/spatial/brute_force.cpp:319-384).
+std::string knn_text(const Cloud& c, u64 k) {
+  const FixedCloud f = fixed_cloud(c);
+  const u64 n = c.bits.size();
+  std::string s;
+  std::vector<std::pair<Big, u64>> nb;
+  for (u64 p = 0; p < n; ++p) {
+    nb.clear();
+    for (u64 q = 0; q < n; ++q)
+      if (q != p) nb.emplace_back(dist2(f, p, q), q);
+    std::sort(nb.begin(), nb.end());
+    const Big cut = nb[k - 1].first;
+    std::string strict, shell;
+    for (const auto& [d, q] : nb) {
+      if (d < cut) strict += std::to_string(q) + " ";
+      else if (d == cut) shell += " " + std::to_string(q);
+      else break;
+    }
+    s += strict + "|" + shell + " | " + reduced(cut, 2 * f.S) + "\n";
+  }
+  return s;
+}
+
+struct Edge {
+  Big D;
+  u64 u, v;
+  bool operator<(const Edge& o) const {
+    if (D != o.D) return D < o.D;
+    if (u != o.u) return u < o.u;
+    return v < o.v;
+  }
+};
+
+struct MinDsu {  // union by least index (src/cpu/hierarchy/k1_forest.cpp:19-62)
+  std::vector<u64> p;
+  u64 count;
+  explicit MinDsu(u64 n) : p(n), count(n) {
+    for (u64 i = 0; i < n; ++i) p[i] = i;
+  }
+  u64 find(u64 x) {
+    while (p[x] != x) x = p[x] = p[p[x]];
+    return x;
+  }
+  bool unite(u64 a, u64 b) {
+    a = find(a);
+    b = find(b);
+    if (a == b) return false;
+    if (a > b) std::swap(a, b);
+    p[b] = a;
+    --count;
+    return true;
+  }
+};
+
+// Exact EMST + Boruvka rounds + compact k=1 forest, text format of
+// ref_emst_forest (oracle/ref_driver.cpp).
+//  * Boruvka rounds with labels frozen to least PointIds and kappa minima
+//    (include/morsehgp3d/hierarchy/boruvka.hpp:1-140), O(n^2) per round;
+//  * the compact forest of build_compact_k1_forest
+//    (src/cpu/hierarchy/k1_forest.cpp:665-845): equal-length batches frozen
+//    pre-batch, one merge node per connected group of >= 2 pre-batch
+//    components, ordered by the group's least PointId, children ordered by
+//    their least PointId, node ids n, n+1, ...
+std::string emst_forest_text(const Cloud& c) {
+  const FixedCloud f = fixed_cloud(c);
+  const u64 n = c.bits.size();
+  const int e2 = 2 * f.S;
+  std::string s, minima_s;
+  std::vector<u64> label(n);
+  for (u64 i = 0; i < n; ++i) label[i] = i;
+  std::vector<Edge> tree;
+  u64 components = n, round = 0;
+  while (components > 1) {
+    std::vector<bool> has(n, false);
+    std::vector<Edge> best(n);
+    std::vector<u64> src(n);
+    for (u64 p = 0; p < n; ++p)
+      for (u64 q = 0; q < n; ++q) {
+        if (label[q] == label[p]) continue;
+        Edge e{dist2(f, p, q), std::min(p, q), std::max(p, q)};
+        const u64 cp = label[p];
+        if (!has[cp] || e < best[cp]) {
+          has[cp] = true;
+          best[cp] = e;
+          src[cp] = p;
+        }
+      }
+    std::vector<Edge> accepted;
+    for (u64 cpn = 0; cpn < n; ++cpn)
+      if (has[cpn]) {
+        const Edge& e = best[cpn];
+        minima_s += "M " + std::to_string(round) + " " + std::to_string(cpn) + " " + std::to_string(src[cpn]) + " " +
+                    std::to_string(e.u) + " " + std::to_string(e.v) + " " + reduced(e.D, e2) + "\n";
+        accepted.push_back(e);
+      }
+    std::sort(accepted.begin(), accepted.end());
+    accepted.erase(std::unique(accepted.begin(), accepted.end(),
+                               [](const Edge& a, const Edge& b) { return a.u == b.u && a.v == b.v; }),
+                   accepted.end());
+    MinDsu d(n);
+    for (u64 p = 0; p < n; ++p) d.unite(p, label[p]);
+    for (const Edge& e : accepted) {
+      minima_s += "A " + std::to_string(round) + " " + std::to_string(e.u) + " " + std::to_string(e.v) + "\n";
+      d.unite(e.u, e.v);
+      tree.push_back(e);
+    }
+    for (u64 p = 0; p < n; ++p) label[p] = d.find(p);
+    components = d.count;
+    ++round;
+  }
+  std::sort(tree.begin(), tree.end());
+  for (const Edge& e : tree)
+    s += "E " + std::to_string(e.u) + " " + std::to_string(e.v) + " " + reduced(e.D, e2) + "\n";
+  s += minima_s;
+  // compact k=1 forest
+  MinDsu comp(n);
+  std::vector<u64> node_of(n), min_pt, cover;  // per root: current node id
+  for (u64 i = 0; i < n; ++i) node_of[i] = i;
+  std::string levels_s, nodes_s, child_s = "C", batches_s;
+  u64 merge_count = 0, child_count_total = 0;
+  auto coverage = [&](u64 id) { return id < n ? u64{1} : cover[id - n]; };
+  for (size_t b = 0, level = 0; b < tree.size(); ++level) {
+    size_t e = b + 1;
+    while (e < tree.size() && tree[e].D == tree[b].D) ++e;
+    levels_s += "L " + reduced(tree[b].D, e2 + 2) + "\n";
+    const u64 pre = comp.count, node_off = merge_count;
+    std::vector<u64> roots;
+    for (size_t i = b; i < e; ++i) {
+      roots.push_back(comp.find(tree[i].u));
+      roots.push_back(comp.find(tree[i].v));
+    }
+    std::sort(roots.begin(), roots.end());
+    roots.erase(std::unique(roots.begin(), roots.end()), roots.end());
+    MinDsu local(roots.size());
+    auto pos = [&](u64 r) { return (u64)(std::lower_bound(roots.begin(), roots.end(), r) - roots.begin()); };
+    for (size_t i = b; i < e; ++i) local.unite(pos(comp.find(tree[i].u)), pos(comp.find(tree[i].v)));
+    std::vector<std::vector<u64>> groups(roots.size());
+    for (u64 li = 0; li < roots.size(); ++li) groups[local.find(li)].push_back(roots[li]);
+    std::vector<std::pair<std::vector<u64>, u64>> pending;
+    for (auto& g : groups) {
+      if (g.empty()) continue;
+      const u64 id = n + merge_count++;
+      u64 cov = 0;
+      for (u64 r : g) {
+        child_s += " " + std::to_string(node_of[r]);
+        cov += coverage(node_of[r]);
+      }
+      nodes_s += "N " + std::to_string(id) + " " + std::to_string(level) + " " + std::to_string(child_count_total) +
+                 " " + std::to_string(g.size()) + " " + std::to_string(g.front()) + " " + std::to_string(cov) + "\n";
+      child_count_total += g.size();
+      cover.push_back(cov);
+      pending.emplace_back(g, id);
+    }
+    for (size_t i = b; i < e; ++i) comp.unite(tree[i].u, tree[i].v);
+    for (auto& [g, id] : pending) node_of[comp.find(g.front())] = id;
+    batches_s += "B " + std::to_string(level) + " " + std::to_string(b) + " " + std::to_string(e - b) + " " +
+                 std::to_string(node_off) + " " + std::to_string(merge_count - node_off) + " " + std::to_string(pre) +
+                 " " + std::to_string(comp.count) + "\n";
+    b = e;
+  }
+  s += levels_s + nodes_s + child_s + "\n" + batches_s + "R " + std::to_string(node_of[comp.find(0)]) + "\n";
+  return s;
+}
+
+u64 put_text(const std::string& s, char* buf, u64 cap) {
+  if (s.size() + 1 > cap) return s.size() + 1;
+  std::memcpy(buf, s.c_str(), s.size() + 1);
+  return 0;
+}
+
 int report(const std::exception& e, char* err, u64 errlen, int code) {
   if (err && errlen) {
     std::strncpy(err, e.what(), errlen - 1);
@@ -256,6 +480,24 @@ int oracle_lbvh_build(const double* xyz, u64 n, u64* source_index, u64* leaves, 
     return report(e, err, errlen, 1);
   } catch (const std::exception& e) {
     return report(e, err, errlen, 2);
+  }
+}
+
+int oracle_knn(const double* xyz, u64 n, u64 k, char* out, u64 cap, u64* needed, char* err, u64 errlen) {
+  try {
+    *needed = put_text(knn_text(canonical_cloud(xyz, n), k), out, cap);
+    return 0;
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 1);
+  }
+}
+
+int oracle_emst_forest(const double* xyz, u64 n, char* out, u64 cap, u64* needed, char* err, u64 errlen) {
+  try {
+    *needed = put_text(emst_forest_text(canonical_cloud(xyz, n)), out, cap);
+    return 0;
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 1);
   }
 }
 

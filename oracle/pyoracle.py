@@ -16,6 +16,7 @@ import ctypes as C
 import os
 
 import numpy as np
+from fractions import Fraction
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATEMENT = os.path.join(HERE, "lib", "libehgp_oracle.so")
@@ -95,3 +96,70 @@ def ref_lbvh_certify(points: np.ndarray, snap) -> tuple[bool, str]:
     rc = fn(C.c_void_p(_p(pts)), C.c_uint64(n), C.c_void_p(_p(leaves)), C.c_void_p(_p(nodes)),
             C.c_void_p(_p(counters)), C.c_void_p(_p(aabb)), C.c_uint64(int(snap.root)), err, C.c_uint64(512))
     return rc == 0, err.value.decode()
+
+
+def _text_call(fn_name: str, which: str, pts: np.ndarray, *extra) -> str:
+    """Calls a text-blob oracle entry point, growing the buffer when needed."""
+    lib = _lib(which)
+    fn = getattr(lib, fn_name)
+    fn.restype = C.c_int
+    pts = np.ascontiguousarray(pts, dtype=np.float64)
+    cap = 1 << 20
+    for _ in range(3):
+        buf = C.create_string_buffer(cap)
+        needed = C.c_uint64(0)
+        err = C.create_string_buffer(512)
+        secs = np.zeros(4)
+        args = [C.c_void_p(_p(pts)), C.c_uint64(len(pts)), *[C.c_uint64(x) for x in extra], buf,
+                C.c_uint64(cap), C.byref(needed)]
+        if which == "reference":
+            args.append(C.c_void_p(_p(secs)))
+        args += [err, C.c_uint64(512)]
+        rc = fn(*args)
+        if rc != 0:
+            raise OracleError(rc, err.value.decode())
+        if needed.value == 0:
+            _text_call.seconds = secs
+            return buf.value.decode()
+        cap = int(needed.value) + 16
+    raise RuntimeError("oracle output did not fit")
+
+
+def knn(points: np.ndarray, k: int, which: str = "restatement") -> list[tuple[list[int], list[int], Fraction]]:
+    """Per PointId p: (strict ids in (d, id) order, shell ids, cutoff squared distance)."""
+    name = "oracle_knn" if which == "restatement" else "ref_knn"
+    out = []
+    for line in _text_call(name, which, points, k).splitlines():
+        strict, shell, cut = line.split("|")
+        num, den = cut.split()
+        out.append(([int(x) for x in strict.split()], [int(x) for x in shell.split()], Fraction(int(num), int(den))))
+    return out
+
+
+def emst_forest(points: np.ndarray, which: str = "restatement") -> dict:
+    """EMST edges, Boruvka minima/accepted per round and the compact k=1 forest."""
+    name = "oracle_emst_forest" if which == "restatement" else "ref_emst_forest"
+    r = {"edges": [], "minima": [], "accepted": [], "levels": [], "nodes": [], "children": [], "batches": [],
+         "root": None}
+    for line in _text_call(name, which, points).splitlines():
+        t = line.split()
+        if not t:
+            continue
+        tag, f = t[0], t[1:]
+        if tag == "E":
+            r["edges"].append((int(f[0]), int(f[1]), Fraction(int(f[2]), int(f[3]))))
+        elif tag == "M":
+            r["minima"].append((int(f[0]), int(f[1]), int(f[2]), int(f[3]), int(f[4]), Fraction(int(f[5]), int(f[6]))))
+        elif tag == "A":
+            r["accepted"].append(tuple(int(x) for x in f))
+        elif tag == "L":
+            r["levels"].append(Fraction(int(f[0]), int(f[1])))
+        elif tag == "N":
+            r["nodes"].append(tuple(int(x) for x in f))
+        elif tag == "C":
+            r["children"] = [int(x) for x in f]
+        elif tag == "B":
+            r["batches"].append(tuple(int(x) for x in f))
+        elif tag == "R":
+            r["root"] = int(f[0])
+    return r

@@ -162,4 +162,106 @@ int ref_lbvh_certify(const double* xyz, uint64_t n, const uint64_t* leaves, cons
   }
 }
 
+// Text-blob outputs below: one record per line, fields separated by spaces.
+// Returns the number of bytes needed when `cap` is too small (nothing written).
+static uint64_t put_text(const std::string& s, char* buf, uint64_t cap) {
+  if (s.size() + 1 > cap) return s.size() + 1;
+  std::memcpy(buf, s.c_str(), s.size() + 1);
+  return 0;
+}
+
+// lbvh_top_k for every point p with exclusions {p}
+// (include/morsehgp3d/spatial/lbvh.hpp:424).  Line p:
+// "<strict ids (d,id) order> | <shell ids> | num den".
+int ref_knn(const double* xyz, uint64_t n, uint64_t k, char* out, uint64_t cap, uint64_t* needed, double* seconds,
+            char* err, uint64_t errlen) {
+  try {
+    using namespace morsehgp3d;
+    const auto pts = points_from(xyz, n);
+    const CanonicalPointCloud cloud = CanonicalPointCloud::rejecting_duplicates(pts);
+    const MortonLbvhIndex index = MortonLbvhIndex::build(cloud);
+    std::string s;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (uint64_t p = 0; p < n; ++p) {
+      const std::vector<spatial::PointId> ex{p};
+      const auto exclusions = spatial::ExclusionSet::from_ids(ex, cloud, 9);
+      const auto part = spatial::lbvh_top_k(index, cloud, cloud.point(p).exact(), k, exclusions);
+      for (const auto& nb : part.strict_below()) s += std::to_string(nb.point_id) + " ";
+      s += "|";
+      for (const auto id : part.cutoff_shell_ids()) s += " " + std::to_string(id);
+      s += " | " + part.cutoff_squared_distance().numerator_string() + " " +
+           part.cutoff_squared_distance().denominator_string() + "\n";
+    }
+    if (seconds) seconds[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *needed = put_text(s, out, cap);
+    return 0;
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 1);
+  }
+}
+
+}  // extern "C"
+
+#include "morsehgp3d/hierarchy/boruvka.hpp"
+#include "morsehgp3d/hierarchy/k1_forest.hpp"
+
+extern "C" {
+
+// build_exact_lbvh_boruvka (include/morsehgp3d/hierarchy/boruvka.hpp:130) and
+// build_compact_k1_forest on its edges (include/morsehgp3d/hierarchy/k1_forest.hpp:108).
+// Lines: "E u v num den" (EMST, canonical order), "M round label source u v num den"
+// (component minima), "A round u v" (accepted), "L num den" (forest levels),
+// "N id level_index child_offset child_count min_point coverage" (merge nodes),
+// "C child..." (child arena), "B level_index edge_off edge_cnt node_off node_cnt pre post",
+// "R root".  seconds[0] = Boruvka, seconds[1] = forest.
+int ref_emst_forest(const double* xyz, uint64_t n, char* out, uint64_t cap, uint64_t* needed, double* seconds,
+                    char* err, uint64_t errlen) {
+  try {
+    using namespace morsehgp3d;
+    const auto pts = points_from(xyz, n);
+    const CanonicalPointCloud cloud = CanonicalPointCloud::rejecting_duplicates(pts);
+    const MortonLbvhIndex index = MortonLbvhIndex::build(cloud);
+    const auto t0 = std::chrono::steady_clock::now();
+    const auto res = hierarchy::build_exact_lbvh_boruvka(index, cloud);
+    const auto t1 = std::chrono::steady_clock::now();
+    const auto forest = hierarchy::build_compact_k1_forest(n, res.emst_edges);
+    const auto t2 = std::chrono::steady_clock::now();
+    if (seconds) {
+      seconds[0] = std::chrono::duration<double>(t1 - t0).count();
+      seconds[1] = std::chrono::duration<double>(t2 - t1).count();
+    }
+    std::string s;
+    for (const auto& e : res.emst_edges)
+      s += "E " + std::to_string(e.u) + " " + std::to_string(e.v) + " " + e.squared_length.numerator_string() + " " +
+           e.squared_length.denominator_string() + "\n";
+    for (const auto& r : res.rounds) {
+      for (const auto& m : r.component_minima)
+        s += "M " + std::to_string(r.round_index) + " " + std::to_string(m.component_label) + " " +
+             std::to_string(m.source_point_id) + " " + std::to_string(m.outgoing_edge.u) + " " +
+             std::to_string(m.outgoing_edge.v) + " " + m.outgoing_edge.squared_length.numerator_string() + " " +
+             m.outgoing_edge.squared_length.denominator_string() + "\n";
+      for (const auto& a : r.accepted_edges)
+        s += "A " + std::to_string(r.round_index) + " " + std::to_string(a.u) + " " + std::to_string(a.v) + "\n";
+    }
+    for (const auto& l : forest.levels) s += "L " + l.numerator_string() + " " + l.denominator_string() + "\n";
+    for (const auto& nd : forest.merge_nodes)
+      s += "N " + std::to_string(nd.id) + " " + std::to_string(nd.level_index) + " " +
+           std::to_string(nd.child_offset) + " " + std::to_string(nd.child_count) + " " +
+           std::to_string(nd.minimum_point_id) + " " + std::to_string(nd.coverage_size) + "\n";
+    s += "C";
+    for (const auto c : forest.child_ids) s += " " + std::to_string(c);
+    s += "\n";
+    for (const auto& b : forest.equal_level_batches)
+      s += "B " + std::to_string(b.level_index) + " " + std::to_string(b.selected_edge_offset) + " " +
+           std::to_string(b.selected_edge_count) + " " + std::to_string(b.merge_node_offset) + " " +
+           std::to_string(b.merge_node_count) + " " + std::to_string(b.pre_batch_component_count) + " " +
+           std::to_string(b.post_batch_component_count) + "\n";
+    s += "R " + std::to_string(forest.root_node_id) + "\n";
+    *needed = put_text(s, out, cap);
+    return 0;
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 1);
+  }
+}
+
 }  // extern "C"

@@ -1,0 +1,88 @@
+"""Helpers shared by the k-NN / EMST / k=1 forest tests: conversion of the
+CUDA path's outputs and of golden fixtures to the oracle's text-record form."""
+from fractions import Fraction
+import json
+
+import numpy as np
+
+import ehgp
+
+
+def load_golden(path):
+    d = json.load(open(path))
+    F = lambda x: Fraction(int(x[0]), int(x[1]))
+    return {
+        "points": np.array(d["points"], dtype=np.float64),
+        "knn11": [(s, sh, F(c)) for s, sh, c in d["knn11"]],
+        "emst": {
+            "edges": [(u, v, F(x)) for u, v, x in d["edges"]],
+            "minima": [(r, l, s, u, v, F(x)) for r, l, s, u, v, x in d["minima"]],
+            "accepted": [tuple(a) for a in d["accepted"]],
+            "levels": [F(x) for x in d["levels"]],
+            "nodes": [tuple(n) for n in d["nodes"]],
+            "children": d["children"],
+            "batches": [tuple(b) for b in d["batches"]],
+            "root": d["root"],
+        },
+    }
+
+
+def gpu_knn_records(ctx, k):
+    """ehgp_knn output as (strict ids, first shell ids, shell size, cutoff) per PointId."""
+    r = ctx.knn(k)
+    out = []
+    for p in range(len(r["ids"])):
+        strict, shell = (int(x) for x in r["meta"][p])
+        ids = [int(x) for x in r["ids"][p]]
+        out.append((ids[:strict], ids[strict:], shell, r["cutoff"][p]))
+    return out
+
+
+def knn_matches(gpu, ref, k):
+    """gpu: gpu_knn_records; ref: oracle (strict, shell, cutoff) list."""
+    assert len(gpu) == len(ref)
+    for p, ((gs, gsh, gshell, gc), (rs, rsh, rc)) in enumerate(zip(gpu, ref)):
+        assert gs == rs, (p, gs, rs)
+        assert gsh == rsh[: k - len(rs)], (p, gsh, rsh)
+        assert gshell == len(rsh), (p, gshell, len(rsh))
+        assert gc == rc, (p, gc, rc)
+
+
+def gpu_emst_forest(ctx):
+    """ehgp_emst + ehgp_k1_forest in the oracle's record form."""
+    S, valid = ctx.scale()
+    assert valid
+    den = 1 << (2 * S)
+    e = ctx.emst()
+    D = [ehgp.limbs_to_int(x) for x in e["D"]]
+    edges = [(int(u), int(v), Fraction(d, den)) for u, v, d in zip(e["u"], e["v"], D)]
+
+    def d2(a, b):
+        return None  # squared lengths of minima come from the edge list
+
+    lengths = {(u, v): x for u, v, x in edges}
+    minima, accepted = [], []
+    for rnd, label, src, tgt in (tuple(int(x) for x in m) for m in e["minima"]):
+        u, v = min(src, tgt), max(src, tgt)
+        minima.append((rnd, label, src, u, v, lengths.get((u, v))))
+    minima.sort()
+    by_round = {}
+    for rnd, _, _, u, v, x in minima:
+        by_round.setdefault(rnd, set()).add((x, u, v))
+    for rnd in sorted(by_round):
+        for x, u, v in sorted(by_round[rnd]):
+            accepted.append((rnd, u, v))
+    f = ctx.k1_forest()
+    levels = [Fraction(ehgp.limbs_to_int(x), den) / 4 for x in f["level_num"]]
+    return {
+        "edges": edges, "minima": minima, "accepted": accepted, "levels": levels,
+        "nodes": [tuple(int(x) for x in nd) for nd in f["nodes"]],
+        "children": [int(x) for x in f["children"]],
+        "batches": [tuple(int(x) for x in b) for b in f["batches"]],
+        "root": f["root"], "rounds": e["rounds"],
+    }
+
+
+def emst_forest_matches(gpu, ref):
+    for key in ("edges", "minima", "accepted", "levels", "nodes", "children", "batches", "root"):
+        assert gpu[key] == ref[key], key

@@ -3,7 +3,7 @@ own CPU code (oracle/_ref/libehgp_ref.so: CanonicalPointCloud::rejecting_duplica
 + MortonLbvhIndex::build, compiled from morsehgp3d/src/cpu against the
 project-written Boost shim).  Run here, where the reference tree exists:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py && python tests/golden/make_golden.py --geom
 """
 import os
 import sys
@@ -46,5 +46,42 @@ def main():
         print(name, len(pts), r["counters"])
 
 
-if __name__ == "__main__":
+if __name__ == "__main__" and "--geom" not in sys.argv:
     main()
+
+
+def geom_cases():
+    yield "uniform64_s2", workloads.uniform_cube(64, 2)
+    yield "lattice4_f32", workloads.jittered_lattice(4, 4).astype(np.float64)
+    g = np.round(workloads.uniform_cube(120, 8) * 4) / 4 + 0.0  # quarter grid: many exact ties
+    yield "grid120", np.unique(g, axis=0)
+
+
+def frac(x):
+    return [str(x.numerator), str(x.denominator)]
+
+
+def main_geom():
+    import json
+    for name, pts in geom_cases():
+        knn = pyoracle.knn(pts, 11, "reference")
+        ef = pyoracle.emst_forest(pts, "reference")
+        doc = {
+            "points": pts.tolist(),
+            "knn11": [[s, sh, frac(c)] for s, sh, c in knn],
+            "edges": [[u, v, frac(d)] for u, v, d in ef["edges"]],
+            "minima": [[r, l, s, u, v, frac(d)] for r, l, s, u, v, d in ef["minima"]],
+            "accepted": [list(a) for a in ef["accepted"]],
+            "levels": [frac(x) for x in ef["levels"]],
+            "nodes": [list(nd) for nd in ef["nodes"]],
+            "children": ef["children"],
+            "batches": [list(b) for b in ef["batches"]],
+            "root": ef["root"],
+        }
+        with open(os.path.join(HERE, f"geom_{name}.json"), "w") as f:
+            json.dump(doc, f, separators=(",", ":"))
+        print(name, len(pts), len(ef["nodes"]))
+
+
+if __name__ == "__main__" and "--geom" in sys.argv:
+    main_geom()
