@@ -138,6 +138,7 @@ int ehgp_ctx_create(int device, const ehgp_limits* limits, ehgp_ctx** out_ctx) {
   }
   if (e == cudaSuccess) e = ehgp::lbvh_alloc(*ctx);
   if (e == cudaSuccess) e = ehgp::geom_alloc(*ctx);
+  if (e == cudaSuccess) e = ehgp::pairs_alloc(*ctx);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) {
     const int st = (e == cudaErrorMemoryAllocation) ? EHGP_ERR_OUT_OF_MEMORY : EHGP_ERR_CUDA;

@@ -164,6 +164,23 @@ struct GeomBuffers {
   uint32_t* sorted_v = nullptr;     // [n]
 };
 
+// Buffers of the pair-support stage.
+struct PairBuffers {
+  uint32_t* W = nullptr;            // [n * 32] witness lists (32 nearest, FP64 order)
+  double* R2 = nullptr;             // [n] squared witness radius
+  void* raw = nullptr;              // [capacity] 64-byte records, unordered
+  void* sorted = nullptr;           // [capacity] records in (u, v) order
+  uint64_t* key = nullptr;          // [capacity]
+  uint32_t* order0 = nullptr;
+  uint32_t* order1 = nullptr;
+  uint64_t* levelD = nullptr;       // [capacity * 4] squared lengths of sorted records
+  uint32_t* counters = nullptr;
+  uint32_t* radix_counts = nullptr;
+  uint32_t capacity = 0;
+  uint32_t count = 0;               // records of the last run
+  uint32_t K = 0;
+};
+
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -188,6 +205,7 @@ struct Ctx {
   bool geom_ready = false;         // traversal nodes + scale built for built_n
   int scale_S = 0;                 // host copy of the cloud scale
   bool scale_valid = false;
+  PairBuffers pb;
   uint32_t emst_rounds = 0;
   uint32_t emst_minima = 0;        // total per-round minima logged
   bool emst_ready = false;
@@ -208,6 +226,10 @@ cudaError_t lbvh_export(Ctx& ctx, uint32_t n, const ehgp_lbvh_out* out);
 cudaError_t geom_alloc(Ctx& ctx);
 // Traversal nodes, leaf map and cloud scale for the resident LBVH.
 uint64_t geom_prepare(Ctx& ctx, uint32_t n);
+
+// Pair supports (ehgp_pairs.cu)
+cudaError_t pairs_alloc(Ctx& ctx);
+int pairs_run(Ctx& ctx, uint32_t K, uint32_t* out_count);
 
 }  // namespace ehgp
 

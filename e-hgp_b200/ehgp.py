@@ -87,6 +87,16 @@ class K1ForestOut(C.Structure):
                 ("batches", C.c_void_p), ("counts", C.c_void_p), ("root_node_id", C.c_void_p)]
 
 
+class PairsOut(C.Structure):
+    _fields_ = [("records", C.c_void_p), ("level_num", C.c_void_p), ("capacity", C.c_uint64),
+                ("count", C.c_void_p)]
+
+
+PAIR_RECORD = np.dtype([("u", "<u4"), ("v", "<u4"), ("interior_count", "<u4"), ("shell_count", "<u4"),
+                        ("extra_shell_witness", "<u4"), ("interior_ids", "<u4", 9), ("reserved", "<u4", 2)])
+assert PAIR_RECORD.itemsize == 64
+
+
 def limbs_to_int(a: np.ndarray) -> int:
     """Little-endian 64-bit limbs -> Python int."""
     v = 0
@@ -121,6 +131,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "ehgp_knn": (C.c_int, [P, C.c_uint32, C.POINTER(KnnOut)]),
         "ehgp_emst": (C.c_int, [P, C.POINTER(EmstOut)]),
         "ehgp_k1_forest": (C.c_int, [P, C.POINTER(K1ForestOut)]),
+        "ehgp_pairs": (C.c_int, [P, C.c_uint32, C.POINTER(PairsOut)]),
         "ehgp_lbvh_build_noalloc": (C.c_int, [P, C.c_uint64, C.POINTER(LbvhOut), P]),
         "ehgp_lbvh_noalloc_max_points": (C.c_uint64, []),
         "ehgp_lbvh_noalloc_scratch_bytes": (C.c_uint64, []),
@@ -292,6 +303,16 @@ class Context:
         self._check(self.lib.ehgp_emst(self._h, C.byref(out)))
         mc = int(mcount[0]) if cap else 0
         return {"u": u[:m], "v": v[:m], "D": D[:m], "rounds": int(rounds[0]), "minima": minima[:mc]}
+
+    def pairs(self, K: int = 10) -> dict:
+        """ehgp_pairs: relevant pair supports in (u, v) order (reference-layout records)."""
+        cnt = np.zeros(1, np.uint64)
+        self._check(self.lib.ehgp_pairs(self._h, K, C.byref(PairsOut(None, None, 0, _ptr(cnt)))))
+        m = int(cnt[0])
+        recs = np.zeros(max(m, 1), PAIR_RECORD)
+        lv = np.zeros((max(m, 1), 4), np.uint64)
+        self._check(self.lib.ehgp_pairs(self._h, K, C.byref(PairsOut(_ptr(recs), _ptr(lv), m, _ptr(cnt)))))
+        return {"records": recs[:m], "level_num": lv[:m]}
 
     def k1_forest(self) -> dict:
         """ehgp_k1_forest on the last EMST: reference-layout compact forest arenas."""

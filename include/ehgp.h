@@ -181,6 +181,37 @@ typedef struct ehgp_k1_forest_out {
  * (include/morsehgp3d/hierarchy/k1_forest.hpp:108) with the same arenas. */
 int ehgp_k1_forest(ehgp_ctx* ctx, const ehgp_k1_forest_out* out);
 
+/* ---- pair critical-sphere supports ------------------------------------------ */
+/* One relevant pair support (64 bytes).  The sphere is the diametral sphere of
+ * (u, v): centre (u + v) / 2, squared level |u - v|^2 / 4.  shell_count == 2
+ * is an ExactPairSupportEvent (closed rank interior_count + 2); a larger shell
+ * is an ExactPairSupportExtraShellDiagnostic
+ * (include/morsehgp3d/hierarchy/pair_support_stream.hpp:256-289). */
+typedef struct ehgp_pair_record {
+  uint32_t u, v;                /* support PointIds, u < v */
+  uint32_t interior_count;      /* strict interior points (<= s_max - 2) */
+  uint32_t shell_count;         /* complete exact shell, supports included */
+  uint32_t extra_shell_witness; /* least extra shell PointId, or 0xffffffff */
+  uint32_t interior_ids[9];     /* ascending; unused slots 0xffffffff */
+  uint32_t reserved[2];
+} ehgp_pair_record;
+
+typedef struct ehgp_pairs_out {
+  ehgp_pair_record* records; /* [capacity], (u, v) order */
+  uint64_t* level_num;       /* [capacity*4]: |u-v|^2 numerators at scale 2^-2S (level = 1/4 of it) */
+  uint64_t capacity;
+  uint64_t* count;           /* [1] */
+} ehgp_pairs_out;
+
+/* Every relevant pair support of the resident cloud for maximum order K <= 10
+ * (s_max = min(min(K, n) + 1, n)).  Replaces
+ * hierarchy::build_exact_pair_support_stream(index, cloud, K, budget)
+ * (include/morsehgp3d/hierarchy/pair_support_stream.hpp:415) run to completion,
+ * and its GPU proposal seam propose_pair_support_phi_on_gpu
+ * (src/cuda/phase9_pair_support_phi_internal.hpp:110-114): decisions are exact
+ * on the device.  records == NULL only counts. */
+int ehgp_pairs(ehgp_ctx* ctx, uint32_t K, const ehgp_pairs_out* out);
+
 /* Allocation-free LBVH build.  No counterpart in the reference: it exists for
  * callers that may not call cudaMalloc (a host framework that owns all device
  * memory through its own pool, or a latency-critical caller that cannot

@@ -12,6 +12,7 @@
 #include <boost/multiprecision/cpp_int.hpp>
 
 #include <algorithm>
+#include <cmath>
 #include <array>
 #include <cstdint>
 #include <cstring>
@@ -421,6 +422,90 @@ std::string emst_forest_text(const Cloud& c) {
   return s;
 }
 
+// Sign of (w - u).(w - v): w inside (<0), on (0) or outside (>0) the closed
+// diametral ball of u, v.  FP64 with a forward error bound first, exact
+// integers at the cloud scale when the bound does not decide.
+int diametral_side(const Cloud& c, const FixedCloud& f, u64 w, u64 u, u64 v) {
+  double acc = 0, mag = 0;
+  for (int a = 0; a < 3; ++a) {
+    double xw, xu, xv;
+    std::memcpy(&xw, &c.bits[w][a], 8);
+    std::memcpy(&xu, &c.bits[u][a], 8);
+    std::memcpy(&xv, &c.bits[v][a], 8);
+    const double t = (xw - xu) * (xw - xv);
+    acc += t;
+    mag += std::fabs(t);
+  }
+  const double bound = 16.0 * 1.1102230246251565e-16 * mag + 1e-300;
+  if (acc > bound) return 1;
+  if (acc < -bound) return -1;
+  Big s = 0;
+  for (int a = 0; a < 3; ++a) s += (f.X[w][a] - f.X[u][a]) * (f.X[w][a] - f.X[v][a]);
+  return s < 0 ? -1 : (s > 0 ? 1 : 0);
+}
+
+std::string center_text(const FixedCloud& f, u64 u, u64 v) {
+  Big num[3];
+  for (int a = 0; a < 3; ++a) num[a] = f.X[u][a] + f.X[v][a];
+  int e = f.S + 1;
+  while (e > 0 && num[0] % 2 == 0 && num[1] % 2 == 0 && num[2] % 2 == 0) {
+    for (auto& x : num) x /= 2;
+    --e;
+  }
+  return num[0].str() + " " + num[1].str() + " " + num[2].str() + " " + (Big(1) << (unsigned)e).str();
+}
+
+// All relevant pair supports by brute force: the outcome of
+// build_exact_pair_support_stream (include/morsehgp3d/hierarchy/pair_support_stream.hpp:415)
+// with its leaf rule classify_leaf_pair / classify_sparse_closed_ball
+// (src/cpu/hierarchy/pair_support_stream.cpp:1781-2094): relevant iff the strict
+// interior count I <= s_max - 2, with s_max = min(min(K, n) + 1, n); a shell of
+// exactly the two supports is an event, a larger shell a diagnostic carrying the
+// complete shell count and the least extra shell PointId.
+std::string pairs_text(const Cloud& c, u64 K) {
+  const FixedCloud f = fixed_cloud(c);
+  const u64 n = c.bits.size();
+  const u64 keff = std::min(K, n);
+  const u64 smax = std::min(keff + 1, n);
+  std::string ev, dg;
+  if (smax < 2) return "S complete\n";
+  const u64 cap = smax - 2;
+  std::vector<u64> interior;
+  for (u64 u = 0; u < n; ++u)
+    for (u64 v = u + 1; v < n; ++v) {
+      interior.clear();
+      u64 shell = 0, extra = ~u64{0};
+      bool reject = false;
+      for (u64 w = 0; w < n; ++w) {
+        const int sd = (w == u || w == v) ? 0 : diametral_side(c, f, w, u, v);
+        if (sd < 0) {
+          interior.push_back(w);
+          if (interior.size() > cap) {
+            reject = true;
+            break;
+          }
+        } else if (sd == 0) {
+          ++shell;
+          if (w != u && w != v) extra = std::min(extra, w);
+        }
+      }
+      if (reject) continue;
+      const u64 I = interior.size();
+      const Big D = dist2(f, u, v);
+      const std::string tail = reduced(D, 2 * f.S + 2) + " " + center_text(f, u, v) + " |";
+      std::string ids;
+      for (u64 w : interior) ids += " " + std::to_string(w);
+      if (shell == 2)
+        ev += "P " + std::to_string(u) + " " + std::to_string(v) + " " + std::to_string(I + 2) + " " +
+              std::to_string(n - I - 2) + " " + tail + ids + "\n";
+      else
+        dg += "D " + std::to_string(u) + " " + std::to_string(v) + " " + std::to_string(shell) + " " +
+              std::to_string(extra) + " " + std::to_string(I + 2) + " " + std::to_string(I + shell) + " " +
+              std::to_string(n - I - shell) + " " + tail + ids + "\n";
+    }
+  return ev + dg + "S complete\n";
+}
+
 u64 put_text(const std::string& s, char* buf, u64 cap) {
   if (s.size() + 1 > cap) return s.size() + 1;
   std::memcpy(buf, s.c_str(), s.size() + 1);
@@ -486,6 +571,15 @@ int oracle_lbvh_build(const double* xyz, u64 n, u64* source_index, u64* leaves, 
 int oracle_knn(const double* xyz, u64 n, u64 k, char* out, u64 cap, u64* needed, char* err, u64 errlen) {
   try {
     *needed = put_text(knn_text(canonical_cloud(xyz, n), k), out, cap);
+    return 0;
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 1);
+  }
+}
+
+int oracle_pairs(const double* xyz, u64 n, u64 K, char* out, u64 cap, u64* needed, char* err, u64 errlen) {
+  try {
+    *needed = put_text(pairs_text(canonical_cloud(xyz, n), K), out, cap);
     return 0;
   } catch (const std::exception& e) {
     return report(e, err, errlen, 1);

@@ -163,3 +163,29 @@ def emst_forest(points: np.ndarray, which: str = "restatement") -> dict:
         elif tag == "R":
             r["root"] = int(f[0])
     return r
+
+
+def parse_pairs(txt: str) -> dict:
+    """Pair-support records: events (u, v, closed_rank, exterior, level, center, interior)
+    and diagnostics (u, v, shell, witness, min_rank, observed_rank, exterior, level, center, interior)."""
+    events, diags, status = [], [], None
+    for line in txt.splitlines():
+        head, _, tail = line.partition("|")
+        t = head.split()
+        if not t:
+            continue
+        ids = tuple(int(x) for x in tail.split())
+        if t[0] == "P":
+            center = tuple(Fraction(int(t[7 + a]), int(t[10])) for a in range(3))
+            events.append((int(t[1]), int(t[2]), int(t[3]), int(t[4]), Fraction(int(t[5]), int(t[6])), center, ids))
+        elif t[0] == "D":
+            center = tuple(Fraction(int(t[10 + a]), int(t[13])) for a in range(3))
+            diags.append((*(int(x) for x in t[1:8]), Fraction(int(t[8]), int(t[9])), center, ids))
+        elif t[0] == "S":
+            status = t[1]
+    return {"events": events, "diagnostics": diags, "status": status}
+
+
+def pairs(points: np.ndarray, K: int = 10, which: str = "restatement") -> dict:
+    name = "oracle_pairs" if which == "restatement" else "ref_pairs"
+    return parse_pairs(_text_call(name, which, points, K))

@@ -204,8 +204,74 @@ int ref_knn(const double* xyz, uint64_t n, uint64_t k, char* out, uint64_t cap, 
 
 #include "morsehgp3d/hierarchy/boruvka.hpp"
 #include "morsehgp3d/hierarchy/k1_forest.hpp"
+#include "morsehgp3d/hierarchy/pair_support_stream.hpp"
+
+namespace {
+
+std::string center_text(const morsehgp3d::exact::ExactCenter3& c) {
+  return c.numerator(0).str() + " " + c.numerator(1).str() + " " + c.numerator(2).str() + " " +
+         c.denominator().str();
+}
+
+std::string ids_text(const std::vector<morsehgp3d::spatial::PointId>& ids) {
+  std::string s;
+  for (const auto id : ids) s += " " + std::to_string(id);
+  return s;
+}
+
+morsehgp3d::hierarchy::ExactPairSupportStreamBudget unlimited_pair_budget() {
+  morsehgp3d::hierarchy::ExactPairSupportStreamBudget b;
+  const std::size_t big = std::size_t{1} << 62;
+  b.maximum_work_unit_count = big;
+  b.maximum_frontier_entry_count = big;
+  b.maximum_auxiliary_frontier_entry_count = big;
+  b.maximum_emitted_record_count = big;
+  b.maximum_emitted_point_id_reference_count = big;
+  b.maximum_global_closed_ball_query_count = big;
+  b.maximum_point_classification_count = big;
+  return b;
+}
+
+}  // namespace
 
 extern "C" {
+
+// build_exact_pair_support_stream (include/morsehgp3d/hierarchy/pair_support_stream.hpp:415)
+// with an unlimited budget.  Lines, in the stream's canonical (u, v) order:
+// "P u v closed_rank exterior lnum lden cx cy cz cden | interior..."  (events)
+// "D u v shell witness min_rank observed exterior lnum lden cx cy cz cden | interior..."
+// (relevant extra-shell diagnostics), then "S complete|budget_exhausted".
+int ref_pairs(const double* xyz, uint64_t n, uint64_t K, char* out, uint64_t cap, uint64_t* needed, double* seconds,
+              char* err, uint64_t errlen) {
+  try {
+    using namespace morsehgp3d;
+    const auto pts = points_from(xyz, n);
+    const CanonicalPointCloud cloud = CanonicalPointCloud::rejecting_duplicates(pts);
+    const MortonLbvhIndex index = MortonLbvhIndex::build(cloud);
+    const auto t0 = std::chrono::steady_clock::now();
+    const auto res = hierarchy::build_exact_pair_support_stream(index, cloud, K, unlimited_pair_budget());
+    if (seconds) seconds[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::string s;
+    for (const auto& e : res.events)
+      s += "P " + std::to_string(e.support_ids[0]) + " " + std::to_string(e.support_ids[1]) + " " +
+           std::to_string(e.closed_rank) + " " + std::to_string(e.exterior_count) + " " +
+           e.squared_level.numerator_string() + " " + e.squared_level.denominator_string() + " " +
+           center_text(e.center) + " |" + ids_text(e.interior_ids) + "\n";
+    for (const auto& d : res.relevant_extra_shell_diagnostics)
+      s += "D " + std::to_string(d.support_ids[0]) + " " + std::to_string(d.support_ids[1]) + " " +
+           std::to_string(d.shell_count) + " " + std::to_string(d.canonical_extra_shell_witness_id) + " " +
+           std::to_string(d.minimum_possible_closed_rank) + " " + std::to_string(d.observed_closed_rank) + " " +
+           std::to_string(d.exterior_count) + " " + d.squared_level.numerator_string() + " " +
+           d.squared_level.denominator_string() + " " + center_text(d.center) + " |" + ids_text(d.interior_ids) +
+           "\n";
+    s += std::string("S ") +
+         (res.status == hierarchy::ExactPairSupportStreamStatus::complete ? "complete" : "budget_exhausted") + "\n";
+    *needed = put_text(s, out, cap);
+    return 0;
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 1);
+  }
+}
 
 // build_exact_lbvh_boruvka (include/morsehgp3d/hierarchy/boruvka.hpp:130) and
 // build_compact_k1_forest on its edges (include/morsehgp3d/hierarchy/k1_forest.hpp:108).

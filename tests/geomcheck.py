@@ -86,3 +86,47 @@ def gpu_emst_forest(ctx):
 def emst_forest_matches(gpu, ref):
     for key in ("edges", "minima", "accepted", "levels", "nodes", "children", "batches", "root"):
         assert gpu[key] == ref[key], key
+
+
+def load_golden_pairs(path):
+    """pairs_*.json (tests/golden/make_golden.py --pairs) -> oracle record tuples."""
+    d = json.load(open(path))
+    F = lambda a, b: Fraction(int(a), int(b))
+    ev = [(u, v, r, ext, F(ln, ld), tuple(F(c, cen[3]) for c in cen[:3]), tuple(ids))
+          for u, v, r, ext, ln, ld, cen, ids in d["events"]]
+    dg = [(u, v, sh, w, mr, orr, ext, F(ln, ld), tuple(F(c, cen[3]) for c in cen[:3]), tuple(ids))
+          for u, v, sh, w, mr, orr, ext, ln, ld, cen, ids in d["diagnostics"]]
+    return np.array(d["points"], dtype=np.float64), d["K"], {"events": ev, "diagnostics": dg, "status": d["status"]}
+
+
+def gpu_pair_records(ctx, K, points_canonical):
+    """ehgp_pairs output converted to the oracle's (events, diagnostics) tuples.
+
+    points_canonical: binary64 coordinates in PointId order (for the exact centre)."""
+    S, valid = ctx.scale()
+    assert valid
+    n = len(points_canonical)
+    r = ctx.pairs(K)
+    ev, dg = [], []
+    for rec, lv in zip(r["records"], r["level_num"]):
+        u, v = int(rec["u"]), int(rec["v"])
+        I, sh = int(rec["interior_count"]), int(rec["shell_count"])
+        level = Fraction(ehgp.limbs_to_int(lv), 1 << (2 * S)) / 4
+        center = tuple((Fraction(float(points_canonical[u][a])) + Fraction(float(points_canonical[v][a]))) / 2
+                       for a in range(3))
+        ids = tuple(int(x) for x in rec["interior_ids"][:I])
+        if sh == 2:
+            ev.append((u, v, I + 2, n - I - 2, level, center, ids))
+        else:
+            dg.append((u, v, sh, int(rec["extra_shell_witness"]), I + 2, I + sh, n - I - sh, level, center, ids))
+    return {"events": ev, "diagnostics": dg, "status": "complete"}
+
+
+def pairs_match(gpu, ref):
+    for key in ("events", "diagnostics"):
+        g, r = gpu[key], ref[key]
+        if g != r:
+            gs, rs = set(g), set(r)
+            raise AssertionError(f"{key}: {len(g)} vs {len(r)}; only gpu {sorted(gs - rs)[:3]}; "
+                                 f"only oracle {sorted(rs - gs)[:3]}")
+    assert ref["status"] == "complete"

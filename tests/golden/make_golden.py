@@ -4,6 +4,7 @@ own CPU code (oracle/_ref/libehgp_ref.so: CanonicalPointCloud::rejecting_duplica
 project-written Boost shim).  Run here, where the reference tree exists:
 
     make -C oracle ref && python tests/golden/make_golden.py && python tests/golden/make_golden.py --geom
+    python tests/golden/make_golden.py --pairs   # slow: the reference pair stream
 """
 import os
 import sys
@@ -46,7 +47,7 @@ def main():
         print(name, len(pts), r["counters"])
 
 
-if __name__ == "__main__" and "--geom" not in sys.argv:
+if __name__ == "__main__" and len(sys.argv) == 1:
     main()
 
 
@@ -85,3 +86,35 @@ def main_geom():
 
 if __name__ == "__main__" and "--geom" in sys.argv:
     main_geom()
+
+
+def parse_pairs(txt):
+    """Records of ref_pairs / oracle_pairs text (see oracle/ref_driver.cpp)."""
+    events, diags, status = [], [], None
+    for line in txt.splitlines():
+        head, _, tail = line.partition("|")
+        t = head.split()
+        if not t:
+            continue
+        ids = [int(x) for x in tail.split()]
+        if t[0] == "P":
+            events.append([int(t[1]), int(t[2]), int(t[3]), int(t[4]), t[5], t[6], t[7:11], ids])
+        elif t[0] == "D":
+            diags.append([int(x) for x in t[1:8]] + [t[8], t[9], t[10:14], ids])
+        elif t[0] == "S":
+            status = t[1]
+    return {"events": events, "diagnostics": diags, "status": status}
+
+
+def main_pairs():
+    import json
+    for name, pts in geom_cases():
+        txt = pyoracle._text_call("ref_pairs", "reference", pts, 10)
+        doc = {"points": pts.tolist(), "K": 10, **parse_pairs(txt)}
+        with open(os.path.join(HERE, f"pairs_{name}.json"), "w") as f:
+            json.dump(doc, f, separators=(",", ":"))
+        print(name, len(pts), len(doc["events"]), len(doc["diagnostics"]), doc["status"], flush=True)
+
+
+if __name__ == "__main__" and "--pairs" in sys.argv:
+    main_pairs()
