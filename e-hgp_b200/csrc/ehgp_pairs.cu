@@ -40,7 +40,7 @@ namespace {
 
 constexpr int kThreads = 128;
 constexpr int kStack = 128;
-constexpr int kW = 32;           // witnesses per point
+constexpr int kW = 64;           // witnesses per point (two per lane)
 constexpr int kMaxInterior = 9;  // s_max - 2 for K >= 10
 
 __host__ __device__ inline uint32_t nblocks(uint64_t n, int t = kThreads) {
@@ -125,7 +125,7 @@ k_witness_knn(uint32_t n, uint32_t kw, uint32_t root, const TNode* __restrict__ 
       if (lr <= thr) stack[top++] = t.right;
     }
   }
-  for (int j = 0; j < (int)kw; ++j) W[(uint64_t)p * kW + j] = j < cnt ? cid[j] : kInvalid32;
+  for (int j = 0; j < kW; ++j) W[(uint64_t)p * kW + j] = j < cnt ? cid[j] : kInvalid32;
   // witness radius: every point strictly closer than R2 is in W (R2 = +inf when W is all other points)
   R2[p] = (cnt >= (int)kw && n - 1 > kw) ? cd[kw - 1] : INFINITY;
 }
@@ -163,80 +163,133 @@ struct PairRec {
 };
 static_assert(sizeof(PairRec) == 64, "pair record is one 64-byte line");
 
-// Classification accumulator of one pair.
-struct Ball {
-  uint32_t interior;
-  uint32_t shell;   // extra shell points (u and v excluded)
-  uint32_t witness;
-  uint32_t ids[kMaxInterior];
-  bool rejected;
-  __device__ void init() {
-    interior = 0;
-    shell = 0;
-    witness = kInvalid32;
-    rejected = false;
-  }
-  __device__ void add(int side, uint32_t w, uint32_t cap) {
-    if (side < 0) {
-      if (interior >= cap) {
-        rejected = true;
-        return;
-      }
-      ids[interior++] = w;
-    } else if (side == 0) {
-      ++shell;
-      witness = min(witness, w);
-    }
-  }
+// ---- warp-per-point enumeration ---------------------------------------------------
+// One warp owns one point u; lane l holds witnesses l and l + 32 of W_u.
+constexpr int kWarpsPerBlock = kThreads / 32;
+constexpr int kQueue = 256;  // warp-cooperative ball-query frontier (power of two)
+
+struct WarpShared {
+  uint32_t stack[kStack];
+  uint32_t queue[kQueue];
+  uint32_t ids[kMaxInterior + 64];
 };
 
-// Global exact closed-ball query over the LBVH with early rejection.
-__device__ void ball_query(Ball& b, uint32_t iu, uint32_t iv, const Pt& u, const Pt& v, uint32_t root,
-                           const TNode* tn, const uint32_t* leaf_pid, const uint32_t* n_begin, const uint32_t* n_end,
-                           const double* px, const double* py, const double* pz, int S, uint32_t cap,
-                           uint32_t* err) {
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Appends the ids of flagged lanes (two flags per lane) to sh.ids[base...];
+// returns the number appended.  Writes only while the total stays <= cap.
+__device__ __forceinline__ uint32_t warp_append(WarpShared& sh, uint32_t base, bool f0, uint32_t id0, bool f1,
+                                                uint32_t id1, uint32_t cap) {
+  const uint32_t b0 = __ballot_sync(0xffffffffu, f0), b1 = __ballot_sync(0xffffffffu, f1);
+  const uint32_t c0 = __popc(b0), total = c0 + __popc(b1);
+  if (base + total <= cap) {
+    const uint32_t lt = lanemask_lt();
+    if (f0) sh.ids[base + __popc(b0 & lt)] = id0;
+    if (f1) sh.ids[base + c0 + __popc(b1 & lt)] = id1;
+  }
+  return total;
+}
+
+struct WarpBall {
+  uint32_t interior;
+  uint32_t shell;    // extra shell points
+  uint32_t witness;  // least extra shell id
+  bool rejected;
+};
+
+// Classifies the two candidates of every lane (w0, w1; kInvalid32 = none).
+__device__ __forceinline__ void warp_classify(WarpBall& b, WarpShared& sh, uint32_t w0, uint32_t w1, uint32_t iu,
+                                              uint32_t iv, const Pt& u, const Pt& v, const double* px,
+                                              const double* py, const double* pz, int S, uint32_t cap) {
+  int s0 = 1, s1 = 1;
+  if (w0 != kInvalid32 && w0 != iu && w0 != iv)
+    s0 = diametral_side(point(px, py, pz, w0), u, v, w0, iu, iv, px, py, pz, S);
+  if (w1 != kInvalid32 && w1 != iu && w1 != iv)
+    s1 = diametral_side(point(px, py, pz, w1), u, v, w1, iu, iv, px, py, pz, S);
+  const uint32_t added = warp_append(sh, b.interior, s0 < 0, w0, s1 < 0, w1, cap);
+  b.interior += added;
+  if (b.interior > cap) b.rejected = true;
+  const uint32_t sb0 = __ballot_sync(0xffffffffu, s0 == 0), sb1 = __ballot_sync(0xffffffffu, s1 == 0);
+  b.shell += __popc(sb0) + __popc(sb1);
+  const uint32_t mw = min(s0 == 0 ? w0 : kInvalid32, s1 == 0 ? w1 : kInvalid32);
+  b.witness = min(b.witness, __reduce_min_sync(0xffffffffu, mw));
+}
+
+// Warp-cooperative exact closed-ball query over the LBVH (breadth-first over
+// the subtrees that straddle the sphere, 32 nodes per step), early rejection.
+__device__ void warp_ball_query(WarpBall& b, WarpShared& sh, uint32_t iu, uint32_t iv, const Pt& u, const Pt& v,
+                                uint32_t root, const TNode* tn, const uint32_t* leaf_pid, const uint32_t* n_begin,
+                                const uint32_t* n_end, const double* px, const double* py, const double* pz, int S,
+                                uint32_t cap, uint32_t* err) {
+  const uint32_t lane = threadIdx.x & 31u;
   const double mx = 0.5 * (u.x + v.x), my = 0.5 * (u.y + v.y), mz = 0.5 * (u.z + v.z);
   const double r2 = 0.25 * d2fp(u.x, u.y, u.z, v.x, v.y, v.z);
   const double r2_hi = r2 * (1.0 + 8.0 * kDistRelErr) + 1e-300, r2_lo = r2 * (1.0 - 8.0 * kDistRelErr);
-  uint32_t stack[kStack];
-  int top = 0;
-  stack[top++] = root;
-  while (top > 0 && !b.rejected) {
-    const uint32_t node = stack[--top];
-    const TNode t = load_node(tn, node);
-    if (t.left == kInvalid32) {
-      const uint32_t w = t.right;
-      if (w == iu || w == iv) continue;
-      b.add(diametral_side(point(px, py, pz, w), u, v, w, iu, iv, px, py, pz, S), w, cap);
-      continue;
-    }
-    if (box_lb(t, mx, my, mz) > r2_hi) continue;  // whole subtree strictly outside
-    if (box_ub(t, mx, my, mz) < r2_lo) {          // whole subtree strictly inside
-      const uint32_t nb = n_begin[node], ne = n_end[node];
-      for (uint32_t q = nb; q < ne && !b.rejected; ++q) {
-        const uint32_t w = leaf_pid[q];
-        if (w == iu || w == iv) continue;  // cannot happen (supports are on the sphere)
-        b.add(-1, w, cap);
+  uint32_t head = 0, tail = 1;
+  if (lane == 0) sh.queue[0] = root;
+  __syncwarp();
+  while (head < tail && !b.rejected) {
+    const uint32_t batch = min(tail - head, 32u);
+    uint32_t node = kInvalid32;
+    if (lane < batch) node = sh.queue[(head + lane) & (kQueue - 1)];
+    __syncwarp();
+    uint32_t leafw = kInvalid32, bulk_b = 0, bulk_e = 0;
+    bool expand = false;
+    TNode t;
+    if (node != kInvalid32) {
+      t = load_node(tn, node);
+      if (t.left == kInvalid32) {
+        leafw = t.right;
+      } else if (box_lb(t, mx, my, mz) <= r2_hi) {
+        if (box_ub(t, mx, my, mz) < r2_lo) {
+          bulk_b = n_begin[node];
+          bulk_e = n_end[node];
+        } else {
+          expand = true;
+        }
       }
-      continue;
     }
-    if (top + 2 > kStack) { atomicOr(err, kErrCapacity); b.rejected = true; return; }
-    stack[top++] = t.right;
-    stack[top++] = t.left;
+    warp_classify(b, sh, leafw, kInvalid32, iu, iv, u, v, px, py, pz, S, cap);
+    // whole subtrees strictly inside
+    uint32_t bulk_total = bulk_e - bulk_b;
+    for (int off = 16; off > 0; off >>= 1) bulk_total += __shfl_xor_sync(0xffffffffu, bulk_total, off);
+    if (bulk_total) {
+      if (b.interior + bulk_total > cap) {
+        b.rejected = true;
+      } else {
+        // append the ids lane by lane (at most cap of them in total)
+        uint32_t before = bulk_e - bulk_b;
+        for (int off = 1; off < 32; off <<= 1) {
+          const uint32_t t2 = __shfl_up_sync(0xffffffffu, before, off);
+          if ((int)lane >= off) before += t2;
+        }
+        before -= (bulk_e - bulk_b);
+        for (uint32_t q = bulk_b; q < bulk_e; ++q) sh.ids[b.interior + before + (q - bulk_b)] = leaf_pid[q];
+        b.interior += bulk_total;
+      }
+    }
+    // children of straddling subtrees
+    const uint32_t eb = __ballot_sync(0xffffffffu, expand);
+    const uint32_t pushes = 2 * __popc(eb);
+    if (tail - head - batch + pushes > kQueue) {
+      if (lane == 0) atomicOr(err, kErrCapacity);
+      b.rejected = true;
+      break;
+    }
+    if (expand) {
+      const uint32_t at = tail + 2 * __popc(eb & lanemask_lt());
+      sh.queue[at & (kQueue - 1)] = t.left;
+      sh.queue[(at + 1) & (kQueue - 1)] = t.right;
+    }
+    __syncwarp();
+    head += batch;
+    tail += pushes;
   }
-}
-
-// Classification from a witness list (valid when the closed diametral ball is
-// inside the strict witness ball of `owner`): every point of the ball is in W.
-__device__ void local_ball(Ball& b, const uint32_t* __restrict__ Wlist, uint32_t other, uint32_t iu, uint32_t iv,
-                           const Pt& u, const Pt& v, const double* px, const double* py, const double* pz, int S,
-                           uint32_t cap) {
-  for (int j = 0; j < kW && !b.rejected; ++j) {
-    const uint32_t w = Wlist[j];
-    if (w == kInvalid32) break;
-    if (w == other) continue;
-    b.add(diametral_side(point(px, py, pz, w), u, v, w, iu, iv, px, py, pz, S), w, cap);
-  }
+  __syncwarp();
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -245,87 +298,99 @@ k_pairs(uint32_t n, uint32_t cap, uint32_t root, const TNode* __restrict__ tn, c
         const double* __restrict__ py, const double* __restrict__ pz, const int* __restrict__ scale,
         const uint32_t* __restrict__ W, const double* __restrict__ R2, PairRec* __restrict__ out,
         uint32_t out_cap, uint32_t* __restrict__ counters, uint32_t* __restrict__ err) {
-  const uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pos >= n) return;
+  __shared__ WarpShared shared[kWarpsPerBlock];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t pos = blockIdx.x * kWarpsPerBlock + warp;
+  if (pos >= n) return;  // uniform per warp
+  WarpShared& sh = shared[warp];
   const uint32_t iu = leaf_pid[pos];
   const Pt u = point(px, py, pz, iu);
   const int S = scale[0];
   const double r2u = R2[iu];
-  // witness offsets relative to u in binary32 for the subtree bound
-  float wx[kW], wy[kW], wz[kW];
-  int nw = 0;
-  for (int j = 0; j < kW; ++j) {
-    const uint32_t w = W[(uint64_t)iu * kW + j];
-    if (w == kInvalid32) break;
-    wx[nw] = (float)(px[w] - u.x);
-    wy[nw] = (float)(py[w] - u.y);
-    wz[nw] = (float)(pz[w] - u.z);
-    ++nw;
-  }
-  const uint32_t need = cap + 1;  // witnesses that make every pair of a subtree irrelevant
-  uint32_t stack[kStack];
-  int top = 0;
-  stack[top++] = root;
+  // this lane's two witnesses of u
+  const uint32_t w0 = W[(uint64_t)iu * kW + lane], w1 = W[(uint64_t)iu * kW + 32 + lane];
+  float ax0 = 0.f, ay0 = 0.f, az0 = 0.f, ax1 = 0.f, ay1 = 0.f, az1 = 0.f;
+  if (w0 != kInvalid32) { ax0 = (float)(px[w0] - u.x); ay0 = (float)(py[w0] - u.y); az0 = (float)(pz[w0] - u.z); }
+  if (w1 != kInvalid32) { ax1 = (float)(px[w1] - u.x); ay1 = (float)(py[w1] - u.y); az1 = (float)(pz[w1] - u.z); }
+  const uint32_t nw = __popc(__ballot_sync(0xffffffffu, w0 != kInvalid32)) +
+                      __popc(__ballot_sync(0xffffffffu, w1 != kInvalid32));
+  const uint32_t need = cap + 1;
+  uint32_t top = 0;
+  if (lane == 0) sh.stack[0] = root;
+  top = 1;
+  __syncwarp();
+  const double lo = 1.0 - 4.0 * kDistRelErr, hi = 1.0 + 4.0 * kDistRelErr;
   while (top > 0) {
-    const uint32_t node = stack[--top];
+    const uint32_t node = sh.stack[top - 1];
+    --top;
+    __syncwarp();
     if (n_end[node] <= pos + 1) continue;  // every partner precedes u in Morton order
     const TNode t = load_node(tn, node);
     if (t.left != kInvalid32) {
-      // rank prune: witnesses strictly inside every diametral ball (u, v in box)
-      if ((uint32_t)nw >= need) {
+      if (nw >= need) {
         const float lx = (float)((double)t.lo[0] - u.x), ly = (float)((double)t.lo[1] - u.y),
                     lz = (float)((double)t.lo[2] - u.z);
         const float hx = (float)((double)t.hi[0] - u.x), hy = (float)((double)t.hi[1] - u.y),
                     hz = (float)((double)t.hi[2] - u.z);
-        uint32_t inside = 0;
-        for (int j = 0; j < nw && inside < need; ++j) {
-          // max over v in box of (w-u).(w-v) = sum_i a_i (a_i - (a_i >= 0 ? lo_i : hi_i)), a = w - u
-          const float ax = wx[j], ay = wy[j], az = wz[j];
+        // max over v in box of (w-u).(w-v) = sum_i a_i (a_i - (a_i >= 0 ? lo_i : hi_i)), a = w - u
+        auto inside = [&](float ax, float ay, float az, bool valid) {
           const float tx = ax * (ax - (ax >= 0.f ? lx : hx));
           const float ty = ay * (ay - (ay >= 0.f ? ly : hy));
           const float tz = az * (az - (az >= 0.f ? lz : hz));
           const float mag = fabsf(tx) + fabsf(ty) + fabsf(tz) + ax * ax + ay * ay + az * az;
-          if (tx + ty + tz < -1e-5f * mag) ++inside;
-        }
-        if (inside >= need) continue;
+          return valid && (tx + ty + tz < -1e-5f * mag);
+        };
+        const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, inside(ax0, ay0, az0, w0 != kInvalid32))) +
+                             __popc(__ballot_sync(0xffffffffu, inside(ax1, ay1, az1, w1 != kInvalid32)));
+        if (cnt >= need) continue;
       }
-      if (top + 2 > kStack) { atomicOr(err, kErrCapacity); return; }
-      stack[top++] = t.right;
-      stack[top++] = t.left;
+      if (top + 2 > kStack) {
+        if (lane == 0) atomicOr(err, kErrCapacity);
+        return;
+      }
+      if (lane == 0) {
+        sh.stack[top] = t.right;
+        sh.stack[top + 1] = t.left;
+      }
+      top += 2;
+      __syncwarp();
       continue;
     }
     const uint32_t iv = t.right;
     const Pt v = point(px, py, pz, iv);
     const double d2 = d2fp(u.x, u.y, u.z, v.x, v.y, v.z);
-    Ball b;
-    b.init();
-    const double lo = 1.0 - 4.0 * kDistRelErr, hi = 1.0 + 4.0 * kDistRelErr;
+    WarpBall b{0u, 0u, kInvalid32, false};
     if (d2 * hi < r2u * lo) {
-      local_ball(b, W + (uint64_t)iu * kW, iv, iu, iv, u, v, px, py, pz, S, cap);
+      warp_classify(b, sh, w0, w1, iu, iv, u, v, px, py, pz, S, cap);
     } else if (d2 * hi < R2[iv] * lo) {
-      local_ball(b, W + (uint64_t)iv * kW, iu, iu, iv, u, v, px, py, pz, S, cap);
+      const uint32_t v0 = W[(uint64_t)iv * kW + lane], v1 = W[(uint64_t)iv * kW + 32 + lane];
+      warp_classify(b, sh, v0, v1, iu, iv, u, v, px, py, pz, S, cap);
     } else {
-      ball_query(b, iu, iv, u, v, root, tn, leaf_pid, n_begin, n_end, px, py, pz, S, cap, err);
+      warp_ball_query(b, sh, iu, iv, u, v, root, tn, leaf_pid, n_begin, n_end, px, py, pz, S, cap, err);
     }
-    if (b.rejected) continue;
-    const uint32_t slot = atomicAdd(counters, 1u);
-    if (slot >= out_cap) continue;  // counted; the host reports the capacity
-    PairRec r;
-    r.u = min(iu, iv);
-    r.v = max(iu, iv);
-    r.interior = b.interior;
-    r.shell = b.shell + 2;
-    r.witness = b.witness;
-    for (uint32_t j = 0; j < kMaxInterior; ++j) r.ids[j] = j < b.interior ? b.ids[j] : kInvalid32;
-    // interior ids ascending (the reference sorts them)
-    for (uint32_t a = 1; a < b.interior; ++a) {
-      const uint32_t x = r.ids[a];
-      uint32_t j = a;
-      while (j > 0 && r.ids[j - 1] > x) { r.ids[j] = r.ids[j - 1]; --j; }
-      r.ids[j] = x;
+    __syncwarp();
+    if (b.rejected || b.interior > cap) continue;
+    if (lane == 0) {
+      const uint32_t slot = atomicAdd(counters, 1u);
+      if (slot < out_cap) {
+        PairRec r;
+        r.u = min(iu, iv);
+        r.v = max(iu, iv);
+        r.interior = b.interior;
+        r.shell = b.shell + 2;
+        r.witness = b.witness;
+        for (uint32_t j = 0; j < kMaxInterior; ++j) r.ids[j] = j < b.interior ? sh.ids[j] : kInvalid32;
+        for (uint32_t a = 1; a < b.interior; ++a) {  // ascending interior ids
+          const uint32_t x = r.ids[a];
+          uint32_t j = a;
+          while (j > 0 && r.ids[j - 1] > x) { r.ids[j] = r.ids[j - 1]; --j; }
+          r.ids[j] = x;
+        }
+        r.pad[0] = r.pad[1] = 0;
+        out[slot] = r;
+      }
     }
-    r.pad[0] = r.pad[1] = 0;
-    out[slot] = r;
+    __syncwarp();
   }
 }
 
@@ -402,7 +467,7 @@ int pairs_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   k_witness_knn<<<nblocks(n), kThreads, 0, st>>>(n, kw, root, g.tnodes, b.leaf_pid, b.px, b.py, b.pz, p.W, p.R2,
                                                   ctx.d_err);
   cudaMemsetAsync(p.counters, 0, 8 * sizeof(uint32_t), st);
-  k_pairs<<<nblocks(n), kThreads, 0, st>>>(n, cap, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end, b.px, b.py, b.pz,
+  k_pairs<<<nblocks(n, kWarpsPerBlock), kThreads, 0, st>>>(n, cap, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end, b.px, b.py, b.pz,
                                             g.scale, p.W, p.R2, (PairRec*)p.raw, p.capacity, p.counters, ctx.d_err);
   launches += 2;
   uint32_t hc[2] = {0, 0};
