@@ -3,22 +3,28 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Workload: the regular volumetric cloud, 37^3 = 50,653 lattice points jittered
-by U[-0.25, 0.25] per axis, binary32 storage, seeded (no dataset involved).
-A step is one pass of the device pipeline over one cloud.  The stages that
-exist so far run inside the step; `config.stages` names them.
+by U[-0.25, 0.25] per axis, binary32 storage, seeded (synthetic; the
+reference names no dataset).  K_max = 10.  A step is one pass of the product
+path over one cloud; `config.stages` lists the stages inside the step:
+canonical cloud + exact Morton LBVH, Boruvka EMST, compact k=1 forest, and
+every relevant pair critical-sphere support (rank <= 11).
 
-value  : p95 over the K timed steps of the device time of one step (CUDA events
-         on the library's stream, inputs already resident in HBM), max over ranks.
-e2e    : p95 over K steps of the same work through the public C ABI with host
-         buffers: pinned host->device copy of the points, the build, and the
-         device->host copy of the full reference-layout result, wall clock.
+value : p95 over the K timed steps of the step time on the device timeline
+        (CUDA events on the library's stream around the whole step; inputs
+        already resident in HBM; the host-side forest sweep is inside).
+e2e   : p95 over K steps of the same step through the public C ABI with host
+        buffers: pinned host input copied in, and every result (EMST edges and
+        exact lengths, forest arenas, pair-support records and levels) copied
+        back to the host; wall clock.
 L2 is flushed (a 512 MiB write) before every timed step.
 
 Multi-GPU: replicas only (one independent cloud per rank, different seeds),
 barrier + max over ranks; no data-path collective.
 
---impl reference times the reference's own CPU code of the same stages
-(oracle/_ref, compiled from the reference sources), on rank 0 only.
+--impl reference times the reference's own CPU code (oracle/_ref, compiled
+from the reference sources) for the same stages on a bounded sample of the
+workload (see `cpu_baseline.sample`), on rank 0 only: its exact pair stream
+costs minutes already at a few hundred points.
 """
 from __future__ import annotations
 
@@ -35,10 +41,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path[:0] = [ROOT, os.path.join(ROOT, "e-hgp_b200")]
 
-METRIC = "warm_e2e_p95_ms_50k_jittered_lattice"
+METRIC = "warm_e2e_p95_ms_50k_jittered_lattice_K10"
 WORKLOAD = "jittered_lattice_37^3_f32"
-STAGES = ["canonical_cloud", "exact_morton_lbvh"]
-BYTES_PER_POINT_LBVH = 310  # algorithmic bytes per point of the Morton/LBVH build
+K_MAX = 10
+STAGES = ["canonical_cloud", "exact_morton_lbvh", "boruvka_emst", "k1_compact_forest", "pair_supports_rank_le_11"]
 
 
 def p95(xs):
@@ -88,7 +94,7 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def dist_setup(args):
+def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -118,50 +124,71 @@ def barrier(world: int):
         dist.barrier()
 
 
-def cpu_reference_time(pts64: np.ndarray, budget_s: float = 10.0, max_reps: int = 20) -> dict:
-    """The reference's own CPU code (oracle/_ref) on the same cloud, 1 thread."""
+# ---- the reference's own CPU code on a bounded sample ---------------------------------
+SAMPLE_SIDE = 4  # a 4^3 = 64-point corner of the jittered lattice
+
+
+def reference_sample(seed: int = 0) -> np.ndarray:
+    import workloads
+    return workloads.jittered_lattice(37, seed).reshape(37, 37, 37, 3)[:SAMPLE_SIDE, :SAMPLE_SIDE, :SAMPLE_SIDE] \
+        .reshape(-1, 3).astype(np.float64)
+
+
+def reference_step_seconds(pts: np.ndarray) -> dict:
+    """Stage times of the reference chain (single thread, as the reference is)."""
     from oracle import pyoracle
-    if not pyoracle.available("reference"):
-        return {"value": None, "unit": "ms", "cores": 1, "kind": "reference", "sample": "oracle/_ref not built"}
-    times = []
-    t_end = time.perf_counter() + budget_s
-    while len(times) < max_reps and (not times or time.perf_counter() < t_end):
-        r = pyoracle.lbvh_build(pts64, "reference")
-        times.append(1e3 * float(r["seconds"].sum()))
-    return {"value": p95(times), "unit": "ms", "cores": 1, "kind": "reference",
-            "sample": f"full {len(pts64)}-point cloud, {len(times)} reps, p95; "
-                      f"CanonicalPointCloud::rejecting_duplicates + MortonLbvhIndex::build, single thread",
-            "host_cores_total": os.cpu_count()}
+    lb = pyoracle.lbvh_build(pts, "reference")["seconds"]
+    pyoracle.emst_forest(pts, "reference")
+    ef = pyoracle._text_call.seconds.copy()
+    pyoracle.pairs(pts, K_MAX, "reference")
+    pr = pyoracle._text_call.seconds.copy()
+    return {"canonical_cloud": lb[0], "exact_morton_lbvh": lb[1], "boruvka_emst": ef[0],
+            "k1_compact_forest": ef[1], "pair_supports_rank_le_11": pr[0]}
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    import workloads
-    pts = workloads.jittered_lattice(37, 0).astype(np.float64)
     from oracle import pyoracle
     if not pyoracle.available("reference"):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libehgp_ref.so was not built"}))
         return
-    for _ in range(args.warmup):
-        pyoracle.lbvh_build(pts, "reference")
+    pts = reference_sample(0)
+    for _ in range(min(args.warmup, 1)):
+        reference_step_seconds(pts)
     times = []
-    for _ in range(args.steps):
-        r = pyoracle.lbvh_build(pts, "reference")
-        times.append(1e3 * float(r["seconds"].sum()))
+    for _ in range(min(args.steps, 3)):
+        times.append(1e3 * sum(reference_step_seconds(pts).values()))
     v = p95(times)
-    line = {"metric": METRIC, "value": v, "unit": "ms", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": float(np.mean(times)), "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "exact", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": WORKLOAD, "points": int(len(pts)), "stages": STAGES, "seed": 0},
-            "cpu_baseline": {"value": v, "unit": "ms", "cores": 1, "kind": "reference",
-                             "sample": f"full cloud, {args.steps} steps, single thread (reference CPU code is single-threaded)"},
+    sample = (f"{len(pts)}-point {SAMPLE_SIDE}^3 corner of the same jittered lattice (the full 50,653-point "
+              f"cloud is out of reach: the reference's exact pair stream alone took 540 s at 256 points); "
+              f"{len(times)} steps, p95; reference CPU code, single thread")
+    line = {"metric": METRIC, "value": v, "unit": "ms", "n_gpus": args.gpus, "steps": len(times),
+            "warmup": min(args.warmup, 1), "ms_per_step": float(np.mean(times)), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "exact", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "points": int(len(pts)), "K_max": K_MAX, "stages": STAGES,
+                       "sample": sample},
+            "cpu_baseline": {"value": v, "unit": "ms", "cores": 1, "kind": "reference", "sample": sample},
             "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
+def cpu_baseline_line(ours_on_sample_ms: float | None) -> dict:
+    from oracle import pyoracle
+    if not pyoracle.available("reference"):
+        return {"value": None, "unit": "ms", "cores": 1, "kind": "reference", "sample": "oracle/_ref not built"}
+    pts = reference_sample(0)
+    st = reference_step_seconds(pts)
+    return {"value": 1e3 * sum(st.values()), "unit": "ms", "cores": 1, "kind": "reference",
+            "sample": f"{len(pts)}-point {SAMPLE_SIDE}^3 corner of the workload, one step of the same stages",
+            "stage_ms": {k: 1e3 * v for k, v in st.items()}, "gpu_same_sample_ms": ours_on_sample_ms,
+            "host_cores_total": os.cpu_count()}
+
+
+# ---- our path ----------------------------------------------------------------------------
 def run_ours(args, world, rank, local):
+    import ctypes as C
+
     import torch
 
     import ehgp
@@ -169,75 +196,136 @@ def run_ours(args, world, rank, local):
     pts = workloads.jittered_lattice(37, rank)  # one independent cloud per rank (replicas)
     n = len(pts)
     ctx = ehgp.Context(max_points=n, device=local)
-    # pinned host copy of the input and host result buffers for the e2e leg
     pinned = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
     pinned.copy_(torch.from_numpy(pts))
     host_pts = pinned.numpy()
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    d_pts = torch.from_numpy(pts.astype(np.float64)).to(f"cuda:{local}")
+    torch.cuda.synchronize(local)
+    lib = ctx.lib
+    m = n - 1
+    forest = {"lv": np.empty((m, 4), np.uint64), "nodes": np.empty((m, 6), np.uint64),
+              "child": np.empty(2 * m, np.uint64), "batches": np.empty((m, 7), np.uint64),
+              "counts": np.zeros(4, np.uint64), "root": np.zeros(1, np.uint64)}
+    fout = ehgp.K1ForestOut(*(forest[k].ctypes.data for k in ("lv", "nodes", "child", "batches", "counts", "root")))
+    none_lbvh = ehgp.LbvhOut(None, None, None, None, None, None)
+    cnt = np.zeros(1, np.uint64)
 
     def l2_flush():
         flush.fill_(1.0)
         torch.cuda.synchronize(local)
 
-    # device-resident leg: inputs already in HBM (widened binary64 on device)
-    d_pts = torch.from_numpy(pts.astype(np.float64)).to(f"cuda:{local}")
-    torch.cuda.synchronize(local)
-    import ctypes as C
-    out_none = ehgp.LbvhOut(None, None, None, None, None, None)
+    def resident_step():
+        """Device-resident step: results stay on the device except what the host forest sweep reads."""
+        ctx.step_begin()
+        ctx._check(lib.ehgp_lbvh_build_device(ctx._h, C.c_void_p(d_pts.data_ptr()), n, C.byref(none_lbvh)))
+        ctx._check(lib.ehgp_emst(ctx._h, None))
+        ctx._check(lib.ehgp_k1_forest(ctx._h, C.byref(fout)))
+        ctx._check(lib.ehgp_pairs(ctx._h, K_MAX, C.byref(ehgp.PairsOut(None, None, 0, cnt.ctypes.data))))
+        return ctx.step_end()
 
-    def device_step():
-        st = ctx.lib.ehgp_lbvh_build_device(ctx._h, C.c_void_p(d_pts.data_ptr()), n, C.byref(out_none))
-        ctx._check(st)
-        return ctx.last_timing()
+    # e2e buffers (host)
+    e_u = np.empty(m, np.uint32)
+    e_v = np.empty(m, np.uint32)
+    e_D = np.empty((m, 4), np.uint64)
+    rounds = np.zeros(1, np.uint32)
+    eout = ehgp.EmstOut(e_u.ctypes.data, e_v.ctypes.data, e_D.ctypes.data, rounds.ctypes.data, None, 0, None)
+    pair_cap = 64 * n
+    recs = np.empty(pair_cap, ehgp.PAIR_RECORD)
+    plv = np.empty((pair_cap, 4), np.uint64)
+    pout = ehgp.PairsOut(recs.ctypes.data, plv.ctypes.data, pair_cap, cnt.ctypes.data)
+
+    def e2e_step():
+        t0 = time.perf_counter()
+        ctx.lbvh_build(host_pts, outputs=False)
+        ctx._check(lib.ehgp_emst(ctx._h, C.byref(eout)))
+        ctx._check(lib.ehgp_k1_forest(ctx._h, C.byref(fout)))
+        ctx._check(lib.ehgp_pairs(ctx._h, K_MAX, C.byref(pout)))
+        return 1e3 * (time.perf_counter() - t0)
 
     for _ in range(max(args.warmup, 3)):
-        device_step()
-        ctx.lbvh_build(host_pts)
+        resident_step()
+        e2e_step()
     barrier(world)
-    dev_ms, e2e_ms, launches = [], [], 0
+    dev_ms, e2e_ms, kern_ms = [], [], []
+    launches = 0
+    stats = None
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
             l2_flush()
-            ms, nl = device_step()
-            dev_ms.append(ms)
-            launches += nl
+            dev_ms.append(resident_step())
+            km, stats = ctx.kernel_stats()
+            kern_ms.append(km)
+            launches += int(ctx.last_timing()[1])
         for _ in range(args.steps):
             l2_flush()
-            t0 = time.perf_counter()
-            snap = ctx.lbvh_build(host_pts)
-            e2e_ms.append(1e3 * (time.perf_counter() - t0))
-            launches += ctx.last_timing()[1]
+            e2e_ms.append(e2e_step())
     barrier(world)
     value = max_over_ranks(p95(dev_ms), world)
     e2e = max_over_ranks(p95(e2e_ms), world)
     if rank != 0:
         ctx.close()
         return
-    d2h = snap.leaves.nbytes + snap.nodes.nbytes + snap.source_index.nbytes + 5 * 8 + 6 * 8 + 8
-    alg_bytes = BYTES_PER_POINT_LBVH * n
-    mean_ms = float(np.mean(dev_ms))
+    records = int(cnt[0])
+    # stage breakdown of one more step (device time per stage)
+    l2_flush()
+    stage_ms = {}
+    ctx._check(lib.ehgp_lbvh_build_device(ctx._h, C.c_void_p(d_pts.data_ptr()), n, C.byref(none_lbvh)))
+    stage_ms["lbvh"], l1 = ctx.last_timing()
+    ctx._check(lib.ehgp_emst(ctx._h, None))
+    stage_ms["emst"], l2 = ctx.last_timing()
+    t0 = time.perf_counter()
+    ctx._check(lib.ehgp_k1_forest(ctx._h, C.byref(fout)))
+    stage_ms["k1_forest_host"] = 1e3 * (time.perf_counter() - t0)
+    ctx._check(lib.ehgp_pairs(ctx._h, K_MAX, C.byref(ehgp.PairsOut(None, None, 0, cnt.ctypes.data))))
+    stage_ms["pairs"], l3 = ctx.last_timing()
+    launches_per_step = int(l1 + l2 + l3)
+    # roofline of the dominant kernel (pair enumeration): algorithmic bytes per launch from
+    # its own work counters: 32 B per LBVH node visit (box + children), 24 B per point whose
+    # side is decided (64 witness coordinates per witness-list classification), 32 B per
+    # ball-query node visit, 64 B per emitted record, 280 B per point of witness list + coordinates.
+    visits, local_pairs, ballq, ball_nodes, emitted = (int(x) for x in stats[:5])
+    alg_bytes = 32 * visits + 64 * 24 * local_pairs + 32 * ball_nodes + 64 * emitted + 280 * n
+    kmean = float(np.mean(kern_ms))
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = alg_bytes / (mean_ms * 1e-3) / 1e9
+    achieved = alg_bytes / (kmean * 1e-3) / 1e9
+    d2h = e_u.nbytes + e_v.nbytes + e_D.nbytes + sum(forest[k].nbytes for k in forest) + records * (64 + 32)
     line = {
         "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64+exact", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "points": n, "stages": STAGES, "seed": "rank", "l2": "flushed 512MiB",
-                   "parallelism": f"replicas{world}"},
+        "warmup": max(args.warmup, 3), "ms_per_step": float(np.mean(dev_ms)), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64+exact", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "points": n, "K_max": K_MAX, "stages": STAGES, "seed": "rank",
+                   "l2": "flushed 512MiB before each step", "parallelism": f"replicas{world}",
+                   "pair_supports": records, "stage_ms": stage_ms},
         "e2e": {"value": e2e, "unit": "ms", "h2d_bytes_per_step": int(pts.nbytes), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
+        "gpu_launches_per_step": launches_per_step,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "kernel": "whole LBVH build (all stages)",
+                     "traffic": None, "kernel": "k_pairs (pair-support enumeration)",
+                     "kernel_ms": kmean, "algorithmic_bytes": alg_bytes,
+                     "work": {"node_visits": visits, "witness_classifications": local_pairs,
+                              "ball_queries": ballq, "ball_query_node_visits": ball_nodes, "records": emitted},
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "clocks": clocks.summary(),
     }
     if world == 1:
-        line["cpu_baseline"] = cpu_reference_time(pts.astype(np.float64))
+        # our own time on the reference's sample, for a like-for-like reading
+        sample = reference_sample(0)
+        with ehgp.Context(max_points=len(sample), device=local) as sctx:
+            ts = []
+            for _ in range(5):
+                t0 = time.perf_counter()
+                sctx.lbvh_build(sample, outputs=False)
+                sctx.emst(with_minima=False)
+                sctx.k1_forest()
+                sctx.pairs(K_MAX)
+                ts.append(1e3 * (time.perf_counter() - t0))
+        line["cpu_baseline"] = cpu_baseline_line(float(np.median(ts)))
     print(json.dumps(line))
     ctx.close()
 
@@ -249,11 +337,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     args = ap.parse_args()
-    world, rank, local = dist_setup(args) if args.impl == "ours" else (
-        int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)
     if args.impl == "reference":
-        run_reference(args, world, rank)
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
         return
+    world, rank, local = dist_setup()
     run_ours(args, world, rank, local)
     if world > 1:
         import torch.distributed as dist

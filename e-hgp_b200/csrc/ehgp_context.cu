@@ -126,6 +126,10 @@ int ehgp_ctx_create(int device, const ehgp_limits* limits, ehgp_ctx** out_ctx) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->evk0);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->evk1);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->evs0);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->evs1);
   if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->h_status, 64 * sizeof(uint32_t));
   if (e == cudaSuccess) e = ehgp::ctx_alloc(*ctx, (void**)&ctx->d_err, sizeof(uint32_t));
   if (e == cudaSuccess) {
@@ -158,6 +162,8 @@ int ehgp_ctx_destroy(ehgp_ctx* ctx) {
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  for (cudaEvent_t ev : {ctx->evk0, ctx->evk1, ctx->evs0, ctx->evs1})
+    if (ev) cudaEventDestroy(ev);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return EHGP_OK;
@@ -192,6 +198,30 @@ int ehgp_lbvh_build_f32(ehgp_ctx* ctx, const float* xyz, uint64_t n, const ehgp_
 }
 int ehgp_lbvh_build_device(ehgp_ctx* ctx, const double* d_xyz, uint64_t n, const ehgp_lbvh_out* out) {
   return lbvh_build_common(ctx, d_xyz, n, out, 2);
+}
+
+int ehgp_step_begin(ehgp_ctx* ctx) {
+  if (!ctx) return EHGP_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  return cudaEventRecord(ctx->evs0, ctx->stream) == cudaSuccess ? EHGP_OK : EHGP_ERR_CUDA;
+}
+
+int ehgp_step_end(ehgp_ctx* ctx, double* elapsed_ms) {
+  if (!ctx) return EHGP_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  if (cudaEventRecord(ctx->evs1, ctx->stream) != cudaSuccess || cudaEventSynchronize(ctx->evs1) != cudaSuccess)
+    return EHGP_ERR_CUDA;
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, ctx->evs0, ctx->evs1) != cudaSuccess) return EHGP_ERR_CUDA;
+  if (elapsed_ms) *elapsed_ms = ms;
+  return EHGP_OK;
+}
+
+int ehgp_kernel_stats(const ehgp_ctx* ctx, double* kernel_ms, uint64_t* stats, uint32_t count) {
+  if (!ctx) return EHGP_ERR_INVALID_ARGUMENT;
+  if (kernel_ms) *kernel_ms = ctx->kernel_ms;
+  for (uint32_t i = 0; stats && i < count && i < 8; ++i) stats[i] = ctx->kernel_stats[i];
+  return EHGP_OK;
 }
 
 int ehgp_last_timing(const ehgp_ctx* ctx, double* device_ms, uint64_t* kernel_launches) {

@@ -175,6 +175,7 @@ struct PairBuffers {
   uint32_t* order1 = nullptr;
   uint64_t* levelD = nullptr;       // [capacity * 4] squared lengths of sorted records
   uint32_t* counters = nullptr;
+  unsigned long long* stats = nullptr;  // [8] work counters of the enumeration kernel
   uint32_t* radix_counts = nullptr;
   uint32_t capacity = 0;
   uint32_t count = 0;               // records of the last run
@@ -206,6 +207,10 @@ struct Ctx {
   int scale_S = 0;                 // host copy of the cloud scale
   bool scale_valid = false;
   PairBuffers pb;
+  // timing of the dominant kernel of the last stage, and of a whole step
+  cudaEvent_t evk0 = nullptr, evk1 = nullptr, evs0 = nullptr, evs1 = nullptr;
+  double kernel_ms = 0.0;
+  uint64_t kernel_stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   uint32_t emst_rounds = 0;
   uint32_t emst_minima = 0;        // total per-round minima logged
   bool emst_ready = false;

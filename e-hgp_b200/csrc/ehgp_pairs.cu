@@ -224,7 +224,7 @@ __device__ __forceinline__ void warp_classify(WarpBall& b, WarpShared& sh, uint3
 __device__ void warp_ball_query(WarpBall& b, WarpShared& sh, uint32_t iu, uint32_t iv, const Pt& u, const Pt& v,
                                 uint32_t root, const TNode* tn, const uint32_t* leaf_pid, const uint32_t* n_begin,
                                 const uint32_t* n_end, const double* px, const double* py, const double* pz, int S,
-                                uint32_t cap, uint32_t* err) {
+                                uint32_t cap, uint32_t* err, unsigned long long& nodes_seen) {
   const uint32_t lane = threadIdx.x & 31u;
   const double mx = 0.5 * (u.x + v.x), my = 0.5 * (u.y + v.y), mz = 0.5 * (u.z + v.z);
   const double r2 = 0.25 * d2fp(u.x, u.y, u.z, v.x, v.y, v.z);
@@ -234,6 +234,7 @@ __device__ void warp_ball_query(WarpBall& b, WarpShared& sh, uint32_t iu, uint32
   __syncwarp();
   while (head < tail && !b.rejected) {
     const uint32_t batch = min(tail - head, 32u);
+    nodes_seen += batch;
     uint32_t node = kInvalid32;
     if (lane < batch) node = sh.queue[(head + lane) & (kQueue - 1)];
     __syncwarp();
@@ -297,8 +298,11 @@ k_pairs(uint32_t n, uint32_t cap, uint32_t root, const TNode* __restrict__ tn, c
         const uint32_t* __restrict__ n_begin, const uint32_t* __restrict__ n_end, const double* __restrict__ px,
         const double* __restrict__ py, const double* __restrict__ pz, const int* __restrict__ scale,
         const uint32_t* __restrict__ W, const double* __restrict__ R2, PairRec* __restrict__ out,
-        uint32_t out_cap, uint32_t* __restrict__ counters, uint32_t* __restrict__ err) {
+        uint32_t out_cap, uint32_t* __restrict__ counters, unsigned long long* __restrict__ stats,
+        uint32_t* __restrict__ err) {
   __shared__ WarpShared shared[kWarpsPerBlock];
+  // work counters (identical in every lane; lane 0 publishes them)
+  unsigned long long visits = 0, local_pairs = 0, ball_queries = 0, ball_nodes = 0, emitted = 0;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t pos = blockIdx.x * kWarpsPerBlock + warp;
   if (pos >= n) return;  // uniform per warp
@@ -326,6 +330,7 @@ k_pairs(uint32_t n, uint32_t cap, uint32_t root, const TNode* __restrict__ tn, c
     __syncwarp();
     if (n_end[node] <= pos + 1) continue;  // every partner precedes u in Morton order
     const TNode t = load_node(tn, node);
+    ++visits;
     if (t.left != kInvalid32) {
       if (nw >= need) {
         const float lx = (float)((double)t.lo[0] - u.x), ly = (float)((double)t.lo[1] - u.y),
@@ -361,15 +366,32 @@ k_pairs(uint32_t n, uint32_t cap, uint32_t root, const TNode* __restrict__ tn, c
     const double d2 = d2fp(u.x, u.y, u.z, v.x, v.y, v.z);
     WarpBall b{0u, 0u, kInvalid32, false};
     if (d2 * hi < r2u * lo) {
+      ++local_pairs;
       warp_classify(b, sh, w0, w1, iu, iv, u, v, px, py, pz, S, cap);
     } else if (d2 * hi < R2[iv] * lo) {
+      ++local_pairs;
       const uint32_t v0 = W[(uint64_t)iv * kW + lane], v1 = W[(uint64_t)iv * kW + 32 + lane];
       warp_classify(b, sh, v0, v1, iu, iv, u, v, px, py, pz, S, cap);
     } else {
-      warp_ball_query(b, sh, iu, iv, u, v, root, tn, leaf_pid, n_begin, n_end, px, py, pz, S, cap, err);
+      // witnesses of u strictly inside this one sphere: enough of them rejects
+      // the pair without a global query
+      auto strictly_inside = [&](uint32_t w, float ax, float ay, float az) {
+        if (w == kInvalid32 || w == iv) return false;
+        const double dx = (double)ax, dy = (double)ay, dz = (double)az;  // w - u (binary32-rounded)
+        const double vx = v.x - u.x, vy = v.y - u.y, vz = v.z - u.z;
+        // (w-u).(w-v) = |a|^2 - a.(v-u); margin covers the binary32 rounding of a
+        const double aa = dx * dx + dy * dy + dz * dz, av = dx * vx + dy * vy + dz * vz;
+        return aa - av < -1e-5 * (aa + fabs(dx * vx) + fabs(dy * vy) + fabs(dz * vz));
+      };
+      const uint32_t inside = __popc(__ballot_sync(0xffffffffu, strictly_inside(w0, ax0, ay0, az0))) +
+                              __popc(__ballot_sync(0xffffffffu, strictly_inside(w1, ax1, ay1, az1)));
+      if (inside >= need) continue;
+      ++ball_queries;
+      warp_ball_query(b, sh, iu, iv, u, v, root, tn, leaf_pid, n_begin, n_end, px, py, pz, S, cap, err, ball_nodes);
     }
     __syncwarp();
     if (b.rejected || b.interior > cap) continue;
+    ++emitted;
     if (lane == 0) {
       const uint32_t slot = atomicAdd(counters, 1u);
       if (slot < out_cap) {
@@ -391,6 +413,13 @@ k_pairs(uint32_t n, uint32_t cap, uint32_t root, const TNode* __restrict__ tn, c
       }
     }
     __syncwarp();
+  }
+  if (lane == 0) {
+    atomicAdd(stats + 0, visits);
+    atomicAdd(stats + 1, local_pairs);
+    atomicAdd(stats + 2, ball_queries);
+    atomicAdd(stats + 3, ball_nodes);
+    atomicAdd(stats + 4, emitted);
   }
 }
 
@@ -440,6 +469,7 @@ cudaError_t pairs_alloc(Ctx& ctx) {
   EHGP_ALLOC(p.order1, (uint64_t)p.capacity * sizeof(uint32_t));
   EHGP_ALLOC(p.levelD, (uint64_t)p.capacity * 4 * sizeof(uint64_t));
   EHGP_ALLOC(p.counters, 8 * sizeof(uint32_t));
+  EHGP_ALLOC(p.stats, 8 * sizeof(unsigned long long));
   EHGP_ALLOC(p.radix_counts, 256ull * ((p.capacity + kRadixTile - 1) / kRadixTile) * sizeof(uint32_t));
 #undef EHGP_ALLOC
   return cudaSuccess;
@@ -467,14 +497,26 @@ int pairs_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   k_witness_knn<<<nblocks(n), kThreads, 0, st>>>(n, kw, root, g.tnodes, b.leaf_pid, b.px, b.py, b.pz, p.W, p.R2,
                                                   ctx.d_err);
   cudaMemsetAsync(p.counters, 0, 8 * sizeof(uint32_t), st);
-  k_pairs<<<nblocks(n, kWarpsPerBlock), kThreads, 0, st>>>(n, cap, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end, b.px, b.py, b.pz,
-                                            g.scale, p.W, p.R2, (PairRec*)p.raw, p.capacity, p.counters, ctx.d_err);
+  cudaMemsetAsync(p.stats, 0, 8 * sizeof(unsigned long long), st);
+  cudaEventRecord(ctx.evk0, st);
+  k_pairs<<<nblocks(n, kWarpsPerBlock), kThreads, 0, st>>>(n, cap, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end,
+                                                           b.px, b.py, b.pz, g.scale, p.W, p.R2, (PairRec*)p.raw,
+                                                           p.capacity, p.counters, p.stats, ctx.d_err);
+  cudaEventRecord(ctx.evk1, st);
   launches += 2;
   uint32_t hc[2] = {0, 0};
+  unsigned long long hs[8];
   cudaMemcpyAsync(hc, p.counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(hc + 1, ctx.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(hs, p.stats, sizeof(hs), cudaMemcpyDeviceToHost, st);
   cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return abi_cuda_fail(&ctx, e, "pair enumeration");
+  {
+    float kms = 0.f;
+    cudaEventElapsedTime(&kms, ctx.evk0, ctx.evk1);
+    ctx.kernel_ms = kms;
+    for (int i = 0; i < 8; ++i) ctx.kernel_stats[i] = hs[i];
+  }
   if (hc[1]) return abi_device_status(&ctx, hc[1]);
   if (hc[0] > p.capacity) return abi_fail(&ctx, EHGP_ERR_CAPACITY, "pair-support records exceed the buffer");
   const uint32_t m = hc[0];

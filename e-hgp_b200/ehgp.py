@@ -132,6 +132,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "ehgp_emst": (C.c_int, [P, C.POINTER(EmstOut)]),
         "ehgp_k1_forest": (C.c_int, [P, C.POINTER(K1ForestOut)]),
         "ehgp_pairs": (C.c_int, [P, C.c_uint32, C.POINTER(PairsOut)]),
+        "ehgp_step_begin": (C.c_int, [P]),
+        "ehgp_step_end": (C.c_int, [P, C.POINTER(C.c_double)]),
+        "ehgp_kernel_stats": (C.c_int, [P, C.POINTER(C.c_double), P, C.c_uint32]),
         "ehgp_lbvh_build_noalloc": (C.c_int, [P, C.c_uint64, C.POINTER(LbvhOut), P]),
         "ehgp_lbvh_noalloc_max_points": (C.c_uint64, []),
         "ehgp_lbvh_noalloc_scratch_bytes": (C.c_uint64, []),
@@ -231,6 +234,20 @@ class Context:
     @property
     def device_bytes(self) -> int:
         return int(self.lib.ehgp_ctx_device_bytes(self._h))
+
+    def step_begin(self) -> None:
+        self._check(self.lib.ehgp_step_begin(self._h))
+
+    def step_end(self) -> float:
+        ms = C.c_double()
+        self._check(self.lib.ehgp_step_end(self._h, C.byref(ms)))
+        return ms.value
+
+    def kernel_stats(self) -> tuple[float, np.ndarray]:
+        ms = C.c_double()
+        st = np.zeros(8, np.uint64)
+        self._check(self.lib.ehgp_kernel_stats(self._h, C.byref(ms), _ptr(st), 8))
+        return ms.value, st
 
     def last_timing(self) -> tuple[float, int]:
         ms, launches = C.c_double(), C.c_uint64()

@@ -233,6 +233,18 @@ uint64_t ehgp_lbvh_noalloc_scratch_bytes(void);
  * the context's stream, and the number of kernel launches it issued. */
 int ehgp_last_timing(const ehgp_ctx* ctx, double* device_ms, uint64_t* kernel_launches);
 
+/* Step timing on the context's stream: ehgp_step_begin records a CUDA event,
+ * ehgp_step_end records a second one, waits for it and returns the elapsed
+ * device-timeline milliseconds (host stages in between included). */
+int ehgp_step_begin(ehgp_ctx* ctx);
+int ehgp_step_end(ehgp_ctx* ctx, double* elapsed_ms);
+
+/* CUDA-event time of the dominant kernel of the last pair stage (the pair
+ * enumeration) and its work counters: [0] LBVH node visits, [1] witness-list
+ * classifications, [2] exact ball queries, [3] ball-query node visits,
+ * [4] emitted records. */
+int ehgp_kernel_stats(const ehgp_ctx* ctx, double* kernel_ms, uint64_t* stats, uint32_t count);
+
 #ifdef __cplusplus
 }
 #endif
