@@ -506,6 +506,221 @@ std::string pairs_text(const Cloud& c, u64 K) {
   return ev + dg + "S complete\n";
 }
 
+// ---- triples and quads ---------------------------------------------------------------
+// A value with a bound m on the sum of absolute values of the terms that built
+// it: after k roundings the FP64 error is at most k*u*m, so |v| > 64*u*m
+// certifies the sign.
+struct Fm {
+  double v, m;
+};
+Fm operator+(Fm a, Fm b) { return {a.v + b.v, a.m + b.m}; }
+Fm operator-(Fm a, Fm b) { return {a.v - b.v, a.m + b.m}; }
+Fm operator*(Fm a, Fm b) { return {a.v * b.v, a.m * b.m}; }
+int fm_sign(Fm x) {
+  const double bound = 64.0 * 1.1102230246251565e-16 * x.m + 1e-300;
+  return x.v > bound ? 1 : (x.v < -bound ? -1 : 2);  // 2 = undecided
+}
+using FV = std::array<Fm, 3>;
+using BV = std::array<Big, 3>;
+template <class T> T dot3(const std::array<T, 3>& a, const std::array<T, 3>& b) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+template <class T> std::array<T, 3> cross3(const std::array<T, 3>& a, const std::array<T, 3>& b) {
+  return {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+}
+template <class T> std::array<T, 3> scale3(const T& s, const std::array<T, 3>& a) { return {s * a[0], s * a[1], s * a[2]}; }
+template <class T> std::array<T, 3> add3(const std::array<T, 3>& a, const std::array<T, 3>& b) {
+  return {a[0] + b[0], a[1] + b[1], a[2] + b[2]};
+}
+
+FV fdiff(const Cloud& c, u64 p, u64 q) {  // p - q in FP64 with magnitudes
+  FV r;
+  for (int a = 0; a < 3; ++a) {
+    double x, y;
+    std::memcpy(&x, &c.bits[p][a], 8);
+    std::memcpy(&y, &c.bits[q][a], 8);
+    r[a] = {x - y, std::fabs(x) + std::fabs(y)};
+  }
+  return r;
+}
+BV bdiff(const FixedCloud& f, u64 p, u64 q) { return {f.X[p][0] - f.X[q][0], f.X[p][1] - f.X[q][1], f.X[p][2] - f.X[q][2]}; }
+
+// Exact geometry of one 3- or 4-point support (the circumcenter analysis of
+// exact::analyze_circumcenter_support, include/morsehgp3d/exact/support.hpp:41,474-479):
+//  triangle: well-centred iff the three angles are acute ((b-a).(c-a) > 0 ...);
+//            centre a + (G22(G11-G12) e1 + G11(G22-G12) e2) / (2 det G);
+//  tetrahedron: centre a + N / (2 det E), N = |e1|^2 e2xe3 + |e2|^2 e3xe1 + |e3|^2 e1xe2,
+//            barycentric signs of the centre from N.(e_j x e_k) and 2 det E^2 - sum.
+// status: 0 minimal, 1 boundary reduced, 2 exterior centre, 3 affinely dependent.
+struct SupportGeo {
+  int status = 3;
+  int size = 0;
+  u64 ids[4]{};
+  // side(w): val(w) = A * |p|^2 - p . Nv with p = w - ids[0]; sign multiplied by sgn
+  Big A;
+  BV Nv;
+  int sgn = 1;
+  FV fN;
+  Fm fA{0, 0};
+};
+
+SupportGeo analyze(const Cloud& c, const FixedCloud& f, const u64* ids, int size) {
+  SupportGeo g;
+  g.size = size;
+  for (int i = 0; i < size; ++i) g.ids[i] = ids[i];
+  if (size == 3) {
+    const BV e1 = bdiff(f, ids[1], ids[0]), e2 = bdiff(f, ids[2], ids[0]);
+    const Big G11 = dot3(e1, e1), G12 = dot3(e1, e2), G22 = dot3(e2, e2);
+    const Big detG = G11 * G22 - G12 * G12;
+    if (detG == 0) return g;
+    const Big da = G12, db = G11 - G12, dc = G22 - G12;
+    if (da < 0 || db < 0 || dc < 0) { g.status = 2; return g; }
+    if (da == 0 || db == 0 || dc == 0) { g.status = 1; return g; }
+    g.status = 0;
+    g.A = detG;
+    g.Nv = add3(scale3(Big(G22 * db), e1), scale3(Big(G11 * dc), e2));
+  } else {
+    const BV e1 = bdiff(f, ids[1], ids[0]), e2 = bdiff(f, ids[2], ids[0]), e3 = bdiff(f, ids[3], ids[0]);
+    const BV c23 = cross3(e2, e3), c31 = cross3(e3, e1), c12 = cross3(e1, e2);
+    const Big detE = dot3(e1, c23);
+    if (detE == 0) return g;
+    const BV N = add3(add3(scale3(dot3(e1, e1), c23), scale3(dot3(e2, e2), c31)), scale3(dot3(e3, e3), c12));
+    const Big l1 = dot3(N, c23), l2 = dot3(N, c31), l3 = dot3(N, c12);
+    const Big l0 = 2 * detE * detE - (l1 + l2 + l3);
+    if (l0 < 0 || l1 < 0 || l2 < 0 || l3 < 0) { g.status = 2; return g; }
+    if (l0 == 0 || l1 == 0 || l2 == 0 || l3 == 0) { g.status = 1; return g; }
+    g.status = 0;
+    g.A = detE;
+    g.Nv = N;
+    g.sgn = detE < 0 ? -1 : 1;
+  }
+  return g;
+}
+
+// FP64 image of the side polynomial, for the filter.
+void analyze_fp(const Cloud& c, SupportGeo& g) {
+  const u64* ids = g.ids;
+  if (g.size == 3) {
+    const FV e1 = fdiff(c, ids[1], ids[0]), e2 = fdiff(c, ids[2], ids[0]);
+    const Fm G11 = dot3(e1, e1), G12 = dot3(e1, e2), G22 = dot3(e2, e2);
+    g.fA = G11 * G22 - G12 * G12;
+    g.fN = add3(scale3(G22 * (G11 - G12), e1), scale3(G11 * (G22 - G12), e2));
+  } else {
+    const FV e1 = fdiff(c, ids[1], ids[0]), e2 = fdiff(c, ids[2], ids[0]), e3 = fdiff(c, ids[3], ids[0]);
+    const FV c23 = cross3(e2, e3), c31 = cross3(e3, e1), c12 = cross3(e1, e2);
+    g.fA = dot3(e1, c23);
+    g.fN = add3(add3(scale3(dot3(e1, e1), c23), scale3(dot3(e2, e2), c31)), scale3(dot3(e3, e3), c12));
+  }
+}
+
+int higher_side(const Cloud& c, const FixedCloud& f, const SupportGeo& g, u64 w) {
+  const FV p = fdiff(c, w, g.ids[0]);
+  const int s = fm_sign(g.fA * dot3(p, p) - dot3(p, g.fN));
+  if (s != 2) return s * g.sgn;
+  const BV q = bdiff(f, w, g.ids[0]);
+  const Big val = g.A * dot3(q, q) - dot3(q, g.Nv);
+  return (val < 0 ? -1 : (val > 0 ? 1 : 0)) * g.sgn;
+}
+
+std::string reduced_vec(BV num, Big den) {  // (num / den), common gcd removed
+  if (den < 0) {
+    den = -den;
+    for (auto& x : num) x = -x;
+  }
+  Big g = den;
+  for (const auto& x : num) {
+    Big a = x < 0 ? Big(-x) : x, b = g;
+    while (b != 0) {
+      Big t = a % b;
+      a = b;
+      b = t;
+    }
+    g = a;
+  }
+  if (g == 0) g = 1;
+  return Big(num[0] / g).str() + " " + Big(num[1] / g).str() + " " + Big(num[2] / g).str() + " " + Big(den / g).str();
+}
+
+std::string reduced_frac(Big num, Big den) {
+  if (den < 0) { den = -den; num = -num; }
+  Big a = num < 0 ? Big(-num) : num, b = den;
+  while (b != 0) {
+    Big t = a % b;
+    a = b;
+    b = t;
+  }
+  return Big(num / a).str() + " " + Big(den / a).str();
+}
+
+// Level and centre of a minimal support: centre = a + Nv / (k A) with k = 2.
+std::string sphere_text(const FixedCloud& f, const SupportGeo& g) {
+  const Big den = 2 * g.A;  // centre offset = Nv / den (both sizes)
+  const Big two_S = Big(1) << (unsigned)f.S;
+  const Big lev_num = dot3(g.Nv, g.Nv);
+  const Big lev_den = den * den * (Big(1) << (unsigned)(2 * f.S));
+  BV cnum;
+  for (int a = 0; a < 3; ++a) cnum[a] = den * f.X[g.ids[0]][a] + g.Nv[a];
+  return reduced_frac(lev_num, lev_den) + " " + reduced_vec(cnum, den * two_S);
+}
+
+// All relevant 3- and 4-point supports by brute force: the outcome of
+// build_exact_higher_support_stream run to completion
+// (include/morsehgp3d/hierarchy/higher_support_stream.hpp:544; leaf rule
+// classify_terminal_support, src/cpu/hierarchy/higher_support_stream.cpp:1992-2110):
+// only minimal (well-centred, affinely independent) supports; relevant iff
+// interior + size <= s_max; event iff the shell is exactly the support.
+std::string higher_text(const Cloud& c, u64 K) {
+  const FixedCloud f = fixed_cloud(c);
+  const u64 n = c.bits.size();
+  const u64 keff = std::min(K, n), smax = std::min(keff + 1, n);
+  std::string ev[2], dg[2];
+  std::vector<u64> interior;
+  auto visit = [&](const u64* ids, int size) {
+    if (smax < (u64)size) return;
+    SupportGeo g = analyze(c, f, ids, size);
+    if (g.status != 0) return;
+    analyze_fp(c, g);
+    const u64 cap = smax - size;
+    interior.clear();
+    u64 shell = size, extra = ~u64{0};
+    for (u64 w = 0; w < n; ++w) {
+      bool sup = false;
+      for (int i = 0; i < size; ++i) sup |= (w == ids[i]);
+      if (sup) continue;
+      const int sd = higher_side(c, f, g, w);
+      if (sd < 0) {
+        interior.push_back(w);
+        if (interior.size() > cap) return;
+      } else if (sd == 0) {
+        ++shell;
+        extra = std::min(extra, w);
+      }
+    }
+    const u64 I = interior.size();
+    std::string head = std::to_string(size);
+    for (int i = 0; i < size; ++i) head += " " + std::to_string(ids[i]);
+    std::string idt;
+    for (u64 w : interior) idt += " " + std::to_string(w);
+    const std::string sph = sphere_text(f, g);
+    if (shell == (u64)size)
+      ev[size - 3] += "H " + head + " " + std::to_string(I + size) + " " + std::to_string(n - I - size) + " " + sph +
+                      " |" + idt + "\n";
+    else
+      dg[size - 3] += "G " + head + " " + std::to_string(shell) + " " + std::to_string(extra) + " " +
+                      std::to_string(I + size) + " " + std::to_string(I + shell) + " " + std::to_string(n - I - shell) +
+                      " " + sph + " |" + idt + "\n";
+  };
+  u64 ids[4];
+  for (ids[0] = 0; ids[0] < n; ++ids[0])
+    for (ids[1] = ids[0] + 1; ids[1] < n; ++ids[1])
+      for (ids[2] = ids[1] + 1; ids[2] < n; ++ids[2]) {
+        visit(ids, 3);
+        for (ids[3] = ids[2] + 1; ids[3] < n; ++ids[3]) visit(ids, 4);
+      }
+  // the stream orders records by (support size, ids): triples before quads
+  return ev[0] + ev[1] + dg[0] + dg[1] + "S complete\n";
+}
+
 u64 put_text(const std::string& s, char* buf, u64 cap) {
   if (s.size() + 1 > cap) return s.size() + 1;
   std::memcpy(buf, s.c_str(), s.size() + 1);
@@ -571,6 +786,15 @@ int oracle_lbvh_build(const double* xyz, u64 n, u64* source_index, u64* leaves, 
 int oracle_knn(const double* xyz, u64 n, u64 k, char* out, u64 cap, u64* needed, char* err, u64 errlen) {
   try {
     *needed = put_text(knn_text(canonical_cloud(xyz, n), k), out, cap);
+    return 0;
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 1);
+  }
+}
+
+int oracle_higher(const double* xyz, u64 n, u64 K, char* out, u64 cap, u64* needed, char* err, u64 errlen) {
+  try {
+    *needed = put_text(higher_text(canonical_cloud(xyz, n), K), out, cap);
     return 0;
   } catch (const std::exception& e) {
     return report(e, err, errlen, 1);

@@ -189,3 +189,33 @@ def parse_pairs(txt: str) -> dict:
 def pairs(points: np.ndarray, K: int = 10, which: str = "restatement") -> dict:
     name = "oracle_pairs" if which == "restatement" else "ref_pairs"
     return parse_pairs(_text_call(name, which, points, K))
+
+
+def parse_higher(txt: str) -> dict:
+    """Higher-support records: events (size, ids, closed_rank, exterior, level, center, interior)
+    and diagnostics (size, ids, shell, witness, min_rank, observed_rank, exterior, level, center, interior)."""
+    events, diags, status = [], [], None
+    for line in txt.splitlines():
+        head, _, tail = line.partition("|")
+        t = head.split()
+        if not t:
+            continue
+        ids = tuple(int(x) for x in tail.split())
+        if t[0] in ("H", "G"):
+            m = int(t[1])
+            sup = tuple(int(x) for x in t[2:2 + m])
+            r = t[2 + m:]
+            if t[0] == "H":
+                center = tuple(Fraction(int(r[4 + a]), int(r[7])) for a in range(3))
+                events.append((m, sup, int(r[0]), int(r[1]), Fraction(int(r[2]), int(r[3])), center, ids))
+            else:
+                center = tuple(Fraction(int(r[7 + a]), int(r[10])) for a in range(3))
+                diags.append((m, sup, *(int(x) for x in r[:5]), Fraction(int(r[5]), int(r[6])), center, ids))
+        elif t[0] == "S":
+            status = t[1]
+    return {"events": events, "diagnostics": diags, "status": status}
+
+
+def higher(points: np.ndarray, K: int = 10, which: str = "restatement") -> dict:
+    name = "oracle_higher" if which == "restatement" else "ref_higher"
+    return parse_higher(_text_call(name, which, points, K))

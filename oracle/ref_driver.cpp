@@ -205,6 +205,7 @@ int ref_knn(const double* xyz, uint64_t n, uint64_t k, char* out, uint64_t cap, 
 #include "morsehgp3d/hierarchy/boruvka.hpp"
 #include "morsehgp3d/hierarchy/k1_forest.hpp"
 #include "morsehgp3d/hierarchy/pair_support_stream.hpp"
+#include "morsehgp3d/hierarchy/higher_support_stream.hpp"
 
 namespace {
 
@@ -235,6 +236,56 @@ morsehgp3d::hierarchy::ExactPairSupportStreamBudget unlimited_pair_budget() {
 }  // namespace
 
 extern "C" {
+
+// build_exact_higher_support_stream (include/morsehgp3d/hierarchy/higher_support_stream.hpp:544)
+// with an unlimited budget.  Lines in the stream's canonical (size, ids) order:
+// "H size a b c [d] closed_rank exterior lnum lden cx cy cz cden | interior..."  (events)
+// "G size a b c [d] shell witness min_rank observed exterior lnum lden cx cy cz cden | interior..."
+// then "S complete|budget_exhausted".
+int ref_higher(const double* xyz, uint64_t n, uint64_t K, char* out, uint64_t cap, uint64_t* needed, double* seconds,
+               char* err, uint64_t errlen) {
+  try {
+    using namespace morsehgp3d;
+    const auto pts = points_from(xyz, n);
+    const CanonicalPointCloud cloud = CanonicalPointCloud::rejecting_duplicates(pts);
+    const MortonLbvhIndex index = MortonLbvhIndex::build(cloud);
+    hierarchy::ExactHigherSupportStreamBudget b;
+    const std::size_t big = std::size_t{1} << 62;
+    b.maximum_work_unit_count = big;
+    b.maximum_frontier_entry_count = big;
+    b.maximum_auxiliary_frontier_entry_count = big;
+    b.maximum_emitted_record_count = big;
+    b.maximum_emitted_point_id_reference_count = big;
+    b.maximum_prune_receipt_count = big;
+    b.maximum_global_closed_ball_query_count = big;
+    b.maximum_point_classification_count = big;
+    const auto t0 = std::chrono::steady_clock::now();
+    const auto res = hierarchy::build_exact_higher_support_stream(index, cloud, K, b);
+    if (seconds) seconds[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::string s;
+    auto ids = [](const auto& r) {
+      std::string t = std::to_string((int)r.support_size);
+      for (int i = 0; i < r.support_size; ++i) t += " " + std::to_string(r.support_ids[i]);
+      return t;
+    };
+    for (const auto& e : res.events)
+      s += "H " + ids(e) + " " + std::to_string(e.closed_rank) + " " + std::to_string(e.exterior_count) + " " +
+           e.squared_level.numerator_string() + " " + e.squared_level.denominator_string() + " " +
+           center_text(e.center) + " |" + ids_text(e.interior_ids) + "\n";
+    for (const auto& d : res.relevant_extra_shell_diagnostics)
+      s += "G " + ids(d) + " " + std::to_string(d.shell_count) + " " + std::to_string(d.canonical_extra_shell_witness_id) +
+           " " + std::to_string(d.minimum_possible_closed_rank) + " " + std::to_string(d.observed_closed_rank) + " " +
+           std::to_string(d.exterior_count) + " " + d.squared_level.numerator_string() + " " +
+           d.squared_level.denominator_string() + " " + center_text(d.center) + " |" + ids_text(d.interior_ids) +
+           "\n";
+    s += std::string("S ") +
+         (res.status == hierarchy::ExactHigherSupportStreamStatus::complete ? "complete" : "budget_exhausted") + "\n";
+    *needed = put_text(s, out, cap);
+    return 0;
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 1);
+  }
+}
 
 // build_exact_pair_support_stream (include/morsehgp3d/hierarchy/pair_support_stream.hpp:415)
 // with an unlimited budget.  Lines, in the stream's canonical (u, v) order:

@@ -5,6 +5,7 @@ project-written Boost shim).  Run here, where the reference tree exists:
 
     make -C oracle ref && python tests/golden/make_golden.py && python tests/golden/make_golden.py --geom
     python tests/golden/make_golden.py --pairs   # slow: the reference pair stream
+    python tests/golden/make_golden.py --higher  # slow: the reference higher-support stream (n = 12)
 """
 import os
 import sys
@@ -118,3 +119,47 @@ def main_pairs():
 
 if __name__ == "__main__" and "--pairs" in sys.argv:
     main_pairs()
+
+
+def higher_cases():
+    yield "uniform12_s2", workloads.uniform_cube(12, 2)
+    yield "lattice12", workloads.jittered_lattice(3, 6).astype(np.float64)[:12]
+    # cube corners + face centres + centre: cospherical ties (extra-shell diagnostics)
+    c = [[x, y, z] for x in (0, 1) for y in (0, 1) for z in (0, 1)] + [[0.5, 0.5, 0.0], [0.5, 0.0, 0.5],
+                                                                         [0.0, 0.5, 0.5], [0.5, 0.5, 0.5]]
+    yield "cube12_ties", np.array(c, dtype=np.float64)
+
+
+def parse_higher(txt):
+    events, diags, status = [], [], None
+    for line in txt.splitlines():
+        head, _, tail = line.partition("|")
+        t = head.split()
+        if not t:
+            continue
+        ids = [int(x) for x in tail.split()]
+        if t[0] in ("H", "G"):
+            m = int(t[1])
+            sup = [int(x) for x in t[2:2 + m]]
+            rest = t[2 + m:]
+            if t[0] == "H":
+                events.append([m, sup, int(rest[0]), int(rest[1]), rest[2], rest[3], rest[4:8], ids])
+            else:
+                diags.append([m, sup] + [int(x) for x in rest[:5]] + [rest[5], rest[6], rest[7:11], ids])
+        elif t[0] == "S":
+            status = t[1]
+    return {"events": events, "diagnostics": diags, "status": status}
+
+
+def main_higher():
+    import json
+    for name, pts in higher_cases():
+        txt = pyoracle._text_call("ref_higher", "reference", pts, 10)
+        doc = {"points": pts.tolist(), "K": 10, **parse_higher(txt)}
+        with open(os.path.join(HERE, f"higher_{name}.json"), "w") as f:
+            json.dump(doc, f, separators=(",", ":"))
+        print(name, len(pts), len(doc["events"]), len(doc["diagnostics"]), doc["status"], flush=True)
+
+
+if __name__ == "__main__" and "--higher" in sys.argv:
+    main_higher()
