@@ -81,6 +81,7 @@ int lbvh_build_common(Ctx* ctx, const void* src, uint64_t n, const ehgp_lbvh_out
   ctx->built_n = 0;
   ctx->geom_ready = false;
   ctx->emst_ready = false;
+  ctx->pb.witness_ready = false;
   if (where == 0) {
     e = cudaMemcpyAsync(b.xyz_in, src, 3 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
   } else if (where == 1) {
@@ -143,6 +144,7 @@ int ehgp_ctx_create(int device, const ehgp_limits* limits, ehgp_ctx** out_ctx) {
   if (e == cudaSuccess) e = ehgp::lbvh_alloc(*ctx);
   if (e == cudaSuccess) e = ehgp::geom_alloc(*ctx);
   if (e == cudaSuccess) e = ehgp::pairs_alloc(*ctx);
+  if (e == cudaSuccess) e = ehgp::higher_alloc(*ctx);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) {
     const int st = (e == cudaErrorMemoryAllocation) ? EHGP_ERR_OUT_OF_MEMORY : EHGP_ERR_CUDA;

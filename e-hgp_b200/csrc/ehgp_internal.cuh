@@ -180,6 +180,32 @@ struct PairBuffers {
   uint32_t capacity = 0;
   uint32_t count = 0;               // records of the last run
   uint32_t K = 0;
+  bool witness_ready = false;       // W / R2 computed for the resident cloud
+};
+
+// Buffers of the triple/quad-support stage.
+struct HigherBuffers {
+  uint32_t* nb = nullptr;           // [n * 512] neighbour lists
+  uint32_t* nbc = nullptr;          // [n]
+  double* gather_r2 = nullptr;      // [n] squared gather radius
+  double* rcap = nullptr;           // [n] certified radius bound
+  uint8_t* todo = nullptr;          // [n]
+  float* dirs = nullptr;            // [642 * 3]
+  double delta = 0;                 // covering angle of dirs
+  void* raw = nullptr;              // [capacity] 64-byte records
+  void* sorted = nullptr;
+  uint64_t* khi = nullptr;
+  uint64_t* klo = nullptr;
+  uint32_t* order0 = nullptr;
+  uint32_t* order1 = nullptr;
+  uint32_t* counters = nullptr;
+  unsigned long long* stats = nullptr;
+  uint32_t* radix_counts = nullptr;
+  uint32_t capacity = 0;
+  uint32_t count = 0;
+  uint32_t K = 0;
+  double kernel_ms = 0;
+  uint64_t stats_host[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 struct Ctx {
@@ -207,6 +233,7 @@ struct Ctx {
   int scale_S = 0;                 // host copy of the cloud scale
   bool scale_valid = false;
   PairBuffers pb;
+  HigherBuffers hb;
   // timing of the dominant kernel of the last stage, and of a whole step
   cudaEvent_t evk0 = nullptr, evk1 = nullptr, evs0 = nullptr, evs1 = nullptr;
   double kernel_ms = 0.0;
@@ -235,6 +262,10 @@ uint64_t geom_prepare(Ctx& ctx, uint32_t n);
 // Pair supports (ehgp_pairs.cu)
 cudaError_t pairs_alloc(Ctx& ctx);
 int pairs_run(Ctx& ctx, uint32_t K, uint32_t* out_count);
+
+// Triple/quad supports (ehgp_higher.cu)
+cudaError_t higher_alloc(Ctx& ctx);
+int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count);
 
 }  // namespace ehgp
 

@@ -541,6 +541,7 @@ int pairs_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   ctx.last_launches = launches;
   p.count = m;
   p.K = K;
+  p.witness_ready = true;
   *out_count = m;
   return EHGP_OK;
 }

@@ -97,6 +97,15 @@ PAIR_RECORD = np.dtype([("u", "<u4"), ("v", "<u4"), ("interior_count", "<u4"), (
 assert PAIR_RECORD.itemsize == 64
 
 
+class HigherOut(C.Structure):
+    _fields_ = [("records", C.c_void_p), ("capacity", C.c_uint64), ("count", C.c_void_p)]
+
+
+HIGHER_RECORD = np.dtype([("size", "<u4"), ("ids", "<u4", 4), ("interior_count", "<u4"), ("shell_count", "<u4"),
+                          ("extra_shell_witness", "<u4"), ("interior_ids", "<u4", 8)])
+assert HIGHER_RECORD.itemsize == 64
+
+
 def limbs_to_int(a: np.ndarray) -> int:
     """Little-endian 64-bit limbs -> Python int."""
     v = 0
@@ -132,6 +141,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "ehgp_emst": (C.c_int, [P, C.POINTER(EmstOut)]),
         "ehgp_k1_forest": (C.c_int, [P, C.POINTER(K1ForestOut)]),
         "ehgp_pairs": (C.c_int, [P, C.c_uint32, C.POINTER(PairsOut)]),
+        "ehgp_higher": (C.c_int, [P, C.c_uint32, C.POINTER(HigherOut)]),
+        "ehgp_higher_stats": (C.c_int, [P, C.POINTER(C.c_double), P, C.c_uint32]),
         "ehgp_step_begin": (C.c_int, [P]),
         "ehgp_step_end": (C.c_int, [P, C.POINTER(C.c_double)]),
         "ehgp_kernel_stats": (C.c_int, [P, C.POINTER(C.c_double), P, C.c_uint32]),
@@ -330,6 +341,21 @@ class Context:
         lv = np.zeros((max(m, 1), 4), np.uint64)
         self._check(self.lib.ehgp_pairs(self._h, K, C.byref(PairsOut(_ptr(recs), _ptr(lv), m, _ptr(cnt)))))
         return {"records": recs[:m], "level_num": lv[:m]}
+
+    def higher(self, K: int = 10) -> np.ndarray:
+        """ehgp_higher: relevant minimal triple/quad supports in (size, ids) order."""
+        cnt = np.zeros(1, np.uint64)
+        self._check(self.lib.ehgp_higher(self._h, K, C.byref(HigherOut(None, 0, _ptr(cnt)))))
+        m = int(cnt[0])
+        recs = np.zeros(max(m, 1), HIGHER_RECORD)
+        self._check(self.lib.ehgp_higher(self._h, K, C.byref(HigherOut(_ptr(recs), m, _ptr(cnt)))))
+        return recs[:m]
+
+    def higher_stats(self) -> tuple[float, np.ndarray]:
+        ms = C.c_double()
+        st = np.zeros(8, np.uint64)
+        self._check(self.lib.ehgp_higher_stats(self._h, C.byref(ms), _ptr(st), 8))
+        return ms.value, st
 
     def k1_forest(self) -> dict:
         """ehgp_k1_forest on the last EMST: reference-layout compact forest arenas."""

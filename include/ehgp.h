@@ -212,6 +212,40 @@ typedef struct ehgp_pairs_out {
  * on the device.  records == NULL only counts. */
 int ehgp_pairs(ehgp_ctx* ctx, uint32_t K, const ehgp_pairs_out* out);
 
+/* ---- triple and quad critical-sphere supports ------------------------------ */
+/* One relevant minimal 3- or 4-point support (64 bytes): an
+ * ExactHigherSupportEvent when shell_count == size, else an
+ * ExactHigherSupportExtraShellDiagnostic
+ * (include/morsehgp3d/hierarchy/higher_support_stream.hpp:283-316).  The sphere
+ * is the circumsphere of the support (for a triangle, the one centred in its
+ * plane); its exact centre and level follow from the support ids. */
+typedef struct ehgp_higher_record {
+  uint32_t size;                /* 3 or 4 */
+  uint32_t ids[4];              /* ascending; unused slot 0 */
+  uint32_t interior_count;      /* <= s_max - size */
+  uint32_t shell_count;         /* complete exact shell, support included */
+  uint32_t extra_shell_witness; /* least extra shell PointId, or 0xffffffff */
+  uint32_t interior_ids[8];     /* ascending; unused slots 0xffffffff */
+} ehgp_higher_record;
+
+typedef struct ehgp_higher_out {
+  ehgp_higher_record* records; /* [capacity], (size, ids) order */
+  uint64_t capacity;
+  uint64_t* count;             /* [1] */
+} ehgp_higher_out;
+
+/* Every relevant minimal triple and quad support of the resident cloud for
+ * maximum order K <= 10.  Replaces hierarchy::build_exact_higher_support_stream
+ * (include/morsehgp3d/hierarchy/higher_support_stream.hpp:544) run to
+ * completion.  EHGP_ERR_CAPACITY when a certified neighbourhood exceeds 512
+ * points.  records == NULL only counts. */
+int ehgp_higher(ehgp_ctx* ctx, uint32_t K, const ehgp_higher_out* out);
+
+/* CUDA-event time of the last triple/quad enumeration kernel and its work
+ * counters: [0] candidate supports tested, [1] closed-ball classifications,
+ * [2] records, [3] neighbour-list entries. */
+int ehgp_higher_stats(const ehgp_ctx* ctx, double* kernel_ms, uint64_t* stats, uint32_t count);
+
 /* Allocation-free LBVH build.  No counterpart in the reference: it exists for
  * callers that may not call cudaMalloc (a host framework that owns all device
  * memory through its own pool, or a latency-critical caller that cannot

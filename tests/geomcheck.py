@@ -130,3 +130,48 @@ def pairs_match(gpu, ref):
             raise AssertionError(f"{key}: {len(g)} vs {len(r)}; only gpu {sorted(gs - rs)[:3]}; "
                                  f"only oracle {sorted(rs - gs)[:3]}")
     assert ref["status"] == "complete"
+
+
+def exact_sphere(P, ids):
+    """Exact circumcentre and squared level of a 3- or 4-point support (Fractions)."""
+    pts = [[Fraction(float(x)) for x in P[i]] for i in ids]
+    a = pts[0]
+    e = [[p[k] - a[k] for k in range(3)] for p in pts[1:]]
+    dot = lambda u, v: sum(x * y for x, y in zip(u, v))
+    cross = lambda u, v: [u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]]
+    if len(ids) == 3:
+        G11, G12, G22 = dot(e[0], e[0]), dot(e[0], e[1]), dot(e[1], e[1])
+        A = G11 * G22 - G12 * G12
+        N = [G22 * (G11 - G12) * e[0][k] + G11 * (G22 - G12) * e[1][k] for k in range(3)]
+    else:
+        c23, c31, c12 = cross(e[1], e[2]), cross(e[2], e[0]), cross(e[0], e[1])
+        A = dot(e[0], c23)
+        N = [dot(e[0], e[0]) * c23[k] + dot(e[1], e[1]) * c31[k] + dot(e[2], e[2]) * c12[k] for k in range(3)]
+    off = [x / (2 * A) for x in N]
+    return tuple(a[k] + off[k] for k in range(3)), dot(off, off)
+
+
+def gpu_higher_records(ctx, K, points_canonical):
+    """ehgp_higher output converted to the oracle's (events, diagnostics) tuples."""
+    n = len(points_canonical)
+    ev, dg = [], []
+    for r in ctx.higher(K):
+        m = int(r["size"])
+        ids = tuple(int(x) for x in r["ids"][:m])
+        I, sh = int(r["interior_count"]), int(r["shell_count"])
+        center, level = exact_sphere(points_canonical, ids)
+        iids = tuple(int(x) for x in r["interior_ids"][:I])
+        if sh == m:
+            ev.append((m, ids, I + m, n - I - m, level, center, iids))
+        else:
+            dg.append((m, ids, sh, int(r["extra_shell_witness"]), I + m, I + sh, n - I - sh, level, center, iids))
+    return {"events": ev, "diagnostics": dg, "status": "complete"}
+
+
+def higher_match(gpu, ref):
+    for key in ("events", "diagnostics"):
+        g, r = gpu[key], ref[key]
+        if g != r:
+            gs, rs = set(g), set(r)
+            raise AssertionError(f"{key}: {len(g)} vs {len(r)}; only gpu {sorted(gs - rs)[:2]}; "
+                                 f"only oracle {sorted(rs - gs)[:2]}")
