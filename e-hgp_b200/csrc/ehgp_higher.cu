@@ -13,19 +13,20 @@
 //
 // B200 design (replacing the reference's CPU branch-and-bound over LBVH node
 // triples/quads with interval Gram/Cramer bounds):
-//  1. Radius certificate.  Any sphere through a point a is the tangent ball
-//     B(a + r u, r).  A neighbour p lies strictly inside it as soon as
+//  1. Direction table.  Any sphere through a point a is the tangent ball
+//     B(a + r u, r); a point p lies strictly inside it as soon as
 //     r > rho_p(u) = |p - a| / (2 cos angle(u, p - a)), and tangent balls with the
-//     same u are nested.  Over 642 sampled directions s with covering angle
-//     delta, shrinking each cap by delta gives a bound valid for every u in the
-//     cone of s: r <= (s_max-2)-th smallest rho_p(s) for a relevant sphere of
-//     size >= 3.  A well-centred sphere also has a support point p with
-//     (p - a).u >= r, so r <= the support function of the cloud's AABB in the
-//     cone.  r_cap(a) = max over s of the smaller bound.
-//  2. Owner-local enumeration.  Every support is enumerated once, by its least
-//     PointId a, from the neighbours of a within 2 r_cap(a) -- a list that
-//     also holds every point of the support's ball (the ball lies in B(a, 2r)),
-//     so the closed-ball classification is exact and local.
+//     same u are nested.  A relevant sphere of size >= 3 has at most s_max - 3
+//     strict interior points, so r <= the (s_max-2)-th smallest rho_p(u).  Over
+//     642 sampled directions s (covering angle delta), caps shrunk by delta give
+//     a bound rho_s(a) valid in the whole cone of s, further capped by the AABB
+//     support function (a well-centred sphere has a support point p with
+//     (p - a).u >= r).  See k_dirtable for the derivation.
+//  2. Candidate set C(a): the points whose lowest threshold in some cone is at
+//     most rho_s(a).  It holds every support, shell and interior point of every
+//     relevant sphere through a, and enough interior points of every other
+//     well-centred sphere to reject it.  Every support is enumerated once, by
+//     its least PointId a, from C(a), and classified exactly against C(a).
 //  3. Exact predicates: FP64 with a tracked error bound, then 832-bit integers
 //     at the cloud scale inside the bound.
 #include "ehgp_internal.cuh"
@@ -39,11 +40,11 @@
 namespace ehgp {
 namespace {
 
-constexpr int kMaxNb = 512;     // neighbour list capacity per point
+constexpr int kMaxNb = 1024;    // neighbour list capacity per point
 constexpr int kDirs = 642;      // direction samples (icosphere, 3 subdivisions)
 constexpr int kWarps = 4;       // warps per block
 constexpr int kThreads = 32 * kWarps;
-constexpr int kQueue = 512;
+constexpr int kQueue = 1024;
 constexpr int kMaxInteriorH = 8;  // s_max - 3 for K = 10
 constexpr double kU = 1.1102230246251565e-16;
 
@@ -335,57 +336,127 @@ k_gather(uint32_t n, uint32_t root, const TNode* __restrict__ tn, const uint32_t
   if (lane == 0) nbc[a] = overflow ? (uint32_t)kMaxNb + 1 : count;
 }
 
-// ---- 2. radius certificate ------------------------------------------------------------------
+// ---- 2. direction table and candidate set --------------------------------------------
+// For owner a and sampled direction s (cone of half-angle delta):
+//   rho_shr_p(s) = |p - a| / (2 cos(angle(s, p - a) + delta))  >= rho_p(u) for u in the cone
+//   rho_lo_p(s)  = |p - a| / (2 cos(max(angle(s, p - a) - delta, 0)))  <= rho_p(u)
+//   rho_s(a)     = min((s_max - 2)-th smallest rho_shr_p(s), ext_s)
+// where ext_s bounds the AABB support function over the cone.  A relevant
+// sphere through a with centre direction u in the cone of s has
+// r <= rho_(s_max-2)(u) <= rho_s(a), so each of its support, shell and strictly
+// interior points p has rho_lo_p(s) <= rho_p(u) <= r <= rho_s(a): the candidate
+// set C(a) = {p : rho_lo_p(s) <= rho_s(a) for some s} holds them all.  A
+// well-centred sphere through a that is NOT relevant has r <= ext_s and at
+// least s_max - 2 points with rho_p(u) < r whose thresholds are the smallest at
+// u; those lie in C(a) too, so classifying against C(a) rejects it.
+// The neighbour list (points within the gather radius L, sorted by distance)
+// certifies rho_s when rho_s <= L / 2: every unlisted point has rho >= L / 2.
+constexpr int kDirWarps = 2;
+constexpr int kMaxCand = 256;  // candidate-set capacity per point
+
 struct CertParams {
   const float* dirs;  // [kDirs * 3] unit vectors
   double delta;       // covering angle of the directions (radians)
   double lo[3], hi[3];  // cloud AABB
-  uint32_t need;        // s_max - 2: strictly interior points that make a sphere irrelevant
+  uint32_t need;        // s_max - 2
 };
 
-constexpr int kRcapWarps = 2;  // 32 KB of neighbour offsets per block
-
-__global__ void __launch_bounds__(32 * kRcapWarps)
-k_rcap(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, const uint32_t* __restrict__ nb,
-       const uint32_t* __restrict__ nbc, const double* __restrict__ px, const double* __restrict__ py,
-       const double* __restrict__ pz, const double* __restrict__ gather_r2, uint8_t* __restrict__ todo,
-       double* __restrict__ rcap) {
-  __shared__ double rel[kRcapWarps][kMaxNb][4];  // x, y, z, |p - a|
+__global__ void __launch_bounds__(32 * kDirWarps)
+k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uint32_t* __restrict__ nb,
+           const uint32_t* __restrict__ nbc, const double* __restrict__ px, const double* __restrict__ py,
+           const double* __restrict__ pz, const double* __restrict__ gather_r2, uint8_t* __restrict__ todo,
+           uint32_t* __restrict__ cand, uint32_t* __restrict__ candc, double* __restrict__ need_r) {
+  __shared__ float4 rel[kDirWarps][kMaxNb];  // x, y, z, |p - a| (binary32 copies; margins below)
+  __shared__ uint32_t ids[kDirWarps][kMaxNb];
+  __shared__ uint32_t mark[kDirWarps][kMaxNb / 32];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t pos = blockIdx.x * kRcapWarps + warp;
+  const uint32_t pos = blockIdx.x * kDirWarps + warp;
   if (pos >= n) return;
   const uint32_t a = leaf_pid[pos];
   if (!todo[a]) return;
   const uint32_t m = nbc[a];
-  if (m > (uint32_t)kMaxNb) {  // list overflow: stays to do, the host reports capacity
-    if (lane == 0) rcap[a] = INFINITY;
+  if (m > (uint32_t)kMaxNb) {
+    if (lane == 0) need_r[a] = INFINITY;
     return;
   }
   const double ax = px[a], ay = py[a], az = pz[a];
   for (uint32_t i = lane; i < m; i += 32) {
     const uint32_t p = nb[(uint64_t)a * kMaxNb + i];
     const double x = px[p] - ax, y = py[p] - ay, z = pz[p] - az;
-    rel[warp][i][0] = x;
-    rel[warp][i][1] = y;
-    rel[warp][i][2] = z;
-    rel[warp][i][3] = sqrt(x * x + y * y + z * z);
+    rel[warp][i] = make_float4((float)x, (float)y, (float)z, (float)sqrt(x * x + y * y + z * z));
+    ids[warp][i] = p;
+  }
+  for (uint32_t i = lane; i < (uint32_t)kMaxNb / 32; i += 32) mark[warp][i] = 0;
+  __syncwarp();
+  // sort by distance (odd-even merge sort over a power-of-two padding, in shared memory)
+  uint32_t P = 1;
+  while (P < m) P <<= 1;
+  for (uint32_t i = m + lane; i < P; i += 32) {
+    rel[warp][i] = make_float4(0.f, 0.f, 0.f, INFINITY);
+    ids[warp][i] = kInvalid32;
   }
   __syncwarp();
+  for (uint32_t k = 2; k <= P; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = lane; i < P; i += 32) {
+        const uint32_t l = i ^ j;
+        if (l > i) {
+          const bool up = (i & k) == 0;
+          const float4 x = rel[warp][i], y = rel[warp][l];
+          if ((x.w > y.w) == up) {
+            rel[warp][i] = y;
+            rel[warp][l] = x;
+            const uint32_t t = ids[warp][i];
+            ids[warp][i] = ids[warp][l];
+            ids[warp][l] = t;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+  // distances are binary32: thresholds carry a relative margin of 1e-5 in the safe direction
+  const double L2 = sqrt(gather_r2[a]) * (1.0 - 1e-9);  // list covers |p - a| <= L
+  const double half_L = 0.5 * L2;
   const double cd = cos(cp.delta), sdl = sin(cp.delta);
   const double A[3] = {ax, ay, az};
-  double worst = 0.0;
+  double worst_needed = 0.0;  // largest certified rho_s (the list must cover 2 rho_s)
+  bool ok = true;
   for (int d = lane; d < kDirs; d += 32) {
     const double s0 = cp.dirs[3 * d], s1 = cp.dirs[3 * d + 1], s2 = cp.dirs[3 * d + 2];
-    // the `need` smallest thresholds
+    // AABB support bound over the cone
+    double ext = 0.0;
+    const double sv[3] = {s0, s1, s2};
+    for (int k = 0; k < 3; ++k) {
+      const double up = cp.hi[k] - A[k], dn = cp.lo[k] - A[k];
+      const double t1 = sv[k] - cp.delta, t2 = sv[k] + cp.delta;
+      const double f1 = t1 >= 0 ? up * t1 : dn * t1, f2 = t2 >= 0 ? up * t2 : dn * t2;
+      ext += fmax(f1, f2);
+    }
+    ext *= (1.0 + 1e-12);
+    // the centre of a well-centred sphere lies in conv(S), inside the AABB: r is at most
+    // the distance at which the ray a + r u leaves the AABB, maximised over the cone
+    // axis by axis (min over axes of the per-axis maxima bounds the max of the min)
+    for (int k = 0; k < 3; ++k) {
+      const double t1 = sv[k] - cp.delta, t2 = sv[k] + cp.delta;
+      if (t1 <= 0.0 && t2 >= 0.0) continue;  // the cone crosses this axis' zero: no bound
+      const double g = t1 > 0.0 ? (cp.hi[k] - A[k]) / t1 : (A[k] - cp.lo[k]) / (-t2);
+      ext = fmin(ext, g * (1.0 + 1e-12));
+    }
+    // the `need` smallest shrunk thresholds (early exit: rho_shr >= |p - a| / 2)
     double best[16];
     uint32_t cnt = 0;
     for (uint32_t i = 0; i < m; ++i) {
-      const double dist = rel[warp][i][3];
-      const double c = (s0 * rel[warp][i][0] + s1 * rel[warp][i][1] + s2 * rel[warp][i][2]) / dist;
-      const double s = sqrt(fmax(0.0, 1.0 - c * c));
-      const double cshr = c * cd - s * sdl;  // cos(angle + delta)
-      if (cshr <= 1e-12) continue;
-      const double rho = dist / (2.0 * cshr) * (1.0 + 1e-12);
+      const float4 r = rel[warp][i];
+      const double dist = (double)r.w;
+      const double kth = cnt >= cp.need ? best[cp.need - 1] : INFINITY;
+      if (0.5 * dist * (1.0 - 1e-5) > fmin(kth, ext)) break;
+      const double c = (s0 * r.x + s1 * r.y + s2 * r.z) / dist;
+      // upper bound of the angle (cosine lowered by the binary32 margin) -> cos(angle + delta) lowered
+      const double cs = fmax(-1.0, c - 1e-5), sn = sqrt(fmax(0.0, 1.0 - cs * cs));
+      const double cshr = cs * cd - sn * sdl;
+      if (cshr <= 1e-9) continue;
+      const double rho = dist / (2.0 * cshr) * (1.0 + 1e-5);
       if (cnt < cp.need) {
         uint32_t j = cnt++;
         while (j > 0 && best[j - 1] > rho) { best[j] = best[j - 1]; --j; }
@@ -396,25 +467,52 @@ k_rcap(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, const u
         best[j] = rho;
       }
     }
-    const double rho_s = (cnt >= cp.need) ? best[cp.need - 1] : INFINITY;
-    // support-function bound of the AABB over the cone
-    double ext = 0.0;
-    const double sv[3] = {s0, s1, s2};
-    for (int k = 0; k < 3; ++k) {
-      const double up = cp.hi[k] - A[k], dn = cp.lo[k] - A[k];
-      const double t1 = sv[k] - cp.delta, t2 = sv[k] + cp.delta;
-      const double f1 = t1 >= 0 ? up * t1 : dn * t1, f2 = t2 >= 0 ? up * t2 : dn * t2;
-      ext += fmax(f1, f2);
+    const double kth = cnt >= cp.need ? best[cp.need - 1] : INFINITY;
+    const double rho_s = fmin(kth, ext);
+    // certified when every unlisted point (rho >= L/2) cannot lower it
+    if (!(rho_s <= half_L)) ok = false;
+    worst_needed = fmax(worst_needed, rho_s);
+    // mark the candidates of this cone: rho_lo_p(s) <= rho_s (rho_lo >= |p - a| / 2)
+    for (uint32_t i = 0; i < m; ++i) {
+      const float4 r = rel[warp][i];
+      const double dist = (double)r.w;
+      if (0.5 * dist * (1.0 - 1e-5) > rho_s) break;
+      const double c = (s0 * r.x + s1 * r.y + s2 * r.z) / dist;
+      // lower bound of the angle (cosine raised by the margin) -> cos(max(angle - delta, 0)) raised
+      const double cs = fmin(1.0, c + 1e-5);
+      const double sn = sqrt(fmax(0.0, 1.0 - cs * cs));
+      const double clo = (cs >= cd) ? 1.0 : cs * cd + sn * sdl;
+      if (clo <= 0.0) continue;
+      const double rho_lo = dist / (2.0 * clo) * (1.0 - 1e-5);
+      if (rho_lo <= rho_s * (1.0 + 1e-9)) atomicOr(&mark[warp][i >> 5], 1u << (i & 31));
     }
-    worst = fmax(worst, fmin(rho_s, ext * (1.0 + 1e-12)));
   }
-  for (int off = 16; off > 0; off >>= 1) worst = fmax(worst, __shfl_xor_sync(0xffffffffu, worst, off));
+  ok = __all_sync(0xffffffffu, ok);
+  for (int off = 16; off > 0; off >>= 1) worst_needed = fmax(worst_needed, __shfl_xor_sync(0xffffffffu, worst_needed, off));
+  __syncwarp();
+  if (!ok) {  // the list must grow to 2 rho_s (with room)
+    if (lane == 0) need_r[a] = worst_needed;
+    return;
+  }
+  // compact the candidate set in distance order
+  uint32_t c = 0;
+  uint32_t* out = cand + (uint64_t)a * kMaxCand;
+  bool overflow = false;
+  for (uint32_t base = 0; base < m; base += 32) {
+    const uint32_t i = base + lane;
+    const bool f = i < m && ((mark[warp][i >> 5] >> (i & 31)) & 1u);
+    const uint32_t b = __ballot_sync(0xffffffffu, f);
+    if (f) {
+      const uint32_t at = c + __popc(b & lanemask_lt());
+      if (at < (uint32_t)kMaxCand) out[at] = ids[warp][i];
+    }
+    c += __popc(b);
+  }
+  overflow = c > (uint32_t)kMaxCand;
   if (lane == 0) {
-    const double r = worst * (1.0 + 1e-9);
-    rcap[a] = r;
-    // the list must cover B(a, 2 r) with room to spare
-    const double cover2 = gather_r2[a] * (1.0 - 64.0 * kU);
-    if (4.0 * r * r * (1.0 + 4e-3) <= cover2) todo[a] = 0;
+    candc[a] = overflow ? (uint32_t)kMaxCand + 1 : c;
+    need_r[a] = worst_needed;
+    todo[a] = overflow ? 2 : 0;  // 2: candidate set too large (reported)
   }
 }
 
@@ -432,14 +530,15 @@ struct Ctl {
   uint32_t cap;  // record capacity
 };
 
-// Classifies every listed neighbour of the owner against s; returns false when rejected.
-__device__ bool classify_list(const Cloud& c, const Sphere& s, const uint32_t* list, uint32_t m, uint32_t icap,
-                              HigherRec& r) {
+// Classifies every point of the candidate set (support excluded) against s;
+// false when the interior exceeds icap.
+__device__ bool classify_set(const Cloud& c, const Sphere& s, const uint32_t* set, uint32_t m, uint32_t icap,
+                             HigherRec& r) {
   r.interior = 0;
   r.shell = (uint32_t)s.size;
   r.witness = kInvalid32;
   for (uint32_t i = 0; i < m; ++i) {
-    const uint32_t w = list[i];
+    const uint32_t w = set[i];
     if (w == s.ids[1] || w == s.ids[2] || (s.size == 4 && w == s.ids[3])) continue;
     const int sd = sphere_side(c, s, w);
     if (sd < 0) {
@@ -456,14 +555,13 @@ __device__ bool classify_list(const Cloud& c, const Sphere& s, const uint32_t* l
 __device__ void emit(HigherRec& r, const Sphere& s, HigherRec* out, uint32_t out_cap, uint32_t* counter) {
   r.size = (uint32_t)s.size;
   for (int i = 0; i < 4; ++i) r.ids[i] = i < s.size ? s.ids[i] : 0u;
-  // canonical: support ids ascending, interior ids ascending
-  for (int i = 1; i < s.size; ++i) {
+  for (int i = 1; i < s.size; ++i) {  // support ids ascending
     const uint32_t x = r.ids[i];
     int j = i;
     while (j > 0 && r.ids[j - 1] > x) { r.ids[j] = r.ids[j - 1]; --j; }
     r.ids[j] = x;
   }
-  for (uint32_t i = 1; i < r.interior; ++i) {
+  for (uint32_t i = 1; i < r.interior; ++i) {  // interior ids ascending
     const uint32_t x = r.iids[i];
     uint32_t j = i;
     while (j > 0 && r.iids[j - 1] > x) { r.iids[j] = r.iids[j - 1]; --j; }
@@ -474,107 +572,79 @@ __device__ void emit(HigherRec& r, const Sphere& s, HigherRec* out, uint32_t out
   if (slot < out_cap) out[slot] = r;
 }
 
+__device__ __forceinline__ void decode_pair(uint64_t t, uint32_t& lo, uint32_t& hi) {
+  uint32_t i = (uint32_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) / 2.0);
+  while ((uint64_t)(i + 1) * i / 2 > t) --i;
+  while ((uint64_t)(i + 2) * (i + 1) / 2 <= t) ++i;
+  lo = (uint32_t)(t - (uint64_t)(i + 1) * i / 2);
+  hi = i + 1;
+}
+
 __global__ void __launch_bounds__(kThreads)
-k_higher(uint32_t n, Ctl ctl, const uint32_t* __restrict__ leaf_pid, const uint32_t* __restrict__ nb,
-         const uint32_t* __restrict__ nbc, const double* __restrict__ rcap, const double* __restrict__ px,
-         const double* __restrict__ py, const double* __restrict__ pz, const int* __restrict__ cloud_scale,
-         HigherRec* __restrict__ out, uint32_t* __restrict__ counter, unsigned long long* __restrict__ stats,
-         uint32_t* __restrict__ err) {
-  __shared__ uint32_t list[kWarps][kMaxNb];   // neighbours within 2 r_cap (classification set)
-  __shared__ uint32_t cand[kWarps][kMaxNb];   // of which id > owner (support candidates)
+k_higher(uint32_t n, Ctl ctl, const uint32_t* __restrict__ leaf_pid, const uint32_t* __restrict__ cand,
+         const uint32_t* __restrict__ candc, const double* __restrict__ px, const double* __restrict__ py,
+         const double* __restrict__ pz, const int* __restrict__ cloud_scale, HigherRec* __restrict__ out,
+         uint32_t* __restrict__ counter, unsigned long long* __restrict__ stats, uint32_t* __restrict__ err) {
+  __shared__ uint32_t set[kWarps][kMaxCand];  // C(a): classification set
+  __shared__ uint32_t sup[kWarps][kMaxCand];  // C(a) with ids > a: support candidates
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t pos = blockIdx.x * kWarps + warp;
   if (pos >= n) return;
   const uint32_t a = leaf_pid[pos];
   const Cloud c{px, py, pz, cloud_scale[0]};
-  const uint32_t m0 = nbc[a];
-  if (m0 > (uint32_t)kMaxNb) return;  // reported by the host through the certificate pass
-  const double rc = rcap[a];
-  const double lim2 = 4.0 * rc * rc * (1.0 + 1e-6);
-  const P3 pa = c.p(a);
-  // compact the neighbours within 2 r_cap, and the candidates among them
-  uint32_t m = 0, mc = 0;
-  for (uint32_t base = 0; base < m0; base += 32) {
+  const uint32_t m = candc[a];
+  if (m > (uint32_t)kMaxCand) return;  // reported by the host
+  uint32_t mc = 0;
+  for (uint32_t base = 0; base < m; base += 32) {
     const uint32_t i = base + lane;
-    uint32_t p = kInvalid32;
-    bool in = false;
-    if (i < m0) {
-      p = nb[(uint64_t)a * kMaxNb + i];
-      const double dx = px[p] - pa.x, dy = py[p] - pa.y, dz = pz[p] - pa.z;
-      in = dx * dx + dy * dy + dz * dz <= lim2;
-    }
-    const uint32_t b1 = __ballot_sync(0xffffffffu, in), b2 = __ballot_sync(0xffffffffu, in && p > a);
-    if (in) list[warp][m + __popc(b1 & lanemask_lt())] = p;
-    if (in && p > a) cand[warp][mc + __popc(b2 & lanemask_lt())] = p;
-    m += __popc(b1);
-    mc += __popc(b2);
+    const uint32_t p = i < m ? cand[(uint64_t)a * kMaxCand + i] : kInvalid32;
+    if (i < m) set[warp][i] = p;
+    const bool f = i < m && p > a;
+    const uint32_t b = __ballot_sync(0xffffffffu, f);
+    if (f) sup[warp][mc + __popc(b & lanemask_lt())] = p;
+    mc += __popc(b);
   }
   __syncwarp();
-  const double rcap2 = rc * rc;
   unsigned long long tested = 0, classified = 0, emitted = 0;
-  // --- triples (a, b, c): lanes over candidate pairs
-  const uint32_t icap3 = ctl.smax >= 3 ? ctl.smax - 3 : 0;
   const uint64_t P2 = (uint64_t)mc * (mc - 1) / 2;
+  // --- triples (a, b, c): lanes over candidate pairs
   if (ctl.smax >= 3) {
+    const uint32_t icap = ctl.smax - 3;
     for (uint64_t t = lane; t < P2; t += 32) {
-      // decode t -> (i < j)
-      uint32_t i = (uint32_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) / 2.0);
-      while ((uint64_t)(i + 1) * i / 2 > t) --i;
-      while ((uint64_t)(i + 2) * (i + 1) / 2 <= t) ++i;
-      const uint32_t j = (uint32_t)(t - (uint64_t)(i + 1) * i / 2);  // j < i + 1
+      uint32_t j, k;
+      decode_pair(t, j, k);
       Sphere s;
       s.size = 3;
       s.ids[0] = a;
-      s.ids[1] = cand[warp][j];
-      s.ids[2] = cand[warp][i + 1];
+      s.ids[1] = sup[warp][j];
+      s.ids[2] = sup[warp][k];
       ++tested;
-      s.status = tri_status(c, s.ids, s);
-      if (s.status != 0) continue;
-      radius_bounds(s);
-      if (s.r2_lo > rcap2) continue;  // certainly beyond the certified radius: irrelevant
-      if (s.r2_hi > lim2 * 0.25) { atomicOr(err, kErrInternal); continue; }
+      if (tri_status(c, s.ids, s) != 0) continue;
       ++classified;
       HigherRec r;
-      if (!classify_list(c, s, list[warp], m, icap3, r)) continue;
+      if (!classify_set(c, s, set[warp], m, icap, r)) continue;
       ++emitted;
       emit(r, s, out, ctl.cap, counter);
     }
   }
-  // --- quads (a, b, c, d): lanes over candidate pairs (b, c), inner loop over d
-  const uint32_t icap4 = ctl.smax >= 4 ? ctl.smax - 4 : 0;
+  // --- quads (a, b, c, d): lanes over pairs (b, c), inner loop over d
   if (ctl.smax >= 4) {
+    const uint32_t icap = ctl.smax - 4;
     for (uint64_t t = lane; t < P2; t += 32) {
-      uint32_t i = (uint32_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) / 2.0);
-      while ((uint64_t)(i + 1) * i / 2 > t) --i;
-      while ((uint64_t)(i + 2) * (i + 1) / 2 <= t) ++i;
-      const uint32_t j = (uint32_t)(t - (uint64_t)(i + 1) * i / 2);
-      const uint32_t b = cand[warp][j], cc = cand[warp][i + 1];
-      // the triangle (a, b, c) lies on the quad's sphere: its circumradius <= r
-      {
-        Sphere tri;
-        tri.size = 3;
-        tri.ids[0] = a; tri.ids[1] = b; tri.ids[2] = cc;
-        const P3 pb = c.p(b), pc = c.p(cc);
-        const FV e1 = fdiff(pb, pa), e2 = fdiff(pc, pa);
-        const Fm G11 = dot(e1, e1), G12 = dot(e1, e2), G22 = dot(e2, e2);
-        tri.A = G11 * G22 - G12 * G12;
-        tri.N = add(scale(G22 * (G11 - G12), e1), scale(G11 * (G22 - G12), e2));
-        radius_bounds(tri);
-        if (tri.r2_lo > rcap2) continue;
-      }
-      for (uint32_t k = i + 2; k < mc; ++k) {
+      uint32_t j, k;
+      decode_pair(t, j, k);
+      for (uint32_t l = k + 1; l < mc; ++l) {
         Sphere s;
         s.size = 4;
-        s.ids[0] = a; s.ids[1] = b; s.ids[2] = cc; s.ids[3] = cand[warp][k];
+        s.ids[0] = a;
+        s.ids[1] = sup[warp][j];
+        s.ids[2] = sup[warp][k];
+        s.ids[3] = sup[warp][l];
         ++tested;
-        s.status = quad_status(c, s.ids, s);
-        if (s.status != 0) continue;
-        radius_bounds(s);
-        if (s.r2_lo > rcap2) continue;
-        if (s.r2_hi > lim2 * 0.25) { atomicOr(err, kErrInternal); continue; }
+        if (quad_status(c, s.ids, s) != 0) continue;
         ++classified;
         HigherRec r;
-        if (!classify_list(c, s, list[warp], m, icap4, r)) continue;
+        if (!classify_set(c, s, set[warp], m, icap, r)) continue;
         ++emitted;
         emit(r, s, out, ctl.cap, counter);
       }
@@ -590,6 +660,7 @@ k_higher(uint32_t n, Ctl ctl, const uint32_t* __restrict__ leaf_pid, const uint3
     atomicAdd(stats + 1, classified);
     atomicAdd(stats + 2, emitted);
     atomicAdd(stats + 3, (unsigned long long)m);
+    atomicAdd(stats + 4, (unsigned long long)mc);
   }
 }
 
@@ -609,6 +680,23 @@ __global__ void k_higher_gather(uint32_t m, const uint32_t* __restrict__ v0, con
                                 HigherRec* __restrict__ sorted) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < m) sorted[i] = recs[radix_result(state, passes, v0, v1)[i]];
+}
+
+__global__ void k_gather_init(uint32_t n, const double* __restrict__ R2w, double* __restrict__ gr2,
+                              uint8_t* __restrict__ todo, double factor2) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  gr2[i] = R2w[i] * factor2;
+  todo[i] = 1;
+}
+
+// Points whose direction table is not yet certified: cover 2 rho_max with room.
+__global__ void k_gather_grow(uint32_t n, double* __restrict__ gr2, const uint8_t* __restrict__ todo,
+                              const double* __restrict__ need_r) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || todo[i] != 1) return;
+  const double want = 4.0 * need_r[i] * need_r[i] * 1.1;
+  gr2[i] = fmax(gr2[i] * 1.44, isfinite(want) ? want : gr2[i] * 4.0);
 }
 
 // Icosphere directions and their covering angle (max angular circumradius of a face).
@@ -644,9 +732,9 @@ void icosphere(std::vector<float>& dirs, double& delta) {
     }
     f = nf;
   }
+  // covering angle: every direction is within the circumradius of its face
   delta = 0.0;
   for (auto& tri : f) {
-    // spherical circumcentre direction: normal of the plane through the three vertices
     const auto& A = v[tri[0]];
     const auto& B = v[tri[1]];
     const auto& C = v[tri[2]];
@@ -659,7 +747,7 @@ void icosphere(std::vector<float>& dirs, double& delta) {
       delta = std::max(delta, std::acos(std::min(1.0, cosang)));
     }
   }
-  delta *= 1.05;  // margin for the float rounding of the stored directions
+  delta *= 1.05;  // margin for the binary32 rounding of the stored directions
   dirs.clear();
   for (auto& p : v)
     for (int k = 0; k < 3; ++k) dirs.push_back((float)p[k]);
@@ -671,11 +759,13 @@ cudaError_t higher_alloc(Ctx& ctx) {
   const uint64_t n = ctx.max_points;
   HigherBuffers& h = ctx.hb;
   cudaError_t e = cudaSuccess;
-  h.capacity = (uint32_t)(192 * n + 4096);
+  h.capacity = (uint32_t)(512 * n + 4096);  // ~225 supports per point in lattices, more with ties
 #define EHGP_ALLOC(ptr, bytes) \
   if ((e = ctx_alloc(ctx, (void**)&(ptr), (bytes))) != cudaSuccess) return e
   EHGP_ALLOC(h.nb, n * kMaxNb * sizeof(uint32_t));
   EHGP_ALLOC(h.nbc, n * sizeof(uint32_t));
+  EHGP_ALLOC(h.cand, n * kMaxCand * sizeof(uint32_t));
+  EHGP_ALLOC(h.candc, n * sizeof(uint32_t));
   EHGP_ALLOC(h.gather_r2, n * sizeof(double));
   EHGP_ALLOC(h.rcap, n * sizeof(double));
   EHGP_ALLOC(h.todo, n * sizeof(uint8_t));
@@ -698,27 +788,6 @@ cudaError_t higher_alloc(Ctx& ctx) {
   return cudaMemcpy(h.dirs, dirs.data(), dirs.size() * sizeof(float), cudaMemcpyHostToDevice);
 }
 
-namespace {
-
-__global__ void k_gather_init(uint32_t n, const double* __restrict__ R2w, double* __restrict__ gr2,
-                              uint8_t* __restrict__ todo, double factor2) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  gr2[i] = R2w[i] * factor2;
-  todo[i] = 1;
-}
-
-__global__ void k_gather_grow(uint32_t n, double* __restrict__ gr2, const uint8_t* __restrict__ todo,
-                              const double* __restrict__ rcap) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || !todo[i]) return;
-  // cover the certified radius found so far, with room, or grow by 2x
-  const double want = 4.0 * rcap[i] * rcap[i] * 1.02;
-  gr2[i] = isfinite(want) && want > gr2[i] ? want : gr2[i] * 4.0;
-}
-
-}  // namespace
-
 int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   const uint32_t n = (uint32_t)ctx.built_n;
   HigherBuffers& h = ctx.hb;
@@ -740,52 +809,67 @@ int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   const uint32_t root = 2 * n - 2;
   uint64_t launches = 0;
   cudaEventRecord(ctx.ev0, st);
-  // neighbour lists + certified radii; up to four rounds for points whose list is too short
-  k_gather_init<<<nblocks(n, 256), 256, 0, st>>>(n, p.R2, h.gather_r2, h.todo, 2.6 * 2.6);
+  k_gather_init<<<nblocks(n, 256), 256, 0, st>>>(n, p.R2, h.gather_r2, h.todo, 1.6 * 1.6);
   launches += 1;
-  double lo[3], hi[3];
+  CertParams cp;
   {
     uint64_t fr[12];
     cudaMemcpyAsync(fr, b.frame, sizeof(fr), cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
     for (int k = 0; k < 3; ++k) {
-      std::memcpy(&lo[k], &fr[k], 8);
-      std::memcpy(&hi[k], &fr[3 + k], 8);
+      std::memcpy(&cp.lo[k], &fr[k], 8);
+      std::memcpy(&cp.hi[k], &fr[3 + k], 8);
     }
   }
-  CertParams cp;
   cp.dirs = h.dirs;
   cp.delta = h.delta;
-  for (int k = 0; k < 3; ++k) { cp.lo[k] = lo[k]; cp.hi[k] = hi[k]; }
   cp.need = smax - 2;
   if (cp.need > 16) return abi_fail(&ctx, EHGP_ERR_INVALID_ARGUMENT, "K above 10 is not supported");
-  uint32_t remaining = n;
-  for (int round = 0; round < 4 && remaining > 0; ++round) {
+  uint32_t pending = n, overflowed = 0;
+  std::vector<uint8_t> todo(n);
+  for (int round = 0; round < 6 && pending > 0; ++round) {
     k_gather<<<nblocks(n, kWarps), kThreads, 0, st>>>(n, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end, b.px, b.py,
                                                       b.pz, h.gather_r2, h.todo, h.nb, h.nbc);
-    k_rcap<<<nblocks(n, kRcapWarps), 32 * kRcapWarps, 0, st>>>(n, cp, b.leaf_pid, h.nb, h.nbc, b.px, b.py, b.pz, h.gather_r2,
-                                                    h.todo, h.rcap);
+    k_dirtable<<<nblocks(n, kDirWarps), 32 * kDirWarps, 0, st>>>(n, cp, b.leaf_pid, h.nb, h.nbc, b.px, b.py, b.pz,
+                                                                  h.gather_r2, h.todo, h.cand, h.candc, h.rcap);
     launches += 2;
-    // count the points still to do
-    std::vector<uint8_t> todo(n);
     cudaMemcpyAsync(todo.data(), h.todo, n, cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return abi_cuda_fail(&ctx, e, "higher-support certificate");
-    remaining = 0;
-    for (uint32_t i = 0; i < n; ++i) remaining += todo[i];
-    if (remaining) {
+    pending = overflowed = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      pending += todo[i] == 1;
+      overflowed += todo[i] == 2;
+    }
+    if (overflowed) break;
+    if (pending) {
       k_gather_grow<<<nblocks(n, 256), 256, 0, st>>>(n, h.gather_r2, h.todo, h.rcap);
       ++launches;
     }
   }
-  if (remaining)
-    return abi_fail(&ctx, EHGP_ERR_CAPACITY, "a certified neighbourhood exceeds 512 points (sparse or clustered cloud)");
+  if (pending || overflowed) {
+    std::vector<uint32_t> cnt(n), cc(n);
+    std::vector<double> need(n), gr(n);
+    cudaMemcpy(cnt.data(), h.nbc, 4ull * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(cc.data(), h.candc, 4ull * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(need.data(), h.rcap, 8ull * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(gr.data(), h.gather_r2, 8ull * n, cudaMemcpyDeviceToHost);
+    uint32_t i = 0;
+    while (i < n && todo[i] == 0) ++i;
+    char msg[320];
+    snprintf(msg, sizeof msg,
+             "a certified neighbourhood exceeds its capacity (%u points pending, %u over %d candidates): e.g. "
+             "PointId %u with %u neighbours, %u candidates, radius bound %.6g, gather radius %.6g",
+             pending, overflowed, kMaxCand, i, i < n ? cnt[i] : 0u, i < n ? cc[i] : 0u, i < n ? need[i] : 0.0,
+             i < n ? std::sqrt(gr[i]) : 0.0);
+    return abi_fail(&ctx, EHGP_ERR_CAPACITY, msg);
+  }
   cudaMemsetAsync(h.counters, 0, 8 * sizeof(uint32_t), st);
   cudaMemsetAsync(h.stats, 0, 8 * sizeof(unsigned long long), st);
   Ctl ctl{smax, h.capacity};
   cudaEventRecord(ctx.evk0, st);
-  k_higher<<<nblocks(n, kWarps), kThreads, 0, st>>>(n, ctl, b.leaf_pid, h.nb, h.nbc, h.rcap, b.px, b.py, b.pz,
-                                                    g.scale, (HigherRec*)h.raw, h.counters, h.stats, ctx.d_err);
+  k_higher<<<nblocks(n, kWarps), kThreads, 0, st>>>(n, ctl, b.leaf_pid, h.cand, h.candc, b.px, b.py, b.pz, g.scale,
+                                                    (HigherRec*)h.raw, h.counters, h.stats, ctx.d_err);
   cudaEventRecord(ctx.evk1, st);
   ++launches;
   uint32_t hc[2];

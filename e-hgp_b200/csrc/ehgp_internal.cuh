@@ -187,8 +187,10 @@ struct PairBuffers {
 struct HigherBuffers {
   uint32_t* nb = nullptr;           // [n * 512] neighbour lists
   uint32_t* nbc = nullptr;          // [n]
+  uint32_t* cand = nullptr;         // [n * 256] candidate sets
+  uint32_t* candc = nullptr;        // [n]
   double* gather_r2 = nullptr;      // [n] squared gather radius
-  double* rcap = nullptr;           // [n] certified radius bound
+  double* rcap = nullptr;           // [n] largest direction bound (radius the list must cover / 2)
   uint8_t* todo = nullptr;          // [n]
   float* dirs = nullptr;            // [642 * 3]
   double delta = 0;                 // covering angle of dirs
