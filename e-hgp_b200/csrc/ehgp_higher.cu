@@ -32,6 +32,7 @@
 #include "ehgp_internal.cuh"
 #include "ehgp_exact.cuh"
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstring>
@@ -69,33 +70,29 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return m;
 }
 
-// ---- FP64 values with a magnitude bound (error <= 64 u m) -------------------------
-struct Fm {
-  double v, m;
-};
-__device__ __forceinline__ Fm operator+(Fm a, Fm b) { return {a.v + b.v, a.m + b.m}; }
-__device__ __forceinline__ Fm operator-(Fm a, Fm b) { return {a.v - b.v, a.m + b.m}; }
-__device__ __forceinline__ Fm operator*(Fm a, Fm b) { return {a.v * b.v, a.m * b.m}; }
-__device__ __forceinline__ int fm_sign(Fm x) {
-  const double bound = 64.0 * kU * x.m + 1e-300;
-  return x.v > bound ? 1 : (x.v < -bound ? -1 : 2);
-}
-struct FV {
-  Fm x, y, z;
-};
-__device__ __forceinline__ Fm dot(const FV& a, const FV& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-__device__ __forceinline__ FV cross(const FV& a, const FV& b) {
-  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
-}
-__device__ __forceinline__ FV scale(Fm s, const FV& a) { return {s * a.x, s * a.y, s * a.z}; }
-__device__ __forceinline__ FV add(const FV& a, const FV& b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+// ---- FP64 filters with per-tuple uniform error bounds ------------------------------
+// Every coordinate difference p - a is one correctly rounded subtraction, so
+// |fl(p - a) - (p - a)| <= u |p - a|.  For a polynomial evaluated in binary64 with
+// at most ~15 roundings on any path, |computed - exact| <= 64 u m where m is the
+// value of the same polynomial with every input replaced by an upper bound of its
+// magnitude and every subtraction by an addition.  With all difference
+// coordinates bounded by M (M >= max |coordinate| (1 + 2u)) that gives, per
+// coordinate or scalar:
+//   dot(e, e')          3 M^2        cross(e, e')       2 M^2
+//   triangle  G12 3 M^2, G11 - G12 6 M^2, detG 18 M^4, N 36 M^5
+//   tetra     detE 6 M^3, N 18 M^4, l_i = N.(e_j x e_k) 108 M^6, l_0 396 M^6
+//   side      A q - p.N with |p| <= Mp:  A_m 3 Mp^2 + 3 Mp N_m
+// 1e-300 absolute covers underflow.  An undecided sign goes to the exact path.
+constexpr double kFilt = 64.0 * kU;
+constexpr double kTiny = 1e-300;
 
-struct P3 {
-  double x, y, z;
+__device__ __forceinline__ int fsign(double v, double bound) { return v > bound ? 1 : (v < -bound ? -1 : 2); }
+
+struct SetPt {
+  double x, y, z, q;  // fl(p - a) and fl(|fl(p - a)|^2) = (x x + y y) + z z
 };
-__device__ __forceinline__ FV fdiff(const P3& p, const P3& q) {
-  return {{p.x - q.x, fabs(p.x) + fabs(q.x)}, {p.y - q.y, fabs(p.y) + fabs(q.y)}, {p.z - q.z, fabs(p.z) + fabs(q.z)}};
-}
+
+__device__ __forceinline__ double ptmax(const SetPt& p) { return fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z))); }
 
 // ---- exact versions (832-bit integers at the cloud scale) --------------------------
 using W = WInt<13>;
@@ -117,7 +114,6 @@ struct Cloud {
   const double* py;
   const double* pz;
   int S;
-  __device__ P3 p(uint32_t i) const { return P3{px[i], py[i], pz[i]}; }
   __device__ WV wdiff(uint32_t i, uint32_t j) const {
     return {W::from_i128(fixed_of(dbits(px[i]), S) - fixed_of(dbits(px[j]), S)),
             W::from_i128(fixed_of(dbits(py[i]), S) - fixed_of(dbits(py[j]), S)),
@@ -125,114 +121,133 @@ struct Cloud {
   }
 };
 
-// A support's side polynomial: side(w) = sgn * sign(A |p|^2 - p.N), p = w - a.
-struct Sphere {
-  uint32_t ids[4];
-  int size;
-  int status;  // 0 minimal, 1 boundary reduced, 2 exterior centre, 3 dependent, 4 undecided in FP
-  Fm A;
-  FV N;
-  int sgn;
-  double r2_lo, r2_hi;  // FP bounds of the squared radius (valid when status == 0)
-};
-
-__device__ void radius_bounds(Sphere& s) {
-  // r^2 = |N|^2 / (4 A^2) with |error| of every quantity <= 64 u m
-  const double g = 64.0 * kU;
-  const double a_lo = fabs(s.A.v) - g * s.A.m, a_hi = fabs(s.A.v) + g * s.A.m;
-  double n_lo = 0, n_hi = 0;
-  const Fm c[3] = {s.N.x, s.N.y, s.N.z};
-  for (int i = 0; i < 3; ++i) {
-    const double lo = fmax(fabs(c[i].v) - g * c[i].m, 0.0), hi = fabs(c[i].v) + g * c[i].m;
-    n_lo += lo * lo;
-    n_hi += hi * hi;
-  }
-  if (a_lo <= 0) {
-    s.r2_lo = 0;
-    s.r2_hi = INFINITY;
-  } else {
-    s.r2_lo = n_lo / (4 * a_hi * a_hi) * (1 - 1e-12);
-    s.r2_hi = n_hi / (4 * a_lo * a_lo) * (1 + 1e-12);
-  }
+// Exact fallbacks, kept out of line so that the FP64 fast paths stay in registers.
+__device__ __noinline__ void tri_signs_exact(const Cloud& c, const uint32_t* id, int* sg) {
+  const WV w1 = c.wdiff(id[1], id[0]), w2 = c.wdiff(id[2], id[0]);
+  const W g11 = wdot(w1, w1), g12 = wdot(w1, w2), g22 = wdot(w2, w2);
+  sg[0] = g12.sign();
+  sg[1] = wsub(g11, g12).sign();
+  sg[2] = wsub(g22, g12).sign();
+  sg[3] = wsub(wmul(g11, g22), wmul(g12, g12)).sign();
 }
 
-// Status of a triangle: minimal iff its three angles are acute.
-__device__ int tri_status(const Cloud& c, const uint32_t* id, Sphere& s) {
-  const P3 a = c.p(id[0]), b = c.p(id[1]), d = c.p(id[2]);
-  const FV e1 = fdiff(b, a), e2 = fdiff(d, a);
-  const Fm G11 = dot(e1, e1), G12 = dot(e1, e2), G22 = dot(e2, e2);
-  const Fm db = G11 - G12, dc = G22 - G12;
-  const Fm detG = G11 * G22 - G12 * G12;
-  int sa = fm_sign(G12), sb = fm_sign(db), sc = fm_sign(dc), sd = fm_sign(detG);
-  if (sa == 2 || sb == 2 || sc == 2 || sd == 2) {
-    const WV w1 = c.wdiff(id[1], id[0]), w2 = c.wdiff(id[2], id[0]);
-    const W g11 = wdot(w1, w1), g12 = wdot(w1, w2), g22 = wdot(w2, w2);
-    sa = g12.sign();
-    sb = wsub(g11, g12).sign();
-    sc = wsub(g22, g12).sign();
-    sd = wsub(wmul(g11, g22), wmul(g12, g12)).sign();
-  }
-  if (sd == 0) return 3;
-  if (sa < 0 || sb < 0 || sc < 0) return 2;
-  if (sa == 0 || sb == 0 || sc == 0) return 1;
-  s.A = detG;
-  s.N = add(scale(G22 * db, e1), scale(G11 * dc, e2));
-  s.sgn = 1;
-  return 0;
+__device__ __noinline__ void quad_signs_exact(const Cloud& c, const uint32_t* id, int* sg) {
+  const WV w1 = c.wdiff(id[1], id[0]), w2 = c.wdiff(id[2], id[0]), w3 = c.wdiff(id[3], id[0]);
+  const WV x23 = wcross(w2, w3), x31 = wcross(w3, w1), x12 = wcross(w1, w2);
+  const WV nn = wvadd(wvadd(wscale(wdot(w1, w1), x23), wscale(wdot(w2, w2), x31)), wscale(wdot(w3, w3), x12));
+  const W de = wdot(w1, x23);
+  const W m1 = wdot(nn, x23), m2 = wdot(nn, x31), m3 = wdot(nn, x12);
+  const W two = W::from_i128(2);
+  const W m0 = wsub(wmul(two, wmul(de, de)), wadd(wadd(m1, m2), m3));
+  sg[0] = de.sign();
+  sg[1] = m0.sign();
+  sg[2] = m1.sign();
+  sg[3] = m2.sign();
+  sg[4] = m3.sign();
 }
 
-// Status of a tetrahedron: minimal iff the four barycentric coordinates of its
-// circumcentre are positive.
-__device__ int quad_status(const Cloud& c, const uint32_t* id, Sphere& s) {
-  const P3 a = c.p(id[0]);
-  const FV e1 = fdiff(c.p(id[1]), a), e2 = fdiff(c.p(id[2]), a), e3 = fdiff(c.p(id[3]), a);
-  const FV c23 = cross(e2, e3), c31 = cross(e3, e1), c12 = cross(e1, e2);
-  const Fm detE = dot(e1, c23);
-  const FV N = add(add(scale(dot(e1, e1), c23), scale(dot(e2, e2), c31)), scale(dot(e3, e3), c12));
-  const Fm l1 = dot(N, c23), l2 = dot(N, c31), l3 = dot(N, c12);
-  const Fm l0 = Fm{2.0, 0.0} * detE * detE - (l1 + l2 + l3);
-  int sd = fm_sign(detE), s0 = fm_sign(l0), s1 = fm_sign(l1), s2 = fm_sign(l2), s3 = fm_sign(l3);
-  if (sd == 2 || s0 == 2 || s1 == 2 || s2 == 2 || s3 == 2) {
-    const WV w1 = c.wdiff(id[1], id[0]), w2 = c.wdiff(id[2], id[0]), w3 = c.wdiff(id[3], id[0]);
-    const WV x23 = wcross(w2, w3), x31 = wcross(w3, w1), x12 = wcross(w1, w2);
-    const W de = wdot(w1, x23);
-    const WV nn = wvadd(wvadd(wscale(wdot(w1, w1), x23), wscale(wdot(w2, w2), x31)), wscale(wdot(w3, w3), x12));
-    const W m1 = wdot(nn, x23), m2 = wdot(nn, x31), m3 = wdot(nn, x12);
-    const W two = W::from_i128(2);
-    const W m0 = wsub(wmul(two, wmul(de, de)), wadd(wadd(m1, m2), m3));
-    sd = de.sign();
-    s0 = m0.sign(); s1 = m1.sign(); s2 = m2.sign(); s3 = m3.sign();
-  }
-  if (sd == 0) return 3;
-  if (s0 < 0 || s1 < 0 || s2 < 0 || s3 < 0) return 2;
-  if (s0 == 0 || s1 == 0 || s2 == 0 || s3 == 0) return 1;
-  s.A = detE;
-  s.N = N;
-  s.sgn = sd;
-  return 0;
-}
-
-// Exact side of w: -1 strictly inside, 0 on the sphere, +1 outside.
-__device__ int sphere_side(const Cloud& c, const Sphere& s, uint32_t w) {
-  const FV p = fdiff(c.p(w), c.p(s.ids[0]));
-  const int fs = fm_sign(s.A * dot(p, p) - dot(p, s.N));
-  if (fs != 2) return fs * s.sgn;
-  const WV q = c.wdiff(w, s.ids[0]);
+// Exact sign of the side polynomial A |w - a|^2 - (w - a).N (before the orientation sign).
+__device__ __noinline__ int side_exact(const Cloud& c, const uint32_t* ids, int size, uint32_t w) {
+  const WV q = c.wdiff(w, ids[0]);
   W val;
-  if (s.size == 3) {
-    const WV w1 = c.wdiff(s.ids[1], s.ids[0]), w2 = c.wdiff(s.ids[2], s.ids[0]);
+  if (size == 3) {
+    const WV w1 = c.wdiff(ids[1], ids[0]), w2 = c.wdiff(ids[2], ids[0]);
     const W g11 = wdot(w1, w1), g12 = wdot(w1, w2), g22 = wdot(w2, w2);
     const W detG = wsub(wmul(g11, g22), wmul(g12, g12));
     const WV n = wvadd(wscale(wmul(g22, wsub(g11, g12)), w1), wscale(wmul(g11, wsub(g22, g12)), w2));
     val = wsub(wmul(detG, wdot(q, q)), wdot(q, n));
   } else {
-    const WV w1 = c.wdiff(s.ids[1], s.ids[0]), w2 = c.wdiff(s.ids[2], s.ids[0]), w3 = c.wdiff(s.ids[3], s.ids[0]);
+    const WV w1 = c.wdiff(ids[1], ids[0]), w2 = c.wdiff(ids[2], ids[0]), w3 = c.wdiff(ids[3], ids[0]);
     const WV x23 = wcross(w2, w3), x31 = wcross(w3, w1), x12 = wcross(w1, w2);
     const W de = wdot(w1, x23);
     const WV nn = wvadd(wvadd(wscale(wdot(w1, w1), x23), wscale(wdot(w2, w2), x31)), wscale(wdot(w3, w3), x12));
     val = wsub(wmul(de, wdot(q, q)), wdot(q, nn));
   }
-  return val.sign() * s.sgn;
+  return val.sign();
+}
+
+// A minimal support waiting for classification: side(w) = sgn * sign(A q - p.N)
+// with p = fl(w - a), q = fl(|p|^2); the FP value is decided outside +-bnd.
+struct QEntry {
+  double A, Nx, Ny, Nz, bnd;
+  uint32_t ids[4];  // ids[0] = owner a; ids[3] = kInvalid32 for a triangle
+  int size, sgn;
+};
+static_assert(sizeof(QEntry) == 64, "queue entries are 64 bytes");
+
+// Triangle (a, a + e1, a + e2): minimal iff its three angles are acute.
+// Returns 0 minimal (E filled), 1 boundary reduced, 2 obtuse, 3 collinear; *adm is
+// false when the circumradius certainly exceeds rmax (no relevant tetrahedron
+// has this face: its circumsphere contains the face's circumcircle).
+__device__ int tri_eval(const Cloud& c, const SetPt& e1, const SetPt& e2, const uint32_t* id, double Mp, double rmax2,
+                        QEntry& E, double& eA, double& eN, bool& adm) {
+  const double M = fmax(ptmax(e1), ptmax(e2)) * (1.0 + 1e-15), M2 = M * M;
+  const double G11 = e1.q, G22 = e2.q, G12 = (e1.x * e2.x + e1.y * e2.y) + e1.z * e2.z;
+  const double db = G11 - G12, dc = G22 - G12;
+  const double detG = G11 * G22 - G12 * G12;
+  const double bG = kFilt * 3.0 * M2 + kTiny, bD = kFilt * 6.0 * M2 + kTiny, b4 = kFilt * 18.0 * M2 * M2 + kTiny;
+  int sg[4] = {fsign(G12, bG), fsign(db, bD), fsign(dc, bD), fsign(detG, b4)};
+  if (sg[0] == 2 || sg[1] == 2 || sg[2] == 2 || sg[3] == 2) tri_signs_exact(c, id, sg);
+  if (sg[3] == 0) {
+    adm = false;
+    return 3;
+  }
+  {  // r^2 = G11 G22 |b - c|^2 / (4 detG): lower bound against rmax^2
+    const double bc = G11 + G22 - 2.0 * G12, ebc = kFilt * 12.0 * M2 + kTiny;
+    const double num = fmax(G11 - bG, 0.0) * fmax(G22 - bG, 0.0) * fmax(bc - ebc, 0.0);
+    const double den = 4.0 * (detG + b4);
+    adm = !(num * (1.0 - 1e-12) > rmax2 * den * (1.0 + 1e-9));
+  }
+  if (sg[0] < 0 || sg[1] < 0 || sg[2] < 0) return 2;
+  if (sg[0] == 0 || sg[1] == 0 || sg[2] == 0) return 1;
+  const double f1 = G22 * db, f2 = G11 * dc;
+  E.A = detG;
+  E.Nx = f1 * e1.x + f2 * e2.x;
+  E.Ny = f1 * e1.y + f2 * e2.y;
+  E.Nz = f1 * e1.z + f2 * e2.z;
+  const double Am = 18.0 * M2 * M2, Nm = 36.0 * M2 * M2 * M;
+  E.bnd = kFilt * (Am * 3.0 * Mp * Mp + 3.0 * Mp * Nm) + kTiny;
+  E.sgn = 1;
+  E.size = 3;
+  eA = kFilt * Am + kTiny;
+  eN = kFilt * Nm + kTiny;
+  return 0;
+}
+
+// Tetrahedron (a, a + e1, a + e2, a + e3): minimal iff the four barycentric
+// coordinates l_i / (2 detE^2) of its circumcentre are positive.
+__device__ int quad_eval(const Cloud& c, const SetPt& e1, const SetPt& e2, const SetPt& e3, const uint32_t* id,
+                         double Mp, QEntry& E, double& eA, double& eN) {
+  const double M = fmax(fmax(ptmax(e1), ptmax(e2)), ptmax(e3)) * (1.0 + 1e-15), M2 = M * M, M3 = M2 * M;
+  const double c23x = e2.y * e3.z - e2.z * e3.y, c23y = e2.z * e3.x - e2.x * e3.z, c23z = e2.x * e3.y - e2.y * e3.x;
+  const double c31x = e3.y * e1.z - e3.z * e1.y, c31y = e3.z * e1.x - e3.x * e1.z, c31z = e3.x * e1.y - e3.y * e1.x;
+  const double c12x = e1.y * e2.z - e1.z * e2.y, c12y = e1.z * e2.x - e1.x * e2.z, c12z = e1.x * e2.y - e1.y * e2.x;
+  const double detE = (e1.x * c23x + e1.y * c23y) + e1.z * c23z;
+  const double Nx = (e1.q * c23x + e2.q * c31x) + e3.q * c12x;
+  const double Ny = (e1.q * c23y + e2.q * c31y) + e3.q * c12y;
+  const double Nz = (e1.q * c23z + e2.q * c31z) + e3.q * c12z;
+  const double l1 = (Nx * c23x + Ny * c23y) + Nz * c23z;
+  const double l2 = (Nx * c31x + Ny * c31y) + Nz * c31z;
+  const double l3 = (Nx * c12x + Ny * c12y) + Nz * c12z;
+  const double l0 = (2.0 * detE) * detE - ((l1 + l2) + l3);
+  const double M6 = M3 * M3;
+  const double bE = kFilt * 6.0 * M3 + kTiny, bl = kFilt * 108.0 * M6 + kTiny, b0 = kFilt * 396.0 * M6 + kTiny;
+  int sg[5] = {fsign(detE, bE), fsign(l0, b0), fsign(l1, bl), fsign(l2, bl), fsign(l3, bl)};
+  if (sg[0] == 2 || sg[1] == 2 || sg[2] == 2 || sg[3] == 2 || sg[4] == 2) quad_signs_exact(c, id, sg);
+  if (sg[0] == 0) return 3;
+  if (sg[1] < 0 || sg[2] < 0 || sg[3] < 0 || sg[4] < 0) return 2;
+  if (sg[1] == 0 || sg[2] == 0 || sg[3] == 0 || sg[4] == 0) return 1;
+  const double Am = 6.0 * M3, Nm = 18.0 * M2 * M2;
+  E.A = detE;
+  E.Nx = Nx;
+  E.Ny = Ny;
+  E.Nz = Nz;
+  E.bnd = kFilt * (Am * 3.0 * Mp * Mp + 3.0 * Mp * Nm) + kTiny;
+  E.sgn = sg[0];
+  E.size = 4;
+  eA = kFilt * Am + kTiny;
+  eN = kFilt * Nm + kTiny;
+  return 0;
 }
 
 // ---- 1. neighbour lists ------------------------------------------------------------------
@@ -365,7 +380,8 @@ __global__ void __launch_bounds__(32 * kDirWarps)
 k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uint32_t* __restrict__ nb,
            const uint32_t* __restrict__ nbc, const double* __restrict__ px, const double* __restrict__ py,
            const double* __restrict__ pz, const double* __restrict__ gather_r2, uint8_t* __restrict__ todo,
-           uint32_t* __restrict__ cand, uint32_t* __restrict__ candc, double* __restrict__ need_r) {
+           uint32_t* __restrict__ cand, uint32_t* __restrict__ candc, double* __restrict__ need_r,
+           float* __restrict__ rho_tab) {
   __shared__ float4 rel[kDirWarps][kMaxNb];  // x, y, z, |p - a| (binary32 copies; margins below)
   __shared__ uint32_t ids[kDirWarps][kMaxNb];
   __shared__ uint32_t mark[kDirWarps][kMaxNb / 32];
@@ -469,6 +485,7 @@ k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uin
     }
     const double kth = cnt >= cp.need ? best[cp.need - 1] : INFINITY;
     const double rho_s = fmin(kth, ext);
+    rho_tab[(uint64_t)a * kDirs + d] = __double2float_ru(rho_s);  // per-cone bound, rounded up
     // certified when every unlisted point (rho >= L/2) cannot lower it
     if (!(rho_s <= half_L)) ok = false;
     worst_needed = fmax(worst_needed, rho_s);
@@ -517,6 +534,14 @@ k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uin
 }
 
 // ---- 3. owner-local enumeration ---------------------------------------------------------
+// One warp per owner a.  C(a) is staged in shared memory as rounded differences
+// p - a; the support candidates are C(a) with ids > a.  Lanes test triangles
+// (pairs j < k) and tetrahedra (triples j < k < l, load-balanced over the pairs
+// whose three a-faces pass the circumradius bound) for minimality; a minimal
+// support whose circumradius certainly exceeds the radius bound of the cone
+// holding its centre direction is dropped, the others are classified against
+// C(a) by the whole warp, 32 points per step, with ballot counts and an early
+// exit once the interior exceeds s_max - size.
 struct HigherRec {
   uint32_t size;
   uint32_t ids[4];
@@ -530,46 +555,128 @@ struct Ctl {
   uint32_t cap;  // record capacity
 };
 
-// Classifies every point of the candidate set (support excluded) against s;
-// false when the interior exceeds icap.
-__device__ bool classify_set(const Cloud& c, const Sphere& s, const uint32_t* set, uint32_t m, uint32_t icap,
-                             HigherRec& r) {
-  r.interior = 0;
-  r.shell = (uint32_t)s.size;
-  r.witness = kInvalid32;
-  for (uint32_t i = 0; i < m; ++i) {
-    const uint32_t w = set[i];
-    if (w == s.ids[1] || w == s.ids[2] || (s.size == 4 && w == s.ids[3])) continue;
-    const int sd = sphere_side(c, s, w);
-    if (sd < 0) {
-      if (r.interior >= icap) return false;
-      r.iids[r.interior++] = w;
-    } else if (sd == 0) {
-      ++r.shell;
-      r.witness = min(r.witness, w);
-    }
+constexpr int kHWarps = 2;      // warps per block in k_higher (shared memory per warp ~22 KB)
+constexpr int kCube = 32;       // cube-map cells per face edge for centre directions
+constexpr int kCellDirs = 8;    // direction slots per cell (0xffff = unused)
+
+struct HigherTables {
+  const float* dirs;       // [kDirs * 3]
+  const uint16_t* cells;   // [6 * kCube * kCube * kCellDirs]
+  const float* rho;        // [n * kDirs] per-cone radius bounds, by PointId
+  double cos_lim;          // cos(delta) raised by a margin: inside the cone for sure
+};
+
+struct WarpSmem {
+  uint32_t sid[kMaxCand];
+  SetPt spt[kMaxCand];
+  uint16_t supi[kMaxCand];
+  uint32_t adm[kMaxCand][kMaxCand / 32];  // adm[j] bit k (j < k): face (a, j, k) within the bound
+  float rho[kDirs];
+  uint32_t iids[kMaxInteriorH];
+  QEntry q[32];
+};
+
+__device__ __forceinline__ int cube_cell(double ux, double uy, double uz) {
+  const double ax = fabs(ux), ay = fabs(uy), az = fabs(uz);
+  int face;
+  double s, t;
+  if (ax >= ay && ax >= az) {
+    face = ux > 0 ? 0 : 1; s = uy / ax; t = uz / ax;
+  } else if (ay >= az) {
+    face = uy > 0 ? 2 : 3; s = ux / ay; t = uz / ay;
+  } else {
+    face = uz > 0 ? 4 : 5; s = ux / az; t = uy / az;
   }
-  return true;
+  const int i = min(kCube - 1, max(0, (int)floor((s + 1.0) * 0.5 * kCube)));
+  const int j = min(kCube - 1, max(0, (int)floor((t + 1.0) * 0.5 * kCube)));
+  return (face * kCube + i) * kCube + j;
 }
 
-__device__ void emit(HigherRec& r, const Sphere& s, HigherRec* out, uint32_t out_cap, uint32_t* counter) {
-  r.size = (uint32_t)s.size;
-  for (int i = 0; i < 4; ++i) r.ids[i] = i < s.size ? s.ids[i] : 0u;
-  for (int i = 1; i < s.size; ++i) {  // support ids ascending
-    const uint32_t x = r.ids[i];
-    int j = i;
-    while (j > 0 && r.ids[j - 1] > x) { r.ids[j] = r.ids[j - 1]; --j; }
-    r.ids[j] = x;
+// True when the sphere's circumradius certainly exceeds the bound of a cone
+// that certainly holds its centre direction: no relevant support.
+__device__ bool cone_rejects(const QEntry& E, double eA, double eN, const float* rho, const HigherTables& tb) {
+  const double nn = sqrt(E.Nx * E.Nx + E.Ny * E.Ny + E.Nz * E.Nz);
+  const double en = eN * 1.7320508075688772;
+  if (!(en <= 1e-7 * nn)) return false;  // direction not well determined
+  const double r_lo = (nn - en) / (2.0 * (fabs(E.A) + eA)) * (1.0 - 1e-12);
+  // centre offset N / (2A); the sign of A is the certified orientation sgn
+  const double inv = (E.sgn > 0 ? 1.0 : -1.0) / nn;
+  const double ux = E.Nx * inv, uy = E.Ny * inv, uz = E.Nz * inv;
+  const uint16_t* cl = tb.cells + (uint64_t)cube_cell(ux, uy, uz) * kCellDirs;
+  double bound = INFINITY;
+  for (int i = 0; i < kCellDirs; ++i) {
+    const uint32_t s = cl[i];
+    if (s == 0xffffu) break;
+    const double cs = (double)tb.dirs[3 * s] * ux + (double)tb.dirs[3 * s + 1] * uy + (double)tb.dirs[3 * s + 2] * uz;
+    if (cs >= tb.cos_lim) bound = fmin(bound, (double)rho[s]);
   }
-  for (uint32_t i = 1; i < r.interior; ++i) {  // interior ids ascending
-    const uint32_t x = r.iids[i];
-    uint32_t j = i;
-    while (j > 0 && r.iids[j - 1] > x) { r.iids[j] = r.iids[j - 1]; --j; }
-    r.iids[j] = x;
+  return r_lo > bound * (1.0 + 1e-9);
+}
+
+// Classifies the queued supports against C(a) with the whole warp and emits the relevant ones.
+__device__ void classify_queue(WarpSmem& S, uint32_t qn, uint32_t m, const Cloud& c, uint32_t smax, HigherRec* out,
+                               uint32_t cap, uint32_t* counter, uint32_t lane, unsigned long long& emitted) {
+  for (uint32_t e = 0; e < qn; ++e) {
+    const QEntry E = S.q[e];
+    const uint32_t icap = smax - (uint32_t)E.size;
+    uint32_t interior = 0, shell = (uint32_t)E.size, wit = kInvalid32;
+    bool reject = false;
+    for (uint32_t base = 0; base < m; base += 32) {
+      const uint32_t i = base + lane;
+      int sd = 1;
+      uint32_t w = kInvalid32;
+      if (i < m) {
+        w = S.sid[i];
+        if (w != E.ids[1] && w != E.ids[2] && w != E.ids[3]) {
+          const SetPt p = S.spt[i];
+          const double v = E.A * p.q - ((p.x * E.Nx + p.y * E.Ny) + p.z * E.Nz);
+          sd = fsign(v, E.bnd);
+          if (sd == 2) sd = side_exact(c, E.ids, E.size, w);
+          sd *= E.sgn;
+        }
+      }
+      const uint32_t bi = __ballot_sync(0xffffffffu, sd < 0), bs = __ballot_sync(0xffffffffu, sd == 0);
+      if (sd < 0) {
+        const uint32_t at = interior + __popc(bi & lanemask_lt());
+        if (at < icap) S.iids[at] = w;
+      }
+      interior += __popc(bi);
+      if (interior > icap) {
+        reject = true;
+        break;
+      }
+      if (bs) {
+        shell += __popc(bs);
+        wit = min(wit, __reduce_min_sync(0xffffffffu, sd == 0 ? w : kInvalid32));
+      }
+    }
+    __syncwarp();
+    if (!reject && lane == 0) {
+      HigherRec r;
+      r.size = (uint32_t)E.size;
+      for (int i = 0; i < 4; ++i) r.ids[i] = i < E.size ? E.ids[i] : 0u;
+      for (int i = 1; i < E.size; ++i) {  // support ids ascending
+        const uint32_t x = r.ids[i];
+        int j = i;
+        while (j > 0 && r.ids[j - 1] > x) { r.ids[j] = r.ids[j - 1]; --j; }
+        r.ids[j] = x;
+      }
+      r.interior = interior;
+      r.shell = shell;
+      r.witness = wit;
+      for (uint32_t i = 0; i < (uint32_t)kMaxInteriorH; ++i) r.iids[i] = i < interior ? S.iids[i] : kInvalid32;
+      for (uint32_t i = 1; i < interior; ++i) {  // interior ids ascending
+        const uint32_t x = r.iids[i];
+        uint32_t j = i;
+        while (j > 0 && r.iids[j - 1] > x) { r.iids[j] = r.iids[j - 1]; --j; }
+        r.iids[j] = x;
+      }
+      const uint32_t slot = atomicAdd(counter, 1u);
+      if (slot < cap) out[slot] = r;
+      ++emitted;
+    }
+    __syncwarp();
   }
-  for (uint32_t i = r.interior; i < (uint32_t)kMaxInteriorH; ++i) r.iids[i] = kInvalid32;
-  const uint32_t slot = atomicAdd(counter, 1u);
-  if (slot < out_cap) out[slot] = r;
 }
 
 __device__ __forceinline__ void decode_pair(uint64_t t, uint32_t& lo, uint32_t& hi) {
@@ -580,80 +687,179 @@ __device__ __forceinline__ void decode_pair(uint64_t t, uint32_t& lo, uint32_t& 
   hi = i + 1;
 }
 
-__global__ void __launch_bounds__(kThreads)
-k_higher(uint32_t n, Ctl ctl, const uint32_t* __restrict__ leaf_pid, const uint32_t* __restrict__ cand,
+// Position of the r-th (0-based) set bit of x; x has more than r set bits.
+__device__ __forceinline__ uint32_t select_bit(uint32_t x, uint32_t r) {
+  uint32_t pos = 0;
+  for (int w = 16; w > 0; w >>= 1) {
+    const uint32_t cnt = __popc(x & ((1u << w) - 1u));
+    if (r >= cnt) {
+      r -= cnt;
+      x >>= w;
+      pos += w;
+    }
+  }
+  return pos;
+}
+
+__global__ void __launch_bounds__(32 * kHWarps)
+k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf_pid, const uint32_t* __restrict__ cand,
          const uint32_t* __restrict__ candc, const double* __restrict__ px, const double* __restrict__ py,
          const double* __restrict__ pz, const int* __restrict__ cloud_scale, HigherRec* __restrict__ out,
-         uint32_t* __restrict__ counter, unsigned long long* __restrict__ stats, uint32_t* __restrict__ err) {
-  __shared__ uint32_t set[kWarps][kMaxCand];  // C(a): classification set
-  __shared__ uint32_t sup[kWarps][kMaxCand];  // C(a) with ids > a: support candidates
+         uint32_t* __restrict__ counter, unsigned long long* __restrict__ stats) {
+  __shared__ WarpSmem smem[kHWarps];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t pos = blockIdx.x * kWarps + warp;
+  const uint32_t pos = blockIdx.x * kHWarps + warp;
   if (pos >= n) return;
+  WarpSmem& S = smem[warp];
   const uint32_t a = leaf_pid[pos];
   const Cloud c{px, py, pz, cloud_scale[0]};
   const uint32_t m = candc[a];
   if (m > (uint32_t)kMaxCand) return;  // reported by the host
+  const double ax = px[a], ay = py[a], az = pz[a];
   uint32_t mc = 0;
+  double Mp = 0.0;
   for (uint32_t base = 0; base < m; base += 32) {
     const uint32_t i = base + lane;
     const uint32_t p = i < m ? cand[(uint64_t)a * kMaxCand + i] : kInvalid32;
-    if (i < m) set[warp][i] = p;
+    if (i < m) {
+      SetPt s;
+      s.x = px[p] - ax;
+      s.y = py[p] - ay;
+      s.z = pz[p] - az;
+      s.q = (s.x * s.x + s.y * s.y) + s.z * s.z;
+      S.sid[i] = p;
+      S.spt[i] = s;
+      Mp = fmax(Mp, ptmax(s));
+    }
     const bool f = i < m && p > a;
     const uint32_t b = __ballot_sync(0xffffffffu, f);
-    if (f) sup[warp][mc + __popc(b & lanemask_lt())] = p;
+    if (f) S.supi[mc + __popc(b & lanemask_lt())] = (uint16_t)i;
     mc += __popc(b);
   }
-  __syncwarp();
-  unsigned long long tested = 0, classified = 0, emitted = 0;
-  const uint64_t P2 = (uint64_t)mc * (mc - 1) / 2;
-  // --- triples (a, b, c): lanes over candidate pairs
-  if (ctl.smax >= 3) {
-    const uint32_t icap = ctl.smax - 3;
-    for (uint64_t t = lane; t < P2; t += 32) {
-      uint32_t j, k;
-      decode_pair(t, j, k);
-      Sphere s;
-      s.size = 3;
-      s.ids[0] = a;
-      s.ids[1] = sup[warp][j];
-      s.ids[2] = sup[warp][k];
-      ++tested;
-      if (tri_status(c, s.ids, s) != 0) continue;
-      ++classified;
-      HigherRec r;
-      if (!classify_set(c, s, set[warp], m, icap, r)) continue;
-      ++emitted;
-      emit(r, s, out, ctl.cap, counter);
-    }
+  float rmax = 0.f;
+  for (uint32_t d = lane; d < (uint32_t)kDirs; d += 32) {
+    const float r = tb.rho[(uint64_t)a * kDirs + d];
+    S.rho[d] = r;
+    rmax = fmaxf(rmax, r);
   }
-  // --- quads (a, b, c, d): lanes over pairs (b, c), inner loop over d
-  if (ctl.smax >= 4) {
-    const uint32_t icap = ctl.smax - 4;
-    for (uint64_t t = lane; t < P2; t += 32) {
+  for (uint32_t i = lane; i < mc * (kMaxCand / 32); i += 32) S.adm[i / (kMaxCand / 32)][i % (kMaxCand / 32)] = 0u;
+  for (int off = 16; off > 0; off >>= 1) {
+    Mp = fmax(Mp, __shfl_xor_sync(0xffffffffu, Mp, off));
+    rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, off));
+  }
+  Mp *= (1.0 + 1e-15);
+  const double rmax2 = (double)rmax * (double)rmax * (1.0 + 1e-12);
+  __syncwarp();
+  unsigned long long tested = 0, minimal = 0, pruned = 0, classified = 0, emitted = 0, admitted = 0;
+  const uint64_t P2 = (uint64_t)mc * (mc - 1) / 2;
+  // --- triangles (a, j, k); also the face bound adm(j, k) for the tetrahedra
+  for (uint64_t t0 = 0; t0 < P2; t0 += 32) {
+    const uint64_t t = t0 + lane;
+    bool push = false;
+    QEntry E;
+    if (t < P2) {
       uint32_t j, k;
       decode_pair(t, j, k);
-      for (uint32_t l = k + 1; l < mc; ++l) {
-        Sphere s;
-        s.size = 4;
-        s.ids[0] = a;
-        s.ids[1] = sup[warp][j];
-        s.ids[2] = sup[warp][k];
-        s.ids[3] = sup[warp][l];
-        ++tested;
-        if (quad_status(c, s.ids, s) != 0) continue;
-        ++classified;
-        HigherRec r;
-        if (!classify_set(c, s, set[warp], m, icap, r)) continue;
-        ++emitted;
-        emit(r, s, out, ctl.cap, counter);
+      const uint32_t ij = S.supi[j], ik = S.supi[k];
+      E.ids[0] = a;
+      E.ids[1] = S.sid[ij];
+      E.ids[2] = S.sid[ik];
+      E.ids[3] = kInvalid32;
+      double eA, eN;
+      bool adm;
+      ++tested;
+      const int st = tri_eval(c, S.spt[ij], S.spt[ik], E.ids, Mp, rmax2, E, eA, eN, adm);
+      if (adm) {
+        atomicOr(&S.adm[j][k >> 5], 1u << (k & 31));
+        ++admitted;
+      }
+      if (st == 0 && ctl.smax >= 3) {
+        ++minimal;
+        if (cone_rejects(E, eA, eN, S.rho, tb)) ++pruned;
+        else push = true;
+      }
+    }
+    const uint32_t b = __ballot_sync(0xffffffffu, push);
+    if (push) S.q[__popc(b & lanemask_lt())] = E;
+    __syncwarp();
+    classified += __popc(b);
+    classify_queue(S, __popc(b), m, c, ctl.smax, out, ctl.cap, counter, lane, emitted);
+  }
+  __syncwarp();
+  // --- tetrahedra (a, j, k, l), j < k < l with adm(j,k), adm(j,l), adm(k,l)
+  if (ctl.smax >= 4) {
+    constexpr uint32_t kWords = kMaxCand / 32;
+    for (uint64_t t0 = 0; t0 < P2; t0 += 32) {
+      const uint64_t t = t0 + lane;
+      uint32_t j = 0, k = 0, cnt = 0;
+      if (t < P2) {
+        decode_pair(t, j, k);
+        if ((S.adm[j][k >> 5] >> (k & 31)) & 1u) {
+          const uint32_t w0 = (k + 1) >> 5;
+          for (uint32_t w = w0; w < kWords; ++w) {
+            uint32_t bits = S.adm[j][w] & S.adm[k][w];
+            if (w == w0) bits &= ((k + 1) & 31) ? (0xffffffffu << ((k + 1) & 31)) : 0xffffffffu;
+            cnt += __popc(bits);
+          }
+        }
+      }
+      uint32_t incl = cnt;
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, off);
+        if ((int)lane >= off) incl += x;
+      }
+      const uint32_t excl = incl - cnt, total = __shfl_sync(0xffffffffu, incl, 31);
+      for (uint32_t q0 = 0; q0 < total; q0 += 32) {
+        const uint32_t q = q0 + lane;
+        // owner lane: the largest o with excl_o <= q
+        uint32_t o = 0;
+        for (uint32_t step = 16; step > 0; step >>= 1) {
+          const uint32_t v = __shfl_sync(0xffffffffu, excl, o + step);
+          if (v <= q) o += step;
+        }
+        const uint32_t oj = __shfl_sync(0xffffffffu, j, o), ok = __shfl_sync(0xffffffffu, k, o);
+        const uint32_t oe = __shfl_sync(0xffffffffu, excl, o);
+        bool push = false;
+        QEntry E;
+        if (q < total) {
+          uint32_t r = q - oe, l = 0;
+          const uint32_t w0 = (ok + 1) >> 5;
+          for (uint32_t w = w0; w < kWords; ++w) {
+            uint32_t bits = S.adm[oj][w] & S.adm[ok][w];
+            if (w == w0) bits &= ((ok + 1) & 31) ? (0xffffffffu << ((ok + 1) & 31)) : 0xffffffffu;
+            const uint32_t pc = __popc(bits);
+            if (r < pc) {
+              l = w * 32 + select_bit(bits, r);
+              break;
+            }
+            r -= pc;
+          }
+          const uint32_t ij = S.supi[oj], ik = S.supi[ok], il = S.supi[l];
+          E.ids[0] = a;
+          E.ids[1] = S.sid[ij];
+          E.ids[2] = S.sid[ik];
+          E.ids[3] = S.sid[il];
+          double eA, eN;
+          ++tested;
+          if (quad_eval(c, S.spt[ij], S.spt[ik], S.spt[il], E.ids, Mp, E, eA, eN) == 0) {
+            ++minimal;
+            if (cone_rejects(E, eA, eN, S.rho, tb)) ++pruned;
+            else push = true;
+          }
+        }
+        const uint32_t b = __ballot_sync(0xffffffffu, push);
+        if (push) S.q[__popc(b & lanemask_lt())] = E;
+        __syncwarp();
+        classified += __popc(b);
+        classify_queue(S, __popc(b), m, c, ctl.smax, out, ctl.cap, counter, lane, emitted);
       }
     }
   }
   for (int off = 16; off > 0; off >>= 1) {
     tested += __shfl_xor_sync(0xffffffffu, tested, off);
-    classified += __shfl_xor_sync(0xffffffffu, classified, off);
-    emitted += __shfl_xor_sync(0xffffffffu, emitted, off);
+    minimal += __shfl_xor_sync(0xffffffffu, minimal, off);
+    pruned += __shfl_xor_sync(0xffffffffu, pruned, off);
+    admitted += __shfl_xor_sync(0xffffffffu, admitted, off);
   }
   if (lane == 0) {
     atomicAdd(stats + 0, tested);
@@ -661,6 +867,9 @@ k_higher(uint32_t n, Ctl ctl, const uint32_t* __restrict__ leaf_pid, const uint3
     atomicAdd(stats + 2, emitted);
     atomicAdd(stats + 3, (unsigned long long)m);
     atomicAdd(stats + 4, (unsigned long long)mc);
+    atomicAdd(stats + 5, minimal);
+    atomicAdd(stats + 6, pruned);
+    atomicAdd(stats + 7, admitted);
   }
 }
 
@@ -753,6 +962,51 @@ void icosphere(std::vector<float>& dirs, double& delta) {
     for (int k = 0; k < 3; ++k) dirs.push_back((float)p[k]);
 }
 
+// Cube-map cells over the sphere of directions (the same face/cell mapping as
+// cube_cell): each cell lists the directions nearest to its centre that lie
+// within delta + the cell's angular radius, so that the direction covering any
+// u in the cell is listed.  The device re-checks every listed cone, so a short
+// list only costs pruning, never correctness.
+void cube_cells(const std::vector<float>& dirs, double delta, std::vector<uint16_t>& cells) {
+  cells.assign((size_t)6 * kCube * kCube * kCellDirs, (uint16_t)0xffff);
+  auto vec = [](int face, double s, double t) {
+    std::array<double, 3> p{};
+    switch (face) {
+      case 0: p = {1, s, t}; break;
+      case 1: p = {-1, s, t}; break;
+      case 2: p = {s, 1, t}; break;
+      case 3: p = {s, -1, t}; break;
+      case 4: p = {s, t, 1}; break;
+      default: p = {s, t, -1}; break;
+    }
+    const double l = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+    return std::array<double, 3>{p[0] / l, p[1] / l, p[2] / l};
+  };
+  auto angle = [](const std::array<double, 3>& x, const std::array<double, 3>& y) {
+    return std::acos(std::max(-1.0, std::min(1.0, x[0] * y[0] + x[1] * y[1] + x[2] * y[2])));
+  };
+  const size_t nd = dirs.size() / 3;
+  for (int face = 0; face < 6; ++face)
+    for (int i = 0; i < kCube; ++i)
+      for (int j = 0; j < kCube; ++j) {
+        const double s0 = -1.0 + 2.0 * i / kCube, s1 = -1.0 + 2.0 * (i + 1) / kCube;
+        const double t0 = -1.0 + 2.0 * j / kCube, t1 = -1.0 + 2.0 * (j + 1) / kCube;
+        const auto ctr = vec(face, 0.5 * (s0 + s1), 0.5 * (t0 + t1));
+        double eps = 0;
+        for (double s : {s0, s1})
+          for (double t : {t0, t1}) eps = std::max(eps, angle(ctr, vec(face, s, t)));
+        std::vector<std::pair<double, uint16_t>> near;
+        for (size_t d = 0; d < nd; ++d) {
+          const std::array<double, 3> dv{dirs[3 * d], dirs[3 * d + 1], dirs[3 * d + 2]};
+          const double g = angle(ctr, dv);
+          if (g <= delta + eps + 1e-6) near.push_back({g, (uint16_t)d});
+        }
+        std::sort(near.begin(), near.end());
+        uint16_t* out = &cells[((size_t)(face * kCube + i) * kCube + j) * kCellDirs];
+        for (size_t q = 0; q < near.size() && q < (size_t)kCellDirs; ++q) out[q] = near[q].second;
+      }
+}
+
 }  // namespace
 
 cudaError_t higher_alloc(Ctx& ctx) {
@@ -782,9 +1036,16 @@ cudaError_t higher_alloc(Ctx& ctx) {
   double delta = 0;
   icosphere(dirs, delta);
   if (dirs.size() != 3 * (size_t)kDirs) return cudaErrorInvalidValue;
+  std::vector<uint16_t> cells;
+  cube_cells(dirs, delta, cells);
   EHGP_ALLOC(h.dirs, dirs.size() * sizeof(float));
+  EHGP_ALLOC(h.cells, cells.size() * sizeof(uint16_t));
+  EHGP_ALLOC(h.rho, n * kDirs * sizeof(float));
 #undef EHGP_ALLOC
   h.delta = delta;
+  h.cos_lim = std::cos(delta) + 1e-6;
+  if ((e = cudaMemcpy(h.cells, cells.data(), cells.size() * sizeof(uint16_t), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return e;
   return cudaMemcpy(h.dirs, dirs.data(), dirs.size() * sizeof(float), cudaMemcpyHostToDevice);
 }
 
@@ -831,7 +1092,8 @@ int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
     k_gather<<<nblocks(n, kWarps), kThreads, 0, st>>>(n, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end, b.px, b.py,
                                                       b.pz, h.gather_r2, h.todo, h.nb, h.nbc);
     k_dirtable<<<nblocks(n, kDirWarps), 32 * kDirWarps, 0, st>>>(n, cp, b.leaf_pid, h.nb, h.nbc, b.px, b.py, b.pz,
-                                                                  h.gather_r2, h.todo, h.cand, h.candc, h.rcap);
+                                                                  h.gather_r2, h.todo, h.cand, h.candc, h.rcap,
+                                                                  h.rho);
     launches += 2;
     cudaMemcpyAsync(todo.data(), h.todo, n, cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
@@ -868,8 +1130,9 @@ int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   cudaMemsetAsync(h.stats, 0, 8 * sizeof(unsigned long long), st);
   Ctl ctl{smax, h.capacity};
   cudaEventRecord(ctx.evk0, st);
-  k_higher<<<nblocks(n, kWarps), kThreads, 0, st>>>(n, ctl, b.leaf_pid, h.cand, h.candc, b.px, b.py, b.pz, g.scale,
-                                                    (HigherRec*)h.raw, h.counters, h.stats, ctx.d_err);
+  const HigherTables tb{h.dirs, h.cells, h.rho, h.cos_lim};
+  k_higher<<<nblocks(n, kHWarps), 32 * kHWarps, 0, st>>>(n, ctl, tb, b.leaf_pid, h.cand, h.candc, b.px, b.py, b.pz,
+                                                         g.scale, (HigherRec*)h.raw, h.counters, h.stats);
   cudaEventRecord(ctx.evk1, st);
   ++launches;
   uint32_t hc[2];

@@ -194,6 +194,9 @@ struct HigherBuffers {
   uint8_t* todo = nullptr;          // [n]
   float* dirs = nullptr;            // [642 * 3]
   double delta = 0;                 // covering angle of dirs
+  double cos_lim = 0;               // cos(delta) + margin
+  uint16_t* cells = nullptr;        // [6 * 32 * 32 * 8] cube-map cell -> nearby directions
+  float* rho = nullptr;             // [n * 642] per-cone radius bounds
   void* raw = nullptr;              // [capacity] 64-byte records
   void* sorted = nullptr;
   uint64_t* khi = nullptr;
