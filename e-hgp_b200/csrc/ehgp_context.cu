@@ -82,6 +82,8 @@ int lbvh_build_common(Ctx* ctx, const void* src, uint64_t n, const ehgp_lbvh_out
   ctx->geom_ready = false;
   ctx->emst_ready = false;
   ctx->pb.witness_ready = false;
+  ctx->pb.K = 0;  // supports are resident for one cloud and one K
+  ctx->hb.K = 0;
   if (where == 0) {
     e = cudaMemcpyAsync(b.xyz_in, src, 3 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
   } else if (where == 1) {
@@ -160,6 +162,7 @@ int ehgp_ctx_destroy(ehgp_ctx* ctx) {
   if (!ctx) return EHGP_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ehgp::hier_free(*ctx);
   for (void* p : ctx->allocations) cudaFree(p);
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);

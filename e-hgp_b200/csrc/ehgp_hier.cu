@@ -1,0 +1,1547 @@
+// Direct Morse hierarchy on sm_100a: terminal facade, Morse event journal,
+// saddle arm seeds, strict-arm descent, frozen-root quotient and the batched
+// hyper-Kruskal forest journal.
+//
+// Reference semantics (Ludwig-H/E-HGP, morsehgp3d/):
+//  facade   src/cpu/hierarchy/direct_support_terminal.cpp:68-300 — accepted events of
+//           arity 2-4 ordered by (exact level, closed rank, interior ids, support ids);
+//           birth_order = rank if rank <= K_eff, saddle_order = rank - 1 if 2 <= rank <= K_eff + 1;
+//  journal  src/cpu/hierarchy/direct_morse_event_journal.cpp:260-400 — n singleton births
+//           (order 1, level 0) plus one role per order, batches of equal (order, exact level);
+//  seeds    src/cpu/hierarchy/direct_saddle_arm_seed_journal.cpp:380-420 — one family per
+//           saddle role, one arm F_u = (I u U) \ {u} per support point u;
+//  forest   src/cpu/hierarchy/direct_morse_forest_journal.cpp:1042-2150 — per batch, strict
+//           arms resolved against the pre-batch locator, transitive carrier quotient,
+//           q_R = 0 reduced birth, 1 continuation, >= 2 multifusion, then unions and births.
+//
+// B200 design:
+//  * events are assembled, given a rigorous FP64 level interval and sorted on the device
+//    (LSD radix over the level bits); only runs whose intervals overlap are settled exactly
+//    on the host (2304-bit level comparisons), so the facade order is exact;
+//  * a stable partition by closed rank gives every order's births and saddle families in
+//    facade order at once; births are hashed by facet on the device;
+//  * each strict arm descends on its own thread: exact facet miniball (FP64 Welzl, then
+//    exact verification, exhaustive exact enumeration as the fallback), LBVH ball query at
+//    the miniball centre, exact top-k with the cutoff shell settled by 832-bit distance
+//    comparisons, the strict level decrease certified, until the facet hits a birth;
+//    the terminal facet does not depend on the locator state (a descent chain only
+//    reaches a minimum, and minima of lower level are bound before the arm's batch), so
+//    every arm of every batch descends in one launch;
+//  * the order-by-order hyper-Kruskal pass over the resolved arms is host code with
+//    incremental carrier counts.
+#include "ehgp_internal.cuh"
+#include "ehgp_exact.cuh"
+#include "ehgp_sphere.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <vector>
+
+namespace ehgp {
+
+struct HierState;
+
+namespace {
+
+constexpr double kU = 1.1102230246251565e-16;
+constexpr double kFilt = 64.0 * kU;
+constexpr double kTiny = 1e-300;
+constexpr int kMaxFacet = 10;
+constexpr int kT = 256;              // threads per block of the elementwise kernels
+constexpr int kCandCap = 64;         // ball-query candidates per descent step
+constexpr int kDStack = 64;          // LBVH traversal stack per descent thread
+constexpr int kDescentSteps = 512;   // descent steps per arm
+
+// Descent status per arm.
+enum ArmStatus : uint8_t {
+  kArmOk = 0,
+  kArmUnresolved = 1,   // canonical top-k choice equals the facet
+  kArmPlateau = 2,      // no strict level decrease
+  kArmCapacity = 3,     // ball query or traversal capacity
+  kArmSteps = 4,        // step budget
+  kArmInternal = 5,     // no miniball or inconsistent top-k
+};
+
+__host__ __device__ inline uint32_t nblk(uint64_t n, int t) {
+  const uint64_t b = (n + t - 1) / t;
+  return b == 0 ? 1u : (uint32_t)b;
+}
+
+// Device layouts of the support records (ehgp_pairs.cu, ehgp_higher.cu).
+struct PairRecD {
+  uint32_t u, v, interior, shell, witness;
+  uint32_t ids[9];
+  uint32_t pad[2];
+};
+struct HigherRecD {
+  uint32_t size;
+  uint32_t ids[4];
+  uint32_t interior, shell, witness;
+  uint32_t iids[8];
+};
+struct EvRec {
+  uint32_t size, ids[4], nint, rank, iids[9];
+};
+static_assert(sizeof(EvRec) == 64 && sizeof(PairRecD) == 64 && sizeof(HigherRecD) == 64, "64-byte records");
+
+__device__ __forceinline__ TNode load_node(const TNode* __restrict__ tn, uint32_t i) {
+  const float4* p = reinterpret_cast<const float4*>(tn + i);
+  const float4 a = __ldg(p), b = __ldg(p + 1);
+  TNode t;
+  t.lo[0] = a.x; t.lo[1] = a.y; t.lo[2] = a.z; t.left = __float_as_uint(a.w);
+  t.hi[0] = b.x; t.hi[1] = b.y; t.hi[2] = b.z; t.right = __float_as_uint(b.w);
+  return t;
+}
+
+__host__ __device__ inline double wdbl(const W& x, int shift) {  // x 2^-shift, relative error ~1e-15
+  const bool neg = x.negative();
+  const W a = neg ? wneg(x) : x;
+  int t = 12;
+  while (t > 0 && a.w[t] == 0) --t;
+  double v = 0.0;
+  for (int i = t; i >= 0 && i >= t - 2; --i) v += ldexp((double)a.w[i], 64 * i - shift);
+  return neg ? -v : v;
+}
+
+// ---- FP64 circumsphere with uniform error bounds ---------------------------------
+// Same bounds as the support kernels: with every difference coordinate bounded by
+// M, |computed - exact| <= 64 u m with m of A: 1 (pair), 18 M^4 (triangle), 6 M^3
+// (tetrahedron) and of each N coordinate: M (pair), 36 M^5, 18 M^4.
+struct FSphere {
+  double ax, ay, az;   // ids[0]
+  double A, Nx, Ny, Nz;
+  double eA, eN;       // error bounds of A and of each N coordinate
+  double M;            // difference coordinate bound
+};
+
+__device__ void fsphere(const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz,
+                        const uint32_t* ids, int size, FSphere& s) {
+  s.ax = px[ids[0]];
+  s.ay = py[ids[0]];
+  s.az = pz[ids[0]];
+  double e[3][3];
+  double M = 0.0;
+  for (int j = 1; j < size; ++j) {
+    e[j - 1][0] = px[ids[j]] - s.ax;
+    e[j - 1][1] = py[ids[j]] - s.ay;
+    e[j - 1][2] = pz[ids[j]] - s.az;
+    M = fmax(M, fmax(fabs(e[j - 1][0]), fmax(fabs(e[j - 1][1]), fabs(e[j - 1][2]))));
+  }
+  M *= (1.0 + 1e-15);
+  s.M = M;
+  const double M2 = M * M;
+  if (size == 1) {
+    s.A = 1.0; s.Nx = s.Ny = s.Nz = 0.0; s.eA = 0.0; s.eN = 0.0;
+  } else if (size == 2) {
+    s.A = 1.0; s.Nx = e[0][0]; s.Ny = e[0][1]; s.Nz = e[0][2];
+    s.eA = 0.0; s.eN = 2.0 * kU * M + kTiny;
+  } else if (size == 3) {
+    const double G11 = (e[0][0] * e[0][0] + e[0][1] * e[0][1]) + e[0][2] * e[0][2];
+    const double G22 = (e[1][0] * e[1][0] + e[1][1] * e[1][1]) + e[1][2] * e[1][2];
+    const double G12 = (e[0][0] * e[1][0] + e[0][1] * e[1][1]) + e[0][2] * e[1][2];
+    const double f1 = G22 * (G11 - G12), f2 = G11 * (G22 - G12);
+    s.A = G11 * G22 - G12 * G12;
+    s.Nx = f1 * e[0][0] + f2 * e[1][0];
+    s.Ny = f1 * e[0][1] + f2 * e[1][1];
+    s.Nz = f1 * e[0][2] + f2 * e[1][2];
+    s.eA = kFilt * 18.0 * M2 * M2 + kTiny;
+    s.eN = kFilt * 36.0 * M2 * M2 * M + kTiny;
+  } else {
+    const double* e1 = e[0];
+    const double* e2 = e[1];
+    const double* e3 = e[2];
+    const double c23x = e2[1] * e3[2] - e2[2] * e3[1], c23y = e2[2] * e3[0] - e2[0] * e3[2], c23z = e2[0] * e3[1] - e2[1] * e3[0];
+    const double c31x = e3[1] * e1[2] - e3[2] * e1[1], c31y = e3[2] * e1[0] - e3[0] * e1[2], c31z = e3[0] * e1[1] - e3[1] * e1[0];
+    const double c12x = e1[1] * e2[2] - e1[2] * e2[1], c12y = e1[2] * e2[0] - e1[0] * e2[2], c12z = e1[0] * e2[1] - e1[1] * e2[0];
+    const double q1 = (e1[0] * e1[0] + e1[1] * e1[1]) + e1[2] * e1[2];
+    const double q2 = (e2[0] * e2[0] + e2[1] * e2[1]) + e2[2] * e2[2];
+    const double q3 = (e3[0] * e3[0] + e3[1] * e3[1]) + e3[2] * e3[2];
+    s.A = (e1[0] * c23x + e1[1] * c23y) + e1[2] * c23z;
+    s.Nx = (q1 * c23x + q2 * c31x) + q3 * c12x;
+    s.Ny = (q1 * c23y + q2 * c31y) + q3 * c12y;
+    s.Nz = (q1 * c23z + q2 * c31z) + q3 * c12z;
+    s.eA = kFilt * 6.0 * M2 * M + kTiny;
+    s.eN = kFilt * 18.0 * M2 * M2 + kTiny;
+  }
+}
+
+// Rigorous interval [lo, hi] of the squared radius |N|^2 / (4 A^2); false when A is not
+// bounded away from 0 in FP64.
+__device__ bool flevel(const FSphere& s, double& lo, double& hi) {
+  const double nn = sqrt(s.Nx * s.Nx + s.Ny * s.Ny + s.Nz * s.Nz);
+  const double en = s.eN * 1.7320508075688772;
+  const double alo = fabs(s.A) - s.eA, ahi = fabs(s.A) + s.eA;
+  if (!(alo > 0.0)) return false;
+  const double nlo = fmax(nn - en, 0.0), nhi = nn + en;
+  lo = nlo * nlo / (4.0 * ahi * ahi) * (1.0 - 1e-14);
+  hi = nhi * nhi / (4.0 * alo * alo) * (1.0 + 1e-14);
+  return isfinite(hi);
+}
+
+// Exact squared radius converted to FP64 (for ill-conditioned supports): 36-limb free.
+__device__ void exact_level_fp(const Cloud& c, const uint32_t* ids, int size, double& lo, double& hi) {
+  W A;
+  WV N;
+  exact_sphere(c, ids, size, A, N);
+  // scale both to moderate magnitude: |N|^2 / (4A^2) 2^-2S
+  int ta = 12, tn = 12;
+  const W aa = A.negative() ? wneg(A) : A;
+  while (ta > 0 && aa.w[ta] == 0) --ta;
+  const W* comp[3] = {&N.x, &N.y, &N.z};
+  int tmax = 0;
+  for (int k = 0; k < 3; ++k) {
+    const W v = comp[k]->negative() ? wneg(*comp[k]) : *comp[k];
+    int t = 12;
+    while (t > 0 && v.w[t] == 0) --t;
+    tmax = max(tmax, t);
+  }
+  tn = tmax;
+  const int sa = 64 * ta, sn = 64 * tn;
+  const double a = wdbl(A, sa);
+  const double nx = wdbl(N.x, sn), ny = wdbl(N.y, sn), nz = wdbl(N.z, sn);
+  const double r = (nx * nx + ny * ny + nz * nz) / (4.0 * a * a);
+  const double L = ldexp(r, 2 * sn - 2 * sa - 2 * c.S);
+  lo = L * (1.0 - 1e-13);
+  hi = L * (1.0 + 1e-13);
+}
+
+// ---- 1. events -------------------------------------------------------------------
+__global__ void k_ev_build(uint32_t np, uint32_t nh, const PairRecD* __restrict__ pr, const HigherRecD* __restrict__ hr,
+                           const double* __restrict__ px, const double* __restrict__ py,
+                           const double* __restrict__ pz, const int* __restrict__ cloud_scale, EvRec* __restrict__ ev,
+                           double* __restrict__ lmid, double* __restrict__ lerr, uint64_t* __restrict__ key,
+                           uint32_t* __restrict__ diag) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np + nh) return;
+  EvRec r;
+  uint32_t shell;
+  if (i < np) {
+    const PairRecD p = pr[i];
+    r.size = 2;
+    r.ids[0] = p.u;
+    r.ids[1] = p.v;
+    r.ids[2] = r.ids[3] = 0;
+    r.nint = p.interior;
+    for (int j = 0; j < 9; ++j) r.iids[j] = j < (int)p.interior ? p.ids[j] : kInvalid32;
+    shell = p.shell;
+  } else {
+    const HigherRecD h = hr[i - np];
+    r.size = h.size;
+    for (int j = 0; j < 4; ++j) r.ids[j] = h.ids[j];
+    r.nint = h.interior;
+    for (int j = 0; j < 9; ++j) r.iids[j] = j < 8 && j < (int)h.interior ? h.iids[j] : kInvalid32;
+    shell = h.shell;
+  }
+  r.rank = r.nint + r.size;
+  ev[i] = r;
+  if (shell != r.size) {  // relevant extra-shell diagnostic: excluded from the facade
+    atomicAdd(diag, 1u);
+    key[i] = ~uint64_t{0};
+    lmid[i] = INFINITY;
+    lerr[i] = 0.0;
+    return;
+  }
+  FSphere s;
+  fsphere(px, py, pz, r.ids, (int)r.size, s);
+  double lo, hi;
+  if (r.size == 2) {
+    const double d2 = (s.Nx * s.Nx + s.Ny * s.Ny) + s.Nz * s.Nz;
+    lo = 0.25 * d2 * (1.0 - 8.0 * kU);
+    hi = 0.25 * d2 * (1.0 + 8.0 * kU);
+  } else if (!flevel(s, lo, hi) || hi - lo > 1e-9 * hi) {
+    const Cloud c{px, py, pz, cloud_scale[0]};
+    exact_level_fp(c, r.ids, (int)r.size, lo, hi);
+  }
+  const double mid = 0.5 * (lo + hi);
+  lmid[i] = mid;
+  lerr[i] = 0.5 * (hi - lo) + 1e-15 * mid;
+  key[i] = dbits(mid);
+}
+
+__global__ void k_ev_gather(uint32_t m, const uint32_t* __restrict__ v0, const uint32_t* __restrict__ v1,
+                            const uint32_t* __restrict__ state, int passes, const EvRec* __restrict__ ev,
+                            const double* __restrict__ lmid, const double* __restrict__ lerr, EvRec* __restrict__ out,
+                            double* __restrict__ omid, double* __restrict__ oerr, uint32_t* __restrict__ perm) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const uint32_t s = radix_result(state, passes, v0, v1)[i];
+  out[i] = ev[s];
+  omid[i] = lmid[s];
+  oerr[i] = lerr[s];
+  perm[i] = s;
+}
+
+// ---- scans (block-local then across blocks) -----------------------------------------
+struct OpMax {
+  __device__ double operator()(double a, double b) const { return fmax(a, b); }
+};
+struct OpMin {
+  __device__ double operator()(double a, double b) const { return fmin(a, b); }
+};
+
+// Inclusive prefix max of hi[i] = mid + err (forward) and suffix min of lo = mid - err
+// (backward), chunked: one block per 1024 items, then a sequential pass over blocks.
+template <class Op>
+__global__ void k_scan_blocks(uint32_t m, const double* __restrict__ mid, const double* __restrict__ err, double sgn,
+                              int reverse, double* __restrict__ out, double* __restrict__ bsum, Op op, double ident) {
+  __shared__ double sh[1024];
+  const uint32_t base = blockIdx.x * 1024u;
+  for (uint32_t t = threadIdx.x; t < 1024; t += blockDim.x) {
+    const uint32_t j = base + t;
+    double v = ident;
+    if (j < m) {
+      const uint32_t idx = reverse ? m - 1 - j : j;
+      v = mid[idx] + sgn * err[idx];
+    }
+    sh[t] = v;
+  }
+  __syncthreads();
+  for (uint32_t off = 1; off < 1024; off <<= 1) {
+    double add[4];
+    int c = 0;
+    for (uint32_t t = threadIdx.x; t < 1024; t += blockDim.x) add[c++] = t >= off ? sh[t - off] : ident;
+    __syncthreads();
+    c = 0;
+    for (uint32_t t = threadIdx.x; t < 1024; t += blockDim.x) {
+      sh[t] = op(sh[t], add[c++]);
+    }
+    __syncthreads();
+  }
+  for (uint32_t t = threadIdx.x; t < 1024; t += blockDim.x) {
+    const uint32_t j = base + t;
+    if (j < m) out[reverse ? m - 1 - j : j] = sh[t];
+  }
+  if (threadIdx.x == 0) bsum[blockIdx.x] = sh[1023];
+}
+
+template <class Op>
+__global__ void k_scan_carry(uint32_t nb, double* __restrict__ bsum, Op op, double ident) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  double run = ident;
+  for (uint32_t b = 0; b < nb; ++b) {
+    const double v = bsum[b];
+    bsum[b] = run;  // exclusive carry
+    run = op(run, v);
+  }
+}
+
+template <class Op>
+__global__ void k_scan_apply(uint32_t m, int reverse, double* __restrict__ out, const double* __restrict__ bsum,
+                             Op op) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const uint32_t idx = reverse ? m - 1 - j : j;
+  out[idx] = op(out[idx], bsum[j / 1024u]);
+}
+
+// A boundary between facade positions p - 1 and p is certain when every level
+// interval before it lies strictly below every one after it.
+__global__ void k_uncertain(uint32_t m, const double* __restrict__ pre_hi, const double* __restrict__ suf_lo,
+                            uint32_t* __restrict__ list, uint32_t cap, uint32_t* __restrict__ count) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p == 0 || p >= m) return;
+  if (pre_hi[p - 1] < suf_lo[p]) return;
+  const uint32_t at = atomicAdd(count, 1u);
+  if (at < cap) list[at] = p;
+}
+
+// ---- 2. level classes, rank partition, births -----------------------------------
+__global__ void k_level_class(uint32_t m, const uint8_t* __restrict__ eqprev, uint32_t* __restrict__ flag) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < m) flag[p] = (p == 0 || !eqprev[p]) ? 1u : 0u;
+}
+
+// Inclusive prefix sum of 32-bit flags (block-local, then carries).
+__global__ void k_sum_blocks(uint32_t m, const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                             uint32_t* __restrict__ bsum) {
+  __shared__ uint32_t sh[1024];
+  const uint32_t base = blockIdx.x * 1024u;
+  for (uint32_t t = threadIdx.x; t < 1024; t += blockDim.x) sh[t] = base + t < m ? in[base + t] : 0u;
+  __syncthreads();
+  for (uint32_t off = 1; off < 1024; off <<= 1) {
+    uint32_t add[4];
+    int c = 0;
+    for (uint32_t t = threadIdx.x; t < 1024; t += blockDim.x) add[c++] = t >= off ? sh[t - off] : 0u;
+    __syncthreads();
+    c = 0;
+    for (uint32_t t = threadIdx.x; t < 1024; t += blockDim.x) sh[t] += add[c++];
+    __syncthreads();
+  }
+  for (uint32_t t = threadIdx.x; t < 1024; t += blockDim.x)
+    if (base + t < m) out[base + t] = sh[t];
+  if (threadIdx.x == 0) bsum[blockIdx.x] = sh[1023];
+}
+
+__global__ void k_sum_carry(uint32_t nb, uint32_t* __restrict__ bsum) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  uint32_t run = 0;
+  for (uint32_t b = 0; b < nb; ++b) {
+    const uint32_t v = bsum[b];
+    bsum[b] = run;
+    run += v;
+  }
+}
+
+__global__ void k_sum_apply(uint32_t m, uint32_t* __restrict__ out, const uint32_t* __restrict__ bsum, int minus1) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < m) out[j] = out[j] + bsum[j / 1024u] - (minus1 ? 1u : 0u);
+}
+
+__global__ void k_rank_key(uint32_t m, const EvRec* __restrict__ ev, uint64_t* __restrict__ key,
+                           uint32_t* __restrict__ iota, uint32_t* __restrict__ hist) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const uint32_t r = ev[i].rank;
+  key[i] = r;
+  iota[i] = i;
+  atomicAdd(&hist[r < 15 ? r : 15], 1u);
+}
+
+__global__ void k_rank_gather(uint32_t m, const uint32_t* __restrict__ v0, const uint32_t* __restrict__ v1,
+                              const uint32_t* __restrict__ state, int passes, uint32_t* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) out[i] = radix_result(state, passes, v0, v1)[i];
+}
+
+__host__ __device__ inline uint32_t facet_hash(const uint32_t* ids, int k) {
+  uint64_t h = 0x9E3779B97F4A7C15ull ^ (uint64_t)k;
+  for (int i = 0; i < k; ++i) {
+    h ^= ids[i];
+    h *= 0xFF51AFD7ED558CCDull;
+    h ^= h >> 33;
+  }
+  h *= 0xC4CEB9FE1A85EC53ull;
+  h ^= h >> 33;
+  return (uint32_t)h;
+}
+
+__device__ __forceinline__ int event_facet(const EvRec& e, uint32_t* F) {  // I u U, ascending
+  int k = 0;
+  for (uint32_t j = 0; j < e.nint; ++j) F[k++] = e.iids[j];
+  for (uint32_t j = 0; j < e.size; ++j) F[k++] = e.ids[j];
+  for (int a = 1; a < k; ++a) {
+    const uint32_t x = F[a];
+    int b = a;
+    while (b > 0 && F[b - 1] > x) { F[b] = F[b - 1]; --b; }
+    F[b] = x;
+  }
+  return k;
+}
+
+// Births of orders >= 2: handle = n + position in the rank partition; facets stored
+// (10 words, unused = kInvalid32) and hashed (open addressing, handle per slot).
+__global__ void k_birth_insert(uint32_t nb, uint32_t n, uint32_t birth_base, const uint32_t* __restrict__ rank_order,
+                               const EvRec* __restrict__ ev, uint32_t* __restrict__ bfac, uint32_t* __restrict__ slots,
+                               uint32_t mask, uint32_t* __restrict__ err) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const uint32_t fi = rank_order[birth_base + b];
+  uint32_t F[kMaxFacet + 1];
+  const int k = event_facet(ev[fi], F);
+  uint32_t* out = bfac + (uint64_t)b * kMaxFacet;
+  for (int j = 0; j < kMaxFacet; ++j) out[j] = j < k ? F[j] : kInvalid32;
+  const uint32_t h = n + b;
+  uint32_t s = facet_hash(F, k) & mask;
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const uint32_t prev = atomicCAS(&slots[s], kInvalid32, h);
+    if (prev == kInvalid32) return;
+    s = (s + 1) & mask;
+  }
+  atomicOr(err, kErrCapacity);
+}
+
+// ---- 3. strict-arm descent ----------------------------------------------------------
+struct DescentParams {
+  uint32_t n, root;
+  const TNode* tn;
+  const double* px;
+  const double* py;
+  const double* pz;
+  int S;
+  const uint32_t* slots;
+  uint32_t mask;
+  const uint32_t* bfac;
+  uint32_t nbirths;
+};
+
+__device__ uint32_t probe_facet(const DescentParams& d, const uint32_t* F, int k) {
+  if (k == 1) return F[0];  // order-one births are the singletons, handle = PointId
+  uint32_t s = facet_hash(F, k) & d.mask;
+  for (uint32_t probe = 0; probe <= d.mask; ++probe) {
+    const uint32_t h = __ldg(d.slots + s);
+    if (h == kInvalid32) return kInvalid32;
+    const uint32_t* f = d.bfac + (uint64_t)(h - d.n) * kMaxFacet;
+    bool eq = true;
+    for (int j = 0; j < kMaxFacet && eq; ++j) eq = __ldg(f + j) == (j < k ? F[j] : kInvalid32);
+    if (eq) return h;
+    s = (s + 1) & d.mask;
+  }
+  return kInvalid32;
+}
+
+// Exact closed-ball membership of w in the circumsphere of T (side <= 0), FP64 first.
+__device__ bool inside_closed(const Cloud& c, const FSphere& fs, const uint32_t* T, int ts, uint32_t w) {
+  const double x = c.px[w] - fs.ax, y = c.py[w] - fs.ay, z = c.pz[w] - fs.az;
+  const double Mp = fmax(fs.M, fmax(fabs(x), fmax(fabs(y), fabs(z)))) * (1.0 + 1e-15);
+  const double q = (x * x + y * y) + z * z;
+  const double v = fs.A * q - ((x * fs.Nx + y * fs.Ny) + z * fs.Nz);
+  const double M2 = fs.M * fs.M, M4 = M2 * M2;
+  const double Am = ts <= 2 ? 1.0 : (ts == 3 ? 18.0 * M4 : 6.0 * M2 * fs.M);
+  const double Nm = ts == 1 ? 0.0 : (ts == 2 ? fs.M : (ts == 3 ? 36.0 * M4 * fs.M : 18.0 * M4));
+  const double bnd = kFilt * (Am * 3.0 * Mp * Mp + 3.0 * Mp * Nm) + kTiny;
+  const int sa = fs.A > fs.eA ? 1 : (fs.A < -fs.eA ? -1 : 0);
+  if (sa != 0) {
+    if (v * sa < -bnd) return true;
+    if (v * sa > bnd) return false;
+  }
+  W A;
+  WV N;
+  exact_sphere(c, T, ts, A, N);
+  const WV dq = c.wdiff(w, T[0]);
+  const int sd = wsub(wmul(A, wdot(dq, dq)), wdot(dq, N)).sign() * A.sign();
+  return sd <= 0;
+}
+
+// Exact: the circumcentre of T lies in the closed convex hull of T and T is affinely independent.
+__device__ bool hull_centre(const Cloud& c, const uint32_t* T, int ts) {
+  if (ts <= 2) return ts == 1 || T[0] != T[1];
+  int sg[5];
+  if (ts == 3) {
+    tri_signs_exact(c, T, sg);
+    return sg[3] != 0 && sg[0] >= 0 && sg[1] >= 0 && sg[2] >= 0;
+  }
+  quad_signs_exact(c, T, sg);
+  return sg[0] != 0 && sg[1] >= 0 && sg[2] >= 0 && sg[3] >= 0 && sg[4] >= 0;
+}
+
+struct Mini {
+  uint32_t T[4];
+  int ts;
+  FSphere fs;
+};
+
+__device__ bool verify_mini(const Cloud& c, const uint32_t* F, int k, Mini& mb) {
+  if (!hull_centre(c, mb.T, mb.ts)) return false;
+  fsphere(c.px, c.py, c.pz, mb.T, mb.ts, mb.fs);
+  for (int i = 0; i < k; ++i) {
+    bool sup = false;
+    for (int j = 0; j < mb.ts; ++j) sup |= mb.T[j] == F[i];
+    if (!sup && !inside_closed(c, mb.fs, mb.T, mb.ts, F[i])) return false;
+  }
+  return true;
+}
+
+// Exact miniball of the facet F (1..10 points): FP64 Welzl proposes the support,
+// exact predicates verify it; exhaustive exact enumeration of 1..4-subsets when the
+// proposal fails (build_exact_facet_miniball, hierarchy/facet_miniball.hpp:86-102).
+__device__ __noinline__ bool facet_miniball(const Cloud& c, const uint32_t* F, int k, Mini& mb) {
+  double P[kMaxFacet][3];
+  for (int i = 0; i < k; ++i) {
+    P[i][0] = c.px[F[i]] - c.px[F[0]];
+    P[i][1] = c.py[F[i]] - c.py[F[0]];
+    P[i][2] = c.pz[F[i]] - c.pz[F[0]];
+  }
+  double cx = 0, cy = 0, cz = 0, r2 = 0;
+  int T[4] = {0, 0, 0, 0}, ts = 1;
+  bool fp_ok = true;
+  auto out = [&](int i) {
+    const double dx = P[i][0] - cx, dy = P[i][1] - cy, dz = P[i][2] - cz;
+    return dx * dx + dy * dy + dz * dz > r2 * (1.0 + 1e-10) + 1e-300;
+  };
+  auto set_ball = [&](const int* idx, int s) {
+    T[0] = idx[0]; T[1] = s > 1 ? idx[1] : 0; T[2] = s > 2 ? idx[2] : 0; T[3] = s > 3 ? idx[3] : 0;
+    ts = s;
+    const double* a = P[idx[0]];
+    if (s == 1) { cx = a[0]; cy = a[1]; cz = a[2]; r2 = 0; return; }
+    double e[3][3];
+    for (int j = 1; j < s; ++j)
+      for (int t = 0; t < 3; ++t) e[j - 1][t] = P[idx[j]][t] - a[t];
+    double A, N0, N1, N2;
+    if (s == 2) {
+      A = 1.0; N0 = e[0][0]; N1 = e[0][1]; N2 = e[0][2];
+    } else if (s == 3) {
+      const double G11 = e[0][0] * e[0][0] + e[0][1] * e[0][1] + e[0][2] * e[0][2];
+      const double G22 = e[1][0] * e[1][0] + e[1][1] * e[1][1] + e[1][2] * e[1][2];
+      const double G12 = e[0][0] * e[1][0] + e[0][1] * e[1][1] + e[0][2] * e[1][2];
+      A = G11 * G22 - G12 * G12;
+      const double f1 = G22 * (G11 - G12), f2 = G11 * (G22 - G12);
+      N0 = f1 * e[0][0] + f2 * e[1][0]; N1 = f1 * e[0][1] + f2 * e[1][1]; N2 = f1 * e[0][2] + f2 * e[1][2];
+    } else {
+      const double* e1 = e[0]; const double* e2 = e[1]; const double* e3 = e[2];
+      const double c23[3] = {e2[1] * e3[2] - e2[2] * e3[1], e2[2] * e3[0] - e2[0] * e3[2], e2[0] * e3[1] - e2[1] * e3[0]};
+      const double c31[3] = {e3[1] * e1[2] - e3[2] * e1[1], e3[2] * e1[0] - e3[0] * e1[2], e3[0] * e1[1] - e3[1] * e1[0]};
+      const double c12[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+      const double q1 = e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2];
+      const double q2 = e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2];
+      const double q3 = e3[0] * e3[0] + e3[1] * e3[1] + e3[2] * e3[2];
+      A = e1[0] * c23[0] + e1[1] * c23[1] + e1[2] * c23[2];
+      N0 = q1 * c23[0] + q2 * c31[0] + q3 * c12[0];
+      N1 = q1 * c23[1] + q2 * c31[1] + q3 * c12[1];
+      N2 = q1 * c23[2] + q2 * c31[2] + q3 * c12[2];
+    }
+    if (!(fabs(A) > 0.0)) { fp_ok = false; A = 1e-300; }
+    const double inv = 0.5 / A;
+    cx = a[0] + N0 * inv; cy = a[1] + N1 * inv; cz = a[2] + N2 * inv;
+    r2 = (N0 * N0 + N1 * N1 + N2 * N2) * inv * inv;
+  };
+  int idx[4];
+  idx[0] = 0;
+  set_ball(idx, 1);
+  for (int i = 1; i < k && fp_ok; ++i) {
+    if (!out(i)) continue;
+    idx[0] = i;
+    set_ball(idx, 1);
+    for (int j = 0; j < i && fp_ok; ++j) {
+      if (!out(j)) continue;
+      idx[0] = i; idx[1] = j;
+      set_ball(idx, 2);
+      for (int l = 0; l < j && fp_ok; ++l) {
+        if (!out(l)) continue;
+        idx[0] = i; idx[1] = j; idx[2] = l;
+        set_ball(idx, 3);
+        for (int m = 0; m < l && fp_ok; ++m) {
+          if (!out(m)) continue;
+          idx[0] = i; idx[1] = j; idx[2] = l; idx[3] = m;
+          set_ball(idx, 4);
+        }
+      }
+    }
+  }
+  if (fp_ok) {
+    mb.ts = ts;
+    for (int j = 0; j < ts; ++j) mb.T[j] = F[T[j]];
+    // canonical support order (ascending ids) for the exact data
+    for (int a = 1; a < ts; ++a) {
+      const uint32_t x = mb.T[a];
+      int b = a;
+      while (b > 0 && mb.T[b - 1] > x) { mb.T[b] = mb.T[b - 1]; --b; }
+      mb.T[b] = x;
+    }
+    if (verify_mini(c, F, k, mb)) return true;
+  }
+  // exhaustive exact enumeration
+  for (int s = (k == 1 ? 1 : 2); s <= 4 && s <= k; ++s) {
+    int id[4] = {0, 1, 2, 3};
+    while (true) {
+      mb.ts = s;
+      for (int j = 0; j < s; ++j) mb.T[j] = F[id[j]];
+      if (verify_mini(c, F, k, mb)) return true;
+      int p = s - 1;
+      while (p >= 0 && id[p] == k - s + p) --p;
+      if (p < 0) break;
+      ++id[p];
+      for (int q = p + 1; q < s; ++q) id[q] = id[q - 1] + 1;
+    }
+  }
+  return false;
+}
+
+// Exact canonical top-k choice at the miniball centre of F.  Returns the status; on
+// success G holds k ascending ids and *cut_below is 1 when the cutoff lies strictly
+// below beta(F), 0 when it equals it.
+__device__ __noinline__ int topk_choice(const DescentParams& d, const Cloud& c, const Mini& mb, int k, uint32_t* G,
+                                        int* cut_below) {
+  const FSphere& fs = mb.fs;
+  double llo, lhi;
+  if (!flevel(fs, llo, lhi)) exact_level_fp(c, mb.T, mb.ts, llo, lhi);
+  // FP64 centre and its error: c~ = a + N / (2A)
+  const double inv = 0.5 / fs.A;
+  const double ox = fs.Nx * inv, oy = fs.Ny * inv, oz = fs.Nz * inv;
+  const double cx = fs.ax + ox, cy = fs.ay + oy, cz = fs.az + oz;
+  const double on = sqrt(ox * ox + oy * oy + oz * oz);
+  const double nn = sqrt(fs.Nx * fs.Nx + fs.Ny * fs.Ny + fs.Nz * fs.Nz);
+  const double relA = fs.eA / fmax(fabs(fs.A) - fs.eA, 1e-300);
+  const double relN = fs.eN * 1.7320508075688772 / fmax(nn, 1e-300);
+  double dc = on * (relA + relN) * 1.01 + 4.0 * kU * (fabs(cx) + fabs(cy) + fabs(cz)) + kTiny;
+  if (!(relA < 0.5) || !isfinite(dc)) dc = 2.0 * sqrt(lhi) + 1e-300;  // centre not trusted: widen the ball
+  const double R = sqrt(lhi) * (1.0 + 1e-12) + dc;
+  const double R2 = R * R * (1.0 + 1e-12);
+  const double ed = 2.0 * R * dc + dc * dc + 8.0 * kU * R2 + kTiny;
+  // ball query
+  uint32_t cid[kCandCap];
+  double cd[kCandCap];
+  int cnt = 0;
+  uint32_t stack[kDStack];
+  int top = 0;
+  stack[top++] = d.root;
+  while (top > 0) {
+    const uint32_t node = stack[--top];
+    const TNode t = load_node(d.tn, node);
+    if (t.left == kInvalid32) {
+      const uint32_t q = t.right;
+      const double dx = c.px[q] - cx, dy = c.py[q] - cy, dz = c.pz[q] - cz;
+      const double dd = dx * dx + dy * dy + dz * dz;
+      if (dd > R2) continue;
+      if (cnt == kCandCap) return kArmCapacity;
+      int j = cnt++;
+      while (j > 0 && cd[j - 1] > dd) { cd[j] = cd[j - 1]; cid[j] = cid[j - 1]; --j; }
+      cd[j] = dd;
+      cid[j] = q;
+      continue;
+    }
+    double lb = 0.0;
+    {
+      const double qv[3] = {cx, cy, cz};
+      for (int a = 0; a < 3; ++a) {
+        const double g = fmax(fmax((double)t.lo[a] - qv[a], qv[a] - (double)t.hi[a]), 0.0);
+        lb += g * g;
+      }
+    }
+    if (lb * (1.0 - 1e-6) > R2) continue;
+    if (top + 2 > kDStack) return kArmCapacity;
+    stack[top++] = t.left;
+    stack[top++] = t.right;
+  }
+  if (cnt < k) return kArmInternal;
+  // partition around the k-th approximate distance
+  const double tk = cd[k - 1];
+  int below = 0, band0 = -1, band1 = -1;
+  for (int i = 0; i < cnt; ++i) {
+    if (cd[i] < tk - 2.0 * ed) below = i + 1;
+    else if (cd[i] <= tk + 2.0 * ed) { if (band0 < 0) band0 = i; band1 = i; }
+  }
+  int nsel = 0;
+  for (int i = 0; i < below; ++i) G[nsel++] = cid[i];
+  uint32_t cut_point;
+  if (band0 == band1) {  // the k-th is isolated
+    G[nsel++] = cid[band0];
+    cut_point = cid[band0];
+  } else {
+    // exact order of the band by (distance, id)
+    int nb = band1 - band0 + 1;
+    uint32_t* B = cid + band0;
+    for (int a = 1; a < nb; ++a) {
+      const uint32_t x = B[a];
+      int b = a;
+      while (b > 0) {
+        const int s = dist_cmp_exact(c, mb.T, mb.ts, B[b - 1], x);
+        if (s < 0 || (s == 0 && B[b - 1] < x)) break;
+        B[b] = B[b - 1];
+        --b;
+      }
+      B[b] = x;
+    }
+    const int need = k - below;  // >= 1
+    cut_point = B[need - 1];
+    // strictly below the cutoff, then the least ids of the shell
+    int j = 0;
+    while (j < nb && dist_cmp_exact(c, mb.T, mb.ts, B[j], cut_point) < 0) G[nsel++] = B[j++];
+    while (nsel < k) G[nsel++] = B[j++];  // shell members in id order
+  }
+  for (int a = 1; a < k; ++a) {
+    const uint32_t x = G[a];
+    int b = a;
+    while (b > 0 && G[b - 1] > x) { G[b] = G[b - 1]; --b; }
+    G[b] = x;
+  }
+  // cutoff versus beta(F) = |T0 - centre|^2
+  bool on_sphere = false;
+  for (int j = 0; j < mb.ts; ++j) on_sphere |= mb.T[j] == cut_point;
+  if (on_sphere) {
+    *cut_below = 0;
+  } else {
+    const int s = dist_cmp_exact(c, mb.T, mb.ts, cut_point, mb.T[0]);
+    if (s > 0) return kArmInternal;
+    *cut_below = s < 0 ? 1 : 0;
+  }
+  return kArmOk;
+}
+
+__global__ void __launch_bounds__(128)
+k_descent(DescentParams d, uint32_t narms, const uint32_t* __restrict__ fam_event,
+          const uint32_t* __restrict__ arm_family, const uint8_t* __restrict__ arm_local, const EvRec* __restrict__ ev,
+          uint32_t* __restrict__ term, uint8_t* __restrict__ status, unsigned long long* __restrict__ stats) {
+  const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= narms) return;
+  const EvRec e = ev[fam_event[arm_family[a]]];
+  const uint32_t removed = e.ids[arm_local[a]];
+  uint32_t F[kMaxFacet + 1];
+  int k = event_facet(e, F);
+  {
+    int w = 0;
+    for (int j = 0; j < k; ++j)
+      if (F[j] != removed) F[w++] = F[j];
+    k = w;
+  }
+  const Cloud c{d.px, d.py, d.pz, d.S};
+  unsigned long long steps = 0;
+  uint8_t st = kArmSteps;
+  uint32_t res = kInvalid32;
+  for (int step = 0; step < kDescentSteps; ++step) {
+    const uint32_t h = probe_facet(d, F, k);
+    if (h != kInvalid32) {
+      res = h;
+      st = kArmOk;
+      break;
+    }
+    ++steps;
+    Mini mb;
+    if (!facet_miniball(c, F, k, mb)) { st = kArmInternal; break; }
+    uint32_t G[kMaxFacet];
+    int cut_below = 0;
+    const int s = topk_choice(d, c, mb, k, G, &cut_below);
+    if (s != kArmOk) { st = (uint8_t)s; break; }
+    bool same = true;
+    for (int j = 0; j < k; ++j) same &= G[j] == F[j];
+    if (same) { st = kArmUnresolved; break; }
+    if (!cut_below) {  // beta(G) <= cutoff = beta(F): the decrease must be strict
+      Mini mg;
+      if (!facet_miniball(c, G, k, mg)) { st = kArmInternal; break; }
+      double glo, ghi, flo, fhi;
+      if (!flevel(mg.fs, glo, ghi)) exact_level_fp(c, mg.T, mg.ts, glo, ghi);
+      if (!flevel(mb.fs, flo, fhi)) exact_level_fp(c, mb.T, mb.ts, flo, fhi);
+      if (!(ghi < flo) && level_cmp_exact(c, mg.T, mg.ts, mb.T, mb.ts) >= 0) { st = kArmPlateau; break; }
+    }
+    for (int j = 0; j < k; ++j) F[j] = G[j];
+  }
+  term[a] = res;
+  status[a] = st;
+  atomicAdd(stats, steps);
+}
+
+}  // namespace
+
+// ---- host state ---------------------------------------------------------------------
+struct HierState {
+  std::vector<void*> allocs;
+  uint64_t cap_events = 0, cap_arms = 0, cap_births = 0, cap_slots = 0;
+  // device
+  EvRec* ev_raw = nullptr;
+  EvRec* ev = nullptr;          // facade order
+  double* lmid_raw = nullptr;
+  double* lerr_raw = nullptr;
+  double* lmid = nullptr;
+  double* lerr = nullptr;
+  uint64_t* key = nullptr;
+  uint32_t* order0 = nullptr;
+  uint32_t* order1 = nullptr;
+  uint32_t* perm = nullptr;
+  double* pre_hi = nullptr;
+  double* suf_lo = nullptr;
+  double* bsum = nullptr;
+  uint32_t* ubsum = nullptr;
+  uint32_t* uncertain = nullptr;
+  uint8_t* eqprev = nullptr;
+  uint32_t* lclass = nullptr;   // level class per facade index
+  uint32_t* rank_order = nullptr;
+  uint32_t* counters = nullptr; // [0] diag, [1] uncertain, [2] err, [3..18] rank histogram
+  uint32_t* radix_counts = nullptr;
+  uint32_t* bfac = nullptr;
+  uint32_t* slots = nullptr;
+  uint32_t* fam_event = nullptr;
+  uint32_t* arm_family = nullptr;
+  uint8_t* arm_local = nullptr;
+  uint32_t* term = nullptr;
+  uint8_t* arm_status = nullptr;
+  unsigned long long* dstats = nullptr;
+  // host results
+  uint32_t n = 0, K = 0, keff = 0;
+  int S = 0;
+  uint64_t events = 0, diagnostics = 0;
+  std::vector<EvRec> h_ev;
+  std::vector<uint32_t> h_class;
+  std::vector<double> h_px, h_py, h_pz;
+  std::vector<ehgp_journal_batch> jbatches;
+  std::vector<ehgp_role_record> roles;
+  std::vector<ehgp_family_record> families;
+  std::vector<uint32_t> arm_removed;
+  std::vector<ehgp_forest_node> nodes;
+  std::vector<uint32_t> children;
+  std::vector<ehgp_forest_birth> births;
+  std::vector<ehgp_forest_binding> bindings;
+  std::vector<ehgp_forest_saddle> saddles;
+  std::vector<ehgp_forest_group> groups;
+  std::vector<ehgp_forest_batch> fbatches;
+  std::vector<ehgp_forest_root> roots;
+  uint32_t decision = EHGP_ERR_NOT_BUILT;
+  double ms_device = 0, ms_forest = 0, ms_descent = 0;
+  uint64_t descent_steps = 0, arms = 0, exact_boundaries = 0;
+};
+
+void hier_free(Ctx& ctx) {
+  if (!ctx.hier) return;
+  for (void* p : ctx.hier->allocs) cudaFree(p);
+  delete ctx.hier;
+  ctx.hier = nullptr;
+}
+
+namespace {
+
+template <class T>
+cudaError_t halloc(HierState& h, T** p, uint64_t count) {
+  void* q = nullptr;
+  const cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 16);
+  if (e != cudaSuccess) return e;
+  h.allocs.push_back(q);
+  *p = (T*)q;
+  return cudaSuccess;
+}
+
+void hfree_all(HierState& h) {
+  for (void* p : h.allocs) cudaFree(p);
+  h.allocs.clear();
+  h.cap_events = h.cap_arms = h.cap_births = h.cap_slots = 0;
+}
+
+cudaError_t ensure_events(HierState& h, uint64_t m) {
+  if (m <= h.cap_events && h.cap_events) return cudaSuccess;
+  hfree_all(h);
+  const uint64_t cap = m + m / 8 + 1024;
+  cudaError_t e;
+#define HA(p, c) if ((e = halloc(h, &(p), (c))) != cudaSuccess) return e
+  HA(h.ev_raw, cap);
+  HA(h.ev, cap);
+  HA(h.lmid_raw, cap);
+  HA(h.lerr_raw, cap);
+  HA(h.lmid, cap);
+  HA(h.lerr, cap);
+  HA(h.key, cap);
+  HA(h.order0, cap);
+  HA(h.order1, cap);
+  HA(h.perm, cap);
+  HA(h.pre_hi, cap);
+  HA(h.suf_lo, cap);
+  HA(h.bsum, cap / 1024 + 2);
+  HA(h.ubsum, cap / 1024 + 2);
+  HA(h.uncertain, 1u << 20);
+  HA(h.eqprev, cap);
+  HA(h.lclass, cap);
+  HA(h.rank_order, cap);
+  HA(h.counters, 32);
+  HA(h.radix_counts, 256ull * ((cap + kRadixTile - 1) / kRadixTile) + 256);
+  HA(h.bfac, cap * kMaxFacet);
+  HA(h.fam_event, cap);
+  HA(h.dstats, 4);
+  const uint64_t arms = 4 * cap;
+  HA(h.arm_family, arms);
+  HA(h.arm_local, arms);
+  HA(h.term, arms);
+  HA(h.arm_status, arms);
+  uint64_t slots = 1;
+  while (slots < 2 * cap + 1024) slots <<= 1;
+  HA(h.slots, slots);
+#undef HA
+  h.cap_events = cap;
+  h.cap_arms = arms;
+  h.cap_slots = slots;
+  return cudaSuccess;
+}
+
+// Exact facade order of events within an uncertain run: (level, rank, interior, support).
+struct HostCmp {
+  const Cloud* c;
+  bool less(const EvRec& a, const EvRec& b, int* lev) const {
+    const int s = level_cmp_exact(*c, a.ids, (int)a.size, b.ids, (int)b.size);
+    if (lev) *lev = s;
+    if (s != 0) return s < 0;
+    if (a.rank != b.rank) return a.rank < b.rank;
+    const uint32_t m = std::min(a.nint, b.nint);
+    for (uint32_t i = 0; i < m; ++i)
+      if (a.iids[i] != b.iids[i]) return a.iids[i] < b.iids[i];
+    if (a.nint != b.nint) return a.nint < b.nint;
+    const uint32_t ms = std::min(a.size, b.size);
+    for (uint32_t i = 0; i < ms; ++i)
+      if (a.ids[i] != b.ids[i]) return a.ids[i] < b.ids[i];
+    return a.size < b.size;
+  }
+};
+
+void scan_minmax(cudaStream_t st, uint32_t m, const double* mid, const double* err, double* out, double* bsum,
+                 bool forward_max, uint64_t* launches) {
+  const uint32_t nb = nblk(m, 1024);
+  if (forward_max) {
+    k_scan_blocks<<<nb, 256, 0, st>>>(m, mid, err, 1.0, 0, out, bsum, OpMax{}, -INFINITY);
+    k_scan_carry<<<1, 1, 0, st>>>(nb, bsum, OpMax{}, -INFINITY);
+    k_scan_apply<<<nblk(m, kT), kT, 0, st>>>(m, 0, out, bsum, OpMax{});
+  } else {
+    k_scan_blocks<<<nb, 256, 0, st>>>(m, mid, err, -1.0, 1, out, bsum, OpMin{}, INFINITY);
+    k_scan_carry<<<1, 1, 0, st>>>(nb, bsum, OpMin{}, INFINITY);
+    k_scan_apply<<<nblk(m, kT), kT, 0, st>>>(m, 1, out, bsum, OpMin{});
+  }
+  *launches += 3;
+}
+
+}  // namespace
+
+int hier_run(Ctx& ctx, uint32_t K) {
+  if (!ctx.hier) ctx.hier = new HierState();
+  HierState& h = *ctx.hier;
+  const uint32_t n = (uint32_t)ctx.built_n;
+  cudaStream_t st = ctx.stream;
+  LbvhBuffers& b = ctx.lb;
+  GeomBuffers& g = ctx.gb;
+  uint64_t launches = 0;
+  h.decision = EHGP_ERR_NOT_BUILT;
+  h.n = n;
+  h.K = K;
+  h.keff = K < n ? K : n;
+  if (K == 0 || K > 10) return abi_fail(&ctx, EHGP_ERR_INVALID_ARGUMENT, "K_max must be in [1, 10]");
+  // supports for this K
+  uint32_t np = 0, nh = 0;
+  if (!(ctx.pb.K == K && ctx.pb.witness_ready)) {  // pair supports of this cloud and K
+    const int s = pairs_run(ctx, K, &np);
+    if (s != EHGP_OK) return s;
+  }
+  np = ctx.pb.count;
+  if (ctx.hb.K != K) {
+    const int s = higher_run(ctx, K, &nh);
+    if (s != EHGP_OK) return s;
+  }
+  nh = ctx.hb.count;
+  const auto t0 = std::chrono::steady_clock::now();
+  cudaEventRecord(ctx.ev0, st);
+  const uint64_t total = (uint64_t)np + nh;
+  cudaError_t e = ensure_events(h, total + 1);
+  if (e != cudaSuccess) return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "hierarchy buffers do not fit the device");
+  cudaMemsetAsync(h.counters, 0, 32 * sizeof(uint32_t), st);
+  cudaMemsetAsync(h.dstats, 0, 4 * sizeof(unsigned long long), st);
+  if (total)
+    k_ev_build<<<nblk(total, kT), kT, 0, st>>>(np, nh, (const PairRecD*)ctx.pb.sorted, (const HigherRecD*)ctx.hb.sorted,
+                                                b.px, b.py, b.pz, g.scale, h.ev_raw, h.lmid_raw, h.lerr_raw, h.key,
+                                                h.counters);
+  ++launches;
+  uint32_t hc[2] = {0, 0};
+  cudaMemcpyAsync(hc, h.counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "hierarchy events");
+  h.diagnostics = hc[0];
+  const uint32_t m = (uint32_t)(total - hc[0]);
+  h.events = m;
+  // facade order by the FP64 level midpoints (diagnostics sort last)
+  RadixScratch rs{h.radix_counts, ctx.radix.state, (uint32_t)((h.cap_events + kRadixTile - 1) / kRadixTile)};
+  if (total) {
+    {
+      std::vector<uint32_t> iota(total);
+      std::iota(iota.begin(), iota.end(), 0u);
+      cudaMemcpyAsync(h.order0, iota.data(), total * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
+      cudaStreamSynchronize(st);
+    }
+    const IndirectKey stages[1] = {{h.key, 0}};
+    const int bits[1] = {64};
+    const int passes = radix_sort_indirect(st, (uint32_t)total, h.order0, h.order1, stages, bits, 1, rs, &launches);
+    k_ev_gather<<<nblk(total, kT), kT, 0, st>>>((uint32_t)total, h.order0, h.order1, ctx.radix.state, passes, h.ev_raw,
+                                                 h.lmid_raw, h.lerr_raw, h.ev, h.lmid, h.lerr, h.perm);
+    ++launches;
+  }
+  // copy the cloud for host-side exact tie resolution
+  h.h_px.resize(n);
+  h.h_py.resize(n);
+  h.h_pz.resize(n);
+  cudaMemcpyAsync(h.h_px.data(), b.px, n * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(h.h_py.data(), b.py, n * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(h.h_pz.data(), b.pz, n * sizeof(double), cudaMemcpyDeviceToHost, st);
+  int scale_h[4];
+  cudaMemcpyAsync(scale_h, g.scale, sizeof(scale_h), cudaMemcpyDeviceToHost, st);
+  cudaMemsetAsync(h.eqprev, 0, m + 1, st);
+  uint32_t unc = 0;
+  if (m > 1) {
+    scan_minmax(st, m, h.lmid, h.lerr, h.pre_hi, h.bsum, true, &launches);
+    scan_minmax(st, m, h.lmid, h.lerr, h.suf_lo, h.bsum, false, &launches);
+    k_uncertain<<<nblk(m, kT), kT, 0, st>>>(m, h.pre_hi, h.suf_lo, h.uncertain, 1u << 20, h.counters + 1);
+    ++launches;
+    cudaMemcpyAsync(&unc, h.counters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+  }
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "hierarchy facade order");
+  h.S = scale_h[0];
+  if (unc > (1u << 20)) return abi_fail(&ctx, EHGP_ERR_CAPACITY, "too many uncertain level boundaries in the facade");
+  if (unc) {
+    std::vector<uint32_t> list(unc);
+    cudaMemcpy(list.data(), h.uncertain, unc * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    std::sort(list.begin(), list.end());
+    const Cloud hc_cloud{h.h_px.data(), h.h_py.data(), h.h_pz.data(), h.S};
+    HostCmp cmp{&hc_cloud};
+    std::vector<uint8_t> eq;
+    for (size_t i = 0; i < list.size();) {
+      const uint32_t s0 = list[i] - 1;
+      uint32_t s1 = list[i];
+      size_t j = i + 1;
+      while (j < list.size() && list[j] == s1 + 1) s1 = list[j++];
+      const uint32_t len = s1 - s0 + 1;
+      std::vector<EvRec> run(len);
+      cudaMemcpy(run.data(), h.ev + s0, len * sizeof(EvRec), cudaMemcpyDeviceToHost);
+      std::sort(run.begin(), run.end(), [&](const EvRec& a, const EvRec& b2) { return cmp.less(a, b2, nullptr); });
+      eq.assign(len, 0);
+      for (uint32_t t = 1; t < len; ++t)
+        eq[t] = level_cmp_exact(hc_cloud, run[t - 1].ids, (int)run[t - 1].size, run[t].ids, (int)run[t].size) == 0;
+      cudaMemcpy(h.ev + s0, run.data(), len * sizeof(EvRec), cudaMemcpyHostToDevice);
+      cudaMemcpy(h.eqprev + s0, eq.data(), len, cudaMemcpyHostToDevice);
+      i = j;
+    }
+  }
+  // level classes
+  if (m) {
+    uint32_t* flag = h.order1;  // scratch
+    k_level_class<<<nblk(m, kT), kT, 0, st>>>(m, h.eqprev, flag);
+    const uint32_t nb = nblk(m, 1024);
+    k_sum_blocks<<<nb, 256, 0, st>>>(m, flag, h.lclass, h.ubsum);
+    k_sum_carry<<<1, 1, 0, st>>>(nb, h.ubsum);
+    k_sum_apply<<<nblk(m, kT), kT, 0, st>>>(m, h.lclass, h.ubsum, 1);
+    launches += 4;
+  }
+  // stable partition by closed rank
+  uint32_t hist[16] = {0};
+  int rpasses = 0;
+  if (m) {
+    k_rank_key<<<nblk(m, kT), kT, 0, st>>>(m, h.ev, h.key, h.order0, h.counters + 3);
+    const IndirectKey stages[1] = {{h.key, 0}};
+    const int bits[1] = {8};
+    rpasses = radix_sort_indirect(st, m, h.order0, h.order1, stages, bits, 1, rs, &launches);
+    k_rank_gather<<<nblk(m, kT), kT, 0, st>>>(m, h.order0, h.order1, ctx.radix.state, rpasses, h.rank_order);
+    launches += 2;
+    cudaMemcpyAsync(hist, h.counters + 3, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+  }
+  // host copies of the facade (events and level classes)
+  h.h_ev.resize(m);
+  h.h_class.resize(m);
+  std::vector<uint32_t> rank_order(m);
+  if (m) {
+    cudaMemcpyAsync(h.h_ev.data(), h.ev, (uint64_t)m * sizeof(EvRec), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(h.h_class.data(), h.lclass, (uint64_t)m * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(rank_order.data(), h.rank_order, (uint64_t)m * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+  }
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "hierarchy facade");
+  if (h.diagnostics) {
+    h.decision = EHGP_ERR_DEGENERATE;
+    return abi_fail(&ctx, EHGP_ERR_DEGENERATE,
+                    "relevant extra-shell diagnostics: the Morse event journal is not built");
+  }
+  const uint32_t keff = h.keff;
+  // rank segments: rb[r] = first position of rank r in rank_order
+  uint64_t rb[18] = {0};
+  for (int r = 0; r < 16; ++r) rb[r + 1] = rb[r] + hist[r];
+  // births (orders 2..keff): handle n + (position - rb[2])
+  const uint64_t nb_higher = rb[keff + 1 > 16 ? 16 : keff + 1] - rb[2];
+  if (nb_higher) {
+    cudaMemsetAsync(h.slots, 0xff, h.cap_slots * sizeof(uint32_t), st);
+    k_birth_insert<<<nblk(nb_higher, kT), kT, 0, st>>>((uint32_t)nb_higher, n, (uint32_t)rb[2], h.rank_order, h.ev,
+                                                       h.bfac, h.slots, (uint32_t)(h.cap_slots - 1), h.counters + 2);
+    ++launches;
+  }
+  // families: saddle events of ranks 2..keff+1 in rank-partition order; arms per support point
+  const uint64_t fam_lo = rb[2], fam_hi = rb[std::min<uint32_t>(keff + 2, 16)];
+  const uint64_t nfam = fam_hi - fam_lo;
+  std::vector<uint32_t> fam_event(nfam), arm_family, arm_off(nfam + 1, 0);
+  std::vector<uint8_t> arm_local;
+  for (uint64_t f = 0; f < nfam; ++f) {
+    fam_event[f] = rank_order[fam_lo + f];
+    const uint32_t sz = h.h_ev[fam_event[f]].size;
+    arm_off[f + 1] = arm_off[f] + sz;
+  }
+  const uint64_t narms = arm_off[nfam];
+  if (narms > h.cap_arms) return abi_fail(&ctx, EHGP_ERR_CAPACITY, "strict arms exceed the hierarchy buffers");
+  arm_family.resize(narms);
+  arm_local.resize(narms);
+  for (uint64_t f = 0; f < nfam; ++f)
+    for (uint32_t j = 0; j < arm_off[f + 1] - arm_off[f]; ++j) {
+      arm_family[arm_off[f] + j] = (uint32_t)f;
+      arm_local[arm_off[f] + j] = (uint8_t)j;
+    }
+  std::vector<uint32_t> term(narms);
+  std::vector<uint8_t> astat(narms);
+  if (narms) {
+    cudaMemcpyAsync(h.fam_event, fam_event.data(), nfam * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(h.arm_family, arm_family.data(), narms * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(h.arm_local, arm_local.data(), narms, cudaMemcpyHostToDevice, st);
+    DescentParams dp{n, 2 * n - 2, g.tnodes, b.px, b.py, b.pz, h.S, h.slots, (uint32_t)(h.cap_slots - 1), h.bfac,
+                     (uint32_t)nb_higher};
+    cudaEventRecord(ctx.evk0, st);
+    k_descent<<<nblk(narms, 128), 128, 0, st>>>(dp, (uint32_t)narms, h.fam_event, h.arm_family, h.arm_local, h.ev,
+                                                h.term, h.arm_status, h.dstats);
+    cudaEventRecord(ctx.evk1, st);
+    ++launches;
+    cudaMemcpyAsync(term.data(), h.term, narms * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(astat.data(), h.arm_status, narms, cudaMemcpyDeviceToHost, st);
+  }
+  uint32_t herr = 0;
+  unsigned long long dsteps = 0;
+  cudaMemcpyAsync(&herr, h.counters + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&dsteps, h.dstats, sizeof(dsteps), cudaMemcpyDeviceToHost, st);
+  cudaEventRecord(ctx.ev1, st);
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "strict-arm descent");
+  {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx.ev0, ctx.ev1);
+    h.ms_device = ms;
+    if (narms) {
+      cudaEventElapsedTime(&ms, ctx.evk0, ctx.evk1);
+      ctx.kernel_ms = ms;
+      h.ms_descent = ms;
+    }
+  }
+  h.descent_steps = dsteps;
+  h.arms = narms;
+  h.exact_boundaries = unc;
+  if (herr) return abi_fail(&ctx, EHGP_ERR_CAPACITY, "the birth facet table is full");
+  for (uint64_t a = 0; a < narms; ++a) {
+    if (astat[a] == kArmOk) continue;
+    static const char* msg[] = {"", "a strict arm descent is unresolved", "a strict arm descent met a plateau",
+                                "a strict arm descent exceeded its ball-query capacity",
+                                "a strict arm descent exceeded its step budget",
+                                "a strict arm descent found no consistent exact miniball or top-k"};
+    h.decision = astat[a] == kArmCapacity ? EHGP_ERR_CAPACITY : EHGP_ERR_DEGENERATE;
+    return abi_fail(&ctx, (int)h.decision, msg[astat[a] < 6 ? astat[a] : 5]);
+  }
+  // ---- host: journal, seeds and the forest journal, order by order
+  const auto t1 = std::chrono::steady_clock::now();
+  h.jbatches.clear();
+  h.roles.clear();
+  h.families.clear();
+  h.arm_removed.clear();
+  h.nodes.clear();
+  h.children.clear();
+  h.births.clear();
+  h.bindings.clear();
+  h.saddles.clear();
+  h.groups.clear();
+  h.fbatches.clear();
+  h.roots.clear();
+  const uint64_t birth_count = n + nb_higher;
+  std::vector<uint32_t> parent(birth_count), border(birth_count, 0), rroot(birth_count, kInvalid32);
+  std::vector<uint8_t> active(birth_count, 0);
+  std::iota(parent.begin(), parent.end(), 0u);
+  auto find = [&](uint32_t x) {
+    while (parent[x] != x) x = parent[x];
+    return x;
+  };
+  std::vector<uint64_t> carriers_of(keff + 2, 0), reduced_of(keff + 2, 0);
+  // journal and forest, order by order
+  std::vector<uint32_t> fam_index_of(nfam);  // family position in the rank partition -> journal family index
+  uint32_t role_count = 0;
+  for (uint32_t k = 1; k <= keff; ++k) {
+    // births of order k: singletons (k = 1) or rank-k events; saddles: rank-(k+1) events
+    const uint64_t b_lo = k == 1 ? 0 : rb[k], b_hi = k == 1 ? 0 : rb[k + 1];
+    const uint64_t s_lo = rb[k + 1], s_hi = rb[k + 2 > 16 ? 16 : k + 2];
+    uint64_t bi = b_lo, si = s_lo;
+    bool singles = k == 1;
+    while (singles || bi < b_hi || si < s_hi) {
+      // next batch: the least level class among the heads (singletons: level 0 first)
+      const uint32_t cls_b = bi < b_hi ? h.h_class[rank_order[bi]] : kInvalid32;
+      const uint32_t cls_s = si < s_hi ? h.h_class[rank_order[si]] : kInvalid32;
+      uint32_t cls;
+      uint32_t lev;
+      if (singles) {
+        cls = kInvalid32;
+        lev = kInvalid32;
+      } else {
+        cls = std::min(cls_b, cls_s);
+        lev = cls_b <= cls_s ? rank_order[bi] : rank_order[si];
+      }
+      const uint32_t bidx = (uint32_t)h.jbatches.size();
+      ehgp_journal_batch jb{k, lev, role_count, 0, 0, 0};
+      ehgp_forest_batch fb{};
+      fb.order = k;
+      fb.level_event = lev;
+      fb.pre_carriers = (uint32_t)carriers_of[k];
+      fb.pre_roots = (uint32_t)reduced_of[k];
+      // roles in projection order: births and saddles of this class
+      struct Role {
+        uint32_t proj, role, fi, pos;
+      };
+      std::vector<Role> batch_roles;
+      if (singles) {
+        for (uint32_t p = 0; p < n; ++p) batch_roles.push_back({p, 0, kInvalid32, p});
+      } else {
+        while (bi < b_hi && h.h_class[rank_order[bi]] == cls) {
+          batch_roles.push_back({n + rank_order[bi], 0, rank_order[bi], (uint32_t)(bi - rb[2])});
+          ++bi;
+        }
+        while (si < s_hi && h.h_class[rank_order[si]] == cls) {
+          batch_roles.push_back({n + rank_order[si], 1, rank_order[si], (uint32_t)(si - fam_lo)});
+          ++si;
+        }
+        std::sort(batch_roles.begin(), batch_roles.end(), [](const Role& x, const Role& y) {
+          return x.proj != y.proj ? x.proj < y.proj : x.role < y.role;
+        });
+      }
+      singles = false;
+      // saddle families of this batch (journal order)
+      struct Arm {
+        uint32_t seed, carrier, prior;
+      };
+      std::vector<uint32_t> fam_ids;
+      for (const Role& r : batch_roles) {
+        h.roles.push_back({bidx, r.proj, r.role});
+        if (r.role == 0) ++jb.birth_roles;
+        else ++jb.saddle_roles;
+        if (r.role == 1) {
+          const EvRec& ev = h.h_ev[r.fi];
+          const uint32_t fidx = (uint32_t)h.families.size();
+          fam_index_of[r.pos] = fidx;
+          h.families.push_back({r.fi, r.proj, role_count + (uint32_t)(&r - batch_roles.data()), bidx, k,
+                                (uint32_t)h.arm_removed.size(), ev.size});
+          for (uint32_t j = 0; j < ev.size; ++j) h.arm_removed.push_back(ev.ids[j]);
+          fam_ids.push_back(r.pos);
+        }
+      }
+      jb.role_count = (uint32_t)batch_roles.size();
+      role_count += jb.role_count;
+      h.jbatches.push_back(jb);
+      // resolve arms against the pre-batch components
+      std::vector<std::vector<Arm>> sad(fam_ids.size());
+      for (size_t q = 0; q < fam_ids.size(); ++q) {
+        const uint32_t fpos = fam_ids[q];
+        const uint32_t fidx = fam_index_of[fpos];
+        for (uint64_t a = arm_off[fpos]; a < arm_off[fpos + 1]; ++a) {
+          if (term[a] >= birth_count || !active[term[a]])
+            return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "a strict arm descended to a minimum that is not yet born");
+          const uint32_t c0 = find(term[a]);
+          sad[q].push_back({h.families[fidx].arm_offset + (uint32_t)(a - arm_off[fpos]), c0, rroot[c0]});
+        }
+      }
+      // frozen-root quotient: transitive classes over the saddles' carriers
+      std::vector<uint32_t> cars;
+      for (auto& as : sad)
+        for (auto& a : as) cars.push_back(a.carrier);
+      std::sort(cars.begin(), cars.end());
+      cars.erase(std::unique(cars.begin(), cars.end()), cars.end());
+      std::vector<uint32_t> qp(cars.size());
+      std::iota(qp.begin(), qp.end(), 0u);
+      auto qi = [&](uint32_t x) { return (uint32_t)(std::lower_bound(cars.begin(), cars.end(), x) - cars.begin()); };
+      auto qf = [&](uint32_t x) {
+        while (qp[x] != x) x = qp[x] = qp[qp[x]];
+        return x;
+      };
+      for (auto& as : sad)
+        for (auto& a : as) {
+          const uint32_t x = qf(qi(as[0].carrier)), y = qf(qi(a.carrier));
+          if (x != y) qp[std::max(x, y)] = std::min(x, y);
+        }
+      // groups ordered by their least carrier; carriers ascending
+      std::vector<int32_t> group_of(cars.size(), -1);
+      struct Plan {
+        std::vector<uint32_t> carriers, priors, saddles;
+        uint32_t kind, created, result;
+      };
+      std::vector<Plan> plans;
+      for (uint32_t i = 0; i < cars.size(); ++i) {
+        const uint32_t r0 = qf(i);
+        if (group_of[r0] < 0) {
+          group_of[r0] = (int32_t)plans.size();
+          plans.push_back({});
+        }
+        Plan& p = plans[group_of[r0]];
+        p.carriers.push_back(cars[i]);
+        if (rroot[cars[i]] != kInvalid32) p.priors.push_back(rroot[cars[i]]);
+      }
+      for (size_t q = 0; q < sad.size(); ++q) plans[group_of[qf(qi(sad[q][0].carrier))]].saddles.push_back((uint32_t)q);
+      uint32_t pending = 0;
+      for (Plan& p : plans) {
+        std::sort(p.priors.begin(), p.priors.end());
+        if (std::adjacent_find(p.priors.begin(), p.priors.end()) != p.priors.end())
+          return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "a frozen carrier class repeats a reduced root");
+        if (p.priors.size() == 1) {
+          p.kind = 1;
+          p.created = kInvalid32;
+          p.result = p.priors[0];
+        } else {
+          if (p.priors.empty() && k == 1) return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "an order-one group has no root");
+          p.kind = p.priors.empty() ? 0 : 2;
+          p.created = (uint32_t)h.nodes.size() + pending++;
+          p.result = p.created;
+        }
+      }
+      fb.saddle_offset = (uint32_t)h.saddles.size();
+      fb.group_offset = (uint32_t)h.groups.size();
+      std::vector<ehgp_forest_node> gnodes;
+      for (Plan& p : plans) {
+        const uint32_t g_soff = (uint32_t)h.saddles.size();
+        const uint32_t gidx = (uint32_t)h.groups.size();
+        for (uint32_t q : p.saddles) {
+          const uint32_t fidx = fam_index_of[fam_ids[q]];
+          const uint32_t arm_o = (uint32_t)h.bindings.size();
+          std::vector<uint32_t> cs, ps;
+          for (const Arm& a : sad[q]) {
+            h.bindings.push_back({a.seed, fidx, a.carrier, a.prior});
+            cs.push_back(a.carrier);
+            if (a.prior != kInvalid32) ps.push_back(a.prior);
+          }
+          std::sort(cs.begin(), cs.end());
+          cs.erase(std::unique(cs.begin(), cs.end()), cs.end());
+          std::sort(ps.begin(), ps.end());
+          ps.erase(std::unique(ps.begin(), ps.end()), ps.end());
+          h.saddles.push_back({fidx, h.families[fidx].event, bidx, arm_o, (uint32_t)sad[q].size(), (uint32_t)cs.size(),
+                               (uint32_t)(cs.size() - ps.size()), (uint32_t)ps.size(), gidx});
+        }
+        const uint32_t ccnt = p.kind == 2 ? (uint32_t)p.priors.size() : 0u;
+        h.groups.push_back({bidx, g_soff, (uint32_t)h.saddles.size() - g_soff, (uint32_t)p.carriers.size(),
+                            (uint32_t)(p.carriers.size() - p.priors.size()), (uint32_t)p.priors.size(),
+                            (uint32_t)h.children.size(), ccnt, p.created, p.result, p.kind});
+        if (p.kind != 1)
+          gnodes.push_back({k, lev, p.kind == 0 ? 1u : 2u, (uint32_t)h.children.size(), ccnt, kInvalid32, gidx});
+        if (p.kind == 2) h.children.insert(h.children.end(), p.priors.begin(), p.priors.end());
+      }
+      h.nodes.insert(h.nodes.end(), gnodes.begin(), gnodes.end());
+      // births of this batch
+      fb.birth_offset = (uint32_t)h.births.size();
+      std::vector<uint32_t> new_births;
+      for (const Role& r : batch_roles) {
+        if (r.role != 0) continue;
+        const uint32_t handle = (uint32_t)h.births.size();
+        uint32_t node = kInvalid32;
+        if (k == 1) {
+          node = (uint32_t)h.nodes.size();
+          h.nodes.push_back({1, kInvalid32, 0, (uint32_t)h.children.size(), 0, handle, kInvalid32});
+        }
+        const uint32_t expect = k == 1 ? r.proj : n + r.pos;
+        if (expect != handle) return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "birth handles left the journal order");
+        h.births.push_back({r.proj, bidx, k, handle, node});
+        new_births.push_back(handle);
+      }
+      // commit: unions (least handle survives), reduced roots, then births
+      for (Plan& p : plans) {
+        uint32_t r0 = find(p.carriers.front());
+        uint32_t had_reduced = rroot[r0] != kInvalid32;
+        for (size_t i = 1; i < p.carriers.size(); ++i) {
+          const uint32_t r1 = find(p.carriers[i]);
+          if (r1 == r0) continue;
+          had_reduced += rroot[r1] != kInvalid32;
+          const uint32_t lo = std::min(r0, r1), hi = std::max(r0, r1);
+          parent[hi] = lo;
+          r0 = lo;
+          --carriers_of[k];
+        }
+        rroot[r0] = p.result;
+        reduced_of[k] = reduced_of[k] - had_reduced + 1;
+      }
+      for (uint32_t hnd : new_births) {
+        active[hnd] = 1;
+        border[hnd] = k;
+        rroot[hnd] = k == 1 ? h.births[hnd].order_one_node : kInvalid32;
+        ++carriers_of[k];
+        if (k == 1) ++reduced_of[k];
+      }
+      fb.birth_count = (uint32_t)new_births.size();
+      fb.saddle_count = (uint32_t)h.saddles.size() - fb.saddle_offset;
+      fb.group_count = (uint32_t)h.groups.size() - fb.group_offset;
+      fb.post_carriers = (uint32_t)carriers_of[k];
+      fb.post_roots = (uint32_t)reduced_of[k];
+      h.fbatches.push_back(fb);
+    }
+  }
+  for (uint64_t hnd = 0; hnd < birth_count; ++hnd)
+    if (active[hnd] && parent[hnd] == hnd && rroot[hnd] != kInvalid32)
+      h.roots.push_back({border[hnd], (uint32_t)hnd, rroot[hnd]});
+  std::sort(h.roots.begin(), h.roots.end(), [](const ehgp_forest_root& x, const ehgp_forest_root& y) {
+    return x.order != y.order ? x.order < y.order : x.node < y.node;
+  });
+  const auto t2 = std::chrono::steady_clock::now();
+  h.ms_forest = std::chrono::duration<double, std::milli>(t2 - t1).count();
+  (void)t0;
+  ctx.last_launches = launches;
+  ctx.last_ms = h.ms_device + h.ms_forest;
+  h.decision = EHGP_OK;
+  return EHGP_OK;
+}
+
+}  // namespace ehgp
+
+extern "C" {
+
+int ehgp_hierarchy(ehgp_ctx* ctx, uint32_t K, ehgp_hier_counts* counts) {
+  if (!ctx) return EHGP_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  ctx->last_error.clear();
+  if (ctx->poisoned) return ehgp::abi_fail(ctx, EHGP_ERR_POISONED, "the context is poisoned by an earlier CUDA failure");
+  if (ctx->built_n == 0) return ehgp::abi_fail(ctx, EHGP_ERR_NOT_BUILT, "ehgp_hierarchy needs a resident LBVH");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return ehgp::abi_cuda_fail(ctx, e, "cudaSetDevice");
+  if (!ctx->geom_ready) {
+    ehgp::geom_prepare(*ctx, (uint32_t)ctx->built_n);
+    if ((e = cudaGetLastError()) != cudaSuccess) return ehgp::abi_cuda_fail(ctx, e, "traversal preparation");
+  }
+  if (!ctx->scale_valid)
+    return ehgp::abi_fail(ctx, EHGP_ERR_NUMERIC_RANGE, "the cloud exceeds the exact fixed-point range");
+  cudaMemsetAsync(ctx->d_err, 0, sizeof(uint32_t), ctx->stream);
+  const int s = ehgp::hier_run(*ctx, K);
+  if (counts) {
+    std::memset(counts, 0, sizeof(*counts));
+    if (ctx->hier) {
+      const ehgp::HierState& h = *ctx->hier;
+      counts->events = h.events;
+      counts->diagnostics = h.diagnostics;
+      counts->journal_batches = h.jbatches.size();
+      counts->role_records = h.roles.size();
+      counts->families = h.families.size();
+      counts->arm_seeds = h.arm_removed.size();
+      counts->birth_records = h.births.size();
+      counts->nodes = h.nodes.size();
+      counts->children = h.children.size();
+      counts->arm_bindings = h.bindings.size();
+      counts->saddle_records = h.saddles.size();
+      counts->atomic_groups = h.groups.size();
+      counts->final_roots = h.roots.size();
+      counts->k_eff = h.keff;
+    }
+    counts->decision = (uint32_t)s;
+  }
+  return s;
+}
+
+int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out) {
+  if (!ctx || !out) return EHGP_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  if (!ctx->hier) return ehgp::abi_fail(ctx, EHGP_ERR_NOT_BUILT, "no hierarchy result is resident");
+  const ehgp::HierState& h = *ctx->hier;
+  auto cp = [](void* dst, const void* src, size_t bytes) {
+    if (dst && bytes) std::memcpy(dst, src, bytes);
+  };
+  if (out->events && !h.h_ev.empty()) cp(out->events, h.h_ev.data(), h.h_ev.size() * sizeof(ehgp::EvRec));
+  cp(out->journal_batches, h.jbatches.data(), h.jbatches.size() * sizeof(ehgp_journal_batch));
+  cp(out->roles, h.roles.data(), h.roles.size() * sizeof(ehgp_role_record));
+  cp(out->families, h.families.data(), h.families.size() * sizeof(ehgp_family_record));
+  cp(out->arm_removed, h.arm_removed.data(), h.arm_removed.size() * sizeof(uint32_t));
+  cp(out->nodes, h.nodes.data(), h.nodes.size() * sizeof(ehgp_forest_node));
+  cp(out->children, h.children.data(), h.children.size() * sizeof(uint32_t));
+  cp(out->births, h.births.data(), h.births.size() * sizeof(ehgp_forest_birth));
+  cp(out->bindings, h.bindings.data(), h.bindings.size() * sizeof(ehgp_forest_binding));
+  cp(out->saddles, h.saddles.data(), h.saddles.size() * sizeof(ehgp_forest_saddle));
+  cp(out->groups, h.groups.data(), h.groups.size() * sizeof(ehgp_forest_group));
+  cp(out->batches, h.fbatches.data(), h.fbatches.size() * sizeof(ehgp_forest_batch));
+  cp(out->roots, h.roots.data(), h.roots.size() * sizeof(ehgp_forest_root));
+  return EHGP_OK;
+}
+
+int ehgp_hier_stats(const ehgp_ctx* ctx, double* ms, uint64_t* stats) {
+  if (!ctx || !ctx->hier) return EHGP_ERR_INVALID_ARGUMENT;
+  const ehgp::HierState& h = *ctx->hier;
+  if (ms) {
+    ms[0] = h.ms_device;
+    ms[1] = h.ms_descent;
+    ms[2] = h.ms_forest;
+  }
+  if (stats) {
+    stats[0] = h.arms;
+    stats[1] = h.descent_steps;
+    stats[2] = h.exact_boundaries;
+    stats[3] = h.events;
+  }
+  return EHGP_OK;
+}
+
+int ehgp_event_level(ehgp_ctx* ctx, uint64_t event, uint64_t* num, uint64_t* den, int32_t* scale) {
+  if (!ctx || !num || !den) return EHGP_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  if (!ctx->hier || event >= ctx->hier->h_ev.size())
+    return ehgp::abi_fail(ctx, EHGP_ERR_INVALID_ARGUMENT, "no such facade event");
+  const ehgp::HierState& h = *ctx->hier;
+  const ehgp::EvRec& r = h.h_ev[event];
+  const ehgp::Cloud c{h.h_px.data(), h.h_py.data(), h.h_pz.data(), h.S};
+  ehgp::W A;
+  ehgp::WV N;
+  ehgp::exact_sphere(c, r.ids, (int)r.size, A, N);
+  using WL = ehgp::WL;
+  const WL x = ehgp::widen<36>(N.x), y = ehgp::widen<36>(N.y), z = ehgp::widen<36>(N.z), a = ehgp::widen<36>(A);
+  const WL nn = ehgp::wadd(ehgp::wadd(ehgp::wmul(x, x), ehgp::wmul(y, y)), ehgp::wmul(z, z));
+  const WL dd = ehgp::wmul(ehgp::wmul(a, a), WL::from_i128(4));
+  for (int i = 0; i < 36; ++i) {
+    num[i] = nn.w[i];
+    den[i] = dd.w[i];
+  }
+  if (scale) *scale = h.S;
+  return EHGP_OK;
+}
+
+}  // extern "C"

@@ -31,6 +31,7 @@
 //     at the cloud scale inside the bound.
 #include "ehgp_internal.cuh"
 #include "ehgp_exact.cuh"
+#include "ehgp_sphere.cuh"
 
 #include <algorithm>
 #include <array>
@@ -53,7 +54,6 @@ __host__ __device__ inline uint32_t nblocks(uint64_t n, int t) {
   const uint64_t b = (n + t - 1) / t;
   return b == 0 ? 1u : (uint32_t)b;
 }
-__device__ __forceinline__ uint64_t dbits(double v) { return (uint64_t)__double_as_longlong(v); }
 
 __device__ __forceinline__ TNode load_node(const TNode* __restrict__ tn, uint32_t i) {
   const float4* p = reinterpret_cast<const float4*>(tn + i);
@@ -93,78 +93,6 @@ struct SetPt {
 };
 
 __device__ __forceinline__ double ptmax(const SetPt& p) { return fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z))); }
-
-// ---- exact versions (832-bit integers at the cloud scale) --------------------------
-using W = WInt<13>;
-struct WV {
-  W x, y, z;
-};
-__device__ __forceinline__ W wdot(const WV& a, const WV& b) {
-  return wadd(wadd(wmul(a.x, b.x), wmul(a.y, b.y)), wmul(a.z, b.z));
-}
-__device__ __forceinline__ WV wcross(const WV& a, const WV& b) {
-  return {wsub(wmul(a.y, b.z), wmul(a.z, b.y)), wsub(wmul(a.z, b.x), wmul(a.x, b.z)),
-          wsub(wmul(a.x, b.y), wmul(a.y, b.x))};
-}
-__device__ __forceinline__ WV wscale(const W& s, const WV& a) { return {wmul(s, a.x), wmul(s, a.y), wmul(s, a.z)}; }
-__device__ __forceinline__ WV wvadd(const WV& a, const WV& b) { return {wadd(a.x, b.x), wadd(a.y, b.y), wadd(a.z, b.z)}; }
-
-struct Cloud {
-  const double* px;
-  const double* py;
-  const double* pz;
-  int S;
-  __device__ WV wdiff(uint32_t i, uint32_t j) const {
-    return {W::from_i128(fixed_of(dbits(px[i]), S) - fixed_of(dbits(px[j]), S)),
-            W::from_i128(fixed_of(dbits(py[i]), S) - fixed_of(dbits(py[j]), S)),
-            W::from_i128(fixed_of(dbits(pz[i]), S) - fixed_of(dbits(pz[j]), S))};
-  }
-};
-
-// Exact fallbacks, kept out of line so that the FP64 fast paths stay in registers.
-__device__ __noinline__ void tri_signs_exact(const Cloud& c, const uint32_t* id, int* sg) {
-  const WV w1 = c.wdiff(id[1], id[0]), w2 = c.wdiff(id[2], id[0]);
-  const W g11 = wdot(w1, w1), g12 = wdot(w1, w2), g22 = wdot(w2, w2);
-  sg[0] = g12.sign();
-  sg[1] = wsub(g11, g12).sign();
-  sg[2] = wsub(g22, g12).sign();
-  sg[3] = wsub(wmul(g11, g22), wmul(g12, g12)).sign();
-}
-
-__device__ __noinline__ void quad_signs_exact(const Cloud& c, const uint32_t* id, int* sg) {
-  const WV w1 = c.wdiff(id[1], id[0]), w2 = c.wdiff(id[2], id[0]), w3 = c.wdiff(id[3], id[0]);
-  const WV x23 = wcross(w2, w3), x31 = wcross(w3, w1), x12 = wcross(w1, w2);
-  const WV nn = wvadd(wvadd(wscale(wdot(w1, w1), x23), wscale(wdot(w2, w2), x31)), wscale(wdot(w3, w3), x12));
-  const W de = wdot(w1, x23);
-  const W m1 = wdot(nn, x23), m2 = wdot(nn, x31), m3 = wdot(nn, x12);
-  const W two = W::from_i128(2);
-  const W m0 = wsub(wmul(two, wmul(de, de)), wadd(wadd(m1, m2), m3));
-  sg[0] = de.sign();
-  sg[1] = m0.sign();
-  sg[2] = m1.sign();
-  sg[3] = m2.sign();
-  sg[4] = m3.sign();
-}
-
-// Exact sign of the side polynomial A |w - a|^2 - (w - a).N (before the orientation sign).
-__device__ __noinline__ int side_exact(const Cloud& c, const uint32_t* ids, int size, uint32_t w) {
-  const WV q = c.wdiff(w, ids[0]);
-  W val;
-  if (size == 3) {
-    const WV w1 = c.wdiff(ids[1], ids[0]), w2 = c.wdiff(ids[2], ids[0]);
-    const W g11 = wdot(w1, w1), g12 = wdot(w1, w2), g22 = wdot(w2, w2);
-    const W detG = wsub(wmul(g11, g22), wmul(g12, g12));
-    const WV n = wvadd(wscale(wmul(g22, wsub(g11, g12)), w1), wscale(wmul(g11, wsub(g22, g12)), w2));
-    val = wsub(wmul(detG, wdot(q, q)), wdot(q, n));
-  } else {
-    const WV w1 = c.wdiff(ids[1], ids[0]), w2 = c.wdiff(ids[2], ids[0]), w3 = c.wdiff(ids[3], ids[0]);
-    const WV x23 = wcross(w2, w3), x31 = wcross(w3, w1), x12 = wcross(w1, w2);
-    const W de = wdot(w1, x23);
-    const WV nn = wvadd(wvadd(wscale(wdot(w1, w1), x23), wscale(wdot(w2, w2), x31)), wscale(wdot(w3, w3), x12));
-    val = wsub(wmul(de, wdot(q, q)), wdot(q, nn));
-  }
-  return val.sign();
-}
 
 // A minimal support waiting for classification: side(w) = sgn * sign(A q - p.N)
 // with p = fl(w - a), q = fl(|p|^2); the FP value is decided outside +-bnd.

@@ -246,6 +246,7 @@ struct Ctx {
   uint32_t emst_rounds = 0;
   uint32_t emst_minima = 0;        // total per-round minima logged
   bool emst_ready = false;
+  struct HierState* hier = nullptr;  // direct hierarchy (ehgp_hier.cu)
 };
 
 // Allocation helper: records the bytes on ctx.
@@ -271,6 +272,10 @@ int pairs_run(Ctx& ctx, uint32_t K, uint32_t* out_count);
 // Triple/quad supports (ehgp_higher.cu)
 cudaError_t higher_alloc(Ctx& ctx);
 int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count);
+
+// Direct Morse hierarchy (ehgp_hier.cu)
+int hier_run(Ctx& ctx, uint32_t K);
+void hier_free(Ctx& ctx);
 
 }  // namespace ehgp
 

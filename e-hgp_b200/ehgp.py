@@ -58,7 +58,11 @@ class NumericRange(EhgpError):
     pass
 
 
-_ERRORS = {1: InvalidArgument, 2: DuplicatePoint, 3: CapacityError, 7: NumericRange}
+class DegenerateError(EhgpError):
+    """Relevant extra-shell diagnostics, or a strict-arm descent that cannot be certified."""
+
+
+_ERRORS = {1: InvalidArgument, 2: DuplicatePoint, 3: CapacityError, 6: DegenerateError, 7: NumericRange}
 
 
 class Limits(C.Structure):
@@ -106,6 +110,48 @@ HIGHER_RECORD = np.dtype([("size", "<u4"), ("ids", "<u4", 4), ("interior_count",
 assert HIGHER_RECORD.itemsize == 64
 
 
+class HierCounts(C.Structure):
+    _fields_ = [(f, C.c_uint64) for f in ("events", "diagnostics", "journal_batches", "role_records", "families",
+                                          "arm_seeds", "birth_records", "nodes", "children", "arm_bindings",
+                                          "saddle_records", "atomic_groups", "final_roots")] + \
+               [("decision", C.c_uint32), ("k_eff", C.c_uint32)]
+
+
+def _u4(*names):
+    return np.dtype([(nm, "<u4") for nm in names])
+
+
+# Record layouts of include/ehgp.h (direct Morse hierarchy).
+EVENT_RECORD = np.dtype([("support_size", "<u4"), ("support_ids", "<u4", 4), ("interior_count", "<u4"),
+                         ("closed_rank", "<u4"), ("interior_ids", "<u4", 9)])
+JOURNAL_BATCH = _u4("order", "level_event", "role_offset", "role_count", "birth_roles", "saddle_roles")
+ROLE_RECORD = _u4("batch", "projection", "role")
+FAMILY_RECORD = _u4("event", "projection", "role_record", "batch", "order", "arm_offset", "arm_count")
+FOREST_NODE = _u4("order", "level_event", "kind", "child_offset", "child_count", "birth_record", "atomic_group")
+FOREST_BIRTH = _u4("projection", "batch", "order", "handle", "order_one_node")
+FOREST_BINDING = _u4("arm_seed", "family", "carrier", "prior_root")
+FOREST_SADDLE = _u4("family", "event", "batch", "arm_offset", "arm_count", "carriers", "latent", "prior_roots",
+                    "group")
+FOREST_GROUP = _u4("batch", "saddle_offset", "saddle_count", "frozen", "latent", "prior_roots", "child_offset",
+                   "child_count", "created_node", "result_node", "kind")
+FOREST_BATCH = _u4("order", "level_event", "birth_offset", "birth_count", "saddle_offset", "saddle_count",
+                   "group_offset", "group_count", "pre_carriers", "pre_roots", "post_carriers", "post_roots")
+FOREST_ROOT = _u4("order", "handle", "node")
+ABSENT = 0xFFFFFFFF
+
+_HIER_FIELDS = [("events", EVENT_RECORD, "events"), ("journal_batches", JOURNAL_BATCH, "journal_batches"),
+                ("roles", ROLE_RECORD, "role_records"), ("families", FAMILY_RECORD, "families"),
+                ("arm_removed", np.dtype("<u4"), "arm_seeds"), ("nodes", FOREST_NODE, "nodes"),
+                ("children", np.dtype("<u4"), "children"), ("births", FOREST_BIRTH, "birth_records"),
+                ("bindings", FOREST_BINDING, "arm_bindings"), ("saddles", FOREST_SADDLE, "saddle_records"),
+                ("groups", FOREST_GROUP, "atomic_groups"), ("batches", FOREST_BATCH, "journal_batches"),
+                ("roots", FOREST_ROOT, "final_roots")]
+
+
+class HierOut(C.Structure):
+    _fields_ = [(name, C.c_void_p) for name, _, _ in _HIER_FIELDS]
+
+
 def limbs_to_int(a: np.ndarray) -> int:
     """Little-endian 64-bit limbs -> Python int."""
     v = 0
@@ -149,6 +195,10 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "ehgp_lbvh_build_noalloc": (C.c_int, [P, C.c_uint64, C.POINTER(LbvhOut), P]),
         "ehgp_lbvh_noalloc_max_points": (C.c_uint64, []),
         "ehgp_lbvh_noalloc_scratch_bytes": (C.c_uint64, []),
+        "ehgp_hierarchy": (C.c_int, [P, C.c_uint32, C.POINTER(HierCounts)]),
+        "ehgp_hier_copy": (C.c_int, [P, C.POINTER(HierOut)]),
+        "ehgp_event_level": (C.c_int, [P, C.c_uint64, P, P, C.POINTER(C.c_int32)]),
+        "ehgp_hier_stats": (C.c_int, [P, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -356,6 +406,46 @@ class Context:
         st = np.zeros(8, np.uint64)
         self._check(self.lib.ehgp_higher_stats(self._h, C.byref(ms), _ptr(st), 8))
         return ms.value, st
+
+    def hierarchy(self, K: int = 10, arrays: bool = True) -> dict:
+        """ehgp_hierarchy: facade, event journal, arm seeds and forest journal on the resident cloud.
+
+        Raises DegenerateError (EHGP_ERR_DEGENERATE) when relevant extra-shell
+        diagnostics stop the chain; `last_hier_counts` then holds the facade counts."""
+        cnt = HierCounts()
+        st = self.lib.ehgp_hierarchy(self._h, K, C.byref(cnt))
+        self.last_hier_counts = {f: getattr(cnt, f) for f, _ in HierCounts._fields_}
+        self._check(st)
+        out = dict(self.last_hier_counts)
+        if arrays:
+            bufs = {}
+            for name, dt, cf in _HIER_FIELDS:
+                bufs[name] = np.zeros(max(int(out[cf]), 1), dt)
+            ho = HierOut(*[_ptr(bufs[name]) for name, _, _ in _HIER_FIELDS])
+            self._check(self.lib.ehgp_hier_copy(self._h, C.byref(ho)))
+            for name, _, cf in _HIER_FIELDS:
+                out[name] = bufs[name][:int(out[cf])]
+        return out
+
+    def hier_stats(self) -> dict:
+        """Timing and work counters of the last hierarchy call."""
+        ms = np.zeros(3)
+        st = np.zeros(4, np.uint64)
+        self._check(self.lib.ehgp_hier_stats(self._h, _ptr(ms), _ptr(st)))
+        return {"device_ms": ms[0], "descent_ms": ms[1], "forest_ms": ms[2], "arms": int(st[0]),
+                "descent_steps": int(st[1]), "exact_boundaries": int(st[2]), "events": int(st[3])}
+
+    def event_level(self, event: int):
+        """Exact level of a facade event as a Fraction (cloud units)."""
+        from fractions import Fraction
+        num = np.zeros(36, np.uint64)
+        den = np.zeros(36, np.uint64)
+        S = C.c_int32()
+        self._check(self.lib.ehgp_event_level(self._h, event, _ptr(num), _ptr(den), C.byref(S)))
+        def signed(a):
+            v = limbs_to_int(a)
+            return v - (1 << (64 * 36)) if v >> (64 * 36 - 1) else v
+        return Fraction(signed(num), signed(den) << (2 * S.value))
 
     def k1_forest(self) -> dict:
         """ehgp_k1_forest on the last EMST: reference-layout compact forest arenas."""

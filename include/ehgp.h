@@ -279,6 +279,119 @@ int ehgp_step_end(ehgp_ctx* ctx, double* elapsed_ms);
  * [4] emitted records. */
 int ehgp_kernel_stats(const ehgp_ctx* ctx, double* kernel_ms, uint64_t* stats, uint32_t count);
 
+/* ---- direct Morse hierarchy ------------------------------------------------
+ * One call runs the reference's direct chain on the resident cloud (pair and
+ * triple/quad supports first when they are not resident for K):
+ *   terminal facade  build_exact_direct_support_terminal_facade
+ *                    (morsehgp3d/include/morsehgp3d/hierarchy/direct_support_terminal.hpp:196)
+ *   event journal    build_exact_direct_morse_event_journal (direct_morse_event_journal.hpp:165)
+ *   arm seeds        build_exact_direct_saddle_arm_seed_journal (direct_saddle_arm_seed_journal.hpp:169)
+ *   forest journal   build_exact_direct_morse_forest_journal (direct_morse_forest_journal.hpp:388),
+ *                    with its strict-arm descent (direct_sparse_facet_descent_step.hpp:239,
+ *                    direct_sparse_facet_descent_closure.hpp:477) and frozen-root quotient
+ *                    (direct_frozen_root_quotient.hpp:176).
+ * Records keep the reference's arena order and index meaning; optional ids
+ * are UINT32_MAX when absent.  Exact levels are referenced by `level_event`,
+ * the facade index of an event at that level (UINT32_MAX: level 0), and are
+ * materialised by ehgp_event_level.  A relevant extra-shell diagnostic stops
+ * the chain after the facade (decision EHGP_ERR_DEGENERATE), as the
+ * reference's no_journal_relevant_extra_shell_diagnostics does. */
+typedef struct ehgp_hier_counts {
+  uint64_t events, diagnostics;                 /* facade */
+  uint64_t journal_batches, role_records;       /* event journal */
+  uint64_t families, arm_seeds;                 /* arm seeds */
+  uint64_t birth_records, nodes, children, arm_bindings, saddle_records, atomic_groups, final_roots;
+  uint32_t decision;                            /* EHGP_OK when the forest journal is complete */
+  uint32_t k_eff;
+} ehgp_hier_counts;
+
+int ehgp_hierarchy(ehgp_ctx* ctx, uint32_t K, ehgp_hier_counts* counts);
+
+/* Facade event (64 bytes), in facade order (exact level, closed rank,
+ * interior ids, support ids). */
+typedef struct ehgp_event_record {
+  uint32_t support_size;
+  uint32_t support_ids[4];
+  uint32_t interior_count;
+  uint32_t closed_rank;
+  uint32_t interior_ids[9];
+} ehgp_event_record;
+
+typedef struct ehgp_journal_batch {  /* ExactDirectMorseH0Batch */
+  uint32_t order, level_event;
+  uint32_t role_offset, role_count, birth_roles, saddle_roles;
+} ehgp_journal_batch;
+
+typedef struct ehgp_role_record {    /* ExactDirectMorseH0RoleRecord */
+  uint32_t batch, projection, role;  /* projection: PointId (< n) or n + event; role 0 birth, 1 saddle */
+} ehgp_role_record;
+
+typedef struct ehgp_family_record {  /* ExactDirectSaddleArmFamilyRecord */
+  uint32_t event, projection, role_record, batch, order, arm_offset, arm_count;
+} ehgp_family_record;
+
+typedef struct ehgp_forest_node {    /* ExactDirectMorseForestNode */
+  uint32_t order, level_event, kind; /* kind: 0 order-one birth, 1 reduced birth, 2 multifusion */
+  uint32_t child_offset, child_count, birth_record, atomic_group;
+} ehgp_forest_node;
+
+typedef struct ehgp_forest_birth {   /* ExactDirectMorseForestBirthRecord */
+  uint32_t projection, batch, order, handle, order_one_node;
+} ehgp_forest_birth;
+
+typedef struct ehgp_forest_binding { /* ExactDirectMorseForestArmRootBinding */
+  uint32_t arm_seed, family, carrier, prior_root;
+} ehgp_forest_binding;
+
+typedef struct ehgp_forest_saddle {  /* ExactDirectMorseForestSaddleRecord */
+  uint32_t family, event, batch, arm_offset, arm_count, carriers, latent, prior_roots, group;
+} ehgp_forest_saddle;
+
+typedef struct ehgp_forest_group {   /* ExactDirectMorseForestAtomicGroup; kind 0 birth, 1 continuation, 2 multifusion */
+  uint32_t batch, saddle_offset, saddle_count, frozen, latent, prior_roots, child_offset, child_count, created_node,
+      result_node, kind;
+} ehgp_forest_group;
+
+typedef struct ehgp_forest_batch {   /* ExactDirectMorseForestBatch */
+  uint32_t order, level_event, birth_offset, birth_count, saddle_offset, saddle_count, group_offset, group_count,
+      pre_carriers, pre_roots, post_carriers, post_roots;
+} ehgp_forest_batch;
+
+typedef struct ehgp_forest_root {    /* ExactDirectMorseForestFinalRoot */
+  uint32_t order, handle, node;
+} ehgp_forest_root;
+
+/* Host copies of the last ehgp_hierarchy result; every pointer may be NULL
+ * and must otherwise hold the count reported in ehgp_hier_counts. */
+typedef struct ehgp_hier_out {
+  ehgp_event_record* events;
+  ehgp_journal_batch* journal_batches;
+  ehgp_role_record* roles;
+  ehgp_family_record* families;
+  uint32_t* arm_removed;             /* [arm_seeds] removed support PointId; family via families[] */
+  ehgp_forest_node* nodes;
+  uint32_t* children;
+  ehgp_forest_birth* births;
+  ehgp_forest_binding* bindings;
+  ehgp_forest_saddle* saddles;
+  ehgp_forest_group* groups;
+  ehgp_forest_batch* batches;
+  ehgp_forest_root* roots;
+} ehgp_hier_out;
+
+int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out);
+
+/* Timing of the last ehgp_hierarchy call: ms[0] device stages (CUDA events),
+ * ms[1] the strict-arm descent kernel, ms[2] the host forest pass;
+ * stats[0] strict arms, [1] descent steps, [2] facade boundaries settled
+ * exactly on the host, [3] facade events. */
+int ehgp_hier_stats(const ehgp_ctx* ctx, double* ms, uint64_t* stats);
+
+/* Exact level of facade event `event` as num / (den 2^(2 scale)), two's
+ * complement little-endian 64-bit limbs, 36 each (num = |N|^2, den = 4 A^2 of
+ * the circumsphere at the cloud scale; not reduced). */
+int ehgp_event_level(ehgp_ctx* ctx, uint64_t event, uint64_t* num, uint64_t* den, int32_t* scale);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,6 +17,7 @@
 #include <cstdint>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -721,6 +722,527 @@ std::string higher_text(const Cloud& c, u64 K) {
   return ev[0] + ev[1] + dg[0] + dg[1] + "S complete\n";
 }
 
+// ---- direct hierarchy: facade, Morse event journal, arm seeds, forest journal --------
+// A brute-force restatement of the reference's direct chain
+//   build_exact_direct_support_terminal_facade (src/cpu/hierarchy/direct_support_terminal.cpp:68-300)
+//   build_exact_direct_morse_event_journal     (src/cpu/hierarchy/direct_morse_event_journal.cpp:260-400)
+//   build_exact_direct_saddle_arm_seed_journal (src/cpu/hierarchy/direct_saddle_arm_seed_journal.cpp:380-420)
+//   build_exact_direct_morse_forest_journal    (src/cpu/hierarchy/direct_morse_forest_journal.cpp:1042-2150)
+// with the descent closure of direct_sparse_facet_descent_{step,closure} restated
+// as: a facet bound in the locator resolves to its birth handle; otherwise its
+// exact miniball centre c_F gives the canonical top-k choice G (strictly closer
+// points, then the least PointIds of the cutoff shell); G = F is unresolved, and
+// beta(G) < beta(F) is required before the descent continues from G.
+struct Rat {
+  Big num, den;  // den > 0
+};
+bool rat_less(const Rat& a, const Rat& b) { return a.num * b.den < b.num * a.den; }
+bool rat_eq(const Rat& a, const Rat& b) { return a.num * b.den == b.num * a.den; }
+std::string rat_text(const Rat& r) { return reduced_frac(r.num, r.den); }
+
+// A ball centred at X[ids0] + Nv / (2A) (cloud-scale integers); level in cloud units.
+struct XBall {
+  int size = 0;
+  u64 ids[4]{};
+  Big A;
+  BV Nv;
+  Rat level;
+};
+
+XBall ball_of(const Cloud& c, const FixedCloud& f, const u64* ids, int size, bool* minimal) {
+  XBall b;
+  b.size = size;
+  for (int i = 0; i < size; ++i) b.ids[i] = ids[i];
+  *minimal = true;
+  if (size == 1) {
+    b.A = 1;
+    b.Nv = {Big(0), Big(0), Big(0)};
+  } else if (size == 2) {
+    b.A = 1;
+    b.Nv = bdiff(f, ids[1], ids[0]);
+  } else {
+    SupportGeo g = analyze(c, f, ids, size);
+    if (g.status != 0) {
+      *minimal = false;
+      return b;
+    }
+    b.A = g.A;
+    b.Nv = g.Nv;
+  }
+  b.level = {dot3(b.Nv, b.Nv), 4 * b.A * b.A * (Big(1) << (unsigned)(2 * f.S))};
+  return b;
+}
+
+// (2A)^2 2^(2S) |p - centre|^2 as an integer
+Big scaled_dist(const FixedCloud& f, const XBall& b, u64 p) {
+  Big s = 0;
+  for (int a = 0; a < 3; ++a) {
+    const Big t = 2 * b.A * (f.X[p][a] - f.X[b.ids[0]][a]) - b.Nv[a];
+    s += t * t;
+  }
+  return s;
+}
+
+// Exact miniball of a facet of 1..10 points (build_exact_facet_miniball,
+// include/morsehgp3d/hierarchy/facet_miniball.hpp:86-102): the enclosing ball of
+// least radius among the circumspheres of 1- to 4-subsets with a relatively
+// interior centre.
+XBall facet_miniball(const Cloud& c, const FixedCloud& f, const std::vector<u64>& F) {
+  const int k = (int)F.size();
+  XBall best;
+  bool have = false;
+  u64 ids[4];
+  auto consider = [&](int size) {
+    bool minimal = false;
+    XBall b = ball_of(c, f, ids, size, &minimal);
+    if (!minimal) return;
+    const Big r2 = dot3(b.Nv, b.Nv);  // (2A)^2 2^(2S) * level
+    for (u64 w : F) {
+      bool sup = false;
+      for (int i = 0; i < size; ++i) sup |= ids[i] == w;
+      if (sup) continue;
+      if (scaled_dist(f, b, w) > r2) return;  // outside the closed ball
+    }
+    if (!have || rat_less(b.level, best.level)) {
+      best = b;
+      have = true;
+    }
+  };
+  for (int i = 0; i < k; ++i) {
+    ids[0] = F[i];
+    if (k == 1) consider(1);
+    for (int j = i + 1; j < k; ++j) {
+      ids[1] = F[j];
+      consider(2);
+      for (int l = j + 1; l < k; ++l) {
+        ids[2] = F[l];
+        consider(3);
+        for (int m = l + 1; m < k; ++m) {
+          ids[3] = F[m];
+          consider(4);
+        }
+      }
+    }
+  }
+  if (!have) throw std::logic_error("a facet has no exact miniball");
+  return best;
+}
+
+struct HEvent {
+  int size = 0;
+  u64 ids[4]{};
+  std::vector<u64> interior;
+  u64 rank = 0;
+  Rat level;
+  int birth = 0, saddle = 0;  // 0 = none
+};
+
+bool hevent_less(const HEvent& a, const HEvent& b) {
+  if (!rat_eq(a.level, b.level)) return rat_less(a.level, b.level);
+  if (a.rank != b.rank) return a.rank < b.rank;
+  if (a.interior != b.interior) return a.interior < b.interior;
+  const int m = std::min(a.size, b.size);
+  for (int i = 0; i < m; ++i)
+    if (a.ids[i] != b.ids[i]) return a.ids[i] < b.ids[i];
+  return a.size < b.size;
+}
+
+std::string hierarchy_text(const Cloud& c, u64 K) {
+  const FixedCloud f = fixed_cloud(c);
+  const u64 n = c.bits.size();
+  const u64 keff = std::min(K, n), smax = std::min(keff + 1, n);
+  std::vector<HEvent> ev;
+  u64 diagnostics = 0;
+  // pair supports
+  if (smax >= 2) {
+    for (u64 u = 0; u < n; ++u)
+      for (u64 v = u + 1; v < n; ++v) {
+        HEvent e;
+        e.size = 2;
+        e.ids[0] = u;
+        e.ids[1] = v;
+        u64 shell = 2;
+        bool reject = false;
+        for (u64 w = 0; w < n && !reject; ++w) {
+          if (w == u || w == v) continue;
+          const int sd = diametral_side(c, f, w, u, v);
+          if (sd < 0) {
+            e.interior.push_back(w);
+            reject = e.interior.size() > smax - 2;
+          } else if (sd == 0) {
+            ++shell;
+          }
+        }
+        if (reject) continue;
+        if (shell != 2) {
+          ++diagnostics;
+          continue;
+        }
+        bool minimal = false;
+        e.level = ball_of(c, f, e.ids, 2, &minimal).level;
+        ev.push_back(std::move(e));
+      }
+  }
+  // triple and quad supports
+  auto visit = [&](const u64* ids, int size) {
+    if (smax < (u64)size) return;
+    SupportGeo g = analyze(c, f, ids, size);
+    if (g.status != 0) return;
+    analyze_fp(c, g);
+    HEvent e;
+    e.size = size;
+    for (int i = 0; i < size; ++i) e.ids[i] = ids[i];
+    u64 shell = size;
+    for (u64 w = 0; w < n; ++w) {
+      bool sup = false;
+      for (int i = 0; i < size; ++i) sup |= (w == ids[i]);
+      if (sup) continue;
+      const int sd = higher_side(c, f, g, w);
+      if (sd < 0) {
+        e.interior.push_back(w);
+        if (e.interior.size() > smax - size) return;
+      } else if (sd == 0) {
+        ++shell;
+      }
+    }
+    if (shell != (u64)size) {
+      ++diagnostics;
+      return;
+    }
+    bool minimal = false;
+    e.level = ball_of(c, f, ids, size, &minimal).level;
+    ev.push_back(std::move(e));
+  };
+  {
+    u64 ids[4];
+    for (ids[0] = 0; ids[0] < n; ++ids[0])
+      for (ids[1] = ids[0] + 1; ids[1] < n; ++ids[1])
+        for (ids[2] = ids[1] + 1; ids[2] < n; ++ids[2]) {
+          visit(ids, 3);
+          for (ids[3] = ids[2] + 1; ids[3] < n; ++ids[3]) visit(ids, 4);
+        }
+  }
+  for (auto& e : ev) {
+    e.rank = e.interior.size() + e.size;
+    e.birth = e.rank <= keff ? (int)e.rank : 0;
+    e.saddle = (e.rank >= 2 && e.rank - 1 <= keff) ? (int)(e.rank - 1) : 0;
+  }
+  std::sort(ev.begin(), ev.end(), hevent_less);
+  std::string s;
+  for (u64 i = 0; i < ev.size(); ++i) {
+    const HEvent& e = ev[i];
+    s += "F " + std::to_string(i) + " " + std::to_string(e.size);
+    for (int j = 0; j < e.size; ++j) s += " " + std::to_string(e.ids[j]);
+    s += " |";
+    for (u64 w : e.interior) s += " " + std::to_string(w);
+    s += " | " + std::to_string(e.rank) + " " + std::to_string(n - e.rank) + " " + rat_text(e.level) + " " +
+         (e.birth ? std::to_string(e.birth) : std::string("-")) + " " +
+         (e.saddle ? std::to_string(e.saddle) : std::string("-")) + "\n";
+  }
+  s += "X " + std::to_string(diagnostics) + "\n";
+  if (diagnostics) {  // journal: no_journal_relevant_extra_shell_diagnostics; seeds and forest reject the source
+    return s + "C\nD 4 3 4\n";
+  }
+  // Morse event journal: projections 0..n-1 are singletons, n + i the facade events
+  struct Seed {
+    u64 order;
+    Rat level;
+    u64 proj;
+    int role;  // 0 birth, 1 saddle
+  };
+  std::vector<Seed> seeds;
+  for (u64 p = 0; p < n; ++p) seeds.push_back({1, {Big(0), Big(1)}, p, 0});
+  for (u64 i = 0; i < ev.size(); ++i) {
+    if (ev[i].birth) seeds.push_back({(u64)ev[i].birth, ev[i].level, n + i, 0});
+    if (ev[i].saddle) seeds.push_back({(u64)ev[i].saddle, ev[i].level, n + i, 1});
+  }
+  std::stable_sort(seeds.begin(), seeds.end(), [](const Seed& a, const Seed& b) {
+    if (a.order != b.order) return a.order < b.order;
+    if (!rat_eq(a.level, b.level)) return rat_less(a.level, b.level);
+    if (a.proj != b.proj) return a.proj < b.proj;
+    return a.role < b.role;
+  });
+  struct JBatch {
+    u64 order;
+    Rat level;
+    u64 off, cnt, births, saddles;
+  };
+  std::vector<JBatch> jb;
+  std::vector<u64> role_batch(seeds.size());
+  for (u64 i = 0; i < seeds.size();) {
+    u64 j = i;
+    JBatch b{seeds[i].order, seeds[i].level, i, 0, 0, 0};
+    while (j < seeds.size() && seeds[j].order == b.order && rat_eq(seeds[j].level, b.level)) {
+      (seeds[j].role ? b.saddles : b.births)++;
+      role_batch[j] = jb.size();
+      ++j;
+    }
+    b.cnt = j - i;
+    jb.push_back(b);
+    i = j;
+  }
+  for (const auto& b : jb)
+    s += "J " + std::to_string(&b - jb.data()) + " " + std::to_string(b.order) + " " + rat_text(b.level) + " " +
+         std::to_string(b.off) + " " + std::to_string(b.cnt) + " " + std::to_string(b.births) + " " +
+         std::to_string(b.saddles) + "\n";
+  for (u64 i = 0; i < seeds.size(); ++i)
+    s += "Q " + std::to_string(i) + " " + std::to_string(role_batch[i]) + " " + std::to_string(seeds[i].proj) + " " +
+         std::to_string(seeds[i].role) + "\n";
+  // saddle families and arm seeds
+  auto facet_of = [&](u64 proj) {  // I u U sorted
+    std::vector<u64> F;
+    if (proj < n) {
+      F.push_back(proj);
+      return F;
+    }
+    const HEvent& e = ev[proj - n];
+    F = e.interior;
+    for (int j = 0; j < e.size; ++j) F.push_back(e.ids[j]);
+    std::sort(F.begin(), F.end());
+    return F;
+  };
+  struct Family {
+    u64 event, proj, role, batch, order, arm_off, arm_cnt;
+  };
+  std::vector<Family> fam;
+  std::vector<std::pair<u64, u64>> arms;  // (family, removed)
+  for (u64 i = 0; i < seeds.size(); ++i) {
+    if (seeds[i].role != 1) continue;
+    const HEvent& e = ev[seeds[i].proj - n];
+    fam.push_back({seeds[i].proj - n, seeds[i].proj, i, role_batch[i], seeds[i].order, arms.size(), (u64)e.size});
+    for (int j = 0; j < e.size; ++j) arms.push_back({fam.size() - 1, e.ids[j]});
+  }
+  for (u64 i = 0; i < fam.size(); ++i)
+    s += "Y " + std::to_string(i) + " " + std::to_string(fam[i].event) + " " + std::to_string(fam[i].proj) + " " +
+         std::to_string(fam[i].role) + " " + std::to_string(fam[i].batch) + " " + std::to_string(fam[i].order) + " " +
+         rat_text(jb[fam[i].batch].level) + " " + std::to_string(fam[i].arm_off) + " " +
+         std::to_string(fam[i].arm_cnt) + "\n";
+  for (u64 i = 0; i < arms.size(); ++i)
+    s += "Z " + std::to_string(i) + " " + std::to_string(arms[i].first) + " " + std::to_string(arms[i].second) + "\n";
+  auto arm_facet = [&](u64 a) {
+    std::vector<u64> F = facet_of(fam[arms[a].first].proj);
+    F.erase(std::find(F.begin(), F.end(), arms[a].second));
+    return F;
+  };
+  // ---- forest journal
+  u64 birth_count = 0;
+  for (const auto& sd : seeds) birth_count += sd.role == 0;
+  std::vector<u64> parent(birth_count), border(birth_count, 0);
+  std::vector<long long> rroot(birth_count, -1);
+  std::vector<char> active(birth_count, 0);
+  for (u64 i = 0; i < birth_count; ++i) parent[i] = i;
+  auto root = [&](u64 h) {
+    while (parent[h] != h) h = parent[h];
+    return h;
+  };
+  auto count_roots = [&](u64 order, bool reduced) {
+    u64 k = 0;
+    for (u64 h = 0; h < birth_count; ++h)
+      if (active[h] && parent[h] == h && border[h] == order && (!reduced || rroot[h] >= 0)) ++k;
+    return k;
+  };
+  std::map<std::vector<u64>, u64> locator;  // bound facet -> birth handle
+  std::string N, C = "C", B, A, S, G, T, R;
+  u64 nodes = 0, children = 0, births = 0, bindings = 0, saddles = 0, groups = 0;
+  auto descend = [&](std::vector<u64> F) -> u64 {
+    for (int guard = 0; guard < 100000; ++guard) {
+      const auto hit = locator.find(F);
+      if (hit != locator.end()) return hit->second;
+      const XBall bf = facet_miniball(c, f, F);
+      const u64 k = F.size();
+      std::vector<std::pair<Big, u64>> d(n);
+      for (u64 p = 0; p < n; ++p) d[p] = {scaled_dist(f, bf, p), p};
+      std::nth_element(d.begin(), d.begin() + (k - 1), d.end(),
+                       [](const auto& x, const auto& y) { return x.first < y.first; });
+      const Big cut = d[k - 1].first;
+      std::vector<u64> below, shell;
+      for (const auto& x : d) {
+        if (x.first < cut) below.push_back(x.second);
+        else if (x.first == cut) shell.push_back(x.second);
+      }
+      std::sort(shell.begin(), shell.end());
+      std::vector<u64> Gs = below;
+      for (u64 i = 0; Gs.size() < k; ++i) Gs.push_back(shell[i]);
+      std::sort(Gs.begin(), Gs.end());
+      if (Gs == F) throw std::logic_error("a strict arm descent is unresolved");
+      const XBall bg = facet_miniball(c, f, Gs);
+      if (!rat_less(bg.level, bf.level)) throw std::logic_error("a strict arm descent met a plateau");
+      F = Gs;
+    }
+    throw std::logic_error("a strict arm descent did not terminate");
+  };
+  auto key_text = [](const std::vector<u64>& F) {
+    std::string t = std::to_string(F.size());
+    for (u64 x : F) t += " " + std::to_string(x);
+    return t;
+  };
+  u64 fam_cursor = 0;
+  for (u64 bi = 0; bi < jb.size(); ++bi) {
+    const JBatch& jbat = jb[bi];
+    const u64 pre_c = count_roots(jbat.order, false), pre_r = count_roots(jbat.order, true);
+    const u64 fam_begin = fam_cursor;
+    while (fam_cursor < fam.size() && fam[fam_cursor].batch == bi) ++fam_cursor;
+    struct Arm {
+      u64 seed, carrier;
+      long long prior;
+      std::vector<u64> key;
+    };
+    std::vector<std::vector<Arm>> sad;
+    std::map<std::vector<u64>, std::pair<u64, long long>> resolved;
+    for (u64 fi = fam_begin; fi < fam_cursor; ++fi) {
+      std::vector<Arm> as;
+      for (u64 a = fam[fi].arm_off; a < fam[fi].arm_off + fam[fi].arm_cnt; ++a) as.push_back({a, 0, -1, arm_facet(a)});
+      sad.push_back(std::move(as));
+    }
+    for (auto& as : sad)
+      for (auto& a : as) {
+        auto it = resolved.find(a.key);
+        if (it == resolved.end()) {
+          const u64 h = root(descend(a.key));
+          it = resolved.emplace(a.key, std::make_pair(h, rroot[h])).first;
+        }
+        a.carrier = it->second.first;
+        a.prior = it->second.second;
+      }
+    // frozen-root quotient: transitive classes of carriers over the saddles
+    std::map<u64, u64> qp;
+    std::function<u64(u64)> qf = [&](u64 x) { return qp[x] == x ? x : (qp[x] = qf(qp[x])); };
+    for (auto& as : sad)
+      for (auto& a : as)
+        if (!qp.count(a.carrier)) qp[a.carrier] = a.carrier;
+    for (auto& as : sad)
+      for (auto& a : as) {
+        const u64 x = qf(as[0].carrier), y = qf(a.carrier);
+        if (x != y) qp[std::max(x, y)] = std::min(x, y);
+      }
+    std::map<u64, std::vector<u64>> cls;  // least carrier -> carriers (sorted)
+    for (auto& kv : qp) cls[qf(kv.first)].push_back(kv.first);
+    struct Plan {
+      std::vector<u64> carriers, priors, saddles;
+      int kind;  // 0 reduced birth, 1 continuation, 2 multifusion
+      long long created = -1;
+      u64 result = 0;
+    };
+    std::vector<Plan> plans;
+    std::map<u64, u64> plan_of;
+    for (auto& kv : cls) {
+      plan_of[kv.first] = plans.size();
+      Plan p;
+      p.carriers = kv.second;
+      for (u64 h : p.carriers)
+        if (rroot[h] >= 0) p.priors.push_back((u64)rroot[h]);
+      std::sort(p.priors.begin(), p.priors.end());
+      plans.push_back(std::move(p));
+    }
+    for (u64 si = 0; si < sad.size(); ++si) plans[plan_of[qf(sad[si][0].carrier)]].saddles.push_back(si);
+    u64 pending_nodes = 0;
+    for (auto& p : plans) {
+      if (p.priors.size() == 1) {
+        p.kind = 1;
+        p.result = p.priors[0];
+      } else {
+        if (p.priors.empty() && jbat.order == 1) throw std::logic_error("an order-one group has no prior root");
+        p.kind = p.priors.empty() ? 0 : 2;
+        p.created = (long long)(nodes + pending_nodes++);
+        p.result = (u64)p.created;
+      }
+    }
+    const u64 s_off0 = saddles, g_off0 = groups;
+    for (auto& p : plans) {
+      const u64 g_s_off = saddles;
+      for (u64 si : p.saddles) {
+        const u64 fi = fam_begin + si;
+        const u64 arm_off = bindings;
+        std::vector<u64> cs, ps;
+        for (auto& a : sad[si]) {
+          A += "A " + std::to_string(bindings++) + " " + std::to_string(a.seed) + " " + std::to_string(fi) + " " +
+               std::to_string(a.carrier) + " " + (a.prior >= 0 ? std::to_string(a.prior) : std::string("-")) +
+               " | " + key_text(a.key) + "\n";
+          cs.push_back(a.carrier);
+          if (a.prior >= 0) ps.push_back((u64)a.prior);
+        }
+        std::sort(cs.begin(), cs.end());
+        cs.erase(std::unique(cs.begin(), cs.end()), cs.end());
+        std::sort(ps.begin(), ps.end());
+        ps.erase(std::unique(ps.begin(), ps.end()), ps.end());
+        S += "S " + std::to_string(saddles++) + " " + std::to_string(fi) + " " + std::to_string(fam[fi].event) + " " +
+             std::to_string(bi) + " " + std::to_string(arm_off) + " " + std::to_string(sad[si].size()) + " " +
+             std::to_string(cs.size()) + " " + std::to_string(cs.size() - ps.size()) + " " +
+             std::to_string(ps.size()) + " " + std::to_string(groups) + "\n";
+      }
+      const u64 child_cnt = p.kind == 2 ? p.priors.size() : 0;
+      G += "G " + std::to_string(groups) + " " + std::to_string(bi) + " " + std::to_string(g_s_off) + " " +
+           std::to_string(saddles - g_s_off) + " " + std::to_string(p.carriers.size()) + " " +
+           std::to_string(p.carriers.size() - p.priors.size()) + " " + std::to_string(p.priors.size()) + " " +
+           std::to_string(children) + " " + std::to_string(child_cnt) + " " +
+           (p.created >= 0 ? std::to_string(p.created) : std::string("-")) + " " + std::to_string(p.result) + " " +
+           std::to_string(p.kind) + "\n";
+      if (p.kind != 1)
+        N += "N " + std::to_string(p.created) + " " + std::to_string(jbat.order) + " " + rat_text(jbat.level) + " " +
+             std::to_string(p.kind == 0 ? 1 : 2) + " " + std::to_string(children) + " " + std::to_string(child_cnt) +
+             " - " + std::to_string(groups) + "\n";
+      if (p.kind == 2)
+        for (u64 x : p.priors) C += " " + std::to_string(x);
+      children += child_cnt;
+      ++groups;
+    }
+    nodes += pending_nodes;
+    // births of this batch (hidden from this batch's descents)
+    struct Birth {
+      u64 handle, order;
+      long long node;
+      std::vector<u64> key;
+    };
+    std::vector<Birth> nb;
+    const u64 b_off0 = births;
+    for (u64 r = jbat.off; r < jbat.off + jbat.cnt; ++r) {
+      if (seeds[r].role != 0) continue;
+      Birth b{births, jbat.order, -1, facet_of(seeds[r].proj)};
+      if (jbat.order == 1) {
+        b.node = (long long)nodes++;
+        N += "N " + std::to_string(b.node) + " 1 " + rat_text(jbat.level) + " 0 " + std::to_string(children) +
+             " 0 " + std::to_string(births) + " -\n";
+      }
+      B += "B " + std::to_string(births) + " " + std::to_string(seeds[r].proj) + " " + std::to_string(bi) + " " +
+           std::to_string(jbat.order) + " " + std::to_string(births) + " " +
+           (b.node >= 0 ? std::to_string(b.node) : std::string("-")) + " | " + key_text(b.key) + "\n";
+      ++births;
+      nb.push_back(std::move(b));
+    }
+    // commit: unions (least handle survives), reduced roots, then births
+    for (auto& p : plans) {
+      u64 r0 = root(p.carriers.front());
+      for (u64 i = 1; i < p.carriers.size(); ++i) {
+        const u64 r1 = root(p.carriers[i]);
+        if (r1 == r0) continue;
+        const u64 lo = std::min(r0, r1), hi = std::max(r0, r1);
+        parent[hi] = lo;
+        r0 = lo;
+      }
+      rroot[r0] = (long long)p.result;
+    }
+    for (auto& b : nb) {
+      active[b.handle] = 1;
+      border[b.handle] = b.order;
+      rroot[b.handle] = b.node;
+      locator[b.key] = b.handle;
+    }
+    T += "T " + std::to_string(bi) + " " + std::to_string(bi) + " " + std::to_string(jbat.order) + " " +
+         rat_text(jbat.level) + " " + std::to_string(b_off0) + " " + std::to_string(births - b_off0) + " " +
+         std::to_string(s_off0) + " " + std::to_string(saddles - s_off0) + " " + std::to_string(g_off0) + " " +
+         std::to_string(groups - g_off0) + " " + std::to_string(pre_c) + " " + std::to_string(pre_r) + " " +
+         std::to_string(count_roots(jbat.order, false)) + " " + std::to_string(count_roots(jbat.order, true)) + "\n";
+  }
+  std::vector<std::array<u64, 3>> fr;  // (order, node, handle)
+  for (u64 h = 0; h < birth_count; ++h)
+    if (active[h] && parent[h] == h && rroot[h] >= 0) fr.push_back({border[h], (u64)rroot[h], h});
+  std::sort(fr.begin(), fr.end());
+  for (u64 i = 0; i < fr.size(); ++i)
+    R += "R " + std::to_string(i) + " " + std::to_string(fr[i][0]) + " " + std::to_string(fr[i][2]) + " " +
+         std::to_string(fr[i][1]) + "\n";
+  return s + N + C + "\n" + B + A + S + G + T + R + "D 5 5 13\n";
+}
+
 u64 put_text(const std::string& s, char* buf, u64 cap) {
   if (s.size() + 1 > cap) return s.size() + 1;
   std::memcpy(buf, s.c_str(), s.size() + 1);
@@ -813,6 +1335,16 @@ int oracle_pairs(const double* xyz, u64 n, u64 K, char* out, u64 cap, u64* neede
 int oracle_emst_forest(const double* xyz, u64 n, char* out, u64 cap, u64* needed, char* err, u64 errlen) {
   try {
     *needed = put_text(emst_forest_text(canonical_cloud(xyz, n)), out, cap);
+    return 0;
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 1);
+  }
+}
+
+
+int oracle_hierarchy(const double* xyz, u64 n, u64 K, char* out, u64 cap, u64* needed, char* err, u64 errlen) {
+  try {
+    *needed = put_text(hierarchy_text(canonical_cloud(xyz, n), K), out, cap);
     return 0;
   } catch (const std::exception& e) {
     return report(e, err, errlen, 1);

@@ -219,3 +219,10 @@ def parse_higher(txt: str) -> dict:
 def higher(points: np.ndarray, K: int = 10, which: str = "restatement") -> dict:
     name = "oracle_higher" if which == "restatement" else "ref_higher"
     return parse_higher(_text_call(name, which, points, K))
+
+
+def hierarchy(pts: np.ndarray, K: int, which: str = "restatement") -> str:
+    """The direct chain (facade, event journal, arm seeds, forest journal) as text:
+    the restatement (oracle_hierarchy) or the reference's own code (ref_hierarchy)."""
+    fn = "oracle_hierarchy" if which == "restatement" else "ref_hierarchy"
+    return _text_call(fn, which, pts, K)

@@ -382,3 +382,197 @@ int ref_emst_forest(const double* xyz, uint64_t n, char* out, uint64_t cap, uint
 }
 
 }  // extern "C"
+
+#include "morsehgp3d/hierarchy/direct_morse_event_journal.hpp"
+#include "morsehgp3d/hierarchy/direct_morse_forest_journal.hpp"
+#include "morsehgp3d/hierarchy/direct_saddle_arm_seed_journal.hpp"
+#include "morsehgp3d/hierarchy/direct_support_terminal.hpp"
+
+namespace {
+
+std::string level_text(const morsehgp3d::exact::ExactLevel& l) {
+  return l.numerator_string() + " " + l.denominator_string();
+}
+
+std::string opt_text(const std::optional<std::size_t>& v) { return v ? std::to_string(*v) : std::string("-"); }
+std::string opt_text(const std::optional<std::uint64_t>& v, int) { return v ? std::to_string(*v) : std::string("-"); }
+
+template <class Key>
+std::string key_text(const Key& k) {
+  std::string t = std::to_string(k.point_count);
+  for (std::size_t i = 0; i < k.point_count; ++i) t += " " + std::to_string(k.point_ids[i]);
+  return t;
+}
+
+}  // namespace
+
+extern "C" {
+
+// The reference's direct hierarchy chain run to completion:
+//   build_exact_pair_support_stream + build_exact_higher_support_stream
+//   -> build_exact_direct_support_terminal_facade (direct_support_terminal.hpp:196)
+//   -> build_exact_direct_morse_event_journal (direct_morse_event_journal.hpp:165)
+//   -> build_exact_direct_saddle_arm_seed_journal (direct_saddle_arm_seed_journal.hpp:169)
+//   -> build_exact_direct_morse_forest_journal (direct_morse_forest_journal.hpp:388).
+// Text lines (one record each, in the reference's own arena order):
+//   F idx size ids.. | interior.. | rank exterior num den birth_order saddle_order   (facade events)
+//   X count                                                                       (relevant extra-shell diagnostics)
+//   J batch order num den role_off role_cnt births saddles                         (journal batches)
+//   Q role batch projection role(0 birth, 1 saddle)                                (role records)
+//   Y family event projection role batch order num den arm_off arm_cnt             (saddle families)
+//   Z seed family removed                                                          (arm seeds)
+//   N node order num den kind child_off child_cnt birth group                      (forest nodes)
+//   C child..                                                                      (child arena)
+//   B birth proj batch order handle one_node | key                                 (birth records)
+//   A binding seed family carrier prior | key                                      (arm-root bindings)
+//   S saddle family event batch arm_off arm_cnt carriers latent prior group         (saddle records)
+//   G group batch s_off s_cnt frozen latent prior c_off c_cnt created result kind  (atomic groups)
+//   T batch src order num den b_off b_cnt s_off s_cnt g_off g_cnt pre_c pre_r post_c post_r
+//   R root order handle node                                                       (final roots)
+//   D journal_decision seed_decision forest_decision
+int ref_hierarchy(const double* xyz, uint64_t n, uint64_t K, char* out, uint64_t cap, uint64_t* needed,
+                  double* seconds, char* err, uint64_t errlen) {
+  try {
+    using namespace morsehgp3d;
+    using namespace morsehgp3d::hierarchy;
+    const auto pts = points_from(xyz, n);
+    const CanonicalPointCloud cloud = CanonicalPointCloud::rejecting_duplicates(pts);
+    const MortonLbvhIndex index = MortonLbvhIndex::build(cloud);
+    const std::size_t big = std::size_t{1} << 40;
+    ExactDirectSupportTerminalBudget tb;
+    tb.pair = unlimited_pair_budget();
+    tb.higher.maximum_work_unit_count = big;
+    tb.higher.maximum_frontier_entry_count = big;
+    tb.higher.maximum_auxiliary_frontier_entry_count = big;
+    tb.higher.maximum_emitted_record_count = big;
+    tb.higher.maximum_emitted_point_id_reference_count = big;
+    tb.higher.maximum_prune_receipt_count = big;
+    tb.higher.maximum_global_closed_ball_query_count = big;
+    tb.higher.maximum_point_classification_count = big;
+    const auto t0 = std::chrono::steady_clock::now();
+    const auto pair = build_exact_pair_support_stream(index, cloud, K, tb.pair);
+    const auto higher = build_exact_higher_support_stream(index, cloud, K, tb.higher);
+    const auto t1 = std::chrono::steady_clock::now();
+    const auto facade = build_exact_direct_support_terminal_facade(index, cloud, K, tb, pair, higher);
+    const auto journal = build_exact_direct_morse_event_journal(cloud, facade);
+    const ExactDirectSaddleArmSeedBudget sb{big, big, big, big};
+    const auto seeds = build_exact_direct_saddle_arm_seed_journal(cloud, facade, journal, sb);
+    ExactDirectMorseForestBudget fb;
+    const std::size_t mid = std::size_t{1} << 22;
+    fb.maximum_source_role_scan_count = big;
+    fb.maximum_source_batch_scan_count = big;
+    fb.maximum_source_family_scan_count = big;
+    fb.maximum_source_arm_seed_scan_count = big;
+    fb.maximum_birth_record_count = big;
+    fb.maximum_arm_root_binding_count = big;
+    fb.maximum_saddle_record_count = big;
+    fb.maximum_atomic_group_count = big;
+    fb.maximum_child_reference_count = big;
+    fb.maximum_batch_record_count = big;
+    fb.maximum_node_count = big;
+    fb.maximum_final_root_count = big;
+    fb.maximum_batch_distinct_arm_count = mid;
+    fb.maximum_logical_output_entry_count = big;
+    fb.maximum_aggregate_closure_node_count = big;
+    fb.maximum_aggregate_closure_step_call_count = big;
+    // the locator sizes its probing table from the binding caps: keep them modest
+    const std::size_t loc = std::size_t{1} << 16, slots = std::size_t{1} << 19;
+    fb.locator_budget = {loc, loc, 16 * loc, loc, loc, loc, loc, loc, 16 * loc, slots, slots};
+    const ExactDirectSparseFacetDescentStepBudget step{
+        ExactDirectSparsePositiveFacetProbeBudget{mid, mid},
+        spatial::ExactLbvhTopKBudget{mid, mid, mid, mid, mid, mid, mid},
+        ExactDirectSparsePositiveFacetProbeBudget{mid, mid}};
+    fb.closure_budget = {direct_sparse_facet_descent_closure_maximum_seed_count,
+                         direct_sparse_facet_descent_closure_maximum_node_count,
+                         direct_sparse_facet_descent_closure_maximum_step_call_count,
+                         direct_sparse_facet_descent_closure_maximum_memo_slot_count, step};
+    fb.quotient_budget = {mid, mid, mid, mid, mid};
+    ExactDirectMorseForestConfig fc;
+    fc.locator_config.external_authority_id = 0x10F0;
+    const auto forest = build_exact_direct_morse_forest_journal(index, cloud, facade, journal, sb, seeds, fb, fc,
+                                                                 spatial::LbvhTraversalOrder::near_first);
+    const auto t2 = std::chrono::steady_clock::now();
+    if (seconds) {
+      seconds[0] = std::chrono::duration<double>(t1 - t0).count();
+      seconds[1] = std::chrono::duration<double>(t2 - t1).count();
+    }
+    std::string s;
+    for (const auto& e : facade.events) {
+      s += "F " + std::to_string(e.event_index) + " " + std::to_string((int)e.support_size);
+      for (int i = 0; i < e.support_size; ++i) s += " " + std::to_string(e.support_ids[i]);
+      s += " |" + ids_text(e.interior_ids) + " | " + std::to_string(e.closed_rank) + " " +
+           std::to_string(e.exterior_count) + " " + level_text(e.squared_level) + " " + opt_text(e.birth_order) + " " +
+           opt_text(e.saddle_order) + "\n";
+    }
+    s += "X " + std::to_string(facade.relevant_extra_shell_diagnostics.size()) + "\n";
+    for (const auto& b : journal.batches)
+      s += "J " + std::to_string(b.batch_index) + " " + std::to_string(b.order) + " " + level_text(b.squared_level) +
+           " " + std::to_string(b.role_record_offset) + " " + std::to_string(b.role_record_count) + " " +
+           std::to_string(b.birth_role_count) + " " + std::to_string(b.saddle_role_count) + "\n";
+    for (const auto& r : journal.role_records)
+      s += "Q " + std::to_string(r.role_record_index) + " " + std::to_string(r.batch_index) + " " +
+           std::to_string(r.event_projection_index) + " " + std::to_string((int)r.role) + "\n";
+    for (const auto& f : seeds.families)
+      s += "Y " + std::to_string(f.family_index) + " " + std::to_string(f.source_event_index) + " " +
+           std::to_string(f.journal_event_projection_index) + " " + std::to_string(f.journal_role_record_index) + " " +
+           std::to_string(f.journal_batch_index) + " " + std::to_string(f.order) + " " +
+           level_text(f.critical_squared_level) + " " + std::to_string(f.arm_seed_offset) + " " +
+           std::to_string(f.arm_seed_count) + "\n";
+    for (const auto& a : seeds.arm_seeds)
+      s += "Z " + std::to_string(a.arm_seed_index) + " " + std::to_string(a.family_index) + " " +
+           std::to_string(a.removed_support_point_id) + "\n";
+    for (const auto& nd : forest.nodes)
+      s += "N " + std::to_string(nd.node_id) + " " + std::to_string(nd.order) + " " + level_text(nd.squared_level) +
+           " " + std::to_string((int)nd.kind) + " " + std::to_string(nd.child_offset) + " " +
+           std::to_string(nd.child_count) + " " + opt_text(nd.birth_record_index) + " " +
+           opt_text(nd.atomic_group_index) + "\n";
+    {
+      std::string c = "C";
+      for (auto id : forest.child_node_ids) c += " " + std::to_string(id);
+      s += c + "\n";
+    }
+    for (const auto& b : forest.birth_records)
+      s += "B " + std::to_string(b.birth_record_index) + " " + std::to_string(b.source_event_projection_index) + " " +
+           std::to_string(b.source_journal_batch_index) + " " + std::to_string(b.order) + " " +
+           std::to_string(b.component_handle) + " " + opt_text(b.order_one_birth_node_id, 0) + " | " +
+           key_text(b.facet_key) + "\n";
+    for (const auto& a : forest.arm_root_bindings)
+      s += "A " + std::to_string(a.binding_index) + " " + std::to_string(a.source_arm_seed_index) + " " +
+           std::to_string(a.source_family_index) + " " + std::to_string(a.frozen_carrier_component_handle) + " " +
+           opt_text(a.prior_reduced_root_node_id, 0) + " | " + key_text(a.strict_arm_key) + "\n";
+    for (const auto& r : forest.saddle_records)
+      s += "S " + std::to_string(r.saddle_record_index) + " " + std::to_string(r.source_family_index) + " " +
+           std::to_string(r.source_event_index) + " " + std::to_string(r.source_journal_batch_index) + " " +
+           std::to_string(r.arm_binding_offset) + " " + std::to_string(r.arm_binding_count) + " " +
+           std::to_string(r.distinct_frozen_carrier_count) + " " + std::to_string(r.distinct_latent_carrier_count) +
+           " " + std::to_string(r.distinct_prior_reduced_root_count) + " " + std::to_string(r.atomic_group_index) +
+           "\n";
+    for (const auto& g : forest.atomic_groups)
+      s += "G " + std::to_string(g.atomic_group_index) + " " + std::to_string(g.batch_index) + " " +
+           std::to_string(g.saddle_record_offset) + " " + std::to_string(g.saddle_record_count) + " " +
+           std::to_string(g.frozen_carrier_count) + " " + std::to_string(g.latent_carrier_count) + " " +
+           std::to_string(g.prior_reduced_root_count) + " " + std::to_string(g.child_offset) + " " +
+           std::to_string(g.child_count) + " " + opt_text(g.created_node_id, 0) + " " +
+           std::to_string(g.resulting_root_node_id) + " " + std::to_string((int)g.kind) + "\n";
+    for (const auto& b : forest.batches)
+      s += "T " + std::to_string(b.batch_index) + " " + std::to_string(b.source_journal_batch_index) + " " +
+           std::to_string(b.order) + " " + level_text(b.squared_level) + " " + std::to_string(b.birth_record_offset) +
+           " " + std::to_string(b.birth_record_count) + " " + std::to_string(b.saddle_record_offset) + " " +
+           std::to_string(b.saddle_record_count) + " " + std::to_string(b.atomic_group_offset) + " " +
+           std::to_string(b.atomic_group_count) + " " + std::to_string(b.strict_pre_batch_carrier_count) + " " +
+           std::to_string(b.strict_pre_batch_reduced_root_count) + " " +
+           std::to_string(b.closed_post_batch_carrier_count) + " " +
+           std::to_string(b.closed_post_batch_reduced_root_count) + "\n";
+    for (const auto& r : forest.final_roots)
+      s += "R " + std::to_string(r.final_root_index) + " " + std::to_string(r.order) + " " +
+           std::to_string(r.component_handle) + " " + std::to_string(r.root_node_id) + "\n";
+    s += "D " + std::to_string((int)journal.decision) + " " + std::to_string((int)seeds.decision) + " " +
+         std::to_string((int)forest.decision) + "\n";
+    *needed = put_text(s, out, cap);
+    return 0;
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 1);
+  }
+}
+
+}  // extern "C"

@@ -175,3 +175,103 @@ def higher_match(gpu, ref):
             gs, rs = set(g), set(r)
             raise AssertionError(f"{key}: {len(g)} vs {len(r)}; only gpu {sorted(gs - rs)[:2]}; "
                                  f"only oracle {sorted(rs - gs)[:2]}")
+
+
+# ---- direct hierarchy ------------------------------------------------------------
+def _frac_text(f: Fraction) -> str:
+    return f"{f.numerator} {f.denominator}"
+
+
+def gpu_hierarchy_text(ctx, K, res=None) -> str:
+    """Renders an ehgp_hierarchy result in the line format of the oracle and of the
+    reference driver (oracle/ref_driver.cpp ref_hierarchy)."""
+    A = ehgp.ABSENT
+    if res is None:
+        res = ctx.hierarchy(K)
+    n = ctx.n
+    keff = int(res["k_eff"])
+    ev = res["events"]
+    lev_cache = {}
+
+    def level(e):
+        if e == A:
+            return "0 1"
+        if e not in lev_cache:
+            lev_cache[e] = _frac_text(ctx.event_level(int(e)))
+        return lev_cache[e]
+
+    def opt(x):
+        return "-" if x == A else str(int(x))
+
+    def facet(proj):
+        if proj < n:
+            return [int(proj)]
+        r = ev[proj - n]
+        f = [int(x) for x in r["interior_ids"][: r["interior_count"]]] + \
+            [int(x) for x in r["support_ids"][: r["support_size"]]]
+        return sorted(f)
+
+    def key(f):
+        return " ".join([str(len(f))] + [str(x) for x in f])
+
+    out = []
+    for i, r in enumerate(ev):
+        rank = int(r["closed_rank"])
+        ids = " ".join(str(int(x)) for x in r["support_ids"][: r["support_size"]])
+        inter = "".join(" " + str(int(x)) for x in r["interior_ids"][: r["interior_count"]])
+        birth = str(rank) if rank <= keff else "-"
+        saddle = str(rank - 1) if 2 <= rank <= keff + 1 else "-"
+        out.append(f"F {i} {int(r['support_size'])} {ids} |{inter} | {rank} {n - rank} {level(i)} {birth} {saddle}")
+    out.append(f"X {int(res['diagnostics'])}")
+    for i, b in enumerate(res["journal_batches"]):
+        out.append(f"J {i} {int(b['order'])} {level(b['level_event'])} {int(b['role_offset'])} {int(b['role_count'])} "
+                   f"{int(b['birth_roles'])} {int(b['saddle_roles'])}")
+    for i, q in enumerate(res["roles"]):
+        out.append(f"Q {i} {int(q['batch'])} {int(q['projection'])} {int(q['role'])}")
+    fam_of_seed = {}
+    for i, f in enumerate(res["families"]):
+        b = res["journal_batches"][f["batch"]]
+        out.append(f"Y {i} {int(f['event'])} {int(f['projection'])} {int(f['role_record'])} {int(f['batch'])} "
+                   f"{int(f['order'])} {level(b['level_event'])} {int(f['arm_offset'])} {int(f['arm_count'])}")
+        for s in range(int(f["arm_offset"]), int(f["arm_offset"] + f["arm_count"])):
+            fam_of_seed[s] = i
+    for s, u in enumerate(res["arm_removed"]):
+        out.append(f"Z {s} {fam_of_seed[s]} {int(u)}")
+    for i, nd in enumerate(res["nodes"]):
+        out.append(f"N {i} {int(nd['order'])} {level(nd['level_event'])} {int(nd['kind'])} {int(nd['child_offset'])} "
+                   f"{int(nd['child_count'])} {opt(nd['birth_record'])} {opt(nd['atomic_group'])}")
+    out.append("C" + "".join(" " + str(int(c)) for c in res["children"]))
+    for i, bt in enumerate(res["births"]):
+        out.append(f"B {i} {int(bt['projection'])} {int(bt['batch'])} {int(bt['order'])} {int(bt['handle'])} "
+                   f"{opt(bt['order_one_node'])} | {key(facet(int(bt['projection'])))}")
+    fams = res["families"]
+    for i, a in enumerate(res["bindings"]):
+        f = fams[a["family"]]
+        removed = int(res["arm_removed"][a["arm_seed"]])
+        arm = [x for x in facet(int(f["projection"])) if x != removed]
+        out.append(f"A {i} {int(a['arm_seed'])} {int(a['family'])} {int(a['carrier'])} {opt(a['prior_root'])} | "
+                   f"{key(arm)}")
+    for i, s in enumerate(res["saddles"]):
+        out.append("S " + " ".join(str(int(x)) for x in [i] + [s[f] for f in ehgp.FOREST_SADDLE.names]))
+    for i, g in enumerate(res["groups"]):
+        vals = [int(g[f]) for f in ehgp.FOREST_GROUP.names]
+        vals[8] = opt(vals[8])
+        out.append("G " + " ".join(str(x) for x in [i] + vals))
+    for i, b in enumerate(res["batches"]):
+        out.append(f"T {i} {i} {int(b['order'])} {level(b['level_event'])} " +
+                   " ".join(str(int(b[f])) for f in ehgp.FOREST_BATCH.names[2:]))
+    for i, r in enumerate(res["roots"]):
+        out.append(f"R {i} {int(r['order'])} {int(r['handle'])} {int(r['node'])}")
+    out.append("D 5 5 13")
+    return "\n".join(out) + "\n"
+
+
+def hierarchy_diff(a: str, b: str) -> str:
+    """First differing line of two hierarchy texts ('' when equal)."""
+    la, lb = a.splitlines(), b.splitlines()
+    for x, y in zip(la, lb):
+        if x != y:
+            return f"gpu: {x[:240]}\nref: {y[:240]}"
+    if len(la) != len(lb):
+        return f"line counts {len(la)} vs {len(lb)}"
+    return ""

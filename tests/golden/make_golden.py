@@ -6,6 +6,7 @@ project-written Boost shim).  Run here, where the reference tree exists:
     make -C oracle ref && python tests/golden/make_golden.py && python tests/golden/make_golden.py --geom
     python tests/golden/make_golden.py --pairs   # slow: the reference pair stream
     python tests/golden/make_golden.py --higher  # slow: the reference higher-support stream (n = 12)
+    python tests/golden/make_golden.py --hierarchy  # slow: the reference direct chain up to the forest journal
 """
 import os
 import sys
@@ -163,3 +164,27 @@ def main_higher():
 
 if __name__ == "__main__" and "--higher" in sys.argv:
     main_higher()
+
+
+def hierarchy_cases():
+    rng = np.random.Generator(np.random.PCG64(11))
+    yield "uniform8_K10", rng.random((8, 3)), 10
+    yield "uniform10_K10", rng.random((10, 3)), 10
+    yield "uniform10_K3", rng.random((10, 3)), 3
+    yield "lattice2_f32_K10", workloads.jittered_lattice(2, 5).astype(np.float64), 10
+    # cube corners: every face and the whole cube are cospherical -> relevant extra shells
+    yield "cube8_K10", np.array([[x, y, z] for x in (0, 1) for y in (0, 1) for z in (0, 1)], float), 10
+
+
+def main_hierarchy():
+    import json
+    for name, pts, K in hierarchy_cases():
+        txt = pyoracle._text_call("ref_hierarchy", "reference", pts, K)
+        doc = {"points": pts.tolist(), "K": K, "text": txt}
+        with open(os.path.join(HERE, f"hier_{name}.json"), "w") as f:
+            json.dump(doc, f, separators=(",", ":"))
+        print(name, len(pts), len(txt.splitlines()), txt.splitlines()[-1], flush=True)
+
+
+if __name__ == "__main__" and "--hierarchy" in sys.argv:
+    main_hierarchy()

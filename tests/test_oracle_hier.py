@@ -1,0 +1,50 @@
+"""The direct-hierarchy oracle (facade -> Morse event journal -> arm seeds ->
+forest journal, with strict-arm descent and frozen-root quotient) pinned
+against the reference's own chain run to completion
+(tests/golden/make_golden.py --hierarchy; the reference needs seconds per
+10 points).  Text lines follow oracle/ref_driver.cpp ref_hierarchy."""
+import glob
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "hier_*.json")))
+
+
+def load_golden_hier(path):
+    d = json.load(open(path))
+    return np.array(d["points"]), d["K"], d["text"]
+
+
+def first_diff(a, b):
+    for x, y in zip(a.splitlines(), b.splitlines()):
+        if x != y:
+            return f"\n  oracle: {x[:200]}\n  golden: {y[:200]}"
+    return f"line counts {len(a.splitlines())} vs {len(b.splitlines())}"
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[5:-5] for p in GOLDEN])
+def test_restatement_hierarchy_matches_golden(path):
+    pts, K, ref = load_golden_hier(path)
+    got = pyoracle.hierarchy(pts, K)
+    assert got == ref, first_diff(got, ref)
+
+
+def test_golden_hierarchy_covers_forest_and_refusal():
+    texts = [load_golden_hier(p)[2] for p in GOLDEN]
+    assert any(t.rstrip().endswith("D 5 5 13") for t in texts)       # complete forests
+    assert any(t.rstrip().endswith("D 4 3 4") for t in texts)        # journal refusal on extra shells
+    assert any("\nG " in t and " 2\n" in t for t in texts)           # multifusion groups
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(pyoracle.__file__), "_ref", "libehgp_ref.so")),
+                    reason="reference build absent")
+def test_restatement_hierarchy_matches_live_reference():
+    pts = np.random.default_rng(23).random((6, 3))
+    a = pyoracle.hierarchy(pts, 10)
+    b = pyoracle.hierarchy(pts, 10, which="reference")
+    assert a == b, first_diff(a, b)
