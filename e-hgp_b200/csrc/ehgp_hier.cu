@@ -509,12 +509,58 @@ __device__ bool inside_closed(const Cloud& c, const FSphere& fs, const uint32_t*
 // Exact: the circumcentre of T lies in the closed convex hull of T and T is affinely independent.
 __device__ bool hull_centre(const Cloud& c, const uint32_t* T, int ts) {
   if (ts <= 2) return ts == 1 || T[0] != T[1];
+  // FP64 signs with the uniform bounds of the support kernels, exact when undecided
+  double e[3][3], M = 0.0;
+  for (int j = 1; j < ts; ++j) {
+    e[j - 1][0] = c.px[T[j]] - c.px[T[0]];
+    e[j - 1][1] = c.py[T[j]] - c.py[T[0]];
+    e[j - 1][2] = c.pz[T[j]] - c.pz[T[0]];
+    M = fmax(M, fmax(fabs(e[j - 1][0]), fmax(fabs(e[j - 1][1]), fabs(e[j - 1][2]))));
+  }
+  M *= (1.0 + 1e-15);
+  const double M2 = M * M;
   int sg[5];
+  bool undecided = false;
+  auto fs = [&](double v, double b) {
+    const int r = v > b ? 1 : (v < -b ? -1 : 2);
+    undecided |= r == 2;
+    return r;
+  };
   if (ts == 3) {
-    tri_signs_exact(c, T, sg);
+    const double G11 = (e[0][0] * e[0][0] + e[0][1] * e[0][1]) + e[0][2] * e[0][2];
+    const double G22 = (e[1][0] * e[1][0] + e[1][1] * e[1][1]) + e[1][2] * e[1][2];
+    const double G12 = (e[0][0] * e[1][0] + e[0][1] * e[1][1]) + e[0][2] * e[1][2];
+    sg[0] = fs(G12, kFilt * 3.0 * M2 + kTiny);
+    sg[1] = fs(G11 - G12, kFilt * 6.0 * M2 + kTiny);
+    sg[2] = fs(G22 - G12, kFilt * 6.0 * M2 + kTiny);
+    sg[3] = fs(G11 * G22 - G12 * G12, kFilt * 18.0 * M2 * M2 + kTiny);
+    if (undecided) tri_signs_exact(c, T, sg);
     return sg[3] != 0 && sg[0] >= 0 && sg[1] >= 0 && sg[2] >= 0;
   }
-  quad_signs_exact(c, T, sg);
+  const double* e1 = e[0];
+  const double* e2 = e[1];
+  const double* e3 = e[2];
+  const double c23x = e2[1] * e3[2] - e2[2] * e3[1], c23y = e2[2] * e3[0] - e2[0] * e3[2], c23z = e2[0] * e3[1] - e2[1] * e3[0];
+  const double c31x = e3[1] * e1[2] - e3[2] * e1[1], c31y = e3[2] * e1[0] - e3[0] * e1[2], c31z = e3[0] * e1[1] - e3[1] * e1[0];
+  const double c12x = e1[1] * e2[2] - e1[2] * e2[1], c12y = e1[2] * e2[0] - e1[0] * e2[2], c12z = e1[0] * e2[1] - e1[1] * e2[0];
+  const double q1 = (e1[0] * e1[0] + e1[1] * e1[1]) + e1[2] * e1[2];
+  const double q2 = (e2[0] * e2[0] + e2[1] * e2[1]) + e2[2] * e2[2];
+  const double q3 = (e3[0] * e3[0] + e3[1] * e3[1]) + e3[2] * e3[2];
+  const double detE = (e1[0] * c23x + e1[1] * c23y) + e1[2] * c23z;
+  const double Nx = (q1 * c23x + q2 * c31x) + q3 * c12x;
+  const double Ny = (q1 * c23y + q2 * c31y) + q3 * c12y;
+  const double Nz = (q1 * c23z + q2 * c31z) + q3 * c12z;
+  const double l1 = (Nx * c23x + Ny * c23y) + Nz * c23z;
+  const double l2 = (Nx * c31x + Ny * c31y) + Nz * c31z;
+  const double l3 = (Nx * c12x + Ny * c12y) + Nz * c12z;
+  const double l0 = (2.0 * detE) * detE - ((l1 + l2) + l3);
+  const double M6 = M2 * M2 * M2;
+  sg[0] = fs(detE, kFilt * 6.0 * M2 * M + kTiny);
+  sg[1] = fs(l0, kFilt * 396.0 * M6 + kTiny);
+  sg[2] = fs(l1, kFilt * 108.0 * M6 + kTiny);
+  sg[3] = fs(l2, kFilt * 108.0 * M6 + kTiny);
+  sg[4] = fs(l3, kFilt * 108.0 * M6 + kTiny);
+  if (undecided) quad_signs_exact(c, T, sg);
   return sg[0] != 0 && sg[1] >= 0 && sg[2] >= 0 && sg[3] >= 0 && sg[4] >= 0;
 }
 
@@ -744,63 +790,92 @@ __device__ __noinline__ int topk_choice(const DescentParams& d, const Cloud& c, 
   if (on_sphere) {
     *cut_below = 0;
   } else {
-    const int s = dist_cmp_exact(c, mb.T, mb.ts, cut_point, mb.T[0]);
-    if (s > 0) return kArmInternal;
-    *cut_below = s < 0 ? 1 : 0;
+    // FP64 first: the cutoff's approximate distance against the radius interval
+    const double dcut = band0 == band1 ? cd[band0] : tk + 2.0 * ed;  // upper bound of the cutoff's FP distance
+    if (dcut + ed < llo) {
+      *cut_below = 1;
+    } else {
+      const int s = dist_cmp_exact(c, mb.T, mb.ts, cut_point, mb.T[0]);
+      if (s > 0) return kArmInternal;
+      *cut_below = s < 0 ? 1 : 0;
+    }
   }
   return kArmOk;
 }
 
-__global__ void __launch_bounds__(128)
-k_descent(DescentParams d, uint32_t narms, const uint32_t* __restrict__ fam_event,
-          const uint32_t* __restrict__ arm_family, const uint8_t* __restrict__ arm_local, const EvRec* __restrict__ ev,
-          uint32_t* __restrict__ term, uint8_t* __restrict__ status, unsigned long long* __restrict__ stats) {
+// Facet of arm a: F_u = (I u U) \ {u}, ascending.
+__device__ __forceinline__ int arm_facet(const EvRec& e, uint32_t removed, uint32_t* F) {
+  int k = event_facet(e, F);
+  int w = 0;
+  for (int j = 0; j < k; ++j)
+    if (F[j] != removed) F[w++] = F[j];
+  return w;
+}
+
+// First probe of every arm: most arms are themselves a birth facet of their order.
+// Misses are queued with their facet for the descent steps.
+__global__ void k_arm_probe(DescentParams d, uint32_t narms, const uint32_t* __restrict__ fam_event,
+                            const uint32_t* __restrict__ arm_family, const uint8_t* __restrict__ arm_local,
+                            const EvRec* __restrict__ ev, uint32_t* __restrict__ term, uint8_t* __restrict__ status,
+                            uint32_t* __restrict__ q_arm, uint32_t* __restrict__ q_fac, uint32_t* __restrict__ q_count) {
   const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= narms) return;
   const EvRec e = ev[fam_event[arm_family[a]]];
-  const uint32_t removed = e.ids[arm_local[a]];
   uint32_t F[kMaxFacet + 1];
-  int k = event_facet(e, F);
-  {
-    int w = 0;
-    for (int j = 0; j < k; ++j)
-      if (F[j] != removed) F[w++] = F[j];
-    k = w;
+  const int k = arm_facet(e, e.ids[arm_local[a]], F);
+  const uint32_t h = probe_facet(d, F, k);
+  term[a] = h;
+  status[a] = kArmOk;
+  if (h != kInvalid32) return;
+  const uint32_t slot = atomicAdd(q_count, 1u);
+  q_arm[slot] = a;
+  for (int j = 0; j < kMaxFacet; ++j) q_fac[(uint64_t)slot * kMaxFacet + j] = j < k ? F[j] : kInvalid32;
+}
+
+// One strict descent step for every queued arm: exact miniball of F, exact canonical
+// top-k choice G at its centre, certified beta(G) < beta(F); G is probed and either
+// binds the arm or is queued for the next step.
+__global__ void __launch_bounds__(128)
+k_arm_step(DescentParams d, uint32_t m, const uint32_t* __restrict__ in_arm, const uint32_t* __restrict__ in_fac,
+           uint32_t* __restrict__ out_arm, uint32_t* __restrict__ out_fac, uint32_t* __restrict__ out_count,
+           uint32_t* __restrict__ term, uint8_t* __restrict__ status, unsigned long long* __restrict__ stats) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const uint32_t a = in_arm[i];
+  uint32_t F[kMaxFacet];
+  int k = 0;
+  for (int j = 0; j < kMaxFacet; ++j) {
+    F[j] = in_fac[(uint64_t)i * kMaxFacet + j];
+    k += F[j] != kInvalid32;
   }
   const Cloud c{d.px, d.py, d.pz, d.S};
-  unsigned long long steps = 0;
-  uint8_t st = kArmSteps;
-  uint32_t res = kInvalid32;
-  for (int step = 0; step < kDescentSteps; ++step) {
-    const uint32_t h = probe_facet(d, F, k);
-    if (h != kInvalid32) {
-      res = h;
-      st = kArmOk;
-      break;
-    }
-    ++steps;
-    Mini mb;
-    if (!facet_miniball(c, F, k, mb)) { st = kArmInternal; break; }
-    uint32_t G[kMaxFacet];
-    int cut_below = 0;
-    const int s = topk_choice(d, c, mb, k, G, &cut_below);
-    if (s != kArmOk) { st = (uint8_t)s; break; }
-    bool same = true;
-    for (int j = 0; j < k; ++j) same &= G[j] == F[j];
-    if (same) { st = kArmUnresolved; break; }
-    if (!cut_below) {  // beta(G) <= cutoff = beta(F): the decrease must be strict
-      Mini mg;
-      if (!facet_miniball(c, G, k, mg)) { st = kArmInternal; break; }
-      double glo, ghi, flo, fhi;
-      if (!flevel(mg.fs, glo, ghi)) exact_level_fp(c, mg.T, mg.ts, glo, ghi);
-      if (!flevel(mb.fs, flo, fhi)) exact_level_fp(c, mb.T, mb.ts, flo, fhi);
-      if (!(ghi < flo) && level_cmp_exact(c, mg.T, mg.ts, mb.T, mb.ts) >= 0) { st = kArmPlateau; break; }
-    }
-    for (int j = 0; j < k; ++j) F[j] = G[j];
+  Mini mb;
+  if (!facet_miniball(c, F, k, mb)) { status[a] = kArmInternal; return; }
+  uint32_t G[kMaxFacet];
+  int cut_below = 0;
+  const int s = topk_choice(d, c, mb, k, G, &cut_below);
+  if (s != kArmOk) { status[a] = (uint8_t)s; return; }
+  bool same = true;
+  for (int j = 0; j < k; ++j) same &= G[j] == F[j];
+  if (same) { status[a] = kArmUnresolved; return; }
+  if (!cut_below) {  // beta(G) <= cutoff = beta(F): the decrease must be strict
+    Mini mg;
+    if (!facet_miniball(c, G, k, mg)) { status[a] = kArmInternal; return; }
+    double glo, ghi, flo, fhi;
+    if (!flevel(mg.fs, glo, ghi)) exact_level_fp(c, mg.T, mg.ts, glo, ghi);
+    if (!flevel(mb.fs, flo, fhi)) exact_level_fp(c, mb.T, mb.ts, flo, fhi);
+    if (!(ghi < flo) && level_cmp_exact(c, mg.T, mg.ts, mb.T, mb.ts) >= 0) { status[a] = kArmPlateau; return; }
+    atomicAdd(stats + 2, 1ull);
   }
-  term[a] = res;
-  status[a] = st;
-  atomicAdd(stats, steps);
+  atomicAdd(stats, 1ull);
+  const uint32_t h = probe_facet(d, G, k);
+  if (h != kInvalid32) {
+    term[a] = h;
+    return;
+  }
+  const uint32_t slot = atomicAdd(out_count, 1u);
+  out_arm[slot] = a;
+  for (int j = 0; j < kMaxFacet; ++j) out_fac[(uint64_t)slot * kMaxFacet + j] = j < k ? G[j] : kInvalid32;
 }
 
 }  // namespace
@@ -838,6 +913,11 @@ struct HierState {
   uint32_t* term = nullptr;
   uint8_t* arm_status = nullptr;
   unsigned long long* dstats = nullptr;
+  uint32_t* qcount = nullptr;   // [0] first-probe misses, [1], [2] step outputs (ping-pong)
+  uint32_t* q_arm[2] = {nullptr, nullptr};
+  uint32_t* q_fac[2] = {nullptr, nullptr};
+  uint64_t q_cap = 0;
+  uint32_t first_misses = 0, descent_rounds = 0;
   // host results
   uint32_t n = 0, K = 0, keff = 0;
   int S = 0;
@@ -865,6 +945,9 @@ struct HierState {
 void hier_free(Ctx& ctx) {
   if (!ctx.hier) return;
   for (void* p : ctx.hier->allocs) cudaFree(p);
+  for (void* p : {(void*)ctx.hier->q_arm[0], (void*)ctx.hier->q_arm[1], (void*)ctx.hier->q_fac[0],
+                  (void*)ctx.hier->q_fac[1]})
+    if (p) cudaFree(p);
   delete ctx.hier;
   ctx.hier = nullptr;
 }
@@ -884,6 +967,7 @@ cudaError_t halloc(HierState& h, T** p, uint64_t count) {
 void hfree_all(HierState& h) {
   for (void* p : h.allocs) cudaFree(p);
   h.allocs.clear();
+  h.qcount = nullptr;
   h.cap_events = h.cap_arms = h.cap_births = h.cap_slots = 0;
 }
 
@@ -1148,10 +1232,43 @@ int hier_run(Ctx& ctx, uint32_t K) {
     DescentParams dp{n, 2 * n - 2, g.tnodes, b.px, b.py, b.pz, h.S, h.slots, (uint32_t)(h.cap_slots - 1), h.bfac,
                      (uint32_t)nb_higher};
     cudaEventRecord(ctx.evk0, st);
-    k_descent<<<nblk(narms, 128), 128, 0, st>>>(dp, (uint32_t)narms, h.fam_event, h.arm_family, h.arm_local, h.ev,
-                                                h.term, h.arm_status, h.dstats);
-    cudaEventRecord(ctx.evk1, st);
+    // first probe; misses queue for descent steps (queue buffers sized by the misses)
+    if (!h.qcount && (e = halloc(h, &h.qcount, 4)) != cudaSuccess)
+      return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "descent queue");
+    cudaMemsetAsync(h.qcount, 0, 4 * sizeof(uint32_t), st);
+    if (h.q_cap < narms) {  // worst case: every arm misses
+      for (void* p : {(void*)h.q_arm[0], (void*)h.q_arm[1], (void*)h.q_fac[0], (void*)h.q_fac[1]})
+        if (p) cudaFree(p);
+      h.q_arm[0] = h.q_arm[1] = h.q_fac[0] = h.q_fac[1] = nullptr;
+      const uint64_t qc = narms + narms / 8 + 1024;
+      if (cudaMalloc(&h.q_arm[0], qc * 4) != cudaSuccess || cudaMalloc(&h.q_arm[1], qc * 4) != cudaSuccess ||
+          cudaMalloc(&h.q_fac[0], qc * 4 * kMaxFacet) != cudaSuccess ||
+          cudaMalloc(&h.q_fac[1], qc * 4 * kMaxFacet) != cudaSuccess)
+        return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "descent queue buffers do not fit the device");
+      h.q_cap = qc;
+    }
+    k_arm_probe<<<nblk(narms, kT), kT, 0, st>>>(dp, (uint32_t)narms, h.fam_event, h.arm_family, h.arm_local, h.ev,
+                                                h.term, h.arm_status, h.q_arm[0], h.q_fac[0], h.qcount);
     ++launches;
+    uint32_t pending = 0;
+    cudaMemcpyAsync(&pending, h.qcount, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "strict-arm probe");
+    h.first_misses = pending;
+    int cur = 0;
+    uint32_t rounds = 0;
+    while (pending) {
+      if (++rounds > (uint32_t)kDescentSteps) return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "a strict arm descent exceeded its step budget");
+      uint32_t* oc = h.qcount + 1 + (1 - cur);
+      cudaMemsetAsync(oc, 0, sizeof(uint32_t), st);
+      k_arm_step<<<nblk(pending, 128), 128, 0, st>>>(dp, pending, h.q_arm[cur], h.q_fac[cur], h.q_arm[1 - cur],
+                                                     h.q_fac[1 - cur], oc, h.term, h.arm_status, h.dstats);
+      ++launches;
+      cudaMemcpyAsync(&pending, oc, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+      if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "strict-arm descent step");
+      cur = 1 - cur;
+    }
+    h.descent_rounds = rounds;
+    cudaEventRecord(ctx.evk1, st);
     cudaMemcpyAsync(term.data(), h.term, narms * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(astat.data(), h.arm_status, narms, cudaMemcpyDeviceToHost, st);
   }
@@ -1186,6 +1303,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
   }
   // ---- host: journal, seeds and the forest journal, order by order
   const auto t1 = std::chrono::steady_clock::now();
+  const uint64_t birth_count = n + nb_higher;
   h.jbatches.clear();
   h.roles.clear();
   h.families.clear();
@@ -1198,34 +1316,54 @@ int hier_run(Ctx& ctx, uint32_t K) {
   h.groups.clear();
   h.fbatches.clear();
   h.roots.clear();
-  const uint64_t birth_count = n + nb_higher;
+  h.roles.reserve(n + 2 * (uint64_t)m);
+  h.jbatches.reserve(n + 2 * (uint64_t)m);
+  h.fbatches.reserve(n + 2 * (uint64_t)m);
+  h.families.reserve(nfam);
+  h.saddles.reserve(nfam);
+  h.groups.reserve(nfam);
+  h.arm_removed.reserve(narms);
+  h.bindings.reserve(narms);
+  h.births.reserve(birth_count);
   std::vector<uint32_t> parent(birth_count), border(birth_count, 0), rroot(birth_count, kInvalid32);
   std::vector<uint8_t> active(birth_count, 0);
   std::iota(parent.begin(), parent.end(), 0u);
   auto find = [&](uint32_t x) {
-    while (parent[x] != x) x = parent[x];
-    return x;
+    uint32_t r = x;
+    while (parent[r] != r) r = parent[r];
+    return r;  // no compression: the least-handle union keeps paths short and the reference has none
   };
   std::vector<uint64_t> carriers_of(keff + 2, 0), reduced_of(keff + 2, 0);
-  // journal and forest, order by order
-  std::vector<uint32_t> fam_index_of(nfam);  // family position in the rank partition -> journal family index
+  std::vector<uint32_t> fam_index_of(nfam);  // rank-partition position -> journal family index
+  // per-batch scratch, reused
+  struct Role {
+    uint32_t proj, role, fi, pos;
+  };
+  struct Arm {
+    uint32_t seed, carrier, prior, saddle;
+  };
+  struct Plan {
+    uint32_t c_off, c_cnt, p_off, p_cnt, s_off, s_cnt, kind, created, result;
+  };
+  std::vector<Role> batch_roles;
+  std::vector<uint32_t> fam_pos;      // batch saddles: rank-partition positions
+  std::vector<Arm> arms_b;            // batch arms
+  std::vector<uint32_t> arm_b_off;    // per batch saddle: first arm
+  std::vector<uint32_t> cars, qp, plan_of, plan_car, plan_prior, plan_sad, tmp;
+  std::vector<Plan> plans;
+  std::vector<ehgp_forest_node> gnodes;
+  std::vector<uint32_t> new_births;
   uint32_t role_count = 0;
   for (uint32_t k = 1; k <= keff; ++k) {
-    // births of order k: singletons (k = 1) or rank-k events; saddles: rank-(k+1) events
     const uint64_t b_lo = k == 1 ? 0 : rb[k], b_hi = k == 1 ? 0 : rb[k + 1];
     const uint64_t s_lo = rb[k + 1], s_hi = rb[k + 2 > 16 ? 16 : k + 2];
     uint64_t bi = b_lo, si = s_lo;
     bool singles = k == 1;
     while (singles || bi < b_hi || si < s_hi) {
-      // next batch: the least level class among the heads (singletons: level 0 first)
-      const uint32_t cls_b = bi < b_hi ? h.h_class[rank_order[bi]] : kInvalid32;
-      const uint32_t cls_s = si < s_hi ? h.h_class[rank_order[si]] : kInvalid32;
-      uint32_t cls;
-      uint32_t lev;
-      if (singles) {
-        cls = kInvalid32;
-        lev = kInvalid32;
-      } else {
+      uint32_t cls = kInvalid32, lev = kInvalid32;
+      if (!singles) {
+        const uint32_t cls_b = bi < b_hi ? h.h_class[rank_order[bi]] : kInvalid32;
+        const uint32_t cls_s = si < s_hi ? h.h_class[rank_order[si]] : kInvalid32;
         cls = std::min(cls_b, cls_s);
         lev = cls_b <= cls_s ? rank_order[bi] : rank_order[si];
       }
@@ -1236,11 +1374,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
       fb.level_event = lev;
       fb.pre_carriers = (uint32_t)carriers_of[k];
       fb.pre_roots = (uint32_t)reduced_of[k];
-      // roles in projection order: births and saddles of this class
-      struct Role {
-        uint32_t proj, role, fi, pos;
-      };
-      std::vector<Role> batch_roles;
+      batch_roles.clear();
       if (singles) {
         for (uint32_t p = 0; p < n; ++p) batch_roles.push_back({p, 0, kInvalid32, p});
       } else {
@@ -1248,135 +1382,162 @@ int hier_run(Ctx& ctx, uint32_t K) {
           batch_roles.push_back({n + rank_order[bi], 0, rank_order[bi], (uint32_t)(bi - rb[2])});
           ++bi;
         }
+        const size_t nbr = batch_roles.size();
         while (si < s_hi && h.h_class[rank_order[si]] == cls) {
           batch_roles.push_back({n + rank_order[si], 1, rank_order[si], (uint32_t)(si - fam_lo)});
           ++si;
         }
-        std::sort(batch_roles.begin(), batch_roles.end(), [](const Role& x, const Role& y) {
-          return x.proj != y.proj ? x.proj < y.proj : x.role < y.role;
-        });
+        if (nbr && nbr < batch_roles.size())  // both kinds: merge by projection (role breaks no tie: distinct events)
+          std::inplace_merge(batch_roles.begin(), batch_roles.begin() + nbr, batch_roles.end(),
+                             [](const Role& x, const Role& y) { return x.proj < y.proj; });
       }
       singles = false;
-      // saddle families of this batch (journal order)
-      struct Arm {
-        uint32_t seed, carrier, prior;
-      };
-      std::vector<uint32_t> fam_ids;
-      for (const Role& r : batch_roles) {
+      // journal roles and saddle families
+      fam_pos.clear();
+      for (size_t q = 0; q < batch_roles.size(); ++q) {
+        const Role& r = batch_roles[q];
         h.roles.push_back({bidx, r.proj, r.role});
-        if (r.role == 0) ++jb.birth_roles;
-        else ++jb.saddle_roles;
-        if (r.role == 1) {
-          const EvRec& ev = h.h_ev[r.fi];
-          const uint32_t fidx = (uint32_t)h.families.size();
-          fam_index_of[r.pos] = fidx;
-          h.families.push_back({r.fi, r.proj, role_count + (uint32_t)(&r - batch_roles.data()), bidx, k,
-                                (uint32_t)h.arm_removed.size(), ev.size});
-          for (uint32_t j = 0; j < ev.size; ++j) h.arm_removed.push_back(ev.ids[j]);
-          fam_ids.push_back(r.pos);
+        if (r.role == 0) {
+          ++jb.birth_roles;
+          continue;
         }
+        ++jb.saddle_roles;
+        const EvRec& ev = h.h_ev[r.fi];
+        const uint32_t fidx = (uint32_t)h.families.size();
+        fam_index_of[r.pos] = fidx;
+        h.families.push_back({r.fi, r.proj, role_count + (uint32_t)q, bidx, k, (uint32_t)h.arm_removed.size(), ev.size});
+        for (uint32_t j = 0; j < ev.size; ++j) h.arm_removed.push_back(ev.ids[j]);
+        fam_pos.push_back(r.pos);
       }
       jb.role_count = (uint32_t)batch_roles.size();
       role_count += jb.role_count;
       h.jbatches.push_back(jb);
-      // resolve arms against the pre-batch components
-      std::vector<std::vector<Arm>> sad(fam_ids.size());
-      for (size_t q = 0; q < fam_ids.size(); ++q) {
-        const uint32_t fpos = fam_ids[q];
+      // arms resolved against the pre-batch components
+      arms_b.clear();
+      arm_b_off.clear();
+      for (uint32_t q = 0; q < fam_pos.size(); ++q) {
+        const uint32_t fpos = fam_pos[q];
         const uint32_t fidx = fam_index_of[fpos];
+        arm_b_off.push_back((uint32_t)arms_b.size());
         for (uint64_t a = arm_off[fpos]; a < arm_off[fpos + 1]; ++a) {
           if (term[a] >= birth_count || !active[term[a]])
             return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "a strict arm descended to a minimum that is not yet born");
           const uint32_t c0 = find(term[a]);
-          sad[q].push_back({h.families[fidx].arm_offset + (uint32_t)(a - arm_off[fpos]), c0, rroot[c0]});
+          arms_b.push_back({h.families[fidx].arm_offset + (uint32_t)(a - arm_off[fpos]), c0, rroot[c0], q});
         }
       }
-      // frozen-root quotient: transitive classes over the saddles' carriers
-      std::vector<uint32_t> cars;
-      for (auto& as : sad)
-        for (auto& a : as) cars.push_back(a.carrier);
-      std::sort(cars.begin(), cars.end());
-      cars.erase(std::unique(cars.begin(), cars.end()), cars.end());
-      std::vector<uint32_t> qp(cars.size());
-      std::iota(qp.begin(), qp.end(), 0u);
-      auto qi = [&](uint32_t x) { return (uint32_t)(std::lower_bound(cars.begin(), cars.end(), x) - cars.begin()); };
-      auto qf = [&](uint32_t x) {
-        while (qp[x] != x) x = qp[x] = qp[qp[x]];
-        return x;
-      };
-      for (auto& as : sad)
-        for (auto& a : as) {
-          const uint32_t x = qf(qi(as[0].carrier)), y = qf(qi(a.carrier));
-          if (x != y) qp[std::max(x, y)] = std::min(x, y);
+      arm_b_off.push_back((uint32_t)arms_b.size());
+      // frozen-root quotient: transitive classes over the saddles' carriers,
+      // groups ordered by their least carrier, carriers ascending
+      plans.clear();
+      plan_car.clear();
+      plan_prior.clear();
+      plan_sad.clear();
+      if (!fam_pos.empty()) {
+        cars.clear();
+        for (const Arm& a : arms_b) cars.push_back(a.carrier);
+        std::sort(cars.begin(), cars.end());
+        cars.erase(std::unique(cars.begin(), cars.end()), cars.end());
+        const uint32_t nc = (uint32_t)cars.size();
+        auto qi = [&](uint32_t x) { return (uint32_t)(std::lower_bound(cars.begin(), cars.end(), x) - cars.begin()); };
+        qp.resize(nc);
+        std::iota(qp.begin(), qp.end(), 0u);
+        auto qf = [&](uint32_t x) {
+          while (qp[x] != x) x = qp[x] = qp[qp[x]];
+          return x;
+        };
+        for (uint32_t q = 0; q + 1 < arm_b_off.size(); ++q) {
+          const uint32_t a0 = qf(qi(arms_b[arm_b_off[q]].carrier));
+          for (uint32_t a = arm_b_off[q] + 1; a < arm_b_off[q + 1]; ++a) {
+            const uint32_t x = qf(a0), y = qf(qi(arms_b[a].carrier));
+            if (x != y) qp[std::max(x, y)] = std::min(x, y);
+          }
         }
-      // groups ordered by their least carrier; carriers ascending
-      std::vector<int32_t> group_of(cars.size(), -1);
-      struct Plan {
-        std::vector<uint32_t> carriers, priors, saddles;
-        uint32_t kind, created, result;
-      };
-      std::vector<Plan> plans;
-      for (uint32_t i = 0; i < cars.size(); ++i) {
-        const uint32_t r0 = qf(i);
-        if (group_of[r0] < 0) {
-          group_of[r0] = (int32_t)plans.size();
-          plans.push_back({});
+        plan_of.assign(nc, kInvalid32);
+        for (uint32_t i = 0; i < nc; ++i) {
+          const uint32_t r0 = qf(i);
+          if (plan_of[r0] == kInvalid32) {
+            plan_of[r0] = (uint32_t)plans.size();
+            plans.push_back({0, 0, 0, 0, 0, 0, 0, kInvalid32, 0});
+          }
         }
-        Plan& p = plans[group_of[r0]];
-        p.carriers.push_back(cars[i]);
-        if (rroot[cars[i]] != kInvalid32) p.priors.push_back(rroot[cars[i]]);
-      }
-      for (size_t q = 0; q < sad.size(); ++q) plans[group_of[qf(qi(sad[q][0].carrier))]].saddles.push_back((uint32_t)q);
-      uint32_t pending = 0;
-      for (Plan& p : plans) {
-        std::sort(p.priors.begin(), p.priors.end());
-        if (std::adjacent_find(p.priors.begin(), p.priors.end()) != p.priors.end())
-          return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "a frozen carrier class repeats a reduced root");
-        if (p.priors.size() == 1) {
-          p.kind = 1;
-          p.created = kInvalid32;
-          p.result = p.priors[0];
-        } else {
-          if (p.priors.empty() && k == 1) return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "an order-one group has no root");
-          p.kind = p.priors.empty() ? 0 : 2;
-          p.created = (uint32_t)h.nodes.size() + pending++;
-          p.result = p.created;
+        // carriers and prior roots per plan (two counting passes keep slices contiguous)
+        for (uint32_t i = 0; i < nc; ++i) {
+          Plan& p = plans[plan_of[qf(i)]];
+          ++p.c_cnt;
+          if (rroot[cars[i]] != kInvalid32) ++p.p_cnt;
+        }
+        for (uint32_t q = 0; q + 1 < arm_b_off.size(); ++q) ++plans[plan_of[qf(qi(arms_b[arm_b_off[q]].carrier))]].s_cnt;
+        uint32_t co = 0, po = 0, so = 0;
+        for (Plan& p : plans) {
+          p.c_off = co; p.p_off = po; p.s_off = so;
+          co += p.c_cnt; po += p.p_cnt; so += p.s_cnt;
+          p.c_cnt = p.p_cnt = p.s_cnt = 0;
+        }
+        plan_car.resize(co);
+        plan_prior.resize(po);
+        plan_sad.resize(so);
+        for (uint32_t i = 0; i < nc; ++i) {
+          Plan& p = plans[plan_of[qf(i)]];
+          plan_car[p.c_off + p.c_cnt++] = cars[i];
+          if (rroot[cars[i]] != kInvalid32) plan_prior[p.p_off + p.p_cnt++] = rroot[cars[i]];
+        }
+        for (uint32_t q = 0; q + 1 < arm_b_off.size(); ++q) {
+          Plan& p = plans[plan_of[qf(qi(arms_b[arm_b_off[q]].carrier))]];
+          plan_sad[p.s_off + p.s_cnt++] = q;
+        }
+        uint32_t pending = 0;
+        for (Plan& p : plans) {
+          uint32_t* pr = plan_prior.data() + p.p_off;
+          std::sort(pr, pr + p.p_cnt);
+          if (std::adjacent_find(pr, pr + p.p_cnt) != pr + p.p_cnt)
+            return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "a frozen carrier class repeats a reduced root");
+          if (p.p_cnt == 1) {
+            p.kind = 1;
+            p.created = kInvalid32;
+            p.result = pr[0];
+          } else {
+            if (p.p_cnt == 0 && k == 1) return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "an order-one group has no root");
+            p.kind = p.p_cnt == 0 ? 0 : 2;
+            p.created = (uint32_t)h.nodes.size() + pending++;
+            p.result = p.created;
+          }
         }
       }
       fb.saddle_offset = (uint32_t)h.saddles.size();
       fb.group_offset = (uint32_t)h.groups.size();
-      std::vector<ehgp_forest_node> gnodes;
-      for (Plan& p : plans) {
+      gnodes.clear();
+      for (const Plan& p : plans) {
         const uint32_t g_soff = (uint32_t)h.saddles.size();
         const uint32_t gidx = (uint32_t)h.groups.size();
-        for (uint32_t q : p.saddles) {
-          const uint32_t fidx = fam_index_of[fam_ids[q]];
+        for (uint32_t t = 0; t < p.s_cnt; ++t) {
+          const uint32_t q = plan_sad[p.s_off + t];
+          const uint32_t fidx = fam_index_of[fam_pos[q]];
           const uint32_t arm_o = (uint32_t)h.bindings.size();
-          std::vector<uint32_t> cs, ps;
-          for (const Arm& a : sad[q]) {
-            h.bindings.push_back({a.seed, fidx, a.carrier, a.prior});
-            cs.push_back(a.carrier);
-            if (a.prior != kInvalid32) ps.push_back(a.prior);
+          tmp.clear();
+          uint32_t nprior = 0;
+          for (uint32_t a = arm_b_off[q]; a < arm_b_off[q + 1]; ++a) {
+            const Arm& am = arms_b[a];
+            h.bindings.push_back({am.seed, fidx, am.carrier, am.prior});
+            tmp.push_back(am.carrier);
           }
-          std::sort(cs.begin(), cs.end());
-          cs.erase(std::unique(cs.begin(), cs.end()), cs.end());
-          std::sort(ps.begin(), ps.end());
-          ps.erase(std::unique(ps.begin(), ps.end()), ps.end());
-          h.saddles.push_back({fidx, h.families[fidx].event, bidx, arm_o, (uint32_t)sad[q].size(), (uint32_t)cs.size(),
-                               (uint32_t)(cs.size() - ps.size()), (uint32_t)ps.size(), gidx});
+          std::sort(tmp.begin(), tmp.end());
+          tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+          for (uint32_t c0 : tmp) nprior += rroot[c0] != kInvalid32;  // carriers are pre-batch roots
+          h.saddles.push_back({fidx, h.families[fidx].event, bidx, arm_o, arm_b_off[q + 1] - arm_b_off[q],
+                               (uint32_t)tmp.size(), (uint32_t)tmp.size() - nprior, nprior, gidx});
         }
-        const uint32_t ccnt = p.kind == 2 ? (uint32_t)p.priors.size() : 0u;
-        h.groups.push_back({bidx, g_soff, (uint32_t)h.saddles.size() - g_soff, (uint32_t)p.carriers.size(),
-                            (uint32_t)(p.carriers.size() - p.priors.size()), (uint32_t)p.priors.size(),
+        const uint32_t ccnt = p.kind == 2 ? p.p_cnt : 0u;
+        h.groups.push_back({bidx, g_soff, (uint32_t)h.saddles.size() - g_soff, p.c_cnt, p.c_cnt - p.p_cnt, p.p_cnt,
                             (uint32_t)h.children.size(), ccnt, p.created, p.result, p.kind});
         if (p.kind != 1)
           gnodes.push_back({k, lev, p.kind == 0 ? 1u : 2u, (uint32_t)h.children.size(), ccnt, kInvalid32, gidx});
-        if (p.kind == 2) h.children.insert(h.children.end(), p.priors.begin(), p.priors.end());
+        if (p.kind == 2) h.children.insert(h.children.end(), plan_prior.begin() + p.p_off, plan_prior.begin() + p.p_off + p.p_cnt);
       }
       h.nodes.insert(h.nodes.end(), gnodes.begin(), gnodes.end());
-      // births of this batch
+      // births of this batch (hidden from this batch's arms)
       fb.birth_offset = (uint32_t)h.births.size();
-      std::vector<uint32_t> new_births;
+      new_births.clear();
       for (const Role& r : batch_roles) {
         if (r.role != 0) continue;
         const uint32_t handle = (uint32_t)h.births.size();
@@ -1391,11 +1552,11 @@ int hier_run(Ctx& ctx, uint32_t K) {
         new_births.push_back(handle);
       }
       // commit: unions (least handle survives), reduced roots, then births
-      for (Plan& p : plans) {
-        uint32_t r0 = find(p.carriers.front());
+      for (const Plan& p : plans) {
+        uint32_t r0 = find(plan_car[p.c_off]);
         uint32_t had_reduced = rroot[r0] != kInvalid32;
-        for (size_t i = 1; i < p.carriers.size(); ++i) {
-          const uint32_t r1 = find(p.carriers[i]);
+        for (uint32_t i = 1; i < p.c_cnt; ++i) {
+          const uint32_t r1 = find(plan_car[p.c_off + i]);
           if (r1 == r0) continue;
           had_reduced += rroot[r1] != kInvalid32;
           const uint32_t lo = std::min(r0, r1), hi = std::max(r0, r1);
@@ -1517,6 +1678,8 @@ int ehgp_hier_stats(const ehgp_ctx* ctx, double* ms, uint64_t* stats) {
     stats[1] = h.descent_steps;
     stats[2] = h.exact_boundaries;
     stats[3] = h.events;
+    stats[4] = h.first_misses;
+    stats[5] = h.descent_rounds;
   }
   return EHGP_OK;
 }

@@ -419,21 +419,23 @@ class Context:
         out = dict(self.last_hier_counts)
         if arrays:
             bufs = {}
+            cnts = self.last_hier_counts
             for name, dt, cf in _HIER_FIELDS:
-                bufs[name] = np.zeros(max(int(out[cf]), 1), dt)
+                bufs[name] = np.zeros(max(int(cnts[cf]), 1), dt)
             ho = HierOut(*[_ptr(bufs[name]) for name, _, _ in _HIER_FIELDS])
             self._check(self.lib.ehgp_hier_copy(self._h, C.byref(ho)))
             for name, _, cf in _HIER_FIELDS:
-                out[name] = bufs[name][:int(out[cf])]
+                out[name] = bufs[name][:int(cnts[cf])]
         return out
 
     def hier_stats(self) -> dict:
         """Timing and work counters of the last hierarchy call."""
         ms = np.zeros(3)
-        st = np.zeros(4, np.uint64)
+        st = np.zeros(6, np.uint64)
         self._check(self.lib.ehgp_hier_stats(self._h, _ptr(ms), _ptr(st)))
         return {"device_ms": ms[0], "descent_ms": ms[1], "forest_ms": ms[2], "arms": int(st[0]),
-                "descent_steps": int(st[1]), "exact_boundaries": int(st[2]), "events": int(st[3])}
+                "descent_steps": int(st[1]), "exact_boundaries": int(st[2]), "events": int(st[3]),
+                "first_misses": int(st[4]), "descent_rounds": int(st[5])}
 
     def event_level(self, event: int):
         """Exact level of a facade event as a Fraction (cloud units)."""

@@ -384,7 +384,8 @@ int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out);
 /* Timing of the last ehgp_hierarchy call: ms[0] device stages (CUDA events),
  * ms[1] the strict-arm descent kernel, ms[2] the host forest pass;
  * stats[0] strict arms, [1] descent steps, [2] facade boundaries settled
- * exactly on the host, [3] facade events. */
+ * exactly on the host, [3] facade events, [4] arms that are not themselves a
+ * birth facet, [5] descent rounds (longest chain); stats holds 6 words. */
 int ehgp_hier_stats(const ehgp_ctx* ctx, double* ms, uint64_t* stats);
 
 /* Exact level of facade event `event` as num / (den 2^(2 scale)), two's
