@@ -39,6 +39,7 @@
 #include <cstring>
 #include <map>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 namespace ehgp {
@@ -1301,62 +1302,66 @@ int hier_run(Ctx& ctx, uint32_t K) {
     h.decision = astat[a] == kArmCapacity ? EHGP_ERR_CAPACITY : EHGP_ERR_DEGENERATE;
     return abi_fail(&ctx, (int)h.decision, msg[astat[a] < 6 ? astat[a] : 5]);
   }
-  // ---- host: journal, seeds and the forest journal, order by order
+  // ---- host: journal, seeds and the forest journal ------------------------------------
+  // Orders are independent (their handles, components and nodes never meet), so each
+  // order runs on its own host thread with local indices; the arenas are then
+  // concatenated in order with the offsets the reference's single pass would give.
   const auto t1 = std::chrono::steady_clock::now();
   const uint64_t birth_count = n + nb_higher;
-  h.jbatches.clear();
-  h.roles.clear();
-  h.families.clear();
-  h.arm_removed.clear();
-  h.nodes.clear();
-  h.children.clear();
-  h.births.clear();
-  h.bindings.clear();
-  h.saddles.clear();
-  h.groups.clear();
-  h.fbatches.clear();
-  h.roots.clear();
-  h.roles.reserve(n + 2 * (uint64_t)m);
-  h.jbatches.reserve(n + 2 * (uint64_t)m);
-  h.fbatches.reserve(n + 2 * (uint64_t)m);
-  h.families.reserve(nfam);
-  h.saddles.reserve(nfam);
-  h.groups.reserve(nfam);
-  h.arm_removed.reserve(narms);
-  h.bindings.reserve(narms);
-  h.births.reserve(birth_count);
   std::vector<uint32_t> parent(birth_count), border(birth_count, 0), rroot(birth_count, kInvalid32);
   std::vector<uint8_t> active(birth_count, 0);
   std::iota(parent.begin(), parent.end(), 0u);
-  auto find = [&](uint32_t x) {
-    uint32_t r = x;
-    while (parent[r] != r) r = parent[r];
-    return r;  // no compression: the least-handle union keeps paths short and the reference has none
+  struct OrderOut {
+    std::vector<ehgp_journal_batch> jb;
+    std::vector<ehgp_role_record> roles;
+    std::vector<ehgp_family_record> fam;
+    std::vector<uint32_t> removed;
+    std::vector<ehgp_forest_node> nodes;
+    std::vector<uint32_t> children;
+    std::vector<ehgp_forest_birth> births;
+    std::vector<ehgp_forest_binding> bindings;
+    std::vector<ehgp_forest_saddle> saddles;
+    std::vector<ehgp_forest_group> groups;
+    std::vector<ehgp_forest_batch> fb;
+    std::vector<ehgp_forest_root> roots;
+    int status = EHGP_OK;
+    const char* msg = "";
   };
-  std::vector<uint64_t> carriers_of(keff + 2, 0), reduced_of(keff + 2, 0);
-  std::vector<uint32_t> fam_index_of(nfam);  // rank-partition position -> journal family index
-  // per-batch scratch, reused
-  struct Role {
-    uint32_t proj, role, fi, pos;
-  };
-  struct Arm {
-    uint32_t seed, carrier, prior, saddle;
-  };
-  struct Plan {
-    uint32_t c_off, c_cnt, p_off, p_cnt, s_off, s_cnt, kind, created, result;
-  };
-  std::vector<Role> batch_roles;
-  std::vector<uint32_t> fam_pos;      // batch saddles: rank-partition positions
-  std::vector<Arm> arms_b;            // batch arms
-  std::vector<uint32_t> arm_b_off;    // per batch saddle: first arm
-  std::vector<uint32_t> cars, qp, plan_of, plan_car, plan_prior, plan_sad, tmp;
-  std::vector<Plan> plans;
-  std::vector<ehgp_forest_node> gnodes;
-  std::vector<uint32_t> new_births;
-  uint32_t role_count = 0;
-  for (uint32_t k = 1; k <= keff; ++k) {
+  std::vector<OrderOut> outs(keff + 1);
+  auto run_order = [&](uint32_t k, OrderOut& o) {
+    auto fail_o = [&](const char* m) {
+      o.status = EHGP_ERR_DEGENERATE;
+      o.msg = m;
+    };
+    auto find = [&](uint32_t x) {  // path halving; roots follow the least-handle union rule alone
+      while (parent[x] != x) {
+        parent[x] = parent[parent[x]];
+        x = parent[x];
+      }
+      return x;
+    };
+    uint64_t carriers = 0, reduced = 0;
     const uint64_t b_lo = k == 1 ? 0 : rb[k], b_hi = k == 1 ? 0 : rb[k + 1];
     const uint64_t s_lo = rb[k + 1], s_hi = rb[k + 2 > 16 ? 16 : k + 2];
+    o.fam.reserve(s_hi - s_lo);
+    o.saddles.reserve(s_hi - s_lo);
+    o.groups.reserve(s_hi - s_lo);
+    o.births.reserve(k == 1 ? n : b_hi - b_lo);
+    struct Role {
+      uint32_t proj, role, fi, pos;
+    };
+    struct Arm {
+      uint32_t seed, carrier, prior;
+    };
+    struct Plan {
+      uint32_t c_off, c_cnt, p_off, p_cnt, s_off, s_cnt, kind, created, result;
+    };
+    std::vector<Role> batch_roles;
+    std::vector<uint32_t> fam_pos, fam_local, arm_b_off, cars, qp, plan_of, plan_car, plan_prior, plan_sad, tmp,
+        new_births;
+    std::vector<Arm> arms_b;
+    std::vector<Plan> plans;
+    std::vector<ehgp_forest_node> gnodes;
     uint64_t bi = b_lo, si = s_lo;
     bool singles = k == 1;
     while (singles || bi < b_hi || si < s_hi) {
@@ -1367,13 +1372,13 @@ int hier_run(Ctx& ctx, uint32_t K) {
         cls = std::min(cls_b, cls_s);
         lev = cls_b <= cls_s ? rank_order[bi] : rank_order[si];
       }
-      const uint32_t bidx = (uint32_t)h.jbatches.size();
-      ehgp_journal_batch jb{k, lev, role_count, 0, 0, 0};
+      const uint32_t bidx = (uint32_t)o.jb.size();
+      ehgp_journal_batch jb{k, lev, (uint32_t)o.roles.size(), 0, 0, 0};
       ehgp_forest_batch fb{};
       fb.order = k;
       fb.level_event = lev;
-      fb.pre_carriers = (uint32_t)carriers_of[k];
-      fb.pre_roots = (uint32_t)reduced_of[k];
+      fb.pre_carriers = (uint32_t)carriers;
+      fb.pre_roots = (uint32_t)reduced;
       batch_roles.clear();
       if (singles) {
         for (uint32_t p = 0; p < n; ++p) batch_roles.push_back({p, 0, kInvalid32, p});
@@ -1387,48 +1392,48 @@ int hier_run(Ctx& ctx, uint32_t K) {
           batch_roles.push_back({n + rank_order[si], 1, rank_order[si], (uint32_t)(si - fam_lo)});
           ++si;
         }
-        if (nbr && nbr < batch_roles.size())  // both kinds: merge by projection (role breaks no tie: distinct events)
+        if (nbr && nbr < batch_roles.size())
           std::inplace_merge(batch_roles.begin(), batch_roles.begin() + nbr, batch_roles.end(),
                              [](const Role& x, const Role& y) { return x.proj < y.proj; });
       }
       singles = false;
       // journal roles and saddle families
       fam_pos.clear();
+      fam_local.clear();
       for (size_t q = 0; q < batch_roles.size(); ++q) {
         const Role& r = batch_roles[q];
-        h.roles.push_back({bidx, r.proj, r.role});
+        const uint32_t ridx = (uint32_t)o.roles.size();
+        o.roles.push_back({bidx, r.proj, r.role});
         if (r.role == 0) {
           ++jb.birth_roles;
           continue;
         }
         ++jb.saddle_roles;
         const EvRec& ev = h.h_ev[r.fi];
-        const uint32_t fidx = (uint32_t)h.families.size();
-        fam_index_of[r.pos] = fidx;
-        h.families.push_back({r.fi, r.proj, role_count + (uint32_t)q, bidx, k, (uint32_t)h.arm_removed.size(), ev.size});
-        for (uint32_t j = 0; j < ev.size; ++j) h.arm_removed.push_back(ev.ids[j]);
+        fam_local.push_back((uint32_t)o.fam.size());
+        o.fam.push_back({r.fi, r.proj, ridx, bidx, k, (uint32_t)o.removed.size(), ev.size});
+        for (uint32_t j = 0; j < ev.size; ++j) o.removed.push_back(ev.ids[j]);
         fam_pos.push_back(r.pos);
       }
       jb.role_count = (uint32_t)batch_roles.size();
-      role_count += jb.role_count;
-      h.jbatches.push_back(jb);
+      o.jb.push_back(jb);
       // arms resolved against the pre-batch components
       arms_b.clear();
       arm_b_off.clear();
       for (uint32_t q = 0; q < fam_pos.size(); ++q) {
         const uint32_t fpos = fam_pos[q];
-        const uint32_t fidx = fam_index_of[fpos];
         arm_b_off.push_back((uint32_t)arms_b.size());
         for (uint64_t a = arm_off[fpos]; a < arm_off[fpos + 1]; ++a) {
-          if (term[a] >= birth_count || !active[term[a]])
-            return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "a strict arm descended to a minimum that is not yet born");
+          if (term[a] >= birth_count || !active[term[a]]) {
+            fail_o("a strict arm descended to a minimum that is not yet born");
+            return;
+          }
           const uint32_t c0 = find(term[a]);
-          arms_b.push_back({h.families[fidx].arm_offset + (uint32_t)(a - arm_off[fpos]), c0, rroot[c0], q});
+          arms_b.push_back({o.fam[fam_local[q]].arm_offset + (uint32_t)(a - arm_off[fpos]), c0, rroot[c0]});
         }
       }
       arm_b_off.push_back((uint32_t)arms_b.size());
-      // frozen-root quotient: transitive classes over the saddles' carriers,
-      // groups ordered by their least carrier, carriers ascending
+      // frozen-root quotient: transitive carrier classes, ordered by least carrier
       plans.clear();
       plan_car.clear();
       plan_prior.clear();
@@ -1461,7 +1466,6 @@ int hier_run(Ctx& ctx, uint32_t K) {
             plans.push_back({0, 0, 0, 0, 0, 0, 0, kInvalid32, 0});
           }
         }
-        // carriers and prior roots per plan (two counting passes keep slices contiguous)
         for (uint32_t i = 0; i < nc; ++i) {
           Plan& p = plans[plan_of[qf(i)]];
           ++p.c_cnt;
@@ -1490,65 +1494,69 @@ int hier_run(Ctx& ctx, uint32_t K) {
         for (Plan& p : plans) {
           uint32_t* pr = plan_prior.data() + p.p_off;
           std::sort(pr, pr + p.p_cnt);
-          if (std::adjacent_find(pr, pr + p.p_cnt) != pr + p.p_cnt)
-            return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "a frozen carrier class repeats a reduced root");
+          if (std::adjacent_find(pr, pr + p.p_cnt) != pr + p.p_cnt) {
+            fail_o("a frozen carrier class repeats a reduced root");
+            return;
+          }
           if (p.p_cnt == 1) {
             p.kind = 1;
             p.created = kInvalid32;
             p.result = pr[0];
           } else {
-            if (p.p_cnt == 0 && k == 1) return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "an order-one group has no root");
+            if (p.p_cnt == 0 && k == 1) {
+              fail_o("an order-one group has no root");
+              return;
+            }
             p.kind = p.p_cnt == 0 ? 0 : 2;
-            p.created = (uint32_t)h.nodes.size() + pending++;
+            p.created = (uint32_t)o.nodes.size() + pending++;
             p.result = p.created;
           }
         }
       }
-      fb.saddle_offset = (uint32_t)h.saddles.size();
-      fb.group_offset = (uint32_t)h.groups.size();
+      fb.saddle_offset = (uint32_t)o.saddles.size();
+      fb.group_offset = (uint32_t)o.groups.size();
       gnodes.clear();
       for (const Plan& p : plans) {
-        const uint32_t g_soff = (uint32_t)h.saddles.size();
-        const uint32_t gidx = (uint32_t)h.groups.size();
+        const uint32_t g_soff = (uint32_t)o.saddles.size();
+        const uint32_t gidx = (uint32_t)o.groups.size();
         for (uint32_t t = 0; t < p.s_cnt; ++t) {
           const uint32_t q = plan_sad[p.s_off + t];
-          const uint32_t fidx = fam_index_of[fam_pos[q]];
-          const uint32_t arm_o = (uint32_t)h.bindings.size();
+          const uint32_t fidx = fam_local[q];
+          const uint32_t arm_o = (uint32_t)o.bindings.size();
           tmp.clear();
           uint32_t nprior = 0;
           for (uint32_t a = arm_b_off[q]; a < arm_b_off[q + 1]; ++a) {
             const Arm& am = arms_b[a];
-            h.bindings.push_back({am.seed, fidx, am.carrier, am.prior});
+            o.bindings.push_back({am.seed, fidx, am.carrier, am.prior});
             tmp.push_back(am.carrier);
           }
           std::sort(tmp.begin(), tmp.end());
           tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
           for (uint32_t c0 : tmp) nprior += rroot[c0] != kInvalid32;  // carriers are pre-batch roots
-          h.saddles.push_back({fidx, h.families[fidx].event, bidx, arm_o, arm_b_off[q + 1] - arm_b_off[q],
+          o.saddles.push_back({fidx, o.fam[fidx].event, bidx, arm_o, arm_b_off[q + 1] - arm_b_off[q],
                                (uint32_t)tmp.size(), (uint32_t)tmp.size() - nprior, nprior, gidx});
         }
         const uint32_t ccnt = p.kind == 2 ? p.p_cnt : 0u;
-        h.groups.push_back({bidx, g_soff, (uint32_t)h.saddles.size() - g_soff, p.c_cnt, p.c_cnt - p.p_cnt, p.p_cnt,
-                            (uint32_t)h.children.size(), ccnt, p.created, p.result, p.kind});
+        o.groups.push_back({bidx, g_soff, (uint32_t)o.saddles.size() - g_soff, p.c_cnt, p.c_cnt - p.p_cnt, p.p_cnt,
+                            (uint32_t)o.children.size(), ccnt, p.created, p.result, p.kind});
         if (p.kind != 1)
-          gnodes.push_back({k, lev, p.kind == 0 ? 1u : 2u, (uint32_t)h.children.size(), ccnt, kInvalid32, gidx});
-        if (p.kind == 2) h.children.insert(h.children.end(), plan_prior.begin() + p.p_off, plan_prior.begin() + p.p_off + p.p_cnt);
+          gnodes.push_back({k, lev, p.kind == 0 ? 1u : 2u, (uint32_t)o.children.size(), ccnt, kInvalid32, gidx});
+        if (p.kind == 2)
+          o.children.insert(o.children.end(), plan_prior.begin() + p.p_off, plan_prior.begin() + p.p_off + p.p_cnt);
       }
-      h.nodes.insert(h.nodes.end(), gnodes.begin(), gnodes.end());
-      // births of this batch (hidden from this batch's arms)
-      fb.birth_offset = (uint32_t)h.births.size();
+      o.nodes.insert(o.nodes.end(), gnodes.begin(), gnodes.end());
+      // births of this batch (hidden from this batch's arms); handles are global
+      fb.birth_offset = (uint32_t)o.births.size();
       new_births.clear();
       for (const Role& r : batch_roles) {
         if (r.role != 0) continue;
-        const uint32_t handle = (uint32_t)h.births.size();
+        const uint32_t handle = k == 1 ? r.proj : n + r.pos;
         uint32_t node = kInvalid32;
         if (k == 1) {
-          node = (uint32_t)h.nodes.size();
-          h.nodes.push_back({1, kInvalid32, 0, (uint32_t)h.children.size(), 0, handle, kInvalid32});
+          node = (uint32_t)o.nodes.size();
+          o.nodes.push_back({1, kInvalid32, 0, (uint32_t)o.children.size(), 0, handle, kInvalid32});
         }
-        const uint32_t expect = k == 1 ? r.proj : n + r.pos;
-        if (expect != handle) return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "birth handles left the journal order");
-        h.births.push_back({r.proj, bidx, k, handle, node});
+        o.births.push_back({r.proj, bidx, k, handle, node});
         new_births.push_back(handle);
       }
       // commit: unions (least handle survives), reduced roots, then births
@@ -1562,32 +1570,141 @@ int hier_run(Ctx& ctx, uint32_t K) {
           const uint32_t lo = std::min(r0, r1), hi = std::max(r0, r1);
           parent[hi] = lo;
           r0 = lo;
-          --carriers_of[k];
+          --carriers;
         }
         rroot[r0] = p.result;
-        reduced_of[k] = reduced_of[k] - had_reduced + 1;
+        reduced = reduced - had_reduced + 1;
       }
-      for (uint32_t hnd : new_births) {
+      for (size_t t = 0; t < new_births.size(); ++t) {
+        const uint32_t hnd = new_births[t];
         active[hnd] = 1;
         border[hnd] = k;
-        rroot[hnd] = k == 1 ? h.births[hnd].order_one_node : kInvalid32;
-        ++carriers_of[k];
-        if (k == 1) ++reduced_of[k];
+        rroot[hnd] = k == 1 ? o.births[fb.birth_offset + t].order_one_node : kInvalid32;
+        ++carriers;
+        if (k == 1) ++reduced;
       }
       fb.birth_count = (uint32_t)new_births.size();
-      fb.saddle_count = (uint32_t)h.saddles.size() - fb.saddle_offset;
-      fb.group_count = (uint32_t)h.groups.size() - fb.group_offset;
-      fb.post_carriers = (uint32_t)carriers_of[k];
-      fb.post_roots = (uint32_t)reduced_of[k];
-      h.fbatches.push_back(fb);
+      fb.saddle_count = (uint32_t)o.saddles.size() - fb.saddle_offset;
+      fb.group_count = (uint32_t)o.groups.size() - fb.group_offset;
+      fb.post_carriers = (uint32_t)carriers;
+      fb.post_roots = (uint32_t)reduced;
+      o.fb.push_back(fb);
     }
+    // final roots of this order (local node ids)
+    const uint64_t h_lo = k == 1 ? 0 : n + (rb[k] - rb[2]), h_hi = k == 1 ? n : n + (rb[k + 1] - rb[2]);
+    for (uint64_t hnd = h_lo; hnd < h_hi; ++hnd)
+      if (active[hnd] && parent[hnd] == hnd && rroot[hnd] != kInvalid32)
+        o.roots.push_back({k, (uint32_t)hnd, rroot[hnd]});
+    std::sort(o.roots.begin(), o.roots.end(),
+              [](const ehgp_forest_root& x, const ehgp_forest_root& y) { return x.node < y.node; });
+  };
+  {
+    std::vector<std::thread> pool;
+    for (uint32_t k = 1; k <= keff; ++k) pool.emplace_back(run_order, k, std::ref(outs[k]));
+    for (auto& t : pool) t.join();
   }
-  for (uint64_t hnd = 0; hnd < birth_count; ++hnd)
-    if (active[hnd] && parent[hnd] == hnd && rroot[hnd] != kInvalid32)
-      h.roots.push_back({border[hnd], (uint32_t)hnd, rroot[hnd]});
-  std::sort(h.roots.begin(), h.roots.end(), [](const ehgp_forest_root& x, const ehgp_forest_root& y) {
-    return x.order != y.order ? x.order < y.order : x.node < y.node;
-  });
+  for (uint32_t k = 1; k <= keff; ++k)
+    if (outs[k].status != EHGP_OK) return abi_fail(&ctx, outs[k].status, outs[k].msg);
+  // concatenate with global offsets
+  {
+    uint64_t tot[12] = {0};
+    for (uint32_t k = 1; k <= keff; ++k) {
+      const OrderOut& o = outs[k];
+      tot[0] += o.jb.size(); tot[1] += o.roles.size(); tot[2] += o.fam.size(); tot[3] += o.removed.size();
+      tot[4] += o.nodes.size(); tot[5] += o.children.size(); tot[6] += o.births.size(); tot[7] += o.bindings.size();
+      tot[8] += o.saddles.size(); tot[9] += o.groups.size(); tot[10] += o.roots.size();
+    }
+    h.jbatches.resize(tot[0]); h.roles.resize(tot[1]); h.families.resize(tot[2]); h.arm_removed.resize(tot[3]);
+    h.nodes.resize(tot[4]); h.children.resize(tot[5]); h.births.resize(tot[6]); h.bindings.resize(tot[7]);
+    h.saddles.resize(tot[8]); h.groups.resize(tot[9]); h.fbatches.resize(tot[0]); h.roots.resize(tot[10]);
+    struct Off {
+      uint32_t jb, role, fam, seed, node, child, birth, bind, sad, grp, root;
+    };
+    std::vector<Off> off(keff + 2);
+    off[1] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t k = 1; k <= keff; ++k) {
+      const OrderOut& o = outs[k];
+      const Off& a = off[k];
+      off[k + 1] = {a.jb + (uint32_t)o.jb.size(), a.role + (uint32_t)o.roles.size(), a.fam + (uint32_t)o.fam.size(),
+                    a.seed + (uint32_t)o.removed.size(), a.node + (uint32_t)o.nodes.size(),
+                    a.child + (uint32_t)o.children.size(), a.birth + (uint32_t)o.births.size(),
+                    a.bind + (uint32_t)o.bindings.size(), a.sad + (uint32_t)o.saddles.size(),
+                    a.grp + (uint32_t)o.groups.size(), a.root + (uint32_t)o.roots.size()};
+    }
+    auto shift = [](uint32_t v, uint32_t d) { return v == kInvalid32 ? v : v + d; };
+    auto merge_order = [&](uint32_t k) {
+      const OrderOut& o = outs[k];
+      const Off& f = off[k];
+      for (size_t i = 0; i < o.jb.size(); ++i) {
+        ehgp_journal_batch x = o.jb[i];
+        x.role_offset += f.role;
+        h.jbatches[f.jb + i] = x;
+        ehgp_forest_batch y = o.fb[i];
+        y.birth_offset += f.birth;
+        y.saddle_offset += f.sad;
+        y.group_offset += f.grp;
+        h.fbatches[f.jb + i] = y;
+      }
+      for (size_t i = 0; i < o.roles.size(); ++i) {
+        ehgp_role_record x = o.roles[i];
+        x.batch += f.jb;
+        h.roles[f.role + i] = x;
+      }
+      for (size_t i = 0; i < o.fam.size(); ++i) {
+        ehgp_family_record x = o.fam[i];
+        x.role_record += f.role;
+        x.batch += f.jb;
+        x.arm_offset += f.seed;
+        h.families[f.fam + i] = x;
+      }
+      std::copy(o.removed.begin(), o.removed.end(), h.arm_removed.begin() + f.seed);
+      for (size_t i = 0; i < o.nodes.size(); ++i) {
+        ehgp_forest_node x = o.nodes[i];
+        x.child_offset += f.child;
+        x.atomic_group = shift(x.atomic_group, f.grp);
+        h.nodes[f.node + i] = x;
+      }
+      for (size_t i = 0; i < o.children.size(); ++i) h.children[f.child + i] = o.children[i] + f.node;
+      for (size_t i = 0; i < o.births.size(); ++i) {
+        ehgp_forest_birth x = o.births[i];
+        x.batch += f.jb;
+        x.order_one_node = shift(x.order_one_node, f.node);
+        h.births[f.birth + i] = x;
+      }
+      for (size_t i = 0; i < o.bindings.size(); ++i) {
+        ehgp_forest_binding x = o.bindings[i];
+        x.arm_seed += f.seed;
+        x.family += f.fam;
+        x.prior_root = shift(x.prior_root, f.node);
+        h.bindings[f.bind + i] = x;
+      }
+      for (size_t i = 0; i < o.saddles.size(); ++i) {
+        ehgp_forest_saddle x = o.saddles[i];
+        x.family += f.fam;
+        x.batch += f.jb;
+        x.arm_offset += f.bind;
+        x.group += f.grp;
+        h.saddles[f.sad + i] = x;
+      }
+      for (size_t i = 0; i < o.groups.size(); ++i) {
+        ehgp_forest_group x = o.groups[i];
+        x.batch += f.jb;
+        x.saddle_offset += f.sad;
+        x.child_offset += f.child;
+        x.created_node = shift(x.created_node, f.node);
+        x.result_node = shift(x.result_node, f.node);
+        h.groups[f.grp + i] = x;
+      }
+      for (size_t i = 0; i < o.roots.size(); ++i) {
+        ehgp_forest_root x = o.roots[i];
+        x.node += f.node;
+        h.roots[f.root + i] = x;
+      }
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t k = 1; k <= keff; ++k) pool.emplace_back(merge_order, k);
+    for (auto& t : pool) t.join();
+  }
   const auto t2 = std::chrono::steady_clock::now();
   h.ms_forest = std::chrono::duration<double, std::milli>(t2 - t1).count();
   (void)t0;
