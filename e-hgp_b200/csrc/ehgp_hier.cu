@@ -57,6 +57,13 @@ constexpr int kCandCap = 64;         // ball-query candidates per descent step
 constexpr int kDStack = 64;          // LBVH traversal stack per descent thread
 constexpr int kDescentSteps = 512;   // descent steps per arm
 
+// Slow-path counters of the descent (read back per call): [0] exhaustive miniball
+// enumerations, [1] exact hull signs, [2] exact closed-ball sides, [3] exact level
+// conversions, [4] exact band orders, [5] exact cutoff comparisons, [6] strictness
+// checks on a cutoff equal to the level.
+__device__ unsigned long long g_descent_slow[8];
+__device__ __forceinline__ void slow(int i) { atomicAdd(&g_descent_slow[i], 1ull); }
+
 // Descent status per arm.
 enum ArmStatus : uint8_t {
   kArmOk = 0,
@@ -455,6 +462,35 @@ __global__ void k_birth_insert(uint32_t nb, uint32_t n, uint32_t birth_base, con
   atomicOr(err, kErrCapacity);
 }
 
+// Rank-partition views read by the host pass in sequence: level class and support size
+// of the event at each rank position.
+__global__ void k_rank_info(uint32_t m, const uint32_t* __restrict__ rank_order, const EvRec* __restrict__ ev,
+                            const uint32_t* __restrict__ lclass, uint32_t* __restrict__ cls_rp,
+                            uint32_t* __restrict__ size_rp) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const uint32_t fi = rank_order[i];
+  cls_rp[i] = lclass[fi];
+  size_rp[i] = ev[fi].size;
+}
+
+// One arm seed per support point of every saddle family (families = rank positions
+// fam_lo.. in journal order; arm_off = exclusive sum of their support sizes).
+__global__ void k_arm_expand(uint32_t nfam, uint32_t fam_lo, const uint32_t* __restrict__ rank_order,
+                             const EvRec* __restrict__ ev, const uint32_t* __restrict__ arm_off,
+                             uint32_t* __restrict__ arm_family, uint8_t* __restrict__ arm_local,
+                             uint32_t* __restrict__ arm_removed) {
+  const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nfam) return;
+  const EvRec& e = ev[rank_order[fam_lo + f]];
+  const uint32_t o = arm_off[f];
+  for (uint32_t j = 0; j < e.size; ++j) {
+    arm_family[o + j] = f;
+    arm_local[o + j] = (uint8_t)j;
+    arm_removed[o + j] = e.ids[j];
+  }
+}
+
 // ---- 3. strict-arm descent ----------------------------------------------------------
 struct DescentParams {
   uint32_t n, root;
@@ -499,6 +535,7 @@ __device__ bool inside_closed(const Cloud& c, const FSphere& fs, const uint32_t*
     if (v * sa < -bnd) return true;
     if (v * sa > bnd) return false;
   }
+  slow(2);
   W A;
   WV N;
   exact_sphere(c, T, ts, A, N);
@@ -535,7 +572,7 @@ __device__ bool hull_centre(const Cloud& c, const uint32_t* T, int ts) {
     sg[1] = fs(G11 - G12, kFilt * 6.0 * M2 + kTiny);
     sg[2] = fs(G22 - G12, kFilt * 6.0 * M2 + kTiny);
     sg[3] = fs(G11 * G22 - G12 * G12, kFilt * 18.0 * M2 * M2 + kTiny);
-    if (undecided) tri_signs_exact(c, T, sg);
+    if (undecided) { slow(1); tri_signs_exact(c, T, sg); }
     return sg[3] != 0 && sg[0] >= 0 && sg[1] >= 0 && sg[2] >= 0;
   }
   const double* e1 = e[0];
@@ -561,7 +598,7 @@ __device__ bool hull_centre(const Cloud& c, const uint32_t* T, int ts) {
   sg[2] = fs(l1, kFilt * 108.0 * M6 + kTiny);
   sg[3] = fs(l2, kFilt * 108.0 * M6 + kTiny);
   sg[4] = fs(l3, kFilt * 108.0 * M6 + kTiny);
-  if (undecided) quad_signs_exact(c, T, sg);
+  if (undecided) { slow(1); quad_signs_exact(c, T, sg); }
   return sg[0] != 0 && sg[1] >= 0 && sg[2] >= 0 && sg[3] >= 0 && sg[4] >= 0;
 }
 
@@ -671,6 +708,7 @@ __device__ __noinline__ bool facet_miniball(const Cloud& c, const uint32_t* F, i
     if (verify_mini(c, F, k, mb)) return true;
   }
   // exhaustive exact enumeration
+  slow(0);
   for (int s = (k == 1 ? 1 : 2); s <= 4 && s <= k; ++s) {
     int id[4] = {0, 1, 2, 3};
     while (true) {
@@ -694,7 +732,7 @@ __device__ __noinline__ int topk_choice(const DescentParams& d, const Cloud& c, 
                                         int* cut_below) {
   const FSphere& fs = mb.fs;
   double llo, lhi;
-  if (!flevel(fs, llo, lhi)) exact_level_fp(c, mb.T, mb.ts, llo, lhi);
+  if (!flevel(fs, llo, lhi)) { slow(3); exact_level_fp(c, mb.T, mb.ts, llo, lhi); }
   // FP64 centre and its error: c~ = a + N / (2A)
   const double inv = 0.5 / fs.A;
   const double ox = fs.Nx * inv, oy = fs.Ny * inv, oz = fs.Nz * inv;
@@ -758,26 +796,67 @@ __device__ __noinline__ int topk_choice(const DescentParams& d, const Cloud& c, 
     G[nsel++] = cid[band0];
     cut_point = cid[band0];
   } else {
-    // exact order of the band by (distance, id)
-    int nb = band1 - band0 + 1;
+    // The band usually holds support points of F's miniball, which lie exactly on
+    // its sphere: relate every band member to beta(F) (support points are equal to it
+    // by construction; others by FP64, exact when undecided).  When the cutoff is
+    // beta(F) the choice needs no mutual order of the members below it.
+    const int nb = band1 - band0 + 1;
     uint32_t* B = cid + band0;
-    for (int a = 1; a < nb; ++a) {
-      const uint32_t x = B[a];
-      int b = a;
-      while (b > 0) {
-        const int s = dist_cmp_exact(c, mb.T, mb.ts, B[b - 1], x);
-        if (s < 0 || (s == 0 && B[b - 1] < x)) break;
-        B[b] = B[b - 1];
-        --b;
+    int rel[kCandCap];
+    int n_lo = 0, n_eq = 0, n_hi = 0;
+    for (int t = 0; t < nb; ++t) {
+      bool sup = false;
+      for (int j = 0; j < mb.ts; ++j) sup |= mb.T[j] == B[t];
+      int r;
+      if (sup) r = 0;
+      else if (cd[band0 + t] + ed < llo) r = -1;
+      else if (cd[band0 + t] - ed > lhi) r = 1;
+      else {
+        slow(5);
+        r = dist_cmp_exact(c, mb.T, mb.ts, B[t], mb.T[0]);
       }
-      B[b] = x;
+      rel[t] = r;
+      n_lo += r < 0;
+      n_eq += r == 0;
+      n_hi += r > 0;
     }
     const int need = k - below;  // >= 1
-    cut_point = B[need - 1];
-    // strictly below the cutoff, then the least ids of the shell
-    int j = 0;
-    while (j < nb && dist_cmp_exact(c, mb.T, mb.ts, B[j], cut_point) < 0) G[nsel++] = B[j++];
-    while (nsel < k) G[nsel++] = B[j++];  // shell members in id order
+    if (need > n_lo && need <= n_lo + n_eq) {
+      // cutoff = beta(F): the lower members, then the least ids at beta(F)
+      for (int t = 0; t < nb; ++t)
+        if (rel[t] < 0) G[nsel++] = B[t];
+      uint32_t eq[kCandCap];
+      int ne = 0;
+      for (int t = 0; t < nb; ++t)
+        if (rel[t] == 0) eq[ne++] = B[t];
+      for (int a = 1; a < ne; ++a) {
+        const uint32_t x = eq[a];
+        int b = a;
+        while (b > 0 && eq[b - 1] > x) { eq[b] = eq[b - 1]; --b; }
+        eq[b] = x;
+      }
+      for (int t = 0; nsel < k; ++t) G[nsel++] = eq[t];
+      cut_point = mb.T[0];
+    } else {
+      // exact order of the band by (distance, id)
+      slow(4);
+      for (int a = 1; a < nb; ++a) {
+        const uint32_t x = B[a];
+        int b = a;
+        while (b > 0) {
+          const int s = dist_cmp_exact(c, mb.T, mb.ts, B[b - 1], x);
+          if (s < 0 || (s == 0 && B[b - 1] < x)) break;
+          B[b] = B[b - 1];
+          --b;
+        }
+        B[b] = x;
+      }
+      cut_point = B[need - 1];
+      // strictly below the cutoff, then the least ids of the shell
+      int j = 0;
+      while (j < nb && dist_cmp_exact(c, mb.T, mb.ts, B[j], cut_point) < 0) G[nsel++] = B[j++];
+      while (nsel < k) G[nsel++] = B[j++];  // shell members in id order
+    }
   }
   for (int a = 1; a < k; ++a) {
     const uint32_t x = G[a];
@@ -796,6 +875,7 @@ __device__ __noinline__ int topk_choice(const DescentParams& d, const Cloud& c, 
     if (dcut + ed < llo) {
       *cut_below = 1;
     } else {
+      slow(5);
       const int s = dist_cmp_exact(c, mb.T, mb.ts, cut_point, mb.T[0]);
       if (s > 0) return kArmInternal;
       *cut_below = s < 0 ? 1 : 0;
@@ -815,7 +895,7 @@ __device__ __forceinline__ int arm_facet(const EvRec& e, uint32_t removed, uint3
 
 // First probe of every arm: most arms are themselves a birth facet of their order.
 // Misses are queued with their facet for the descent steps.
-__global__ void k_arm_probe(DescentParams d, uint32_t narms, const uint32_t* __restrict__ fam_event,
+__global__ void k_arm_probe(DescentParams d, uint32_t narms, const uint32_t* __restrict__ fam_event /* rank_order + fam_lo */,
                             const uint32_t* __restrict__ arm_family, const uint8_t* __restrict__ arm_local,
                             const EvRec* __restrict__ ev, uint32_t* __restrict__ term, uint8_t* __restrict__ status,
                             uint32_t* __restrict__ q_arm, uint32_t* __restrict__ q_fac, uint32_t* __restrict__ q_count) {
@@ -860,6 +940,7 @@ k_arm_step(DescentParams d, uint32_t m, const uint32_t* __restrict__ in_arm, con
   for (int j = 0; j < k; ++j) same &= G[j] == F[j];
   if (same) { status[a] = kArmUnresolved; return; }
   if (!cut_below) {  // beta(G) <= cutoff = beta(F): the decrease must be strict
+    slow(6);
     Mini mg;
     if (!facet_miniball(c, G, k, mg)) { status[a] = kArmInternal; return; }
     double glo, ghi, flo, fhi;
@@ -882,6 +963,27 @@ k_arm_step(DescentParams d, uint32_t m, const uint32_t* __restrict__ in_arm, con
 }  // namespace
 
 // ---- host state ---------------------------------------------------------------------
+struct HierDsu {
+  uint32_t parent, rroot, order;  // order 0: not yet born
+};
+
+struct HierOrderOut {  // one order's journal and forest arenas, local indices
+  std::vector<ehgp_journal_batch> jb;
+  std::vector<ehgp_role_record> roles;
+  std::vector<ehgp_family_record> fam;
+  std::vector<ehgp_forest_node> nodes;
+  std::vector<uint32_t> children;
+  std::vector<ehgp_forest_birth> births;
+  std::vector<ehgp_forest_binding> bindings;
+  std::vector<ehgp_forest_saddle> saddles;
+  std::vector<ehgp_forest_group> groups;
+  std::vector<ehgp_forest_batch> fb;
+  std::vector<ehgp_forest_root> roots;
+  int status = EHGP_OK;
+  const char* msg = "";
+  double ms = 0;
+};
+
 struct HierState {
   std::vector<void*> allocs;
   uint64_t cap_events = 0, cap_arms = 0, cap_births = 0, cap_slots = 0;
@@ -919,12 +1021,24 @@ struct HierState {
   uint32_t* q_fac[2] = {nullptr, nullptr};
   uint64_t q_cap = 0;
   uint32_t first_misses = 0, descent_rounds = 0;
+  unsigned long long slow[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   // host results
   uint32_t n = 0, K = 0, keff = 0;
   int S = 0;
   uint64_t events = 0, diagnostics = 0;
-  std::vector<EvRec> h_ev;
-  std::vector<uint32_t> h_class;
+  std::vector<HierOrderOut> outs;     // per-order arenas (capacity kept across calls)
+  std::vector<HierDsu> dsu;
+  uint64_t pin_m = 0, pin_arms = 0;   // pinned host views of the last call
+  uint32_t* p_rank = nullptr;
+  uint32_t* p_cls = nullptr;
+  uint32_t* p_armoff = nullptr;
+  uint32_t* p_removed = nullptr;
+  uint32_t* p_term = nullptr;
+  uint8_t* p_stat = nullptr;
+  uint32_t* d_cls_rp = nullptr;       // device views (event capacity)
+  uint32_t* d_size_rp = nullptr;
+  uint32_t* d_armoff = nullptr;
+  uint32_t* d_removed = nullptr;
   std::vector<double> h_px, h_py, h_pz;
   std::vector<ehgp_journal_batch> jbatches;
   std::vector<ehgp_role_record> roles;
@@ -939,7 +1053,7 @@ struct HierState {
   std::vector<ehgp_forest_batch> fbatches;
   std::vector<ehgp_forest_root> roots;
   uint32_t decision = EHGP_ERR_NOT_BUILT;
-  double ms_device = 0, ms_forest = 0, ms_descent = 0;
+  double ms_device = 0, ms_forest = 0, ms_descent = 0, ms_orders = 0;
   uint64_t descent_steps = 0, arms = 0, exact_boundaries = 0;
 };
 
@@ -949,6 +1063,9 @@ void hier_free(Ctx& ctx) {
   for (void* p : {(void*)ctx.hier->q_arm[0], (void*)ctx.hier->q_arm[1], (void*)ctx.hier->q_fac[0],
                   (void*)ctx.hier->q_fac[1]})
     if (p) cudaFree(p);
+  for (void* p : {(void*)ctx.hier->p_rank, (void*)ctx.hier->p_cls, (void*)ctx.hier->p_armoff,
+                  (void*)ctx.hier->p_removed, (void*)ctx.hier->p_term, (void*)ctx.hier->p_stat})
+    if (p) cudaFreeHost(p);
   delete ctx.hier;
   ctx.hier = nullptr;
 }
@@ -1000,12 +1117,16 @@ cudaError_t ensure_events(HierState& h, uint64_t m) {
   HA(h.radix_counts, 256ull * ((cap + kRadixTile - 1) / kRadixTile) + 256);
   HA(h.bfac, cap * kMaxFacet);
   HA(h.fam_event, cap);
+  HA(h.d_cls_rp, cap);
+  HA(h.d_size_rp, cap);
+  HA(h.d_armoff, cap + 1);
   HA(h.dstats, 4);
   const uint64_t arms = 4 * cap;
   HA(h.arm_family, arms);
   HA(h.arm_local, arms);
   HA(h.term, arms);
   HA(h.arm_status, arms);
+  HA(h.d_removed, arms);
   uint64_t slots = 1;
   while (slots < 2 * cap + 1024) slots <<= 1;
   HA(h.slots, slots);
@@ -1084,6 +1205,10 @@ int hier_run(Ctx& ctx, uint32_t K) {
   if (e != cudaSuccess) return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "hierarchy buffers do not fit the device");
   cudaMemsetAsync(h.counters, 0, 32 * sizeof(uint32_t), st);
   cudaMemsetAsync(h.dstats, 0, 4 * sizeof(unsigned long long), st);
+  {
+    const unsigned long long zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    cudaMemcpyToSymbolAsync(g_descent_slow, zero, sizeof(zero), 0, cudaMemcpyHostToDevice, st);
+  }
   if (total)
     k_ev_build<<<nblk(total, kT), kT, 0, st>>>(np, nh, (const PairRecD*)ctx.pb.sorted, (const HigherRecD*)ctx.hb.sorted,
                                                 b.px, b.py, b.pz, g.scale, h.ev_raw, h.lmid_raw, h.lerr_raw, h.key,
@@ -1178,15 +1303,6 @@ int hier_run(Ctx& ctx, uint32_t K) {
     launches += 2;
     cudaMemcpyAsync(hist, h.counters + 3, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
   }
-  // host copies of the facade (events and level classes)
-  h.h_ev.resize(m);
-  h.h_class.resize(m);
-  std::vector<uint32_t> rank_order(m);
-  if (m) {
-    cudaMemcpyAsync(h.h_ev.data(), h.ev, (uint64_t)m * sizeof(EvRec), cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(h.h_class.data(), h.lclass, (uint64_t)m * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(rank_order.data(), h.rank_order, (uint64_t)m * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-  }
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "hierarchy facade");
   if (h.diagnostics) {
     h.decision = EHGP_ERR_DEGENERATE;
@@ -1208,28 +1324,56 @@ int hier_run(Ctx& ctx, uint32_t K) {
   // families: saddle events of ranks 2..keff+1 in rank-partition order; arms per support point
   const uint64_t fam_lo = rb[2], fam_hi = rb[std::min<uint32_t>(keff + 2, 16)];
   const uint64_t nfam = fam_hi - fam_lo;
-  std::vector<uint32_t> fam_event(nfam), arm_family, arm_off(nfam + 1, 0);
-  std::vector<uint8_t> arm_local;
-  for (uint64_t f = 0; f < nfam; ++f) {
-    fam_event[f] = rank_order[fam_lo + f];
-    const uint32_t sz = h.h_ev[fam_event[f]].size;
-    arm_off[f + 1] = arm_off[f] + sz;
+  uint64_t narms = 0;
+  if (m) {
+    k_rank_info<<<nblk(m, kT), kT, 0, st>>>(m, h.rank_order, h.ev, h.lclass, h.d_cls_rp, h.d_size_rp);
+    ++launches;
   }
-  const uint64_t narms = arm_off[nfam];
+  if (nfam) {  // arm offsets: inclusive sum of the family sizes into d_armoff + 1
+    const uint32_t nb = nblk(nfam, 1024);
+    k_sum_blocks<<<nb, 256, 0, st>>>((uint32_t)nfam, h.d_size_rp + fam_lo, h.d_armoff + 1, h.ubsum);
+    k_sum_carry<<<1, 1, 0, st>>>(nb, h.ubsum);
+    k_sum_apply<<<nblk(nfam, kT), kT, 0, st>>>((uint32_t)nfam, h.d_armoff + 1, h.ubsum, 0);
+    cudaMemsetAsync(h.d_armoff, 0, sizeof(uint32_t), st);
+    launches += 3;
+    uint32_t na = 0;
+    cudaMemcpyAsync(&na, h.d_armoff + nfam, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "arm offsets");
+    narms = na;
+  }
   if (narms > h.cap_arms) return abi_fail(&ctx, EHGP_ERR_CAPACITY, "strict arms exceed the hierarchy buffers");
-  arm_family.resize(narms);
-  arm_local.resize(narms);
-  for (uint64_t f = 0; f < nfam; ++f)
-    for (uint32_t j = 0; j < arm_off[f + 1] - arm_off[f]; ++j) {
-      arm_family[arm_off[f] + j] = (uint32_t)f;
-      arm_local[arm_off[f] + j] = (uint8_t)j;
+  // pinned host views
+  if (h.pin_m < m + 1 || h.pin_arms < narms + 1) {
+    for (void* p : {(void*)h.p_rank, (void*)h.p_cls, (void*)h.p_armoff, (void*)h.p_removed, (void*)h.p_term,
+                    (void*)h.p_stat})
+      if (p) cudaFreeHost(p);
+    h.p_rank = h.p_cls = h.p_armoff = h.p_removed = h.p_term = nullptr;
+    h.p_stat = nullptr;
+    const uint64_t pm = (m + 1) + (m + 1) / 8, pa = (narms + 1) + (narms + 1) / 8;
+    if (cudaMallocHost(&h.p_rank, pm * 4) != cudaSuccess || cudaMallocHost(&h.p_cls, pm * 4) != cudaSuccess ||
+        cudaMallocHost(&h.p_armoff, pm * 4) != cudaSuccess || cudaMallocHost(&h.p_removed, pa * 4) != cudaSuccess ||
+        cudaMallocHost(&h.p_term, pa * 4) != cudaSuccess || cudaMallocHost(&h.p_stat, pa) != cudaSuccess) {
+      h.pin_m = h.pin_arms = 0;
+      return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "pinned host buffers for the hierarchy");
     }
-  std::vector<uint32_t> term(narms);
-  std::vector<uint8_t> astat(narms);
+    h.pin_m = pm;
+    h.pin_arms = pa;
+  }
+  const uint32_t* rank_order = h.p_rank;
+  const uint32_t* cls_rp = h.p_cls;
+  const uint32_t* arm_off = h.p_armoff;
+  const uint32_t* term = h.p_term;
+  const uint8_t* astat = h.p_stat;
+  if (m) {
+    cudaMemcpyAsync(h.p_rank, h.rank_order, (uint64_t)m * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(h.p_cls, h.d_cls_rp, (uint64_t)m * 4, cudaMemcpyDeviceToHost, st);
+  }
+  if (nfam) cudaMemcpyAsync(h.p_armoff, h.d_armoff, (nfam + 1) * 4, cudaMemcpyDeviceToHost, st);
   if (narms) {
-    cudaMemcpyAsync(h.fam_event, fam_event.data(), nfam * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(h.arm_family, arm_family.data(), narms * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(h.arm_local, arm_local.data(), narms, cudaMemcpyHostToDevice, st);
+    k_arm_expand<<<nblk(nfam, kT), kT, 0, st>>>((uint32_t)nfam, (uint32_t)fam_lo, h.rank_order, h.ev, h.d_armoff,
+                                               h.arm_family, h.arm_local, h.d_removed);
+    ++launches;
+    cudaMemcpyAsync(h.p_removed, h.d_removed, narms * 4, cudaMemcpyDeviceToHost, st);
     DescentParams dp{n, 2 * n - 2, g.tnodes, b.px, b.py, b.pz, h.S, h.slots, (uint32_t)(h.cap_slots - 1), h.bfac,
                      (uint32_t)nb_higher};
     cudaEventRecord(ctx.evk0, st);
@@ -1248,7 +1392,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
         return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "descent queue buffers do not fit the device");
       h.q_cap = qc;
     }
-    k_arm_probe<<<nblk(narms, kT), kT, 0, st>>>(dp, (uint32_t)narms, h.fam_event, h.arm_family, h.arm_local, h.ev,
+    k_arm_probe<<<nblk(narms, kT), kT, 0, st>>>(dp, (uint32_t)narms, h.rank_order + fam_lo, h.arm_family, h.arm_local, h.ev,
                                                 h.term, h.arm_status, h.q_arm[0], h.q_fac[0], h.qcount);
     ++launches;
     uint32_t pending = 0;
@@ -1270,13 +1414,14 @@ int hier_run(Ctx& ctx, uint32_t K) {
     }
     h.descent_rounds = rounds;
     cudaEventRecord(ctx.evk1, st);
-    cudaMemcpyAsync(term.data(), h.term, narms * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(astat.data(), h.arm_status, narms, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(h.p_term, h.term, narms * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(h.p_stat, h.arm_status, narms, cudaMemcpyDeviceToHost, st);
   }
   uint32_t herr = 0;
   unsigned long long dsteps = 0;
   cudaMemcpyAsync(&herr, h.counters + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(&dsteps, h.dstats, sizeof(dsteps), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyFromSymbolAsync(h.slow, g_descent_slow, sizeof(h.slow), 0, cudaMemcpyDeviceToHost, st);
   cudaEventRecord(ctx.ev1, st);
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "strict-arm descent");
   {
@@ -1308,45 +1453,48 @@ int hier_run(Ctx& ctx, uint32_t K) {
   // concatenated in order with the offsets the reference's single pass would give.
   const auto t1 = std::chrono::steady_clock::now();
   const uint64_t birth_count = n + nb_higher;
-  std::vector<uint32_t> parent(birth_count), border(birth_count, 0), rroot(birth_count, kInvalid32);
-  std::vector<uint8_t> active(birth_count, 0);
-  std::iota(parent.begin(), parent.end(), 0u);
-  struct OrderOut {
-    std::vector<ehgp_journal_batch> jb;
-    std::vector<ehgp_role_record> roles;
-    std::vector<ehgp_family_record> fam;
-    std::vector<uint32_t> removed;
-    std::vector<ehgp_forest_node> nodes;
-    std::vector<uint32_t> children;
-    std::vector<ehgp_forest_birth> births;
-    std::vector<ehgp_forest_binding> bindings;
-    std::vector<ehgp_forest_saddle> saddles;
-    std::vector<ehgp_forest_group> groups;
-    std::vector<ehgp_forest_batch> fb;
-    std::vector<ehgp_forest_root> roots;
-    int status = EHGP_OK;
-    const char* msg = "";
-  };
-  std::vector<OrderOut> outs(keff + 1);
-  auto run_order = [&](uint32_t k, OrderOut& o) {
+  // union-find state packed per birth handle: one cache line touch per arm
+  h.dsu.resize(birth_count);
+  for (uint64_t i = 0; i < birth_count; ++i) h.dsu[i] = {(uint32_t)i, kInvalid32, 0};
+  HierDsu* dsu = h.dsu.data();
+  // per-order arenas and union-find state persist across calls (no page faults when warm)
+  if (h.outs.size() < keff + 1) h.outs.resize(keff + 1);
+  auto& outs = h.outs;
+  for (uint32_t k = 1; k <= keff; ++k) {
+    HierOrderOut& o = outs[k];
+    o.jb.clear(); o.roles.clear(); o.fam.clear(); o.nodes.clear(); o.children.clear(); o.births.clear();
+    o.bindings.clear(); o.saddles.clear(); o.groups.clear(); o.fb.clear(); o.roots.clear();
+    o.status = EHGP_OK;
+    o.msg = "";
+  }
+  auto run_order = [&](uint32_t k, HierOrderOut& o) {
+    const auto to0 = std::chrono::steady_clock::now();
     auto fail_o = [&](const char* m) {
       o.status = EHGP_ERR_DEGENERATE;
       o.msg = m;
     };
     auto find = [&](uint32_t x) {  // path halving; roots follow the least-handle union rule alone
-      while (parent[x] != x) {
-        parent[x] = parent[parent[x]];
-        x = parent[x];
+      while (dsu[x].parent != x) {
+        dsu[x].parent = dsu[dsu[x].parent].parent;
+        x = dsu[x].parent;
       }
       return x;
     };
     uint64_t carriers = 0, reduced = 0;
     const uint64_t b_lo = k == 1 ? 0 : rb[k], b_hi = k == 1 ? 0 : rb[k + 1];
     const uint64_t s_lo = rb[k + 1], s_hi = rb[k + 2 > 16 ? 16 : k + 2];
+    const uint64_t arm_hi = s_hi > s_lo ? arm_off[s_hi - fam_lo] : 0;  // arms of this order end here
     o.fam.reserve(s_hi - s_lo);
     o.saddles.reserve(s_hi - s_lo);
     o.groups.reserve(s_hi - s_lo);
     o.births.reserve(k == 1 ? n : b_hi - b_lo);
+    {
+      const uint64_t nroles = (k == 1 ? n : b_hi - b_lo) + (s_hi - s_lo);
+      o.roles.reserve(nroles);
+      o.jb.reserve(nroles);
+      o.fb.reserve(nroles);
+      if (s_hi > s_lo) o.bindings.reserve(arm_off[s_hi - fam_lo] - arm_off[s_lo - fam_lo]);
+    }
     struct Role {
       uint32_t proj, role, fi, pos;
     };
@@ -1367,10 +1515,110 @@ int hier_run(Ctx& ctx, uint32_t K) {
     while (singles || bi < b_hi || si < s_hi) {
       uint32_t cls = kInvalid32, lev = kInvalid32;
       if (!singles) {
-        const uint32_t cls_b = bi < b_hi ? h.h_class[rank_order[bi]] : kInvalid32;
-        const uint32_t cls_s = si < s_hi ? h.h_class[rank_order[si]] : kInvalid32;
+        const uint32_t cls_b = bi < b_hi ? cls_rp[bi] : kInvalid32;
+        const uint32_t cls_s = si < s_hi ? cls_rp[si] : kInvalid32;
         cls = std::min(cls_b, cls_s);
         lev = cls_b <= cls_s ? rank_order[bi] : rank_order[si];
+        // fast paths: the batch holds exactly one role (almost every batch off ties)
+        const bool one_b = cls_b == cls && !(bi + 1 < b_hi && cls_rp[bi + 1] == cls) && cls_s != cls;
+        const bool one_s = cls_s == cls && !(si + 1 < s_hi && cls_rp[si + 1] == cls) && cls_b != cls;
+        if (one_b) {
+          const uint32_t bidx = (uint32_t)o.jb.size();
+          const uint32_t pos = (uint32_t)(bi - rb[2]), fi = rank_order[bi];
+          const uint32_t handle = n + pos;
+          o.jb.push_back({k, lev, (uint32_t)o.roles.size(), 1, 1, 0});
+          o.roles.push_back({bidx, n + fi, 0});
+          ehgp_forest_batch fb{k, lev, (uint32_t)o.births.size(), 1, (uint32_t)o.saddles.size(), 0,
+                               (uint32_t)o.groups.size(), 0, (uint32_t)carriers, (uint32_t)reduced, 0, 0};
+          o.births.push_back({n + fi, bidx, k, handle, kInvalid32});
+          dsu[handle].order = k;
+          dsu[handle].rroot = kInvalid32;
+          ++carriers;
+          fb.post_carriers = (uint32_t)carriers;
+          fb.post_roots = (uint32_t)reduced;
+          o.fb.push_back(fb);
+          ++bi;
+          continue;
+        }
+        if (one_s) {
+          const uint32_t bidx = (uint32_t)o.jb.size();
+          const uint32_t pos = (uint32_t)(si - fam_lo), fi = rank_order[si];
+          const uint32_t ridx = (uint32_t)o.roles.size();
+          o.jb.push_back({k, lev, ridx, 1, 0, 1});
+          o.roles.push_back({bidx, n + fi, 1});
+          const uint32_t a0 = arm_off[pos], a1 = arm_off[pos + 1];
+          const uint32_t fidx = (uint32_t)o.fam.size();
+          o.fam.push_back({fi, n + fi, ridx, bidx, k, a0, a1 - a0});
+          uint32_t car[4], dc[4];
+          int ndc = 0;
+          for (uint32_t a = a0; a < a1; ++a) {
+            if (a + 64 < arm_hi) __builtin_prefetch(&dsu[term[a + 64] < birth_count ? term[a + 64] : 0]);
+            if (a + 32 < arm_hi && term[a + 32] < birth_count) __builtin_prefetch(&dsu[dsu[term[a + 32]].parent]);
+            if (term[a] >= birth_count || !dsu[term[a]].order) {
+              fail_o("a strict arm descended to a minimum that is not yet born");
+              return;
+            }
+            const uint32_t c0 = find(term[a]);
+            car[a - a0] = c0;
+            int j = ndc;
+            bool dup = false;
+            for (int t = 0; t < ndc; ++t) dup |= dc[t] == c0;
+            if (!dup) {
+              while (j > 0 && dc[j - 1] > c0) { dc[j] = dc[j - 1]; --j; }
+              dc[j] = c0;
+              ++ndc;
+            }
+          }
+          uint32_t pr[4];
+          int np = 0;
+          for (int t = 0; t < ndc; ++t)
+            if (dsu[dc[t]].rroot != kInvalid32) {
+              const uint32_t x = dsu[dc[t]].rroot;
+              int j = np++;
+              while (j > 0 && pr[j - 1] > x) { pr[j] = pr[j - 1]; --j; }
+              pr[j] = x;
+            }
+          for (int t = 1; t < np; ++t)
+            if (pr[t] == pr[t - 1]) {
+              fail_o("a frozen carrier class repeats a reduced root");
+              return;
+            }
+          uint32_t kind, created = kInvalid32, result;
+          if (np == 1) {
+            kind = 1;
+            result = pr[0];
+          } else {
+            if (np == 0 && k == 1) {
+              fail_o("an order-one group has no root");
+              return;
+            }
+            kind = np == 0 ? 0 : 2;
+            created = (uint32_t)o.nodes.size();
+            result = created;
+          }
+          const uint32_t gidx = (uint32_t)o.groups.size(), sidx = (uint32_t)o.saddles.size();
+          const uint32_t bind0 = (uint32_t)o.bindings.size();
+          for (uint32_t a = a0; a < a1; ++a)
+            o.bindings.push_back({a, fidx, car[a - a0], dsu[car[a - a0]].rroot});
+          o.saddles.push_back({fidx, fi, bidx, bind0, a1 - a0, (uint32_t)ndc, (uint32_t)(ndc - np), (uint32_t)np, gidx});
+          const uint32_t ccnt = kind == 2 ? (uint32_t)np : 0u;
+          o.groups.push_back({bidx, sidx, 1, (uint32_t)ndc, (uint32_t)(ndc - np), (uint32_t)np,
+                              (uint32_t)o.children.size(), ccnt, created, result, kind});
+          if (kind != 1) o.nodes.push_back({k, lev, kind == 0 ? 1u : 2u, (uint32_t)o.children.size(), ccnt, kInvalid32, gidx});
+          if (kind == 2) o.children.insert(o.children.end(), pr, pr + np);
+          ehgp_forest_batch fb{k, lev, (uint32_t)o.births.size(), 0, sidx, 1, gidx, 1, (uint32_t)carriers,
+                               (uint32_t)reduced, 0, 0};
+          // commit: the distinct carriers are pre-batch roots; the least survives
+          for (int t = 1; t < ndc; ++t) dsu[dc[t]].parent = dc[0];
+          carriers -= (uint64_t)(ndc - 1);
+          dsu[dc[0]].rroot = result;
+          reduced = reduced - (uint64_t)np + 1;
+          fb.post_carriers = (uint32_t)carriers;
+          fb.post_roots = (uint32_t)reduced;
+          o.fb.push_back(fb);
+          ++si;
+          continue;
+        }
       }
       const uint32_t bidx = (uint32_t)o.jb.size();
       ehgp_journal_batch jb{k, lev, (uint32_t)o.roles.size(), 0, 0, 0};
@@ -1383,12 +1631,12 @@ int hier_run(Ctx& ctx, uint32_t K) {
       if (singles) {
         for (uint32_t p = 0; p < n; ++p) batch_roles.push_back({p, 0, kInvalid32, p});
       } else {
-        while (bi < b_hi && h.h_class[rank_order[bi]] == cls) {
+        while (bi < b_hi && cls_rp[bi] == cls) {
           batch_roles.push_back({n + rank_order[bi], 0, rank_order[bi], (uint32_t)(bi - rb[2])});
           ++bi;
         }
         const size_t nbr = batch_roles.size();
-        while (si < s_hi && h.h_class[rank_order[si]] == cls) {
+        while (si < s_hi && cls_rp[si] == cls) {
           batch_roles.push_back({n + rank_order[si], 1, rank_order[si], (uint32_t)(si - fam_lo)});
           ++si;
         }
@@ -1409,10 +1657,9 @@ int hier_run(Ctx& ctx, uint32_t K) {
           continue;
         }
         ++jb.saddle_roles;
-        const EvRec& ev = h.h_ev[r.fi];
+        // arm seeds follow the rank partition: the family at position p owns seeds arm_off[p]..
         fam_local.push_back((uint32_t)o.fam.size());
-        o.fam.push_back({r.fi, r.proj, ridx, bidx, k, (uint32_t)o.removed.size(), ev.size});
-        for (uint32_t j = 0; j < ev.size; ++j) o.removed.push_back(ev.ids[j]);
+        o.fam.push_back({r.fi, r.proj, ridx, bidx, k, arm_off[r.pos], arm_off[r.pos + 1] - arm_off[r.pos]});
         fam_pos.push_back(r.pos);
       }
       jb.role_count = (uint32_t)batch_roles.size();
@@ -1424,12 +1671,15 @@ int hier_run(Ctx& ctx, uint32_t K) {
         const uint32_t fpos = fam_pos[q];
         arm_b_off.push_back((uint32_t)arms_b.size());
         for (uint64_t a = arm_off[fpos]; a < arm_off[fpos + 1]; ++a) {
-          if (term[a] >= birth_count || !active[term[a]]) {
+          // two-stage prefetch: the arm's record 64 arms ahead, its parent's 32 ahead
+          if (a + 64 < arm_hi) __builtin_prefetch(&dsu[term[a + 64] < birth_count ? term[a + 64] : 0]);
+          if (a + 32 < arm_hi && term[a + 32] < birth_count) __builtin_prefetch(&dsu[dsu[term[a + 32]].parent]);
+          if (term[a] >= birth_count || !dsu[term[a]].order) {
             fail_o("a strict arm descended to a minimum that is not yet born");
             return;
           }
           const uint32_t c0 = find(term[a]);
-          arms_b.push_back({o.fam[fam_local[q]].arm_offset + (uint32_t)(a - arm_off[fpos]), c0, rroot[c0]});
+          arms_b.push_back({(uint32_t)a, c0, dsu[c0].rroot});
         }
       }
       arm_b_off.push_back((uint32_t)arms_b.size());
@@ -1469,7 +1719,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
         for (uint32_t i = 0; i < nc; ++i) {
           Plan& p = plans[plan_of[qf(i)]];
           ++p.c_cnt;
-          if (rroot[cars[i]] != kInvalid32) ++p.p_cnt;
+          if (dsu[cars[i]].rroot != kInvalid32) ++p.p_cnt;
         }
         for (uint32_t q = 0; q + 1 < arm_b_off.size(); ++q) ++plans[plan_of[qf(qi(arms_b[arm_b_off[q]].carrier))]].s_cnt;
         uint32_t co = 0, po = 0, so = 0;
@@ -1484,7 +1734,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
         for (uint32_t i = 0; i < nc; ++i) {
           Plan& p = plans[plan_of[qf(i)]];
           plan_car[p.c_off + p.c_cnt++] = cars[i];
-          if (rroot[cars[i]] != kInvalid32) plan_prior[p.p_off + p.p_cnt++] = rroot[cars[i]];
+          if (dsu[cars[i]].rroot != kInvalid32) plan_prior[p.p_off + p.p_cnt++] = dsu[cars[i]].rroot;
         }
         for (uint32_t q = 0; q + 1 < arm_b_off.size(); ++q) {
           Plan& p = plans[plan_of[qf(qi(arms_b[arm_b_off[q]].carrier))]];
@@ -1532,7 +1782,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
           }
           std::sort(tmp.begin(), tmp.end());
           tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
-          for (uint32_t c0 : tmp) nprior += rroot[c0] != kInvalid32;  // carriers are pre-batch roots
+          for (uint32_t c0 : tmp) nprior += dsu[c0].rroot != kInvalid32;  // carriers are pre-batch roots
           o.saddles.push_back({fidx, o.fam[fidx].event, bidx, arm_o, arm_b_off[q + 1] - arm_b_off[q],
                                (uint32_t)tmp.size(), (uint32_t)tmp.size() - nprior, nprior, gidx});
         }
@@ -1562,24 +1812,23 @@ int hier_run(Ctx& ctx, uint32_t K) {
       // commit: unions (least handle survives), reduced roots, then births
       for (const Plan& p : plans) {
         uint32_t r0 = find(plan_car[p.c_off]);
-        uint32_t had_reduced = rroot[r0] != kInvalid32;
+        uint32_t had_reduced = dsu[r0].rroot != kInvalid32;
         for (uint32_t i = 1; i < p.c_cnt; ++i) {
           const uint32_t r1 = find(plan_car[p.c_off + i]);
           if (r1 == r0) continue;
-          had_reduced += rroot[r1] != kInvalid32;
+          had_reduced += dsu[r1].rroot != kInvalid32;
           const uint32_t lo = std::min(r0, r1), hi = std::max(r0, r1);
-          parent[hi] = lo;
+          dsu[hi].parent = lo;
           r0 = lo;
           --carriers;
         }
-        rroot[r0] = p.result;
+        dsu[r0].rroot = p.result;
         reduced = reduced - had_reduced + 1;
       }
       for (size_t t = 0; t < new_births.size(); ++t) {
         const uint32_t hnd = new_births[t];
-        active[hnd] = 1;
-        border[hnd] = k;
-        rroot[hnd] = k == 1 ? o.births[fb.birth_offset + t].order_one_node : kInvalid32;
+        dsu[hnd].order = k;
+        dsu[hnd].rroot = k == 1 ? o.births[fb.birth_offset + t].order_one_node : kInvalid32;
         ++carriers;
         if (k == 1) ++reduced;
       }
@@ -1593,10 +1842,11 @@ int hier_run(Ctx& ctx, uint32_t K) {
     // final roots of this order (local node ids)
     const uint64_t h_lo = k == 1 ? 0 : n + (rb[k] - rb[2]), h_hi = k == 1 ? n : n + (rb[k + 1] - rb[2]);
     for (uint64_t hnd = h_lo; hnd < h_hi; ++hnd)
-      if (active[hnd] && parent[hnd] == hnd && rroot[hnd] != kInvalid32)
-        o.roots.push_back({k, (uint32_t)hnd, rroot[hnd]});
+      if (dsu[hnd].order && dsu[hnd].parent == hnd && dsu[hnd].rroot != kInvalid32)
+        o.roots.push_back({k, (uint32_t)hnd, dsu[hnd].rroot});
     std::sort(o.roots.begin(), o.roots.end(),
               [](const ehgp_forest_root& x, const ehgp_forest_root& y) { return x.node < y.node; });
+    o.ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - to0).count();
   };
   {
     std::vector<std::thread> pool;
@@ -1605,16 +1855,18 @@ int hier_run(Ctx& ctx, uint32_t K) {
   }
   for (uint32_t k = 1; k <= keff; ++k)
     if (outs[k].status != EHGP_OK) return abi_fail(&ctx, outs[k].status, outs[k].msg);
+  h.ms_orders = 0;
+  for (uint32_t k = 1; k <= keff; ++k) h.ms_orders = std::max(h.ms_orders, outs[k].ms);
   // concatenate with global offsets
   {
     uint64_t tot[12] = {0};
     for (uint32_t k = 1; k <= keff; ++k) {
-      const OrderOut& o = outs[k];
-      tot[0] += o.jb.size(); tot[1] += o.roles.size(); tot[2] += o.fam.size(); tot[3] += o.removed.size();
+      const HierOrderOut& o = outs[k];
+      tot[0] += o.jb.size(); tot[1] += o.roles.size(); tot[2] += o.fam.size();
       tot[4] += o.nodes.size(); tot[5] += o.children.size(); tot[6] += o.births.size(); tot[7] += o.bindings.size();
       tot[8] += o.saddles.size(); tot[9] += o.groups.size(); tot[10] += o.roots.size();
     }
-    h.jbatches.resize(tot[0]); h.roles.resize(tot[1]); h.families.resize(tot[2]); h.arm_removed.resize(tot[3]);
+    h.jbatches.resize(tot[0]); h.roles.resize(tot[1]); h.families.resize(tot[2]); h.arm_removed.assign(h.p_removed, h.p_removed + narms);
     h.nodes.resize(tot[4]); h.children.resize(tot[5]); h.births.resize(tot[6]); h.bindings.resize(tot[7]);
     h.saddles.resize(tot[8]); h.groups.resize(tot[9]); h.fbatches.resize(tot[0]); h.roots.resize(tot[10]);
     struct Off {
@@ -1623,17 +1875,17 @@ int hier_run(Ctx& ctx, uint32_t K) {
     std::vector<Off> off(keff + 2);
     off[1] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t k = 1; k <= keff; ++k) {
-      const OrderOut& o = outs[k];
+      const HierOrderOut& o = outs[k];
       const Off& a = off[k];
       off[k + 1] = {a.jb + (uint32_t)o.jb.size(), a.role + (uint32_t)o.roles.size(), a.fam + (uint32_t)o.fam.size(),
-                    a.seed + (uint32_t)o.removed.size(), a.node + (uint32_t)o.nodes.size(),
+                    0u, a.node + (uint32_t)o.nodes.size(),
                     a.child + (uint32_t)o.children.size(), a.birth + (uint32_t)o.births.size(),
                     a.bind + (uint32_t)o.bindings.size(), a.sad + (uint32_t)o.saddles.size(),
                     a.grp + (uint32_t)o.groups.size(), a.root + (uint32_t)o.roots.size()};
     }
     auto shift = [](uint32_t v, uint32_t d) { return v == kInvalid32 ? v : v + d; };
     auto merge_order = [&](uint32_t k) {
-      const OrderOut& o = outs[k];
+      const HierOrderOut& o = outs[k];
       const Off& f = off[k];
       for (size_t i = 0; i < o.jb.size(); ++i) {
         ehgp_journal_batch x = o.jb[i];
@@ -1654,10 +1906,8 @@ int hier_run(Ctx& ctx, uint32_t K) {
         ehgp_family_record x = o.fam[i];
         x.role_record += f.role;
         x.batch += f.jb;
-        x.arm_offset += f.seed;
         h.families[f.fam + i] = x;
       }
-      std::copy(o.removed.begin(), o.removed.end(), h.arm_removed.begin() + f.seed);
       for (size_t i = 0; i < o.nodes.size(); ++i) {
         ehgp_forest_node x = o.nodes[i];
         x.child_offset += f.child;
@@ -1673,7 +1923,6 @@ int hier_run(Ctx& ctx, uint32_t K) {
       }
       for (size_t i = 0; i < o.bindings.size(); ++i) {
         ehgp_forest_binding x = o.bindings[i];
-        x.arm_seed += f.seed;
         x.family += f.fam;
         x.prior_root = shift(x.prior_root, f.node);
         h.bindings[f.bind + i] = x;
@@ -1766,7 +2015,10 @@ int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out) {
   auto cp = [](void* dst, const void* src, size_t bytes) {
     if (dst && bytes) std::memcpy(dst, src, bytes);
   };
-  if (out->events && !h.h_ev.empty()) cp(out->events, h.h_ev.data(), h.h_ev.size() * sizeof(ehgp::EvRec));
+  if (out->events && h.events) {
+    const cudaError_t e = cudaMemcpy(out->events, h.ev, h.events * sizeof(ehgp::EvRec), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return ehgp::abi_cuda_fail(ctx, e, "facade copy");
+  }
   cp(out->journal_batches, h.jbatches.data(), h.jbatches.size() * sizeof(ehgp_journal_batch));
   cp(out->roles, h.roles.data(), h.roles.size() * sizeof(ehgp_role_record));
   cp(out->families, h.families.data(), h.families.size() * sizeof(ehgp_family_record));
@@ -1789,6 +2041,7 @@ int ehgp_hier_stats(const ehgp_ctx* ctx, double* ms, uint64_t* stats) {
     ms[0] = h.ms_device;
     ms[1] = h.ms_descent;
     ms[2] = h.ms_forest;
+    ms[3] = h.ms_orders;
   }
   if (stats) {
     stats[0] = h.arms;
@@ -1797,6 +2050,7 @@ int ehgp_hier_stats(const ehgp_ctx* ctx, double* ms, uint64_t* stats) {
     stats[3] = h.events;
     stats[4] = h.first_misses;
     stats[5] = h.descent_rounds;
+    for (int i = 0; i < 7; ++i) stats[6 + i] = h.slow[i];
   }
   return EHGP_OK;
 }
@@ -1804,10 +2058,12 @@ int ehgp_hier_stats(const ehgp_ctx* ctx, double* ms, uint64_t* stats) {
 int ehgp_event_level(ehgp_ctx* ctx, uint64_t event, uint64_t* num, uint64_t* den, int32_t* scale) {
   if (!ctx || !num || !den) return EHGP_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(ctx->mutex);
-  if (!ctx->hier || event >= ctx->hier->h_ev.size())
+  if (!ctx->hier || event >= ctx->hier->events)
     return ehgp::abi_fail(ctx, EHGP_ERR_INVALID_ARGUMENT, "no such facade event");
   const ehgp::HierState& h = *ctx->hier;
-  const ehgp::EvRec& r = h.h_ev[event];
+  ehgp::EvRec r;
+  const cudaError_t ce = cudaMemcpy(&r, h.ev + event, sizeof r, cudaMemcpyDeviceToHost);
+  if (ce != cudaSuccess) return ehgp::abi_cuda_fail(ctx, ce, "facade event copy");
   const ehgp::Cloud c{h.h_px.data(), h.h_py.data(), h.h_pz.data(), h.S};
   ehgp::W A;
   ehgp::WV N;

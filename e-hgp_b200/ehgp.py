@@ -430,12 +430,15 @@ class Context:
 
     def hier_stats(self) -> dict:
         """Timing and work counters of the last hierarchy call."""
-        ms = np.zeros(3)
-        st = np.zeros(6, np.uint64)
+        ms = np.zeros(4)
+        st = np.zeros(13, np.uint64)
         self._check(self.lib.ehgp_hier_stats(self._h, _ptr(ms), _ptr(st)))
-        return {"device_ms": ms[0], "descent_ms": ms[1], "forest_ms": ms[2], "arms": int(st[0]),
+        return {"device_ms": ms[0], "descent_ms": ms[1], "forest_ms": ms[2], "slowest_order_ms": ms[3],
+                "arms": int(st[0]),
                 "descent_steps": int(st[1]), "exact_boundaries": int(st[2]), "events": int(st[3]),
-                "first_misses": int(st[4]), "descent_rounds": int(st[5])}
+                "first_misses": int(st[4]), "descent_rounds": int(st[5]),
+                "slow": {k: int(v) for k, v in zip(("exhaustive_miniball", "exact_hull", "exact_side", "exact_level",
+                                                    "exact_band", "exact_cutoff", "equal_cutoff"), st[6:13])}}
 
     def event_level(self, event: int):
         """Exact level of a facade event as a Fraction (cloud units)."""

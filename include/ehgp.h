@@ -382,10 +382,14 @@ typedef struct ehgp_hier_out {
 int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out);
 
 /* Timing of the last ehgp_hierarchy call: ms[0] device stages (CUDA events),
- * ms[1] the strict-arm descent kernel, ms[2] the host forest pass;
+ * ms[1] the strict-arm descent kernels, ms[2] the host forest pass, ms[3] its
+ * slowest order (orders run on parallel host threads); ms holds 4 doubles;
  * stats[0] strict arms, [1] descent steps, [2] facade boundaries settled
  * exactly on the host, [3] facade events, [4] arms that are not themselves a
- * birth facet, [5] descent rounds (longest chain); stats holds 6 words. */
+ * birth facet, [5] descent rounds (longest chain), [6..12] slow-path counts of
+ * the descent (exhaustive miniball enumerations, exact hull signs, exact
+ * closed-ball sides, exact level conversions, exact band orders, exact cutoff
+ * comparisons, strictness checks at an equal cutoff); stats holds 13 words. */
 int ehgp_hier_stats(const ehgp_ctx* ctx, double* ms, uint64_t* stats);
 
 /* Exact level of facade event `event` as num / (den 2^(2 scale)), two's
