@@ -6,16 +6,19 @@ Workload: the regular volumetric cloud, 37^3 = 50,653 lattice points jittered
 by U[-0.25, 0.25] per axis, binary32 storage, seeded (synthetic; the
 reference names no dataset).  K_max = 10.  A step is one pass of the product
 path over one cloud; `config.stages` lists the stages inside the step:
-canonical cloud + exact Morton LBVH, Boruvka EMST, compact k=1 forest, and
-every relevant pair critical-sphere support (rank <= 11).
+canonical cloud + exact Morton LBVH, Boruvka EMST, compact k=1 forest, every
+relevant pair and triple/quad critical-sphere support (rank <= 11), and the
+direct Morse hierarchy (terminal facade, event journal, arm seeds, strict-arm
+descent, frozen-root quotient, hyper-Kruskal forest journal for orders 1..10).
 
 value : p95 over the K timed steps of the step time on the device timeline
         (CUDA events on the library's stream around the whole step; inputs
         already resident in HBM; the host-side forest sweep is inside).
 e2e   : p95 over K steps of the same step through the public C ABI with host
-        buffers: pinned host input copied in, and every result (EMST edges and
-        exact lengths, forest arenas, pair-support records and levels) copied
-        back to the host; wall clock.
+        buffers: pinned host input copied in, and the results (EMST edges and
+        exact lengths, k=1 forest arenas, pair- and higher-support records,
+        the hgp_reduced forest nodes, child arena, forest batches and final
+        roots of every order) copied back to host memory; wall clock.
 L2 is flushed (a 512 MiB write) before every timed step.
 
 Multi-GPU: replicas only (one independent cloud per rank, different seeds),
@@ -24,7 +27,8 @@ barrier + max over ranks; no data-path collective.
 --impl reference times the reference's own CPU code (oracle/_ref, compiled
 from the reference sources) for the same stages on a bounded sample of the
 workload (see `cpu_baseline.sample`), on rank 0 only: its exact pair stream
-costs minutes already at a few hundred points.
+costs minutes already at a few hundred points and its direct chain up to the
+forest journal seconds at ten points.
 """
 from __future__ import annotations
 
@@ -44,7 +48,8 @@ sys.path[:0] = [ROOT, os.path.join(ROOT, "e-hgp_b200")]
 METRIC = "warm_e2e_p95_ms_50k_jittered_lattice_K10"
 WORKLOAD = "jittered_lattice_37^3_f32"
 K_MAX = 10
-STAGES = ["canonical_cloud", "exact_morton_lbvh", "boruvka_emst", "k1_compact_forest", "pair_supports_rank_le_11"]
+STAGES = ["canonical_cloud", "exact_morton_lbvh", "boruvka_emst", "k1_compact_forest", "pair_supports_rank_le_11",
+          "higher_supports_rank_le_11", "direct_morse_hierarchy_orders_1_10"]
 
 
 def p95(xs):
@@ -125,7 +130,7 @@ def barrier(world: int):
 
 
 # ---- the reference's own CPU code on a bounded sample ---------------------------------
-SAMPLE_SIDE = 4  # a 4^3 = 64-point corner of the jittered lattice
+SAMPLE_SIDE = 2  # a 2^3 = 8-point corner of the jittered lattice: the reference's full chain takes seconds
 
 
 def reference_sample(seed: int = 0) -> np.ndarray:
@@ -140,10 +145,10 @@ def reference_step_seconds(pts: np.ndarray) -> dict:
     lb = pyoracle.lbvh_build(pts, "reference")["seconds"]
     pyoracle.emst_forest(pts, "reference")
     ef = pyoracle._text_call.seconds.copy()
-    pyoracle.pairs(pts, K_MAX, "reference")
-    pr = pyoracle._text_call.seconds.copy()
+    pyoracle.hierarchy(pts, K_MAX, "reference")
+    hi = pyoracle._text_call.seconds.copy()
     return {"canonical_cloud": lb[0], "exact_morton_lbvh": lb[1], "boruvka_emst": ef[0],
-            "k1_compact_forest": ef[1], "pair_supports_rank_le_11": pr[0]}
+            "k1_compact_forest": ef[1], "pair_and_higher_supports": hi[0], "direct_morse_hierarchy": hi[1]}
 
 
 def run_reference(args, world, rank):
@@ -161,8 +166,8 @@ def run_reference(args, world, rank):
         times.append(1e3 * sum(reference_step_seconds(pts).values()))
     v = p95(times)
     sample = (f"{len(pts)}-point {SAMPLE_SIDE}^3 corner of the same jittered lattice (the full 50,653-point "
-              f"cloud is out of reach: the reference's exact pair stream alone took 540 s at 256 points); "
-              f"{len(times)} steps, p95; reference CPU code, single thread")
+              f"cloud is out of reach: the reference's exact pair stream alone took 540 s at 256 points and its "
+              f"direct chain ~20 s at 10 points); {len(times)} steps, p95; reference CPU code, single thread")
     line = {"metric": METRIC, "value": v, "unit": "ms", "n_gpus": args.gpus, "steps": len(times),
             "warmup": min(args.warmup, 1), "ms_per_step": float(np.mean(times)), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "exact", "data": "synthetic", "impl": "reference",
@@ -210,30 +215,51 @@ def run_ours(args, world, rank, local):
     fout = ehgp.K1ForestOut(*(forest[k].ctypes.data for k in ("lv", "nodes", "child", "batches", "counts", "root")))
     none_lbvh = ehgp.LbvhOut(None, None, None, None, None, None)
     cnt = np.zeros(1, np.uint64)
+    hcnt = np.zeros(1, np.uint64)
+    hc = ehgp.HierCounts()
+
+    def pinned_np(count, dtype):
+        nbytes = int(count) * np.dtype(dtype).itemsize
+        t = torch.empty(max(nbytes, 1), dtype=torch.uint8, pin_memory=True)
+        return t.numpy().view(dtype)[:count]
 
     def l2_flush():
         flush.fill_(1.0)
         torch.cuda.synchronize(local)
 
     def resident_step():
-        """Device-resident step: results stay on the device except what the host forest sweep reads."""
+        """Device-resident step: supports stay in HBM; the hierarchy's host passes are inside."""
         ctx.step_begin()
         ctx._check(lib.ehgp_lbvh_build_device(ctx._h, C.c_void_p(d_pts.data_ptr()), n, C.byref(none_lbvh)))
         ctx._check(lib.ehgp_emst(ctx._h, None))
         ctx._check(lib.ehgp_k1_forest(ctx._h, C.byref(fout)))
         ctx._check(lib.ehgp_pairs(ctx._h, K_MAX, C.byref(ehgp.PairsOut(None, None, 0, cnt.ctypes.data))))
+        ctx._check(lib.ehgp_higher(ctx._h, K_MAX, C.byref(ehgp.HigherOut(None, 0, hcnt.ctypes.data))))
+        ctx._check(lib.ehgp_hierarchy(ctx._h, K_MAX, C.byref(hc)))
         return ctx.step_end()
 
-    # e2e buffers (host)
-    e_u = np.empty(m, np.uint32)
-    e_v = np.empty(m, np.uint32)
-    e_D = np.empty((m, 4), np.uint64)
+    # one untimed pass sizes the host buffers of the e2e step
+    resident_step()
+    counts = {f: int(getattr(hc, f)) for f, _ in ehgp.HierCounts._fields_}
+    e_u = pinned_np(m, np.uint32)
+    e_v = pinned_np(m, np.uint32)
+    e_D = pinned_np(m * 4, np.uint64).reshape(m, 4)
     rounds = np.zeros(1, np.uint32)
     eout = ehgp.EmstOut(e_u.ctypes.data, e_v.ctypes.data, e_D.ctypes.data, rounds.ctypes.data, None, 0, None)
-    pair_cap = 64 * n
-    recs = np.empty(pair_cap, ehgp.PAIR_RECORD)
-    plv = np.empty((pair_cap, 4), np.uint64)
+    pair_cap = int(cnt[0]) + 1024
+    recs = pinned_np(pair_cap, ehgp.PAIR_RECORD)
+    plv = pinned_np(pair_cap * 4, np.uint64).reshape(pair_cap, 4)
     pout = ehgp.PairsOut(recs.ctypes.data, plv.ctypes.data, pair_cap, cnt.ctypes.data)
+    higher_cap = int(hcnt[0]) + 1024
+    hrecs = pinned_np(higher_cap, ehgp.HIGHER_RECORD)
+    hout = ehgp.HigherOut(hrecs.ctypes.data, higher_cap, hcnt.ctypes.data)
+    slack = 1.05
+    f_nodes = pinned_np(int(counts["nodes"] * slack) + 64, ehgp.FOREST_NODE)
+    f_child = pinned_np(int(counts["children"] * slack) + 64, np.uint32)
+    f_batch = pinned_np(int(counts["journal_batches"] * slack) + 64, ehgp.FOREST_BATCH)
+    f_root = pinned_np(64, ehgp.FOREST_ROOT)
+    hier_out = ehgp.HierOut(None, None, None, None, None, f_nodes.ctypes.data, f_child.ctypes.data, None, None,
+                            None, None, f_batch.ctypes.data, f_root.ctypes.data)
 
     def e2e_step():
         t0 = time.perf_counter()
@@ -241,6 +267,12 @@ def run_ours(args, world, rank, local):
         ctx._check(lib.ehgp_emst(ctx._h, C.byref(eout)))
         ctx._check(lib.ehgp_k1_forest(ctx._h, C.byref(fout)))
         ctx._check(lib.ehgp_pairs(ctx._h, K_MAX, C.byref(pout)))
+        ctx._check(lib.ehgp_higher(ctx._h, K_MAX, C.byref(hout)))
+        ctx._check(lib.ehgp_hierarchy(ctx._h, K_MAX, C.byref(hc)))
+        if (hc.nodes > len(f_nodes) or hc.children > len(f_child) or hc.journal_batches > len(f_batch)
+                or hc.final_roots > len(f_root)):
+            raise RuntimeError("the hierarchy payload outgrew its host buffers")
+        ctx._check(lib.ehgp_hier_copy(ctx._h, C.byref(hier_out)))
         return 1e3 * (time.perf_counter() - t0)
 
     for _ in range(max(args.warmup, 3)):
@@ -248,15 +280,13 @@ def run_ours(args, world, rank, local):
         e2e_step()
     barrier(world)
     dev_ms, e2e_ms, kern_ms = [], [], []
-    launches = 0
-    stats = None
+    hstats = None
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
             l2_flush()
             dev_ms.append(resident_step())
-            km, stats = ctx.kernel_stats()
+            km, hstats = ctx.higher_stats()
             kern_ms.append(km)
-            launches += int(ctx.last_timing()[1])
         for _ in range(args.steps):
             l2_flush()
             e2e_ms.append(e2e_step())
@@ -266,26 +296,40 @@ def run_ours(args, world, rank, local):
     if rank != 0:
         ctx.close()
         return
-    records = int(cnt[0])
-    # stage breakdown of one more step (device time per stage)
+    # stage breakdown of one more step (device time per stage; host stages on the host clock)
     l2_flush()
     stage_ms = {}
+    launches_per_step = 0
     ctx._check(lib.ehgp_lbvh_build_device(ctx._h, C.c_void_p(d_pts.data_ptr()), n, C.byref(none_lbvh)))
-    stage_ms["lbvh"], l1 = ctx.last_timing()
+    stage_ms["lbvh"], l = ctx.last_timing()
+    launches_per_step += l
     ctx._check(lib.ehgp_emst(ctx._h, None))
-    stage_ms["emst"], l2 = ctx.last_timing()
+    stage_ms["emst"], l = ctx.last_timing()
+    launches_per_step += l
     t0 = time.perf_counter()
     ctx._check(lib.ehgp_k1_forest(ctx._h, C.byref(fout)))
     stage_ms["k1_forest_host"] = 1e3 * (time.perf_counter() - t0)
     ctx._check(lib.ehgp_pairs(ctx._h, K_MAX, C.byref(ehgp.PairsOut(None, None, 0, cnt.ctypes.data))))
-    stage_ms["pairs"], l3 = ctx.last_timing()
-    launches_per_step = int(l1 + l2 + l3)
-    # roofline of the dominant kernel (pair enumeration): algorithmic bytes per launch from
-    # its own work counters: 32 B per LBVH node visit (box + children), 24 B per point whose
-    # side is decided (64 witness coordinates per witness-list classification), 32 B per
-    # ball-query node visit, 64 B per emitted record, 280 B per point of witness list + coordinates.
-    visits, local_pairs, ballq, ball_nodes, emitted = (int(x) for x in stats[:5])
-    alg_bytes = 32 * visits + 64 * 24 * local_pairs + 32 * ball_nodes + 64 * emitted + 280 * n
+    stage_ms["pairs"], l = ctx.last_timing()
+    launches_per_step += l
+    ctx._check(lib.ehgp_higher(ctx._h, K_MAX, C.byref(ehgp.HigherOut(None, 0, hcnt.ctypes.data))))
+    stage_ms["higher"], l = ctx.last_timing()
+    launches_per_step += l
+    t0 = time.perf_counter()
+    ctx._check(lib.ehgp_hierarchy(ctx._h, K_MAX, C.byref(hc)))
+    stage_ms["hierarchy_wall"] = 1e3 * (time.perf_counter() - t0)
+    _, l = ctx.last_timing()
+    launches_per_step += l
+    hs = ctx.hier_stats()
+    stage_ms["hierarchy_device"] = float(hs["device_ms"])
+    stage_ms["hierarchy_descent"] = float(hs["descent_ms"])
+    stage_ms["hierarchy_forest_host"] = float(hs["forest_ms"])
+    launches = launches_per_step * args.steps
+    # roofline of the dominant device kernel of the step (triple/quad enumeration, k_higher):
+    # algorithmic bytes per launch from its counters: 28 B per candidate-set entry staged
+    # (PointId + FP64 coordinates), 2568 B per point of per-cone radius table, 64 B per record.
+    tested, classified, emitted, set_entries = (int(x) for x in hstats[:4])
+    alg_bytes = 28 * set_entries + 2568 * n + 64 * emitted
     kmean = float(np.mean(kern_ms))
     peaks = {}
     try:
@@ -294,22 +338,28 @@ def run_ours(args, world, rank, local):
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved = alg_bytes / (kmean * 1e-3) / 1e9
-    d2h = e_u.nbytes + e_v.nbytes + e_D.nbytes + sum(forest[k].nbytes for k in forest) + records * (64 + 32)
+    d2h = (e_u.nbytes + e_v.nbytes + e_D.nbytes + sum(forest[k].nbytes for k in forest) + int(cnt[0]) * (64 + 32)
+           + int(hcnt[0]) * 64 + int(hc.nodes) * f_nodes.itemsize + int(hc.children) * 4
+           + int(hc.journal_batches) * f_batch.itemsize + int(hc.final_roots) * f_root.itemsize)
     line = {
         "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": float(np.mean(dev_ms)), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64+exact", "data": "synthetic",
         "config": {"workload": WORKLOAD, "points": n, "K_max": K_MAX, "stages": STAGES, "seed": "rank",
                    "l2": "flushed 512MiB before each step", "parallelism": f"replicas{world}",
-                   "pair_supports": records, "stage_ms": stage_ms},
+                   "pair_supports": int(cnt[0]), "higher_supports": int(hcnt[0]),
+                   "hierarchy": {k: counts[k] for k in ("events", "journal_batches", "arm_seeds", "nodes",
+                                                       "final_roots")},
+                   "stage_ms": stage_ms},
         "e2e": {"value": e2e, "unit": "ms", "h2d_bytes_per_step": int(pts.nbytes), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
-        "gpu_launches_per_step": launches_per_step,
+        "gpu_launches_per_step": int(launches_per_step),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "kernel": "k_pairs (pair-support enumeration)",
+                     "traffic": None, "kernel": "k_higher (triple/quad support enumeration)",
                      "kernel_ms": kmean, "algorithmic_bytes": alg_bytes,
-                     "work": {"node_visits": visits, "witness_classifications": local_pairs,
-                              "ball_queries": ballq, "ball_query_node_visits": ball_nodes, "records": emitted},
+                     "work": {"status_tests": tested, "classified": classified, "records": emitted,
+                              "candidate_set_entries": set_entries},
+                     "note": "FP64 predicate-bound, not byte-bound: see DESIGN.md",
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "clocks": clocks.summary(),
     }
@@ -323,7 +373,7 @@ def run_ours(args, world, rank, local):
                 sctx.lbvh_build(sample, outputs=False)
                 sctx.emst(with_minima=False)
                 sctx.k1_forest()
-                sctx.pairs(K_MAX)
+                sctx.hierarchy(K_MAX, arrays=False)
                 ts.append(1e3 * (time.perf_counter() - t0))
         line["cpu_baseline"] = cpu_baseline_line(float(np.median(ts)))
     print(json.dumps(line))
@@ -333,8 +383,8 @@ def run_ours(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     args = ap.parse_args()
     if args.impl == "reference":

@@ -310,7 +310,7 @@ k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uin
            const double* __restrict__ pz, const double* __restrict__ gather_r2, uint8_t* __restrict__ todo,
            uint32_t* __restrict__ cand, uint32_t* __restrict__ candc, double* __restrict__ need_r,
            float* __restrict__ rho_tab) {
-  __shared__ float4 rel[kDirWarps][kMaxNb];  // x, y, z, |p - a| (binary32 copies; margins below)
+  __shared__ float4 rel[kDirWarps][kMaxNb];  // unit direction of p - a and |p - a| (binary32; margins below)
   __shared__ uint32_t ids[kDirWarps][kMaxNb];
   __shared__ uint32_t mark[kDirWarps][kMaxNb / 32];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -327,7 +327,9 @@ k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uin
   for (uint32_t i = lane; i < m; i += 32) {
     const uint32_t p = nb[(uint64_t)a * kMaxNb + i];
     const double x = px[p] - ax, y = py[p] - ay, z = pz[p] - az;
-    rel[warp][i] = make_float4((float)x, (float)y, (float)z, (float)sqrt(x * x + y * y + z * z));
+    const double dd = sqrt(x * x + y * y + z * z);
+    const double inv = dd > 0.0 ? 1.0 / dd : 0.0;
+    rel[warp][i] = make_float4((float)(x * inv), (float)(y * inv), (float)(z * inv), (float)dd);  // unit direction, |p - a|
     ids[warp][i] = p;
   }
   for (uint32_t i = lane; i < (uint32_t)kMaxNb / 32; i += 32) mark[warp][i] = 0;
@@ -395,7 +397,7 @@ k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uin
       const double dist = (double)r.w;
       const double kth = cnt >= cp.need ? best[cp.need - 1] : INFINITY;
       if (0.5 * dist * (1.0 - 1e-5) > fmin(kth, ext)) break;
-      const double c = (s0 * r.x + s1 * r.y + s2 * r.z) / dist;
+      const double c = s0 * r.x + s1 * r.y + s2 * r.z;
       // upper bound of the angle (cosine lowered by the binary32 margin) -> cos(angle + delta) lowered
       const double cs = fmax(-1.0, c - 1e-5), sn = sqrt(fmax(0.0, 1.0 - cs * cs));
       const double cshr = cs * cd - sn * sdl;
@@ -422,7 +424,7 @@ k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uin
       const float4 r = rel[warp][i];
       const double dist = (double)r.w;
       if (0.5 * dist * (1.0 - 1e-5) > rho_s) break;
-      const double c = (s0 * r.x + s1 * r.y + s2 * r.z) / dist;
+      const double c = s0 * r.x + s1 * r.y + s2 * r.z;
       // lower bound of the angle (cosine raised by the margin) -> cos(max(angle - delta, 0)) raised
       const double cs = fmin(1.0, c + 1e-5);
       const double sn = sqrt(fmax(0.0, 1.0 - cs * cs));

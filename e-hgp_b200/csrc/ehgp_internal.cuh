@@ -54,6 +54,8 @@ constexpr int kRadixThreads = 256;
 constexpr int kRadixItems = 4;
 constexpr int kRadixTile = kRadixThreads * kRadixItems;
 constexpr int kRadixMaxPasses = 32;
+// State words: per pass (input buffer, trivial flag), then 256 digit totals.
+constexpr int kRadixStateWords = 2 * (kRadixMaxPasses + 1) + 256;
 
 // Key source for one sorting stage: key(v) = order_key(words[v]) when
 // `order` is set, else words[v].

@@ -765,7 +765,7 @@ cudaError_t lbvh_alloc(Ctx& ctx) {
   const uint32_t tiles = (uint32_t)((n + kRadixTile - 1) / kRadixTile);
   ctx.radix.max_tiles = tiles;
   EHGP_ALLOC(ctx.radix.counts, 256ull * tiles * sizeof(uint32_t));
-  EHGP_ALLOC(ctx.radix.state, 2 * (kRadixMaxPasses + 1) * sizeof(uint32_t));
+  EHGP_ALLOC(ctx.radix.state, kRadixStateWords * sizeof(uint32_t));
 #undef EHGP_ALLOC
   return cudaMemsetAsync(b.frame_done, 0, sizeof(uint32_t), ctx.stream);
 }

@@ -68,7 +68,7 @@ constexpr uint64_t scratch_bytes() {
   L.take(8 * 4);                // stats
   L.take(2 * n * sizeof(ehgp_lbvh_node) + n * sizeof(ehgp_lbvh_leaf) + n * 8);  // export
   L.take(256ull * ((n + ehgp::kRadixTile - 1) / ehgp::kRadixTile) * 4);         // radix counts
-  L.take(2 * (ehgp::kRadixMaxPasses + 1) * 4);  // radix state
+  L.take(ehgp::kRadixStateWords * 4);  // radix state
   L.take(4);                    // error word
   return L.off;
 }
@@ -130,7 +130,7 @@ void carve(ehgp::Ctx& c, unsigned char* base) {
   b.export_buf = at(b.export_bytes);
   c.radix.max_tiles = (uint32_t)((n + ehgp::kRadixTile - 1) / ehgp::kRadixTile);
   c.radix.counts = (uint32_t*)at(256ull * c.radix.max_tiles * 4);
-  c.radix.state = (uint32_t*)at(2 * (ehgp::kRadixMaxPasses + 1) * 4);
+  c.radix.state = (uint32_t*)at(ehgp::kRadixStateWords * 4);
   c.d_err = (uint32_t*)at(4);
   c.max_points = n;
 }

@@ -7,9 +7,9 @@
 //    morton_leaf_less (src/cpu/spatial/lbvh.cpp:93-100,512) -- stability of
 //    the LSD passes over an input in PointId order gives the PointId tie-break.
 //
-// Each 8-bit pass is three kernels: a per-tile histogram (upsweep), a
-// single-CTA scan that also detects a pass in which every key has the same
-// digit, and a stable scatter (downsweep).  Trivial passes are skipped on the
+// Each 8-bit pass is four kernels: a per-tile histogram (upsweep), a row scan
+// of the histogram (one block per digit), a digit-base scan that also detects a
+// pass in which every key has the same digit, and a stable scatter (downsweep).  Trivial passes are skipped on the
 // device (the scatter returns at once and the ping-pong buffer is not
 // flipped), so the host never synchronises inside a sort and the whole
 // sequence can be captured in a CUDA graph.
@@ -43,20 +43,50 @@ k_radix_upsweep(uint32_t n, const uint32_t* __restrict__ vals0, const uint32_t* 
   counts[threadIdx.x * tiles + tile] = hist[threadIdx.x];
 }
 
-// One CTA of 256 threads: thread d owns digit d.
+// Row scan: block d turns row d of the tile histogram (counts[d * tiles ..]) into
+// exclusive offsets within the digit and stores the digit total (coalesced, one
+// block per digit).
 __global__ void __launch_bounds__(256)
-k_radix_scan(uint32_t n, uint32_t* __restrict__ counts, uint32_t tiles, uint32_t* __restrict__ state,
-             int pass) {
+k_radix_rowscan(uint32_t* __restrict__ counts, uint32_t tiles, uint32_t* __restrict__ state) {
+  __shared__ uint32_t warp_tot[8];
+  __shared__ uint32_t carry;
+  const uint32_t d = blockIdx.x, tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  uint32_t* row = counts + (uint64_t)d * tiles;
+  if (tid == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < tiles; base += 256) {
+    const uint32_t t = base + tid;
+    const uint32_t v = t < tiles ? row[t] : 0u;
+    uint32_t x = v;  // inclusive warp scan
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+      if ((int)lane >= off) x += y;
+    }
+    if (lane == 31) warp_tot[warp] = x;
+    __syncthreads();
+    uint32_t wbase = 0;
+    for (uint32_t w = 0; w < warp; ++w) wbase += warp_tot[w];
+    const uint32_t c0 = carry;
+    if (t < tiles) row[t] = c0 + wbase + x - v;
+    __syncthreads();
+    if (tid == 255) carry = c0 + wbase + x;
+    __syncthreads();
+  }
+  if (tid == 0) state[2 * (kRadixMaxPasses + 1) + d] = carry;
+}
+
+// Digit bases: exclusive scan of the 256 digit totals; a pass whose keys share one
+// digit is marked trivial (its scatter is skipped and the buffers do not flip).
+__global__ void __launch_bounds__(256)
+k_radix_digits(uint32_t n, uint32_t* __restrict__ state, int pass) {
   __shared__ uint32_t totals[256];
   __shared__ uint32_t trivial;
   const uint32_t d = threadIdx.x;
   if (d == 0) trivial = 0;
-  uint32_t sum = 0;
-  for (uint32_t t = 0; t < tiles; ++t) sum += counts[d * tiles + t];
+  const uint32_t sum = state[2 * (kRadixMaxPasses + 1) + d];
   totals[d] = sum;
   __syncthreads();
   if (sum == n) trivial = 1;
-  // exclusive scan of the 256 digit totals (Hillis-Steele in shared memory)
   uint32_t v = sum;
   for (int off = 1; off < 256; off <<= 1) {
     __syncthreads();
@@ -66,12 +96,7 @@ k_radix_scan(uint32_t n, uint32_t* __restrict__ counts, uint32_t tiles, uint32_t
     totals[d] = v;
   }
   __syncthreads();
-  uint32_t run = v - sum;  // exclusive base of digit d
-  for (uint32_t t = 0; t < tiles; ++t) {
-    const uint32_t c = counts[d * tiles + t];
-    counts[d * tiles + t] = run;
-    run += c;
-  }
+  state[2 * (kRadixMaxPasses + 1) + d] = v - sum;  // exclusive base of digit d
   __syncthreads();
   if (d == 0) {
     const uint32_t cur = state[2 * pass];
@@ -92,7 +117,7 @@ k_radix_downsweep(uint32_t n, uint32_t* __restrict__ vals0, uint32_t* __restrict
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   const uint32_t* in = state[2 * pass] ? vals1 : vals0;
   uint32_t* out = state[2 * pass] ? vals0 : vals1;
-  base[tid] = counts[tid * tiles + tile];
+  base[tid] = counts[tid * tiles + tile] + state[2 * (kRadixMaxPasses + 1) + tid];
   const uint32_t lanemask_lt = (1u << lane) - 1u;
   for (int r = 0; r < kRadixItems; ++r) {
     const uint32_t i = tile * kRadixTile + r * kRadixThreads + tid;
@@ -139,10 +164,11 @@ int radix_sort_indirect(cudaStream_t stream, uint32_t n, uint32_t* vals0, uint32
     for (int shift = 0; shift < stage_bits[s]; shift += 8) {
       k_radix_upsweep<<<tiles, kRadixThreads, 0, stream>>>(n, vals0, vals1, stages[s], shift, scratch.state,
                                                            pass, scratch.counts, tiles);
-      k_radix_scan<<<1, 256, 0, stream>>>(n, scratch.counts, tiles, scratch.state, pass);
+      k_radix_rowscan<<<256, 256, 0, stream>>>(scratch.counts, tiles, scratch.state);
+      k_radix_digits<<<1, 256, 0, stream>>>(n, scratch.state, pass);
       k_radix_downsweep<<<tiles, kRadixThreads, 0, stream>>>(n, vals0, vals1, stages[s], shift, scratch.state,
                                                              pass, scratch.counts, tiles);
-      *launches += 3;
+      *launches += 4;
       ++pass;
     }
   }
