@@ -275,3 +275,48 @@ def hierarchy_diff(a: str, b: str) -> str:
     if len(la) != len(lb):
         return f"line counts {len(la)} vs {len(lb)}"
     return ""
+
+
+# ---- the normative hgp_reduced definition ------------------------------------------
+def forests_from_hier_text(text: str) -> list[dict]:
+    """Per-order forests (the definition's layout) from a direct-hierarchy text:
+    nodes of each order in creation order as [kind, num, den, child indices within
+    the order] (order-one and reduced births are 'birth', multifusions 'merge'), and
+    the final roots as indices within the order."""
+    nodes, children, roots = [], [], []
+    for line in text.splitlines():
+        f = line.split()
+        if not f:
+            continue
+        if f[0] == "N":
+            nodes.append((int(f[1]), int(f[2]), f[3], f[4], int(f[5]), int(f[6]), int(f[7])))
+        elif f[0] == "C":
+            children = [int(x) for x in f[1:]]
+        elif f[0] == "R":
+            roots.append((int(f[2]), int(f[4])))
+    orders = sorted({nd[1] for nd in nodes} | {o for o, _ in roots})
+    out = []
+    for k in orders:
+        ids = [nd[0] for nd in nodes if nd[1] == k]
+        local = {g: i for i, g in enumerate(ids)}
+        fn = []
+        for nd in nodes:
+            if nd[1] != k:
+                continue
+            _, _, num, den, kind, off, cnt = nd
+            fn.append(["birth" if kind in (0, 1) else "merge", num, den, [local[c] for c in children[off:off + cnt]]])
+        out.append({"order": k, "nodes": fn, "roots": sorted(local[g] for o, g in roots if o == k)})
+    return out
+
+
+def definition_match(ours: list[dict], golden: list[dict]) -> str:
+    """'' when every order of the golden definition forest equals ours (orders with no
+    node on either side compare equal)."""
+    by = {f["order"]: f for f in ours}
+    for g in golden:
+        o = by.get(g["order"], {"nodes": [], "roots": []})
+        if o["nodes"] != g["nodes"]:
+            return f"order {g['order']}: nodes differ\n ours {o['nodes'][:6]}\n def  {g['nodes'][:6]}"
+        if o["roots"] != g["roots"]:
+            return f"order {g['order']}: roots {o['roots']} vs {g['roots']}"
+    return ""

@@ -7,6 +7,7 @@ project-written Boost shim).  Run here, where the reference tree exists:
     python tests/golden/make_golden.py --pairs   # slow: the reference pair stream
     python tests/golden/make_golden.py --higher  # slow: the reference higher-support stream (n = 12)
     python tests/golden/make_golden.py --hierarchy  # slow: the reference direct chain up to the forest journal
+    python tests/golden/make_golden.py --definition  # the Python exhaustive-Gamma hgp_reduced forests
 """
 import os
 import sys
@@ -188,3 +189,43 @@ def main_hierarchy():
 
 if __name__ == "__main__" and "--hierarchy" in sys.argv:
     main_hierarchy()
+
+
+# ---- the normative hgp_reduced definition (Python exhaustive-Gamma oracle) ------------
+REF_PY = "/root/reference/reference"  # morsehgp3d_oracle, stdlib only; run here, where the reference exists
+
+
+def definition_cases():
+    rng = np.random.Generator(np.random.PCG64(29))
+    yield "uniform6_K10", rng.random((6, 3)), 10
+    yield "uniform7_K10", rng.random((7, 3)), 10
+    yield "uniform8_K10", rng.random((8, 3)), 10
+    yield "uniform8_K3", rng.random((8, 3)), 3
+    yield "lattice2_f32_K10", workloads.jittered_lattice(2, 9).astype(np.float64), 10
+
+
+def main_definition():
+    """Forests of run_oracle(points, K, profile='hgp_reduced')
+    (reference/morsehgp3d_oracle/oracle.py:211, hierarchy.py:309-498): per order the
+    nodes in creation order as (kind, level numerator, level denominator, child indices
+    within the order), and the final root indices."""
+    import json
+    sys.path.insert(0, REF_PY)
+    from morsehgp3d_oracle.oracle import run_oracle
+    for name, pts, K in definition_cases():
+        res = run_oracle([tuple(float(x) for x in p) for p in pts], K, profile="hgp_reduced")
+        forests = []
+        for o in res.orders:
+            f = o.forest
+            index = {nd.node_id: i for i, nd in enumerate(f.nodes)}
+            nodes = [[nd.kind, str(nd.squared_level.numerator), str(nd.squared_level.denominator),
+                      [index[c] for c in nd.child_ids]] for nd in f.nodes]
+            forests.append({"order": o.order, "nodes": nodes, "roots": sorted(index[r] for r in f.root_ids)})
+        doc = {"points": pts.tolist(), "K": K, "k_eff": res.k_eff, "forests": forests}
+        with open(os.path.join(HERE, f"definition_{name}.json"), "w") as fh:
+            json.dump(doc, fh, separators=(",", ":"))
+        print(name, len(pts), [len(f["nodes"]) for f in forests], flush=True)
+
+
+if __name__ == "__main__" and "--definition" in sys.argv:
+    main_definition()

@@ -86,3 +86,18 @@ def test_gpu_hierarchy_structure_at_scale(ctx):
     assert int(merges["child_count"].sum()) - len(merges) == n - 1
     assert len(r["bindings"]) == len(r["arm_removed"])
     assert np.all(r["bindings"]["carrier"] < r["birth_records"])
+
+
+DEFINITION = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "definition_*.json")))
+
+
+@pytest.mark.parametrize("path", DEFINITION, ids=[os.path.basename(p)[11:-5] for p in DEFINITION])
+def test_gpu_forest_matches_hgp_reduced_definition(ctx, path):
+    """Device forest journal against the normative hgp_reduced forests of the
+    exhaustive-Gamma Python oracle (kinds, exact levels, children, final roots)."""
+    from geomcheck import definition_match, forests_from_hier_text
+    d = json.load(open(path))
+    ctx.lbvh_build(np.array(d["points"]), outputs=False)
+    got = forests_from_hier_text(gpu_hierarchy_text(ctx, d["K"]))
+    msg = definition_match(got, d["forests"])
+    assert msg == "", msg

@@ -48,3 +48,19 @@ def test_restatement_hierarchy_matches_live_reference():
     a = pyoracle.hierarchy(pts, 10)
     b = pyoracle.hierarchy(pts, 10, which="reference")
     assert a == b, first_diff(a, b)
+
+
+DEFINITION = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "definition_*.json")))
+
+
+@pytest.mark.parametrize("path", DEFINITION, ids=[os.path.basename(p)[11:-5] for p in DEFINITION])
+def test_restatement_forest_matches_hgp_reduced_definition(path):
+    """The direct forest journal's nodes equal the normative hgp_reduced forests of the
+    exhaustive-Gamma Python oracle (reference/morsehgp3d_oracle, run_oracle(...,
+    profile='hgp_reduced'); tests/golden/make_golden.py --definition): kinds, exact
+    levels, children and final roots, order by order."""
+    from geomcheck import definition_match, forests_from_hier_text
+    d = json.load(open(path))
+    got = forests_from_hier_text(pyoracle.hierarchy(np.array(d["points"]), d["K"]))
+    msg = definition_match(got, d["forests"])
+    assert msg == "", msg
