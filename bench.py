@@ -18,7 +18,8 @@ e2e   : p95 over K steps of the same step through the public C ABI with host
         buffers: pinned host input copied in, and the results (EMST edges and
         exact lengths, k=1 forest arenas, pair- and higher-support records,
         the hgp_reduced forest nodes, child arena, forest batches and final
-        roots of every order) copied back to host memory; wall clock.
+        roots of every order, and the vertical maps between adjacent orders)
+        copied back to host memory; wall clock.
 L2 is flushed (a 512 MiB write) before every timed step.
 
 Multi-GPU: replicas only (one independent cloud per rank, different seeds),
@@ -49,7 +50,8 @@ METRIC = "warm_e2e_p95_ms_50k_jittered_lattice_K10"
 WORKLOAD = "jittered_lattice_37^3_f32"
 K_MAX = 10
 STAGES = ["canonical_cloud", "exact_morton_lbvh", "boruvka_emst", "k1_compact_forest", "pair_supports_rank_le_11",
-          "higher_supports_rank_le_11", "direct_morse_hierarchy_orders_1_10"]
+          "higher_supports_rank_le_11", "direct_morse_hierarchy_orders_1_10",
+          "vertical_maps_orders_2_10"]
 
 
 def p95(xs):
@@ -258,8 +260,9 @@ def run_ours(args, world, rank, local):
     f_child = pinned_np(int(counts["children"] * slack) + 64, np.uint32)
     f_batch = pinned_np(int(counts["journal_batches"] * slack) + 64, ehgp.FOREST_BATCH)
     f_root = pinned_np(64, ehgp.FOREST_ROOT)
+    f_vert = pinned_np(int(counts["vertical_assignments"] * slack) + 64, ehgp.VERTICAL_ASSIGNMENT)
     hier_out = ehgp.HierOut(None, None, None, None, None, f_nodes.ctypes.data, f_child.ctypes.data, None, None,
-                            None, None, f_batch.ctypes.data, f_root.ctypes.data)
+                            None, None, f_batch.ctypes.data, f_root.ctypes.data, f_vert.ctypes.data)
 
     def e2e_step():
         t0 = time.perf_counter()
@@ -270,7 +273,7 @@ def run_ours(args, world, rank, local):
         ctx._check(lib.ehgp_higher(ctx._h, K_MAX, C.byref(hout)))
         ctx._check(lib.ehgp_hierarchy(ctx._h, K_MAX, C.byref(hc)))
         if (hc.nodes > len(f_nodes) or hc.children > len(f_child) or hc.journal_batches > len(f_batch)
-                or hc.final_roots > len(f_root)):
+                or hc.final_roots > len(f_root) or hc.vertical_assignments > len(f_vert)):
             raise RuntimeError("the hierarchy payload outgrew its host buffers")
         ctx._check(lib.ehgp_hier_copy(ctx._h, C.byref(hier_out)))
         return 1e3 * (time.perf_counter() - t0)
@@ -340,7 +343,8 @@ def run_ours(args, world, rank, local):
     achieved = alg_bytes / (kmean * 1e-3) / 1e9
     d2h = (e_u.nbytes + e_v.nbytes + e_D.nbytes + sum(forest[k].nbytes for k in forest) + int(cnt[0]) * (64 + 32)
            + int(hcnt[0]) * 64 + int(hc.nodes) * f_nodes.itemsize + int(hc.children) * 4
-           + int(hc.journal_batches) * f_batch.itemsize + int(hc.final_roots) * f_root.itemsize)
+           + int(hc.journal_batches) * f_batch.itemsize + int(hc.final_roots) * f_root.itemsize
+           + int(hc.vertical_assignments) * f_vert.itemsize)
     line = {
         "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": float(np.mean(dev_ms)), "higher_is_better": False,

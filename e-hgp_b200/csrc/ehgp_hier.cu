@@ -1052,6 +1052,8 @@ struct HierState {
   std::vector<ehgp_forest_group> groups;
   std::vector<ehgp_forest_batch> fbatches;
   std::vector<ehgp_forest_root> roots;
+  std::vector<ehgp_vertical_assignment> vertical;
+  std::vector<uint32_t> h_class;  // level class by facade index
   uint32_t decision = EHGP_ERR_NOT_BUILT;
   double ms_device = 0, ms_forest = 0, ms_descent = 0, ms_orders = 0;
   uint64_t descent_steps = 0, arms = 0, exact_boundaries = 0;
@@ -1954,6 +1956,82 @@ int hier_run(Ctx& ctx, uint32_t K) {
     for (uint32_t k = 1; k <= keff; ++k) pool.emplace_back(merge_order, k);
     for (auto& t : pool) t.join();
   }
+  // ---- vertical maps: each reduced node of order k >= 2 at level a maps, on the closed
+  // cut at a, to the root of order k - 1 whose component contains it.  A carrier birth of
+  // the node's group is an event of rank k; that event is a saddle of order k - 1, whose
+  // group's resulting root (level <= a) is climbed through multifusion parents of level <= a
+  // (the contract serializer's assignment, reference/morsehgp3d_oracle/serialization.py:1040-1099).
+  {
+    h.h_class.resize(m);
+    if (m && (e = cudaMemcpy(h.h_class.data(), h.lclass, (uint64_t)m * 4, cudaMemcpyDeviceToHost)) != cudaSuccess)
+      return abi_cuda_fail(&ctx, e, "level classes");
+    const uint64_t nn = h.nodes.size();
+    std::vector<uint32_t> evfam(m, kInvalid32), sad_of_fam(h.families.size(), kInvalid32);
+    for (uint64_t f = 0; f < h.families.size(); ++f) evfam[h.families[f].event] = (uint32_t)f;
+    for (uint64_t sd = 0; sd < h.saddles.size(); ++sd) sad_of_fam[h.saddles[sd].family] = (uint32_t)sd;
+    auto cls = [&](uint32_t node) -> int64_t {
+      const uint32_t le = h.nodes[node].level_event;
+      return le == kInvalid32 ? -1 : (int64_t)h.h_class[le];
+    };
+    std::vector<uint64_t> order_begin(keff + 2, nn);
+    for (uint64_t i = nn; i-- > 0;) order_begin[h.nodes[i].order] = i;
+    for (uint32_t k = keff + 1; k-- > 1;)
+      if (order_begin[k] == nn) order_begin[k] = order_begin[k + 1];
+    std::vector<std::vector<ehgp_vertical_assignment>> vo(keff + 1);
+    std::vector<int> vstat(keff + 1, EHGP_OK);
+    // Offline sweep per source order: node ids grow with level in both forests, so the
+    // target forest's parent links are united in id (= level) order as the source levels
+    // rise; the image is then one find with path compression.
+    auto run_v = [&](uint32_t k) {
+      const uint64_t t_lo = order_begin[k - 1], t_hi = order_begin[k];
+      std::vector<uint32_t> up(t_hi - t_lo);
+      for (uint64_t x = 0; x < up.size(); ++x) up[x] = (uint32_t)x;
+      auto find_up = [&](uint32_t x) {  // local target index
+        while (up[x] != x) {
+          up[x] = up[up[x]];
+          x = up[x];
+        }
+        return x;
+      };
+      uint64_t sweep = t_lo;  // next target node whose child links are not yet united
+      for (uint64_t i = order_begin[k]; i < order_begin[k + 1]; ++i) {
+        const ehgp_forest_node& nd = h.nodes[i];
+        const ehgp_forest_group& g = h.groups[nd.atomic_group];
+        const uint32_t carrier = h.bindings[h.saddles[g.saddle_offset].arm_offset].carrier;
+        const uint32_t proj = h.births[carrier].projection;
+        const uint32_t f = proj >= n ? evfam[proj - n] : kInvalid32;
+        if (f == kInvalid32 || h.families[f].order != k - 1 || sad_of_fam[f] == kInvalid32) {
+          vstat[k] = EHGP_ERR_DEGENERATE;
+          return;
+        }
+        const uint32_t R = h.groups[h.saddles[sad_of_fam[f]].group].result_node;
+        const int64_t lev = cls((uint32_t)i);
+        if (R < t_lo || R >= t_hi || cls(R) > lev) {
+          vstat[k] = EHGP_ERR_DEGENERATE;
+          return;
+        }
+        while (sweep < t_hi && cls((uint32_t)sweep) <= lev) {
+          const ehgp_forest_node& p = h.nodes[sweep];
+          if (p.kind == 2)
+            for (uint32_t c = 0; c < p.child_count; ++c) {
+              const uint32_t ch = h.children[p.child_offset + c];
+              up[find_up(ch - (uint32_t)t_lo)] = (uint32_t)(sweep - t_lo);
+            }
+          ++sweep;
+        }
+        vo[k].push_back({(uint32_t)i, (uint32_t)t_lo + find_up(R - (uint32_t)t_lo), k, nd.level_event});
+      }
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t k = 2; k <= keff; ++k) pool.emplace_back(run_v, k);
+    for (auto& t : pool) t.join();
+    h.vertical.clear();
+    for (uint32_t k = 2; k <= keff; ++k) {
+      if (vstat[k] != EHGP_OK)
+        return abi_fail(&ctx, vstat[k], "a reduced node has no lower-order image through its carrier saddle");
+      h.vertical.insert(h.vertical.end(), vo[k].begin(), vo[k].end());
+    }
+  }
   const auto t2 = std::chrono::steady_clock::now();
   h.ms_forest = std::chrono::duration<double, std::milli>(t2 - t1).count();
   (void)t0;
@@ -2000,6 +2078,7 @@ int ehgp_hierarchy(ehgp_ctx* ctx, uint32_t K, ehgp_hier_counts* counts) {
       counts->saddle_records = h.saddles.size();
       counts->atomic_groups = h.groups.size();
       counts->final_roots = h.roots.size();
+      counts->vertical_assignments = h.vertical.size();
       counts->k_eff = h.keff;
     }
     counts->decision = (uint32_t)s;
@@ -2031,6 +2110,7 @@ int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out) {
   cp(out->groups, h.groups.data(), h.groups.size() * sizeof(ehgp_forest_group));
   cp(out->batches, h.fbatches.data(), h.fbatches.size() * sizeof(ehgp_forest_batch));
   cp(out->roots, h.roots.data(), h.roots.size() * sizeof(ehgp_forest_root));
+  cp(out->vertical, h.vertical.data(), h.vertical.size() * sizeof(ehgp_vertical_assignment));
   return EHGP_OK;
 }
 

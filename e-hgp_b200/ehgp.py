@@ -114,7 +114,7 @@ class HierCounts(C.Structure):
     _fields_ = [(f, C.c_uint64) for f in ("events", "diagnostics", "journal_batches", "role_records", "families",
                                           "arm_seeds", "birth_records", "nodes", "children", "arm_bindings",
                                           "saddle_records", "atomic_groups", "final_roots")] + \
-               [("decision", C.c_uint32), ("k_eff", C.c_uint32)]
+               [("decision", C.c_uint32), ("k_eff", C.c_uint32), ("vertical_assignments", C.c_uint64)]
 
 
 def _u4(*names):
@@ -137,6 +137,7 @@ FOREST_GROUP = _u4("batch", "saddle_offset", "saddle_count", "frozen", "latent",
 FOREST_BATCH = _u4("order", "level_event", "birth_offset", "birth_count", "saddle_offset", "saddle_count",
                    "group_offset", "group_count", "pre_carriers", "pre_roots", "post_carriers", "post_roots")
 FOREST_ROOT = _u4("order", "handle", "node")
+VERTICAL_ASSIGNMENT = _u4("source_node", "target_node", "source_order", "level_event")
 ABSENT = 0xFFFFFFFF
 
 _HIER_FIELDS = [("events", EVENT_RECORD, "events"), ("journal_batches", JOURNAL_BATCH, "journal_batches"),
@@ -145,7 +146,8 @@ _HIER_FIELDS = [("events", EVENT_RECORD, "events"), ("journal_batches", JOURNAL_
                 ("children", np.dtype("<u4"), "children"), ("births", FOREST_BIRTH, "birth_records"),
                 ("bindings", FOREST_BINDING, "arm_bindings"), ("saddles", FOREST_SADDLE, "saddle_records"),
                 ("groups", FOREST_GROUP, "atomic_groups"), ("batches", FOREST_BATCH, "journal_batches"),
-                ("roots", FOREST_ROOT, "final_roots")]
+                ("roots", FOREST_ROOT, "final_roots"),
+                ("vertical", VERTICAL_ASSIGNMENT, "vertical_assignments")]
 
 
 class HierOut(C.Structure):

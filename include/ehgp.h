@@ -303,6 +303,7 @@ typedef struct ehgp_hier_counts {
   uint64_t birth_records, nodes, children, arm_bindings, saddle_records, atomic_groups, final_roots;
   uint32_t decision;                            /* EHGP_OK when the forest journal is complete */
   uint32_t k_eff;
+  uint64_t vertical_assignments;                /* vertical maps, orders 2..k_eff */
 } ehgp_hier_counts;
 
 int ehgp_hierarchy(ehgp_ctx* ctx, uint32_t K, ehgp_hier_counts* counts);
@@ -361,6 +362,16 @@ typedef struct ehgp_forest_root {    /* ExactDirectMorseForestFinalRoot */
   uint32_t order, handle, node;
 } ehgp_forest_root;
 
+/* Vertical map v_{k-1,a} of the tower (contract-v2 VerticalAssignment,
+ * morsehgp3d/schemas/morsehgp3d-contract-v2.schema.json $defs.VerticalAssignment; the
+ * reference's direct vertical journal, direct_morse_vertical_journal.hpp:287, takes these
+ * images as external proposals): every reduced node of order k >= 2 maps, at its own level
+ * on the closed cut, to the root of order k - 1 whose component contains it.  Ordered by
+ * source node; source_order = k, target order k - 1. */
+typedef struct ehgp_vertical_assignment {
+  uint32_t source_node, target_node, source_order, level_event;
+} ehgp_vertical_assignment;
+
 /* Host copies of the last ehgp_hierarchy result; every pointer may be NULL
  * and must otherwise hold the count reported in ehgp_hier_counts. */
 typedef struct ehgp_hier_out {
@@ -377,6 +388,7 @@ typedef struct ehgp_hier_out {
   ehgp_forest_group* groups;
   ehgp_forest_batch* batches;
   ehgp_forest_root* roots;
+  ehgp_vertical_assignment* vertical;
 } ehgp_hier_out;
 
 int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out);

@@ -320,3 +320,60 @@ def definition_match(ours: list[dict], golden: list[dict]) -> str:
         if o["roots"] != g["roots"]:
             return f"order {g['order']}: roots {o['roots']} vs {g['roots']}"
     return ""
+
+
+def vertical_from_hier_text(text: str) -> list[list[int]]:
+    """Vertical assignments [source order, source index, target index] (indices within
+    their orders) derived from a direct-hierarchy text: a reduced node N of order k at
+    level a takes a carrier birth of its group; that birth's event is also a saddle of
+    order k - 1, whose group's resulting root, climbed through multifusion parents whose
+    level is <= a (closed cut), is the image of N."""
+    from fractions import Fraction
+    N, C, B, A, S, G, Y = [], [], [], [], [], [], []
+    for line in text.splitlines():
+        f = line.split()
+        if not f:
+            continue
+        t = f[0]
+        if t == "N":
+            N.append((int(f[2]), Fraction(int(f[3]), int(f[4])), int(f[5]), int(f[6]), int(f[7]), f[9]))
+        elif t == "C":
+            C = [int(x) for x in f[1:]]
+        elif t == "B":
+            B.append(int(f[2]))  # projection, indexed by handle
+        elif t == "A":
+            A.append(int(f[4]))  # carrier
+        elif t == "S":
+            S.append((int(f[2]), int(f[5]), int(f[10])))  # family, arm offset, group
+        elif t == "G":
+            G.append(int(f[11]))  # resulting root node
+        elif t == "Y":
+            Y.append((int(f[2]), int(f[6])))  # event, order
+    n = sum(1 for nd in N if nd[0] == 1 and nd[2] == 0)
+    parent = {}
+    for i, nd in enumerate(N):
+        if nd[2] == 2:
+            for c in C[nd[3]:nd[3] + nd[4]]:
+                parent[c] = i
+    fam_of = {(ev, order): fi for fi, (ev, order) in enumerate(Y)}
+    sad_of_fam = {s[0]: si for si, s in enumerate(S)}
+    first_sad_of_group = {}
+    for si, s in enumerate(S):
+        first_sad_of_group.setdefault(s[2], si)
+    local, counter = {}, {}
+    for i, nd in enumerate(N):
+        local[i] = counter.get(nd[0], 0)
+        counter[nd[0]] = local[i] + 1
+    out = []
+    for i, nd in enumerate(N):
+        k, lev, kind = nd[0], nd[1], nd[2]
+        if k < 2:
+            continue
+        g = int(nd[5])
+        carrier = A[S[first_sad_of_group[g]][1]]
+        ev = B[carrier] - n
+        R = G[S[sad_of_fam[fam_of[(ev, k - 1)]]][2]]
+        while R in parent and N[parent[R]][1] <= lev:
+            R = parent[R]
+        out.append([k, local[i], local[R]])
+    return out

@@ -221,7 +221,22 @@ def main_definition():
             nodes = [[nd.kind, str(nd.squared_level.numerator), str(nd.squared_level.denominator),
                       [index[c] for c in nd.child_ids]] for nd in f.nodes]
             forests.append({"order": o.order, "nodes": nodes, "roots": sorted(index[r] for r in f.root_ids)})
-        doc = {"points": pts.tolist(), "K": K, "k_eff": res.k_eff, "forests": forests}
+        # vertical assignments as the contract serializer forms them
+        # (reference/morsehgp3d_oracle/serialization.py:1040-1099): every source node maps, at
+        # its own level on the closed cut, to the lower-order root whose component contains it
+        vertical = []
+        for fam in res.vertical_maps:
+            src = res.for_order(fam.source_order).forest
+            tgt = res.for_order(fam.target_order).forest
+            sidx = {nd.node_id: i for i, nd in enumerate(src.nodes)}
+            tidx = {nd.node_id: i for i, nd in enumerate(tgt.nodes)}
+            closed = {mp.squared_level: mp for mp in fam.maps if mp.closed}
+            for nd in src.nodes:
+                comp = [c for c in src.cut(nd.squared_level, closed=True).components if c.root_id == nd.node_id]
+                tf = closed[nd.squared_level].assignment_by_source[comp[0].facet_point_ids]
+                cand = [c for c in tgt.cut(nd.squared_level, closed=True).components if c.facet_point_ids == tf]
+                vertical.append([fam.source_order, sidx[nd.node_id], tidx[cand[0].root_id]])
+        doc = {"points": pts.tolist(), "K": K, "k_eff": res.k_eff, "forests": forests, "vertical": vertical}
         with open(os.path.join(HERE, f"definition_{name}.json"), "w") as fh:
             json.dump(doc, fh, separators=(",", ":"))
         print(name, len(pts), [len(f["nodes"]) for f in forests], flush=True)

@@ -98,6 +98,56 @@ def test_gpu_forest_matches_hgp_reduced_definition(ctx, path):
     from geomcheck import definition_match, forests_from_hier_text
     d = json.load(open(path))
     ctx.lbvh_build(np.array(d["points"]), outputs=False)
-    got = forests_from_hier_text(gpu_hierarchy_text(ctx, d["K"]))
+    res = ctx.hierarchy(d["K"])
+    got = forests_from_hier_text(gpu_hierarchy_text(ctx, d["K"], res))
     msg = definition_match(got, d["forests"])
     assert msg == "", msg
+    # vertical maps: (source order, source index, target index) within their orders
+    orders = res["nodes"]["order"]
+    local = np.zeros(len(orders), np.int64)
+    seen = {}
+    for i, o in enumerate(orders):
+        local[i] = seen.get(int(o), 0)
+        seen[int(o)] = local[i] + 1
+    vert = sorted([int(v["source_order"]), int(local[v["source_node"]]), int(local[v["target_node"]])]
+                  for v in res["vertical"])
+    assert vert == sorted(d["vertical"])
+
+
+def test_gpu_vertical_maps_natural_at_scale(ctx):
+    """n = 4096: every reduced node of order k >= 2 has an image of order k - 1 at a level
+    no higher than its own, and the images commute with the horizontal maps: a node's
+    parent maps to the root, at the parent's level, of the node's image (naturality)."""
+    pts = workloads.jittered_lattice(16, 3).astype(np.float64)
+    ctx.lbvh_build(pts, outputs=False)
+    r = ctx.hierarchy(10)
+    nodes, ch, vert = r["nodes"], r["children"], r["vertical"]
+    expect = int(((nodes["order"] >= 2)).sum())
+    assert len(vert) == expect
+    parent = np.full(len(nodes), -1, np.int64)
+    for i in np.nonzero(nodes["kind"] == 2)[0]:
+        parent[ch[nodes["child_offset"][i]:nodes["child_offset"][i] + nodes["child_count"][i]]] = i
+    lev = {}
+
+    def level(i):
+        e = int(nodes["level_event"][i])
+        if e == ehgp.ABSENT:
+            return 0
+        if e not in lev:
+            lev[e] = ctx.event_level(e)
+        return lev[e]
+
+    img = {int(v["source_node"]): int(v["target_node"]) for v in vert}
+    checked = 0
+    for s, t in list(img.items())[:400]:
+        assert nodes["order"][t] == nodes["order"][s] - 1
+        assert level(t) <= level(s)
+        p = parent[s]
+        if p < 0:
+            continue
+        x = t
+        while parent[x] >= 0 and level(parent[x]) <= level(p):
+            x = parent[x]
+        assert img[int(p)] == x
+        checked += 1
+    assert checked > 50

@@ -61,6 +61,18 @@ def test_restatement_forest_matches_hgp_reduced_definition(path):
     levels, children and final roots, order by order."""
     from geomcheck import definition_match, forests_from_hier_text
     d = json.load(open(path))
-    got = forests_from_hier_text(pyoracle.hierarchy(np.array(d["points"]), d["K"]))
+    text = pyoracle.hierarchy(np.array(d["points"]), d["K"])
+    got = forests_from_hier_text(text)
     msg = definition_match(got, d["forests"])
     assert msg == "", msg
+
+
+@pytest.mark.parametrize("path", DEFINITION, ids=[os.path.basename(p)[11:-5] for p in DEFINITION])
+def test_vertical_maps_from_journal_match_definition(path):
+    """Vertical maps derived from the direct journal (a group's carrier birth is a saddle
+    one order down; its group's root, climbed on the closed cut) equal the contract
+    serializer's assignments of the exhaustive-Gamma oracle."""
+    from geomcheck import vertical_from_hier_text
+    d = json.load(open(path))
+    got = vertical_from_hier_text(pyoracle.hierarchy(np.array(d["points"]), d["K"]))
+    assert sorted(got) == sorted(d["vertical"])
