@@ -377,3 +377,70 @@ def vertical_from_hier_text(text: str) -> list[list[int]]:
             R = parent[R]
         out.append([k, local[i], local[R]])
     return out
+
+
+def hier_dict_from_text(text: str, n: int, keff: int) -> dict:
+    """The arrays of ehgp.Context.hierarchy rebuilt from a direct-hierarchy text
+    (restatement or reference), vertical maps included (global node ids)."""
+    from fractions import Fraction
+    L = {t: [] for t in "FJQYZNBASGTR"}
+    C = []
+    for line in text.splitlines():
+        f = line.split()
+        if not f:
+            continue
+        if f[0] == "C":
+            C = [int(x) for x in f[1:]]
+        elif f[0] in L:
+            L[f[0]].append(f)
+    first_at = {}
+    events = np.zeros(len(L["F"]), ehgp.EVENT_RECORD)
+    for i, f in enumerate(L["F"]):
+        size = int(f[2])
+        sup = [int(x) for x in f[3:3 + size]]
+        bar = f.index("|", 3 + size)
+        bar2 = f.index("|", bar + 1)
+        inter = [int(x) for x in f[bar + 1:bar2]]
+        rank, num, den = int(f[bar2 + 1]), int(f[bar2 + 3]), int(f[bar2 + 4])
+        events[i]["support_size"] = size
+        events[i]["support_ids"][:size] = sup
+        events[i]["interior_count"] = len(inter)
+        events[i]["interior_ids"][:len(inter)] = inter
+        events[i]["closed_rank"] = rank
+        first_at.setdefault(Fraction(num, den), i)
+
+    def lev(num, den):
+        v = Fraction(int(num), int(den))
+        return ehgp.ABSENT if v == 0 else first_at[v]
+
+    def arr(rows, dtype):
+        a = np.zeros(len(rows), dtype)
+        for i, r in enumerate(rows):
+            for name, v in zip(dtype.names, r):
+                a[i][name] = ehgp.ABSENT if v == "-" else int(v)
+        return a
+
+    opt = lambda x: ehgp.ABSENT if x == "-" else int(x)
+    jb = arr([(f[2], lev(f[3], f[4]), f[5], f[6], f[7], f[8]) for f in L["J"]], ehgp.JOURNAL_BATCH)
+    roles = arr([(f[2], f[3], f[4]) for f in L["Q"]], ehgp.ROLE_RECORD)
+    fams = arr([(f[2], f[3], f[4], f[5], f[6], f[9], f[10]) for f in L["Y"]], ehgp.FAMILY_RECORD)
+    removed = np.array([int(f[3]) for f in L["Z"]], np.uint32)
+    nodes = arr([(f[2], lev(f[3], f[4]), f[5], f[6], f[7], opt(f[8]), opt(f[9])) for f in L["N"]], ehgp.FOREST_NODE)
+    births = arr([(f[2], f[3], f[4], f[5], opt(f[6])) for f in L["B"]], ehgp.FOREST_BIRTH)
+    binds = arr([(f[2], f[3], f[4], opt(f[5])) for f in L["A"]], ehgp.FOREST_BINDING)
+    sads = arr([f[2:11] for f in L["S"]], ehgp.FOREST_SADDLE)
+    grps = arr([f[2:10] + [opt(f[10]), f[11], f[12]] for f in L["G"]], ehgp.FOREST_GROUP)
+    fb = arr([(f[3], lev(f[4], f[5])) + tuple(f[6:16]) for f in L["T"]], ehgp.FOREST_BATCH)
+    roots = arr([(f[2], f[3], f[4]) for f in L["R"]], ehgp.FOREST_ROOT)
+    # vertical maps in global node ids
+    order_start = {}
+    for i, nd in enumerate(nodes):
+        order_start.setdefault(int(nd["order"]), i)
+    vert = []
+    for k, si, ti in vertical_from_hier_text(text):
+        s = order_start[k] + si
+        vert.append((s, order_start[k - 1] + ti, k, int(nodes[s]["level_event"])))
+    vertical = arr(sorted(vert), ehgp.VERTICAL_ASSIGNMENT)
+    return {"k_eff": keff, "events": events, "journal_batches": jb, "roles": roles, "families": fams,
+            "arm_removed": removed, "nodes": nodes, "children": np.array(C, np.uint32), "births": births,
+            "bindings": binds, "saddles": sads, "groups": grps, "batches": fb, "roots": roots, "vertical": vertical}

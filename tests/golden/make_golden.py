@@ -236,7 +236,11 @@ def main_definition():
                 tf = closed[nd.squared_level].assignment_by_source[comp[0].facet_point_ids]
                 cand = [c for c in tgt.cut(nd.squared_level, closed=True).components if c.facet_point_ids == tf]
                 vertical.append([fam.source_order, sidx[nd.node_id], tidx[cand[0].root_id]])
-        doc = {"points": pts.tolist(), "K": K, "k_eff": res.k_eff, "forests": forests, "vertical": vertical}
+        # the contract serializer's critical catalogue (serialization.py:723-793)
+        from morsehgp3d_oracle.serialization import serialize_oracle_result
+        catalog = serialize_oracle_result(res, run_id="0" * 64)["critical_catalog"]
+        doc = {"points": pts.tolist(), "K": K, "k_eff": res.k_eff, "forests": forests, "vertical": vertical,
+               "catalog": catalog}
         with open(os.path.join(HERE, f"definition_{name}.json"), "w") as fh:
             json.dump(doc, fh, separators=(",", ":"))
         print(name, len(pts), [len(f["nodes"]) for f in forests], flush=True)
