@@ -361,6 +361,13 @@ k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uin
       __syncwarp();
     }
   }
+  // the sorted list keeps 1 / |p - a| in .w from here on (binary32)
+  for (uint32_t i = lane; i < P; i += 32) {
+    float4 r = rel[warp][i];
+    r.w = i < m ? 1.0f / r.w : 0.0f;
+    rel[warp][i] = r;
+  }
+  __syncwarp();
   // distances are binary32: thresholds carry a relative margin of 1e-5 in the safe direction
   const double L2 = sqrt(gather_r2[a]) * (1.0 - 1e-9);  // list covers |p - a| <= L
   const double half_L = 0.5 * L2;
@@ -389,49 +396,54 @@ k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uin
       const double g = t1 > 0.0 ? (cp.hi[k] - A[k]) / t1 : (A[k] - cp.lo[k]) / (-t2);
       ext = fmin(ext, g * (1.0 + 1e-12));
     }
-    // the `need` smallest shrunk thresholds (early exit: rho_shr >= |p - a| / 2)
-    double best[16];
+    // The `need` smallest shrunk thresholds, kept as the `need` largest lower bounds of
+    // 1 / rho_shr (binary32, no divides):  1/rho_p(u) >= 2 cos(angle + delta) / |p - a|.  Every
+    // binary32 rounding (about 1e-7 relative) is covered by the 1e-5 margins and the 1e-6
+    // absolute slack on the cosines, always in the safe direction.
+    const float cdf = (float)cd, sdlf = (float)sdl;
+    const float s0f = (float)s0, s1f = (float)s1, s2f = (float)s2;
+    const float ext_f = __double2float_ru(ext);
+    float best[16];
     uint32_t cnt = 0;
     for (uint32_t i = 0; i < m; ++i) {
-      const float4 r = rel[warp][i];
-      const double dist = (double)r.w;
-      const double kth = cnt >= cp.need ? best[cp.need - 1] : INFINITY;
-      if (0.5 * dist * (1.0 - 1e-5) > fmin(kth, ext)) break;
-      const double c = s0 * r.x + s1 * r.y + s2 * r.z;
-      // upper bound of the angle (cosine lowered by the binary32 margin) -> cos(angle + delta) lowered
-      const double cs = fmax(-1.0, c - 1e-5), sn = sqrt(fmax(0.0, 1.0 - cs * cs));
-      const double cshr = cs * cd - sn * sdl;
-      if (cshr <= 1e-9) continue;
-      const double rho = dist / (2.0 * cshr) * (1.0 + 1e-5);
+      const float4 r = rel[warp][i];  // r.w = 1 / |p - a|
+      const float kth_inv = cnt >= cp.need ? best[cp.need - 1] : 0.0f;
+      // early exit: every later point has rho >= |p - a| / 2 > min(kth, ext)
+      if (0.5f * (1.0f - 1e-5f) * fmaxf(kth_inv, 1.0f / ext_f) > r.w) break;
+      const float c = s0f * r.x + s1f * r.y + s2f * r.z;
+      const float cs = fmaxf(-1.0f, c - 1e-5f);  // cosine of an upper bound of the angle
+      const float sn = sqrtf(fmaxf(0.0f, (1.0f - cs) * (1.0f + cs)));
+      const float cshr = cs * cdf - sn * sdlf - 1e-6f;  // lower bound of cos(angle + delta)
+      if (cshr <= 1e-6f) continue;
+      const float inv = 2.0f * cshr * r.w * (1.0f - 1e-5f);  // lower bound of 1 / rho_p(u)
       if (cnt < cp.need) {
         uint32_t j = cnt++;
-        while (j > 0 && best[j - 1] > rho) { best[j] = best[j - 1]; --j; }
-        best[j] = rho;
-      } else if (rho < best[cp.need - 1]) {
+        while (j > 0 && best[j - 1] < inv) { best[j] = best[j - 1]; --j; }
+        best[j] = inv;
+      } else if (inv > best[cp.need - 1]) {
         uint32_t j = cp.need - 1;
-        while (j > 0 && best[j - 1] > rho) { best[j] = best[j - 1]; --j; }
-        best[j] = rho;
+        while (j > 0 && best[j - 1] < inv) { best[j] = best[j - 1]; --j; }
+        best[j] = inv;
       }
     }
-    const double kth = cnt >= cp.need ? best[cp.need - 1] : INFINITY;
+    const double kth = cnt >= cp.need && best[cp.need - 1] > 0.0f ? (1.0 / (double)best[cp.need - 1]) * (1.0 + 1e-12)
+                                                                 : INFINITY;
     const double rho_s = fmin(kth, ext);
     rho_tab[(uint64_t)a * kDirs + d] = __double2float_ru(rho_s);  // per-cone bound, rounded up
     // certified when every unlisted point (rho >= L/2) cannot lower it
     if (!(rho_s <= half_L)) ok = false;
     worst_needed = fmax(worst_needed, rho_s);
-    // mark the candidates of this cone: rho_lo_p(s) <= rho_s (rho_lo >= |p - a| / 2)
+    // mark the candidates of this cone: rho_lo_p(s) <= rho_s, i.e. 2 cos(max(angle - delta, 0)) rho_s >= |p - a|
+    const float rho_sf = __double2float_ru(rho_s);
     for (uint32_t i = 0; i < m; ++i) {
       const float4 r = rel[warp][i];
-      const double dist = (double)r.w;
-      if (0.5 * dist * (1.0 - 1e-5) > rho_s) break;
-      const double c = s0 * r.x + s1 * r.y + s2 * r.z;
-      // lower bound of the angle (cosine raised by the margin) -> cos(max(angle - delta, 0)) raised
-      const double cs = fmin(1.0, c + 1e-5);
-      const double sn = sqrt(fmax(0.0, 1.0 - cs * cs));
-      const double clo = (cs >= cd) ? 1.0 : cs * cd + sn * sdl;
-      if (clo <= 0.0) continue;
-      const double rho_lo = dist / (2.0 * clo) * (1.0 - 1e-5);
-      if (rho_lo <= rho_s * (1.0 + 1e-9)) atomicOr(&mark[warp][i >> 5], 1u << (i & 31));
+      if (0.5f * (1.0f - 1e-5f) > rho_sf * r.w) break;  // rho_lo >= |p - a| / 2 > rho_s
+      const float c = s0f * r.x + s1f * r.y + s2f * r.z;
+      const float cs = fminf(1.0f, c + 1e-5f);  // cosine of a lower bound of the angle
+      const float sn = sqrtf(fmaxf(0.0f, (1.0f - cs) * (1.0f + cs)));
+      const float clo = (cs >= cdf) ? 1.0f : cs * cdf + sn * sdlf + 1e-6f;  // upper bound of cos(max(angle - delta, 0))
+      if (clo <= 0.0f) continue;
+      if (2.0f * clo * rho_sf * r.w * (1.0f + 2e-5f) >= 1.0f) atomicOr(&mark[warp][i >> 5], 1u << (i & 31));
     }
   }
   ok = __all_sync(0xffffffffu, ok);
