@@ -294,8 +294,9 @@ k_gather(uint32_t n, uint32_t root, const TNode* __restrict__ tn, const uint32_t
 // u; those lie in C(a) too, so classifying against C(a) rejects it.
 // The neighbour list (points within the gather radius L, sorted by distance)
 // certifies rho_s when rho_s <= L / 2: every unlisted point has rho >= L / 2.
-constexpr int kDirWarps = 2;
-constexpr int kMaxCand = 256;  // candidate-set capacity per point
+constexpr int kDirThreads = 128;  // one block per point: four warps share its sorted list
+constexpr int kMaxCand = 256;     // candidate-set capacity per point
+constexpr int kMaxNeed = kMaxInteriorH + 1;  // s_max - 2 for K = 10
 
 struct CertParams {
   const float* dirs;  // [kDirs * 3] unit vectors
@@ -304,131 +305,139 @@ struct CertParams {
   uint32_t need;        // s_max - 2
 };
 
-__global__ void __launch_bounds__(32 * kDirWarps)
+// Largest (s_k +- delta)-weighted excursion from a along axis k inside the cloud AABB:
+// sum over k bounds the support of the AABB over a cone of directions around s.
+__device__ __forceinline__ double cone_ext(const CertParams& cp, double sk, double ak, int k) {
+  const double up = cp.hi[k] - ak, dn = cp.lo[k] - ak;
+  const double t1 = sk - cp.delta, t2 = sk + cp.delta;
+  const double f1 = t1 >= 0 ? up * t1 : dn * t1, f2 = t2 >= 0 ? up * t2 : dn * t2;
+  return fmax(f1, f2);
+}
+
+// Distance along the cone (direction s, half-angle delta) at which a ray from a leaves the
+// AABB across axis k; infinite when the cone crosses that axis' zero.
+__device__ __forceinline__ double cone_exit(const CertParams& cp, double sk, double ak, int k) {
+  const double t1 = sk - cp.delta, t2 = sk + cp.delta;
+  if (t1 <= 0.0 && t2 >= 0.0) return INFINITY;
+  const double g = t1 > 0.0 ? (cp.hi[k] - ak) / t1 : (ak - cp.lo[k]) / (-t2);
+  return g * (1.0 + 1e-12);
+}
+
+// best[] holds the NEED largest values seen so far in descending order (zeros while
+// fewer were seen); inserting v keeps the NEED largest of best[] and v.  Unrolled over a
+// compile-time NEED so that best[] stays in registers.
+template <int NEED>
+__device__ __forceinline__ void keep_largest(float (&best)[NEED], float v) {
+#pragma unroll
+  for (int j = NEED - 1; j > 0; --j) best[j] = fmaxf(fminf(best[j - 1], v), best[j]);
+  best[0] = fmaxf(best[0], v);
+}
+
+template <int NEED>
+__global__ void __launch_bounds__(kDirThreads)
 k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uint32_t* __restrict__ nb,
            const uint32_t* __restrict__ nbc, const double* __restrict__ px, const double* __restrict__ py,
            const double* __restrict__ pz, const double* __restrict__ gather_r2, uint8_t* __restrict__ todo,
            uint32_t* __restrict__ cand, uint32_t* __restrict__ candc, double* __restrict__ need_r,
            float* __restrict__ rho_tab) {
-  __shared__ float4 rel[kDirWarps][kMaxNb];  // unit direction of p - a and |p - a| (binary32; margins below)
-  __shared__ uint32_t ids[kDirWarps][kMaxNb];
-  __shared__ uint32_t mark[kDirWarps][kMaxNb / 32];
-  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t pos = blockIdx.x * kDirWarps + warp;
+  __shared__ float4 rel[kMaxNb];  // unit direction of p - a and |p - a| (binary32; margins below)
+  __shared__ uint32_t ids[kMaxNb];
+  __shared__ uint32_t mark[kMaxNb / 32];
+  __shared__ double worst_w[kDirThreads / 32];
+  const uint32_t t = threadIdx.x, warp = t >> 5, lane = t & 31u;
+  const uint32_t pos = blockIdx.x;
   if (pos >= n) return;
   const uint32_t a = leaf_pid[pos];
   if (!todo[a]) return;
   const uint32_t m = nbc[a];
   if (m > (uint32_t)kMaxNb) {
-    if (lane == 0) need_r[a] = INFINITY;
+    if (t == 0) need_r[a] = INFINITY;
     return;
   }
   const double ax = px[a], ay = py[a], az = pz[a];
-  for (uint32_t i = lane; i < m; i += 32) {
+  for (uint32_t i = t; i < m; i += kDirThreads) {
     const uint32_t p = nb[(uint64_t)a * kMaxNb + i];
     const double x = px[p] - ax, y = py[p] - ay, z = pz[p] - az;
     const double dd = sqrt(x * x + y * y + z * z);
     const double inv = dd > 0.0 ? 1.0 / dd : 0.0;
-    rel[warp][i] = make_float4((float)(x * inv), (float)(y * inv), (float)(z * inv), (float)dd);  // unit direction, |p - a|
-    ids[warp][i] = p;
+    rel[i] = make_float4((float)(x * inv), (float)(y * inv), (float)(z * inv), (float)dd);  // unit direction, |p - a|
+    ids[i] = p;
   }
-  for (uint32_t i = lane; i < (uint32_t)kMaxNb / 32; i += 32) mark[warp][i] = 0;
-  __syncwarp();
-  // sort by distance (odd-even merge sort over a power-of-two padding, in shared memory)
+  if (t < (uint32_t)kMaxNb / 32) mark[t] = 0;
+  // sort by distance (bitonic network over a power-of-two padding, in shared memory)
   uint32_t P = 1;
   while (P < m) P <<= 1;
-  for (uint32_t i = m + lane; i < P; i += 32) {
-    rel[warp][i] = make_float4(0.f, 0.f, 0.f, INFINITY);
-    ids[warp][i] = kInvalid32;
+  for (uint32_t i = m + t; i < P; i += kDirThreads) {
+    rel[i] = make_float4(0.f, 0.f, 0.f, INFINITY);
+    ids[i] = kInvalid32;
   }
-  __syncwarp();
+  __syncthreads();
   for (uint32_t k = 2; k <= P; k <<= 1) {
     for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-      for (uint32_t i = lane; i < P; i += 32) {
+      for (uint32_t i = t; i < P; i += kDirThreads) {
         const uint32_t l = i ^ j;
         if (l > i) {
           const bool up = (i & k) == 0;
-          const float4 x = rel[warp][i], y = rel[warp][l];
+          const float4 x = rel[i], y = rel[l];
           if ((x.w > y.w) == up) {
-            rel[warp][i] = y;
-            rel[warp][l] = x;
-            const uint32_t t = ids[warp][i];
-            ids[warp][i] = ids[warp][l];
-            ids[warp][l] = t;
+            rel[i] = y;
+            rel[l] = x;
+            const uint32_t tmp = ids[i];
+            ids[i] = ids[l];
+            ids[l] = tmp;
           }
         }
       }
-      __syncwarp();
+      __syncthreads();
     }
   }
   // the sorted list keeps 1 / |p - a| in .w from here on (binary32)
-  for (uint32_t i = lane; i < P; i += 32) {
-    float4 r = rel[warp][i];
+  for (uint32_t i = t; i < P; i += kDirThreads) {
+    float4 r = rel[i];
     r.w = i < m ? 1.0f / r.w : 0.0f;
-    rel[warp][i] = r;
+    rel[i] = r;
   }
-  __syncwarp();
+  __syncthreads();
   // distances are binary32: thresholds carry a relative margin of 1e-5 in the safe direction
   const double L2 = sqrt(gather_r2[a]) * (1.0 - 1e-9);  // list covers |p - a| <= L
   const double half_L = 0.5 * L2;
   const double cd = cos(cp.delta), sdl = sin(cp.delta);
-  const double A[3] = {ax, ay, az};
+  const float cdf = (float)cd, sdlf = (float)sdl;
   double worst_needed = 0.0;  // largest certified rho_s (the list must cover 2 rho_s)
   bool ok = true;
-  for (int d = lane; d < kDirs; d += 32) {
+  for (int d = t; d < kDirs; d += kDirThreads) {
     const double s0 = cp.dirs[3 * d], s1 = cp.dirs[3 * d + 1], s2 = cp.dirs[3 * d + 2];
     // AABB support bound over the cone
-    double ext = 0.0;
-    const double sv[3] = {s0, s1, s2};
-    for (int k = 0; k < 3; ++k) {
-      const double up = cp.hi[k] - A[k], dn = cp.lo[k] - A[k];
-      const double t1 = sv[k] - cp.delta, t2 = sv[k] + cp.delta;
-      const double f1 = t1 >= 0 ? up * t1 : dn * t1, f2 = t2 >= 0 ? up * t2 : dn * t2;
-      ext += fmax(f1, f2);
-    }
-    ext *= (1.0 + 1e-12);
+    const double ext = cone_ext(cp, s0, ax, 0) + cone_ext(cp, s1, ay, 1) + cone_ext(cp, s2, az, 2);
     // the centre of a well-centred sphere lies in conv(S), inside the AABB: r is at most
     // the distance at which the ray a + r u leaves the AABB, maximised over the cone
     // axis by axis (min over axes of the per-axis maxima bounds the max of the min)
-    for (int k = 0; k < 3; ++k) {
-      const double t1 = sv[k] - cp.delta, t2 = sv[k] + cp.delta;
-      if (t1 <= 0.0 && t2 >= 0.0) continue;  // the cone crosses this axis' zero: no bound
-      const double g = t1 > 0.0 ? (cp.hi[k] - A[k]) / t1 : (A[k] - cp.lo[k]) / (-t2);
-      ext = fmin(ext, g * (1.0 + 1e-12));
-    }
+    const double exit_r = fmin(fmin(cone_exit(cp, s0, ax, 0), cone_exit(cp, s1, ay, 1)), cone_exit(cp, s2, az, 2));
+    const double ext_c = fmin(ext * (1.0 + 1e-12), exit_r);
     // The `need` smallest shrunk thresholds, kept as the `need` largest lower bounds of
     // 1 / rho_shr (binary32, no divides):  1/rho_p(u) >= 2 cos(angle + delta) / |p - a|.  Every
     // binary32 rounding (about 1e-7 relative) is covered by the 1e-5 margins and the 1e-6
     // absolute slack on the cosines, always in the safe direction.
-    const float cdf = (float)cd, sdlf = (float)sdl;
     const float s0f = (float)s0, s1f = (float)s1, s2f = (float)s2;
-    const float ext_f = __double2float_ru(ext);
-    float best[16];
-    uint32_t cnt = 0;
+    const float ext_f = __double2float_ru(ext_c);
+    const float inv_ext = 1.0f / ext_f;
+    float best[NEED];
+#pragma unroll
+    for (int j = 0; j < NEED; ++j) best[j] = 0.0f;
     for (uint32_t i = 0; i < m; ++i) {
-      const float4 r = rel[warp][i];  // r.w = 1 / |p - a|
-      const float kth_inv = cnt >= cp.need ? best[cp.need - 1] : 0.0f;
+      const float4 r = rel[i];  // r.w = 1 / |p - a|
       // early exit: every later point has rho >= |p - a| / 2 > min(kth, ext)
-      if (0.5f * (1.0f - 1e-5f) * fmaxf(kth_inv, 1.0f / ext_f) > r.w) break;
+      if (0.5f * (1.0f - 1e-5f) * fmaxf(best[NEED - 1], inv_ext) > r.w) break;
       const float c = s0f * r.x + s1f * r.y + s2f * r.z;
       const float cs = fmaxf(-1.0f, c - 1e-5f);  // cosine of an upper bound of the angle
       const float sn = sqrtf(fmaxf(0.0f, (1.0f - cs) * (1.0f + cs)));
       const float cshr = cs * cdf - sn * sdlf - 1e-6f;  // lower bound of cos(angle + delta)
       if (cshr <= 1e-6f) continue;
       const float inv = 2.0f * cshr * r.w * (1.0f - 1e-5f);  // lower bound of 1 / rho_p(u)
-      if (cnt < cp.need) {
-        uint32_t j = cnt++;
-        while (j > 0 && best[j - 1] < inv) { best[j] = best[j - 1]; --j; }
-        best[j] = inv;
-      } else if (inv > best[cp.need - 1]) {
-        uint32_t j = cp.need - 1;
-        while (j > 0 && best[j - 1] < inv) { best[j] = best[j - 1]; --j; }
-        best[j] = inv;
-      }
+      if (inv > best[NEED - 1]) keep_largest<NEED>(best, inv);
     }
-    const double kth = cnt >= cp.need && best[cp.need - 1] > 0.0f ? (1.0 / (double)best[cp.need - 1]) * (1.0 + 1e-12)
-                                                                 : INFINITY;
-    const double rho_s = fmin(kth, ext);
+    const double kth = best[NEED - 1] > 0.0f ? (1.0 / (double)best[NEED - 1]) * (1.0 + 1e-12) : INFINITY;
+    const double rho_s = fmin(kth, ext_c);
     rho_tab[(uint64_t)a * kDirs + d] = __double2float_ru(rho_s);  // per-cone bound, rounded up
     // certified when every unlisted point (rho >= L/2) cannot lower it
     if (!(rho_s <= half_L)) ok = false;
@@ -436,43 +445,72 @@ k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uin
     // mark the candidates of this cone: rho_lo_p(s) <= rho_s, i.e. 2 cos(max(angle - delta, 0)) rho_s >= |p - a|
     const float rho_sf = __double2float_ru(rho_s);
     for (uint32_t i = 0; i < m; ++i) {
-      const float4 r = rel[warp][i];
+      const float4 r = rel[i];
       if (0.5f * (1.0f - 1e-5f) > rho_sf * r.w) break;  // rho_lo >= |p - a| / 2 > rho_s
       const float c = s0f * r.x + s1f * r.y + s2f * r.z;
       const float cs = fminf(1.0f, c + 1e-5f);  // cosine of a lower bound of the angle
       const float sn = sqrtf(fmaxf(0.0f, (1.0f - cs) * (1.0f + cs)));
       const float clo = (cs >= cdf) ? 1.0f : cs * cdf + sn * sdlf + 1e-6f;  // upper bound of cos(max(angle - delta, 0))
       if (clo <= 0.0f) continue;
-      if (2.0f * clo * rho_sf * r.w * (1.0f + 2e-5f) >= 1.0f) atomicOr(&mark[warp][i >> 5], 1u << (i & 31));
+      if (2.0f * clo * rho_sf * r.w * (1.0f + 2e-5f) >= 1.0f) atomicOr(&mark[i >> 5], 1u << (i & 31));
     }
   }
-  ok = __all_sync(0xffffffffu, ok);
   for (int off = 16; off > 0; off >>= 1) worst_needed = fmax(worst_needed, __shfl_xor_sync(0xffffffffu, worst_needed, off));
-  __syncwarp();
+  if (lane == 0) worst_w[warp] = worst_needed;
+  ok = __syncthreads_and(ok);  // also publishes mark[] and worst_w[]
+#pragma unroll
+  for (int w = 0; w < kDirThreads / 32; ++w) worst_needed = fmax(worst_needed, worst_w[w]);
   if (!ok) {  // the list must grow to 2 rho_s (with room)
-    if (lane == 0) need_r[a] = worst_needed;
+    if (t == 0) need_r[a] = worst_needed;
     return;
   }
+  if (warp != 0) return;
   // compact the candidate set in distance order
   uint32_t c = 0;
   uint32_t* out = cand + (uint64_t)a * kMaxCand;
-  bool overflow = false;
   for (uint32_t base = 0; base < m; base += 32) {
     const uint32_t i = base + lane;
-    const bool f = i < m && ((mark[warp][i >> 5] >> (i & 31)) & 1u);
+    const bool f = i < m && ((mark[i >> 5] >> (i & 31)) & 1u);
     const uint32_t b = __ballot_sync(0xffffffffu, f);
     if (f) {
       const uint32_t at = c + __popc(b & lanemask_lt());
-      if (at < (uint32_t)kMaxCand) out[at] = ids[warp][i];
+      if (at < (uint32_t)kMaxCand) out[at] = ids[i];
     }
     c += __popc(b);
   }
-  overflow = c > (uint32_t)kMaxCand;
+  const bool overflow = c > (uint32_t)kMaxCand;
   if (lane == 0) {
     candc[a] = overflow ? (uint32_t)kMaxCand + 1 : c;
     need_r[a] = worst_needed;
     todo[a] = overflow ? 2 : 0;  // 2: candidate set too large (reported)
   }
+}
+
+// One launch of k_dirtable<need> (need = s_max - 2 in 1..kMaxNeed).
+void launch_dirtable(uint32_t need, uint32_t n, const CertParams& cp, const uint32_t* leaf_pid, uint32_t* nb,
+                     const uint32_t* nbc, const double* px, const double* py, const double* pz,
+                     const double* gather_r2, uint8_t* todo, uint32_t* cand, uint32_t* candc, double* need_r,
+                     float* rho_tab, cudaStream_t st) {
+  static_assert(kMaxNeed == 9, "dispatch below covers need 1..9");
+#define EHGP_DIRTABLE(N)                                                                                         \
+  case N:                                                                                                        \
+    k_dirtable<N><<<n, kDirThreads, 0, st>>>(n, cp, leaf_pid, nb, nbc, px, py, pz, gather_r2, todo, cand, candc, \
+                                             need_r, rho_tab);                                                   \
+    break;
+  switch (need) {
+    EHGP_DIRTABLE(1)
+    EHGP_DIRTABLE(2)
+    EHGP_DIRTABLE(3)
+    EHGP_DIRTABLE(4)
+    EHGP_DIRTABLE(5)
+    EHGP_DIRTABLE(6)
+    EHGP_DIRTABLE(7)
+    EHGP_DIRTABLE(8)
+    EHGP_DIRTABLE(9)
+    default:
+      break;
+  }
+#undef EHGP_DIRTABLE
 }
 
 // ---- 3. owner-local enumeration ---------------------------------------------------------
@@ -1027,15 +1065,14 @@ int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   cp.dirs = h.dirs;
   cp.delta = h.delta;
   cp.need = smax - 2;
-  if (cp.need > 16) return abi_fail(&ctx, EHGP_ERR_INVALID_ARGUMENT, "K above 10 is not supported");
+  if (cp.need < 1 || cp.need > (uint32_t)kMaxNeed) return abi_fail(&ctx, EHGP_ERR_INVALID_ARGUMENT, "K above 10 is not supported");
   uint32_t pending = n, overflowed = 0;
   std::vector<uint8_t> todo(n);
   for (int round = 0; round < 6 && pending > 0; ++round) {
     k_gather<<<nblocks(n, kWarps), kThreads, 0, st>>>(n, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end, b.px, b.py,
                                                       b.pz, h.gather_r2, h.todo, h.nb, h.nbc);
-    k_dirtable<<<nblocks(n, kDirWarps), 32 * kDirWarps, 0, st>>>(n, cp, b.leaf_pid, h.nb, h.nbc, b.px, b.py, b.pz,
-                                                                  h.gather_r2, h.todo, h.cand, h.candc, h.rcap,
-                                                                  h.rho);
+    launch_dirtable(cp.need, n, cp, b.leaf_pid, h.nb, h.nbc, b.px, b.py, b.pz, h.gather_r2, h.todo, h.cand,
+                    h.candc, h.rcap, h.rho, st);
     launches += 2;
     cudaMemcpyAsync(todo.data(), h.todo, n, cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
