@@ -323,17 +323,33 @@ __device__ __forceinline__ double cone_exit(const CertParams& cp, double sk, dou
   return g * (1.0 + 1e-12);
 }
 
-// best[] holds the NEED largest values seen so far in descending order (zeros while
-// fewer were seen); inserting v keeps the NEED largest of best[] and v.  Unrolled over a
-// compile-time NEED so that best[] stays in registers.
-template <int NEED>
-__device__ __forceinline__ void keep_largest(float (&best)[NEED], float v) {
+// Bitonic sort of one value per lane, descending across the warp (lane 0 the largest).
+__device__ __forceinline__ float warp_sort_desc(float v, uint32_t lane) {
 #pragma unroll
-  for (int j = NEED - 1; j > 0; --j) best[j] = fmaxf(fminf(best[j - 1], v), best[j]);
-  best[0] = fmaxf(best[0], v);
+  for (uint32_t k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      const float o = __shfl_xor_sync(0xffffffffu, v, j);
+      v = (((lane & j) == 0) == ((lane & k) == 0)) ? fmaxf(v, o) : fminf(v, o);
+    }
+  }
+  return v;
 }
 
-template <int NEED>
+// top holds the 32 largest values seen so far, descending across the warp; merges in one
+// value per lane: the larger of top[j] and the j-th smallest new value forms a bitonic
+// sequence that holds the 32 largest of both, and a bitonic merge orders it.
+__device__ __forceinline__ float warp_top_merge(float top, float v, uint32_t lane) {
+  const float s = warp_sort_desc(v, lane);
+  float x = fmaxf(top, __shfl_sync(0xffffffffu, s, 31u - lane));
+#pragma unroll
+  for (uint32_t j = 16; j > 0; j >>= 1) {
+    const float o = __shfl_xor_sync(0xffffffffu, x, j);
+    x = ((lane & j) == 0) ? fmaxf(x, o) : fminf(x, o);
+  }
+  return x;
+}
+
 __global__ void __launch_bounds__(kDirThreads)
 k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uint32_t* __restrict__ nb,
            const uint32_t* __restrict__ nbc, const double* __restrict__ px, const double* __restrict__ py,
@@ -403,57 +419,88 @@ k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uin
   const double half_L = 0.5 * L2;
   const double cd = cos(cp.delta), sdl = sin(cp.delta);
   const float cdf = (float)cd, sdlf = (float)sdl;
+  const uint32_t need = cp.need;
   double worst_needed = 0.0;  // largest certified rho_s (the list must cover 2 rho_s)
   bool ok = true;
-  for (int d = t; d < kDirs; d += kDirThreads) {
-    const double s0 = cp.dirs[3 * d], s1 = cp.dirs[3 * d + 1], s2 = cp.dirs[3 * d + 2];
-    // AABB support bound over the cone
-    const double ext = cone_ext(cp, s0, ax, 0) + cone_ext(cp, s1, ay, 1) + cone_ext(cp, s2, az, 2);
-    // the centre of a well-centred sphere lies in conv(S), inside the AABB: r is at most
-    // the distance at which the ray a + r u leaves the AABB, maximised over the cone
-    // axis by axis (min over axes of the per-axis maxima bounds the max of the min)
-    const double exit_r = fmin(fmin(cone_exit(cp, s0, ax, 0), cone_exit(cp, s1, ay, 1)), cone_exit(cp, s2, az, 2));
-    const double ext_c = fmin(ext * (1.0 + 1e-12), exit_r);
-    // The `need` smallest shrunk thresholds, kept as the `need` largest lower bounds of
-    // 1 / rho_shr (binary32, no divides):  1/rho_p(u) >= 2 cos(angle + delta) / |p - a|.  Every
-    // binary32 rounding (about 1e-7 relative) is covered by the 1e-5 margins and the 1e-6
-    // absolute slack on the cosines, always in the safe direction.
-    const float s0f = (float)s0, s1f = (float)s1, s2f = (float)s2;
-    const float ext_f = __double2float_ru(ext_c);
-    const float inv_ext = 1.0f / ext_f;
-    float best[NEED];
-#pragma unroll
-    for (int j = 0; j < NEED; ++j) best[j] = 0.0f;
-    for (uint32_t i = 0; i < m; ++i) {
-      const float4 r = rel[i];  // r.w = 1 / |p - a|
-      // early exit: every later point has rho >= |p - a| / 2 > min(kth, ext)
-      if (0.5f * (1.0f - 1e-5f) * fmaxf(best[NEED - 1], inv_ext) > r.w) break;
-      const float c = s0f * r.x + s1f * r.y + s2f * r.z;
-      const float cs = fmaxf(-1.0f, c - 1e-5f);  // cosine of an upper bound of the angle
-      const float sn = sqrtf(fmaxf(0.0f, (1.0f - cs) * (1.0f + cs)));
-      const float cshr = cs * cdf - sn * sdlf - 1e-6f;  // lower bound of cos(angle + delta)
-      if (cshr <= 1e-6f) continue;
-      const float inv = 2.0f * cshr * r.w * (1.0f - 1e-5f);  // lower bound of 1 / rho_p(u)
-      if (inv > best[NEED - 1]) keep_largest<NEED>(best, inv);
+  // Each warp takes batches of 32 directions; lane j prepares direction j of the batch, then
+  // the warp scans the sorted list for one direction at a time, 32 points per step.
+  for (uint32_t dbase = warp * 32u; dbase < (uint32_t)kDirs; dbase += kDirThreads) {
+    const uint32_t dl = dbase + lane;
+    float s0f = 0.f, s1f = 0.f, s2f = 0.f;
+    double ext_c = 0.0;
+    if (dl < (uint32_t)kDirs) {
+      const double s0 = cp.dirs[3 * dl], s1 = cp.dirs[3 * dl + 1], s2 = cp.dirs[3 * dl + 2];
+      s0f = (float)s0;
+      s1f = (float)s1;
+      s2f = (float)s2;
+      // AABB support bound over the cone
+      const double ext = cone_ext(cp, s0, ax, 0) + cone_ext(cp, s1, ay, 1) + cone_ext(cp, s2, az, 2);
+      // the centre of a well-centred sphere lies in conv(S), inside the AABB: r is at most
+      // the distance at which the ray a + r u leaves the AABB, maximised over the cone
+      // axis by axis (min over axes of the per-axis maxima bounds the max of the min)
+      const double exit_r = fmin(fmin(cone_exit(cp, s0, ax, 0), cone_exit(cp, s1, ay, 1)), cone_exit(cp, s2, az, 2));
+      ext_c = fmin(ext * (1.0 + 1e-12), exit_r);
     }
-    const double kth = best[NEED - 1] > 0.0f ? (1.0 / (double)best[NEED - 1]) * (1.0 + 1e-12) : INFINITY;
-    const double rho_s = fmin(kth, ext_c);
-    rho_tab[(uint64_t)a * kDirs + d] = __double2float_ru(rho_s);  // per-cone bound, rounded up
-    // certified when every unlisted point (rho >= L/2) cannot lower it
-    if (!(rho_s <= half_L)) ok = false;
-    worst_needed = fmax(worst_needed, rho_s);
-    // mark the candidates of this cone: rho_lo_p(s) <= rho_s, i.e. 2 cos(max(angle - delta, 0)) rho_s >= |p - a|
-    const float rho_sf = __double2float_ru(rho_s);
-    for (uint32_t i = 0; i < m; ++i) {
-      const float4 r = rel[i];
-      if (0.5f * (1.0f - 1e-5f) > rho_sf * r.w) break;  // rho_lo >= |p - a| / 2 > rho_s
-      const float c = s0f * r.x + s1f * r.y + s2f * r.z;
-      const float cs = fminf(1.0f, c + 1e-5f);  // cosine of a lower bound of the angle
-      const float sn = sqrtf(fmaxf(0.0f, (1.0f - cs) * (1.0f + cs)));
-      const float clo = (cs >= cdf) ? 1.0f : cs * cdf + sn * sdlf + 1e-6f;  // upper bound of cos(max(angle - delta, 0))
-      if (clo <= 0.0f) continue;
-      if (2.0f * clo * rho_sf * r.w * (1.0f + 2e-5f) >= 1.0f) atomicOr(&mark[i >> 5], 1u << (i & 31));
+    const uint32_t nd = min(32u, (uint32_t)kDirs - dbase);
+    float my_rho = 0.f;
+    for (uint32_t jd = 0; jd < nd; ++jd) {
+      const float u0 = __shfl_sync(0xffffffffu, s0f, jd), u1 = __shfl_sync(0xffffffffu, s1f, jd),
+                  u2 = __shfl_sync(0xffffffffu, s2f, jd);
+      const double ext_d = __shfl_sync(0xffffffffu, ext_c, jd);
+      // The `need` smallest shrunk thresholds, kept as the `need` largest lower bounds of
+      // 1 / rho_shr (binary32, no divides):  1/rho_p(u) >= 2 cos(angle + delta) / |p - a|.
+      // Every binary32 rounding (about 1e-7 relative) is covered by the 1e-5 margins and the
+      // 1e-6 absolute slack on the cosines, always in the safe direction.  The scan stops at
+      // the first step whose nearest point has rho >= |p - a| / 2 > min(kth, ext); points
+      // past that bound can neither enter the `need` largest nor lower min(kth, ext).
+      const float inv_ext = 1.0f / __double2float_ru(ext_d);
+      float top = 0.0f;  // lane j: the j-th largest lower bound so far
+      float thr = 0.0f;  // top[need - 1]
+      for (uint32_t base = 0; base < m; base += 32) {
+        const uint32_t i = base + lane;
+        const float lim = 0.5f * (1.0f - 1e-5f) * fmaxf(thr, inv_ext);
+        const float4 r = i < m ? rel[i] : make_float4(0.f, 0.f, 0.f, 0.f);  // r.w = 1 / |p - a|
+        if (lim > __shfl_sync(0xffffffffu, r.w, 0)) break;
+        float inv = 0.0f;
+        if (i < m && !(lim > r.w)) {
+          const float c = u0 * r.x + u1 * r.y + u2 * r.z;
+          const float cs = fmaxf(-1.0f, c - 1e-5f);  // cosine of an upper bound of the angle
+          const float sn = sqrtf(fmaxf(0.0f, (1.0f - cs) * (1.0f + cs)));
+          const float cshr = cs * cdf - sn * sdlf - 1e-6f;  // lower bound of cos(angle + delta)
+          if (cshr > 1e-6f) inv = 2.0f * cshr * r.w * (1.0f - 1e-5f);  // lower bound of 1 / rho_p(u)
+        }
+        if (__any_sync(0xffffffffu, inv > thr)) {
+          top = warp_top_merge(top, inv, lane);
+          thr = __shfl_sync(0xffffffffu, top, need - 1);
+        }
+      }
+      const double kth = thr > 0.0f ? (1.0 / (double)thr) * (1.0 + 1e-12) : INFINITY;
+      const double rho_s = fmin(kth, ext_d);
+      const float rho_sf = __double2float_ru(rho_s);  // per-cone bound, rounded up
+      if (lane == jd) my_rho = rho_sf;
+      // certified when every unlisted point (rho >= L/2) cannot lower it
+      if (!(rho_s <= half_L)) ok = false;
+      worst_needed = fmax(worst_needed, rho_s);
+      // mark the candidates of this cone: rho_lo_p(s) <= rho_s, i.e. 2 cos(max(angle - delta, 0)) rho_s >= |p - a|;
+      // rho_lo >= |p - a| / 2 > rho_s stops the scan (monotone along the sorted list)
+      for (uint32_t base = 0; base < m; base += 32) {
+        const uint32_t i = base + lane;
+        const float4 r = i < m ? rel[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const bool stop = !(i < m) || (0.5f * (1.0f - 1e-5f) > rho_sf * r.w);
+        if (__shfl_sync(0xffffffffu, stop, 0)) break;
+        bool f = false;
+        if (!stop) {
+          const float c = u0 * r.x + u1 * r.y + u2 * r.z;
+          const float cs = fminf(1.0f, c + 1e-5f);  // cosine of a lower bound of the angle
+          const float sn = sqrtf(fmaxf(0.0f, (1.0f - cs) * (1.0f + cs)));
+          const float clo = (cs >= cdf) ? 1.0f : cs * cdf + sn * sdlf + 1e-6f;  // upper bound of cos(max(angle - delta, 0))
+          f = clo > 0.0f && 2.0f * clo * rho_sf * r.w * (1.0f + 2e-5f) >= 1.0f;
+        }
+        const uint32_t bits = __ballot_sync(0xffffffffu, f);
+        if (lane == 0 && bits) atomicOr(&mark[base >> 5], bits);
+      }
     }
+    if (lane < nd) rho_tab[(uint64_t)a * kDirs + dl] = my_rho;
   }
   for (int off = 16; off > 0; off >>= 1) worst_needed = fmax(worst_needed, __shfl_xor_sync(0xffffffffu, worst_needed, off));
   if (lane == 0) worst_w[warp] = worst_needed;
@@ -486,32 +533,7 @@ k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uin
   }
 }
 
-// One launch of k_dirtable<need> (need = s_max - 2 in 1..kMaxNeed).
-void launch_dirtable(uint32_t need, uint32_t n, const CertParams& cp, const uint32_t* leaf_pid, uint32_t* nb,
-                     const uint32_t* nbc, const double* px, const double* py, const double* pz,
-                     const double* gather_r2, uint8_t* todo, uint32_t* cand, uint32_t* candc, double* need_r,
-                     float* rho_tab, cudaStream_t st) {
-  static_assert(kMaxNeed == 9, "dispatch below covers need 1..9");
-#define EHGP_DIRTABLE(N)                                                                                         \
-  case N:                                                                                                        \
-    k_dirtable<N><<<n, kDirThreads, 0, st>>>(n, cp, leaf_pid, nb, nbc, px, py, pz, gather_r2, todo, cand, candc, \
-                                             need_r, rho_tab);                                                   \
-    break;
-  switch (need) {
-    EHGP_DIRTABLE(1)
-    EHGP_DIRTABLE(2)
-    EHGP_DIRTABLE(3)
-    EHGP_DIRTABLE(4)
-    EHGP_DIRTABLE(5)
-    EHGP_DIRTABLE(6)
-    EHGP_DIRTABLE(7)
-    EHGP_DIRTABLE(8)
-    EHGP_DIRTABLE(9)
-    default:
-      break;
-  }
-#undef EHGP_DIRTABLE
-}
+
 
 // ---- 3. owner-local enumeration ---------------------------------------------------------
 // One warp per owner a.  C(a) is staged in shared memory as rounded differences
@@ -1071,8 +1093,8 @@ int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   for (int round = 0; round < 6 && pending > 0; ++round) {
     k_gather<<<nblocks(n, kWarps), kThreads, 0, st>>>(n, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end, b.px, b.py,
                                                       b.pz, h.gather_r2, h.todo, h.nb, h.nbc);
-    launch_dirtable(cp.need, n, cp, b.leaf_pid, h.nb, h.nbc, b.px, b.py, b.pz, h.gather_r2, h.todo, h.cand,
-                    h.candc, h.rcap, h.rho, st);
+    k_dirtable<<<n, kDirThreads, 0, st>>>(n, cp, b.leaf_pid, h.nb, h.nbc, b.px, b.py, b.pz, h.gather_r2, h.todo,
+                                          h.cand, h.candc, h.rcap, h.rho);
     launches += 2;
     cudaMemcpyAsync(todo.data(), h.todo, n, cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
