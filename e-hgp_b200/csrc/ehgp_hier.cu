@@ -36,7 +36,9 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <atomic>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <numeric>
 #include <thread>
@@ -984,6 +986,10 @@ struct HierOrderOut {  // one order's journal and forest arenas, local indices
   double ms = 0;
 };
 
+struct HierOff {
+  uint32_t jb, role, fam, node, child, birth, bind, sad, grp, root, vert;
+};
+
 struct HierState {
   std::vector<void*> allocs;
   uint64_t cap_events = 0, cap_arms = 0, cap_births = 0, cap_slots = 0;
@@ -1040,22 +1046,18 @@ struct HierState {
   uint32_t* d_armoff = nullptr;
   uint32_t* d_removed = nullptr;
   std::vector<double> h_px, h_py, h_pz;
-  std::vector<ehgp_journal_batch> jbatches;
-  std::vector<ehgp_role_record> roles;
-  std::vector<ehgp_family_record> families;
-  std::vector<uint32_t> arm_removed;
-  std::vector<ehgp_forest_node> nodes;
-  std::vector<uint32_t> children;
-  std::vector<ehgp_forest_birth> births;
-  std::vector<ehgp_forest_binding> bindings;
-  std::vector<ehgp_forest_saddle> saddles;
-  std::vector<ehgp_forest_group> groups;
-  std::vector<ehgp_forest_batch> fbatches;
-  std::vector<ehgp_forest_root> roots;
-  std::vector<ehgp_vertical_assignment> vertical;
+  // The result stays in the per-order arenas (local indices); off[k] holds the global
+  // offsets of order k's records, off[keff + 1] the totals.  Records take their global
+  // indices when they are copied out.  An empty `off` means no result.
+  std::vector<HierOff> off;
+  uint64_t arm_seeds = 0;  // p_removed holds the removed point of each arm seed
+  std::vector<std::vector<ehgp_vertical_assignment>> vert;  // per source order, global node ids
+  std::vector<uint32_t> evfam;                              // saddle event -> family (local to its order)
+  std::vector<std::vector<uint32_t>> sad_of_fam;            // per order: family -> saddle (local)
   std::vector<uint32_t> h_class;  // level class by facade index
   uint32_t decision = EHGP_ERR_NOT_BUILT;
   double ms_device = 0, ms_forest = 0, ms_descent = 0, ms_orders = 0;
+  double ms_host[4] = {0, 0, 0, 0};  // union-find init, order passes, concatenation, vertical maps
   uint64_t descent_steps = 0, arms = 0, exact_boundaries = 0;
 };
 
@@ -1184,6 +1186,8 @@ int hier_run(Ctx& ctx, uint32_t K) {
   GeomBuffers& g = ctx.gb;
   uint64_t launches = 0;
   h.decision = EHGP_ERR_NOT_BUILT;
+  h.off.clear();
+  h.arm_seeds = 0;
   h.n = n;
   h.K = K;
   h.keff = K < n ? K : n;
@@ -1469,6 +1473,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
     o.status = EHGP_OK;
     o.msg = "";
   }
+  const auto t_init = std::chrono::steady_clock::now();
   auto run_order = [&](uint32_t k, HierOrderOut& o) {
     const auto to0 = std::chrono::steady_clock::now();
     auto fail_o = [&](const char* m) {
@@ -1855,107 +1860,24 @@ int hier_run(Ctx& ctx, uint32_t K) {
     for (uint32_t k = 1; k <= keff; ++k) pool.emplace_back(run_order, k, std::ref(outs[k]));
     for (auto& t : pool) t.join();
   }
+  const auto t_orders = std::chrono::steady_clock::now();
   for (uint32_t k = 1; k <= keff; ++k)
     if (outs[k].status != EHGP_OK) return abi_fail(&ctx, outs[k].status, outs[k].msg);
   h.ms_orders = 0;
   for (uint32_t k = 1; k <= keff; ++k) h.ms_orders = std::max(h.ms_orders, outs[k].ms);
-  // concatenate with global offsets
-  {
-    uint64_t tot[12] = {0};
-    for (uint32_t k = 1; k <= keff; ++k) {
-      const HierOrderOut& o = outs[k];
-      tot[0] += o.jb.size(); tot[1] += o.roles.size(); tot[2] += o.fam.size();
-      tot[4] += o.nodes.size(); tot[5] += o.children.size(); tot[6] += o.births.size(); tot[7] += o.bindings.size();
-      tot[8] += o.saddles.size(); tot[9] += o.groups.size(); tot[10] += o.roots.size();
-    }
-    h.jbatches.resize(tot[0]); h.roles.resize(tot[1]); h.families.resize(tot[2]); h.arm_removed.assign(h.p_removed, h.p_removed + narms);
-    h.nodes.resize(tot[4]); h.children.resize(tot[5]); h.births.resize(tot[6]); h.bindings.resize(tot[7]);
-    h.saddles.resize(tot[8]); h.groups.resize(tot[9]); h.fbatches.resize(tot[0]); h.roots.resize(tot[10]);
-    struct Off {
-      uint32_t jb, role, fam, seed, node, child, birth, bind, sad, grp, root;
-    };
-    std::vector<Off> off(keff + 2);
-    off[1] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (uint32_t k = 1; k <= keff; ++k) {
-      const HierOrderOut& o = outs[k];
-      const Off& a = off[k];
-      off[k + 1] = {a.jb + (uint32_t)o.jb.size(), a.role + (uint32_t)o.roles.size(), a.fam + (uint32_t)o.fam.size(),
-                    0u, a.node + (uint32_t)o.nodes.size(),
-                    a.child + (uint32_t)o.children.size(), a.birth + (uint32_t)o.births.size(),
-                    a.bind + (uint32_t)o.bindings.size(), a.sad + (uint32_t)o.saddles.size(),
-                    a.grp + (uint32_t)o.groups.size(), a.root + (uint32_t)o.roots.size()};
-    }
-    auto shift = [](uint32_t v, uint32_t d) { return v == kInvalid32 ? v : v + d; };
-    auto merge_order = [&](uint32_t k) {
-      const HierOrderOut& o = outs[k];
-      const Off& f = off[k];
-      for (size_t i = 0; i < o.jb.size(); ++i) {
-        ehgp_journal_batch x = o.jb[i];
-        x.role_offset += f.role;
-        h.jbatches[f.jb + i] = x;
-        ehgp_forest_batch y = o.fb[i];
-        y.birth_offset += f.birth;
-        y.saddle_offset += f.sad;
-        y.group_offset += f.grp;
-        h.fbatches[f.jb + i] = y;
-      }
-      for (size_t i = 0; i < o.roles.size(); ++i) {
-        ehgp_role_record x = o.roles[i];
-        x.batch += f.jb;
-        h.roles[f.role + i] = x;
-      }
-      for (size_t i = 0; i < o.fam.size(); ++i) {
-        ehgp_family_record x = o.fam[i];
-        x.role_record += f.role;
-        x.batch += f.jb;
-        h.families[f.fam + i] = x;
-      }
-      for (size_t i = 0; i < o.nodes.size(); ++i) {
-        ehgp_forest_node x = o.nodes[i];
-        x.child_offset += f.child;
-        x.atomic_group = shift(x.atomic_group, f.grp);
-        h.nodes[f.node + i] = x;
-      }
-      for (size_t i = 0; i < o.children.size(); ++i) h.children[f.child + i] = o.children[i] + f.node;
-      for (size_t i = 0; i < o.births.size(); ++i) {
-        ehgp_forest_birth x = o.births[i];
-        x.batch += f.jb;
-        x.order_one_node = shift(x.order_one_node, f.node);
-        h.births[f.birth + i] = x;
-      }
-      for (size_t i = 0; i < o.bindings.size(); ++i) {
-        ehgp_forest_binding x = o.bindings[i];
-        x.family += f.fam;
-        x.prior_root = shift(x.prior_root, f.node);
-        h.bindings[f.bind + i] = x;
-      }
-      for (size_t i = 0; i < o.saddles.size(); ++i) {
-        ehgp_forest_saddle x = o.saddles[i];
-        x.family += f.fam;
-        x.batch += f.jb;
-        x.arm_offset += f.bind;
-        x.group += f.grp;
-        h.saddles[f.sad + i] = x;
-      }
-      for (size_t i = 0; i < o.groups.size(); ++i) {
-        ehgp_forest_group x = o.groups[i];
-        x.batch += f.jb;
-        x.saddle_offset += f.sad;
-        x.child_offset += f.child;
-        x.created_node = shift(x.created_node, f.node);
-        x.result_node = shift(x.result_node, f.node);
-        h.groups[f.grp + i] = x;
-      }
-      for (size_t i = 0; i < o.roots.size(); ++i) {
-        ehgp_forest_root x = o.roots[i];
-        x.node += f.node;
-        h.roots[f.root + i] = x;
-      }
-    };
-    std::vector<std::thread> pool;
-    for (uint32_t k = 1; k <= keff; ++k) pool.emplace_back(merge_order, k);
-    for (auto& t : pool) t.join();
+  // global offsets of each order's records (the reference's single pass emits orders in turn)
+  std::vector<HierOff> off(keff + 2);
+  off[1] = HierOff{0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (uint32_t k = 1; k <= keff; ++k) {
+    const HierOrderOut& o = outs[k];
+    const HierOff& a = off[k];
+    off[k + 1] = {a.jb + (uint32_t)o.jb.size(),         a.role + (uint32_t)o.roles.size(),
+                  a.fam + (uint32_t)o.fam.size(),       a.node + (uint32_t)o.nodes.size(),
+                  a.child + (uint32_t)o.children.size(), a.birth + (uint32_t)o.births.size(),
+                  a.bind + (uint32_t)o.bindings.size(), a.sad + (uint32_t)o.saddles.size(),
+                  a.grp + (uint32_t)o.groups.size(),    a.root + (uint32_t)o.roots.size(), 0u};
   }
+  const auto t_merge = std::chrono::steady_clock::now();
   // ---- vertical maps: each reduced node of order k >= 2 at level a maps, on the closed
   // cut at a, to the root of order k - 1 whose component contains it.  A carrier birth of
   // the node's group is an event of rank k; that event is a saddle of order k - 1, whose
@@ -1963,80 +1885,113 @@ int hier_run(Ctx& ctx, uint32_t K) {
   // (the contract serializer's assignment, reference/morsehgp3d_oracle/serialization.py:1040-1099).
   {
     h.h_class.resize(m);
-    if (m && (e = cudaMemcpy(h.h_class.data(), h.lclass, (uint64_t)m * 4, cudaMemcpyDeviceToHost)) != cudaSuccess)
+    if (m && (e = cudaMemcpyAsync(h.h_class.data(), h.lclass, (uint64_t)m * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
       return abi_cuda_fail(&ctx, e, "level classes");
-    const uint64_t nn = h.nodes.size();
-    std::vector<uint32_t> evfam(m, kInvalid32), sad_of_fam(h.families.size(), kInvalid32);
-    for (uint64_t f = 0; f < h.families.size(); ++f) evfam[h.families[f].event] = (uint32_t)f;
-    for (uint64_t sd = 0; sd < h.saddles.size(); ++sd) sad_of_fam[h.saddles[sd].family] = (uint32_t)sd;
-    auto cls = [&](uint32_t node) -> int64_t {
-      const uint32_t le = h.nodes[node].level_event;
-      return le == kInvalid32 ? -1 : (int64_t)h.h_class[le];
+    // event -> family and family -> saddle, local to each order (one host thread per order)
+    h.evfam.resize(m);
+    if (h.sad_of_fam.size() < keff + 1) h.sad_of_fam.resize(keff + 1);
+    {
+      std::vector<std::thread> pool;
+      const uint32_t nt = keff;
+      for (uint32_t k = 1; k <= keff; ++k)
+        pool.emplace_back([&, k] {
+          const uint64_t lo = (uint64_t)m * (k - 1) / nt, hi = (uint64_t)m * k / nt;
+          std::fill(h.evfam.begin() + lo, h.evfam.begin() + hi, kInvalid32);
+        });
+      for (auto& t : pool) t.join();
+      pool.clear();
+      for (uint32_t k = 1; k <= keff; ++k)
+        pool.emplace_back([&, k] {
+          const HierOrderOut& o = outs[k];
+          for (uint64_t f = 0; f < o.fam.size(); ++f) h.evfam[o.fam[f].event] = (uint32_t)f;
+          std::vector<uint32_t>& sof = h.sad_of_fam[k];
+          sof.assign(o.fam.size(), kInvalid32);
+          for (uint64_t sd = 0; sd < o.saddles.size(); ++sd) sof[o.saddles[sd].family] = (uint32_t)sd;
+        });
+      for (auto& t : pool) t.join();
+    }
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "level classes");
+    auto cls = [&](const ehgp_forest_node& nd) -> int64_t {
+      return nd.level_event == kInvalid32 ? -1 : (int64_t)h.h_class[nd.level_event];
     };
-    std::vector<uint64_t> order_begin(keff + 2, nn);
-    for (uint64_t i = nn; i-- > 0;) order_begin[h.nodes[i].order] = i;
-    for (uint32_t k = keff + 1; k-- > 1;)
-      if (order_begin[k] == nn) order_begin[k] = order_begin[k + 1];
-    std::vector<std::vector<ehgp_vertical_assignment>> vo(keff + 1);
+    if (h.vert.size() < keff + 1) h.vert.resize(keff + 1);
     std::vector<int> vstat(keff + 1, EHGP_OK);
     // Offline sweep per source order: node ids grow with level in both forests, so the
     // target forest's parent links are united in id (= level) order as the source levels
     // rise; the image is then one find with path compression.
     auto run_v = [&](uint32_t k) {
-      const uint64_t t_lo = order_begin[k - 1], t_hi = order_begin[k];
-      std::vector<uint32_t> up(t_hi - t_lo);
-      for (uint64_t x = 0; x < up.size(); ++x) up[x] = (uint32_t)x;
-      auto find_up = [&](uint32_t x) {  // local target index
+      const HierOrderOut& src = outs[k];
+      const HierOrderOut& tgt = outs[k - 1];
+      const std::vector<uint32_t>& sof = h.sad_of_fam[k - 1];
+      std::vector<ehgp_vertical_assignment>& vo = h.vert[k];
+      vo.clear();
+      const uint64_t h_lo = n + (rb[k] - rb[2]);  // first birth handle of order k
+      const uint32_t t_n = (uint32_t)tgt.nodes.size();
+      std::vector<uint32_t> up(t_n);
+      std::iota(up.begin(), up.end(), 0u);
+      auto find_up = [&](uint32_t x) {
         while (up[x] != x) {
           up[x] = up[up[x]];
           x = up[x];
         }
         return x;
       };
-      uint64_t sweep = t_lo;  // next target node whose child links are not yet united
-      for (uint64_t i = order_begin[k]; i < order_begin[k + 1]; ++i) {
-        const ehgp_forest_node& nd = h.nodes[i];
-        const ehgp_forest_group& g = h.groups[nd.atomic_group];
-        const uint32_t carrier = h.bindings[h.saddles[g.saddle_offset].arm_offset].carrier;
-        const uint32_t proj = h.births[carrier].projection;
-        const uint32_t f = proj >= n ? evfam[proj - n] : kInvalid32;
-        if (f == kInvalid32 || h.families[f].order != k - 1 || sad_of_fam[f] == kInvalid32) {
+      uint32_t sweep = 0;  // next target node whose child links are not yet united
+      for (uint64_t i = 0; i < src.nodes.size(); ++i) {
+        const ehgp_forest_node& nd = src.nodes[i];
+        const ehgp_forest_group& g = src.groups[nd.atomic_group];
+        const uint64_t carrier = src.bindings[src.saddles[g.saddle_offset].arm_offset].carrier;
+        if (carrier < h_lo || carrier - h_lo >= src.births.size()) {
           vstat[k] = EHGP_ERR_DEGENERATE;
           return;
         }
-        const uint32_t R = h.groups[h.saddles[sad_of_fam[f]].group].result_node;
-        const int64_t lev = cls((uint32_t)i);
-        if (R < t_lo || R >= t_hi || cls(R) > lev) {
+        const uint32_t proj = src.births[carrier - h_lo].projection;
+        const uint32_t f = proj >= n && proj - n < m ? h.evfam[proj - n] : kInvalid32;
+        if (f == kInvalid32 || f >= tgt.fam.size() || tgt.fam[f].event != proj - n || sof[f] == kInvalid32) {
           vstat[k] = EHGP_ERR_DEGENERATE;
           return;
         }
-        while (sweep < t_hi && cls((uint32_t)sweep) <= lev) {
-          const ehgp_forest_node& p = h.nodes[sweep];
+        const uint32_t R = tgt.groups[tgt.saddles[sof[f]].group].result_node;
+        const int64_t lev = cls(nd);
+        if (R >= t_n || cls(tgt.nodes[R]) > lev) {
+          vstat[k] = EHGP_ERR_DEGENERATE;
+          return;
+        }
+        while (sweep < t_n && cls(tgt.nodes[sweep]) <= lev) {
+          const ehgp_forest_node& p = tgt.nodes[sweep];
           if (p.kind == 2)
-            for (uint32_t c = 0; c < p.child_count; ++c) {
-              const uint32_t ch = h.children[p.child_offset + c];
-              up[find_up(ch - (uint32_t)t_lo)] = (uint32_t)(sweep - t_lo);
-            }
+            for (uint32_t c = 0; c < p.child_count; ++c) up[find_up(tgt.children[p.child_offset + c])] = sweep;
           ++sweep;
         }
-        vo[k].push_back({(uint32_t)i, (uint32_t)t_lo + find_up(R - (uint32_t)t_lo), k, nd.level_event});
+        vo.push_back({(uint32_t)i + off[k].node, find_up(R) + off[k - 1].node, k, nd.level_event});
       }
     };
     std::vector<std::thread> pool;
     for (uint32_t k = 2; k <= keff; ++k) pool.emplace_back(run_v, k);
     for (auto& t : pool) t.join();
-    h.vertical.clear();
-    for (uint32_t k = 2; k <= keff; ++k) {
-      if (vstat[k] != EHGP_OK)
+    uint32_t vtot = 0;
+    for (uint32_t k = 1; k <= keff; ++k) {
+      if (k >= 2 && vstat[k] != EHGP_OK)
         return abi_fail(&ctx, vstat[k], "a reduced node has no lower-order image through its carrier saddle");
-      h.vertical.insert(h.vertical.end(), vo[k].begin(), vo[k].end());
+      off[k].vert = vtot;
+      if (k >= 2) vtot += (uint32_t)h.vert[k].size();
     }
+    off[keff + 1].vert = vtot;
   }
   const auto t2 = std::chrono::steady_clock::now();
   h.ms_forest = std::chrono::duration<double, std::milli>(t2 - t1).count();
+  {
+    using msd = std::chrono::duration<double, std::milli>;
+    h.ms_host[0] = msd(t_init - t1).count();
+    h.ms_host[1] = msd(t_orders - t_init).count();
+    h.ms_host[2] = msd(t_merge - t_orders).count();
+    h.ms_host[3] = msd(t2 - t_merge).count();
+  }
   (void)t0;
   ctx.last_launches = launches;
   ctx.last_ms = h.ms_device + h.ms_forest;
+  h.off = std::move(off);
+  h.arm_seeds = narms;
   h.decision = EHGP_OK;
   return EHGP_OK;
 }
@@ -2067,18 +2022,21 @@ int ehgp_hierarchy(ehgp_ctx* ctx, uint32_t K, ehgp_hier_counts* counts) {
       const ehgp::HierState& h = *ctx->hier;
       counts->events = h.events;
       counts->diagnostics = h.diagnostics;
-      counts->journal_batches = h.jbatches.size();
-      counts->role_records = h.roles.size();
-      counts->families = h.families.size();
-      counts->arm_seeds = h.arm_removed.size();
-      counts->birth_records = h.births.size();
-      counts->nodes = h.nodes.size();
-      counts->children = h.children.size();
-      counts->arm_bindings = h.bindings.size();
-      counts->saddle_records = h.saddles.size();
-      counts->atomic_groups = h.groups.size();
-      counts->final_roots = h.roots.size();
-      counts->vertical_assignments = h.vertical.size();
+      if (!h.off.empty()) {
+        const ehgp::HierOff& t = h.off.back();
+        counts->journal_batches = t.jb;
+        counts->role_records = t.role;
+        counts->families = t.fam;
+        counts->arm_seeds = h.arm_seeds;
+        counts->birth_records = t.birth;
+        counts->nodes = t.node;
+        counts->children = t.child;
+        counts->arm_bindings = t.bind;
+        counts->saddle_records = t.sad;
+        counts->atomic_groups = t.grp;
+        counts->final_roots = t.root;
+        counts->vertical_assignments = t.vert;
+      }
       counts->k_eff = h.keff;
     }
     counts->decision = (uint32_t)s;
@@ -2091,26 +2049,112 @@ int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out) {
   std::lock_guard<std::mutex> lock(ctx->mutex);
   if (!ctx->hier) return ehgp::abi_fail(ctx, EHGP_ERR_NOT_BUILT, "no hierarchy result is resident");
   const ehgp::HierState& h = *ctx->hier;
-  auto cp = [](void* dst, const void* src, size_t bytes) {
-    if (dst && bytes) std::memcpy(dst, src, bytes);
-  };
   if (out->events && h.events) {
     const cudaError_t e = cudaMemcpy(out->events, h.ev, h.events * sizeof(ehgp::EvRec), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return ehgp::abi_cuda_fail(ctx, e, "facade copy");
   }
-  cp(out->journal_batches, h.jbatches.data(), h.jbatches.size() * sizeof(ehgp_journal_batch));
-  cp(out->roles, h.roles.data(), h.roles.size() * sizeof(ehgp_role_record));
-  cp(out->families, h.families.data(), h.families.size() * sizeof(ehgp_family_record));
-  cp(out->arm_removed, h.arm_removed.data(), h.arm_removed.size() * sizeof(uint32_t));
-  cp(out->nodes, h.nodes.data(), h.nodes.size() * sizeof(ehgp_forest_node));
-  cp(out->children, h.children.data(), h.children.size() * sizeof(uint32_t));
-  cp(out->births, h.births.data(), h.births.size() * sizeof(ehgp_forest_birth));
-  cp(out->bindings, h.bindings.data(), h.bindings.size() * sizeof(ehgp_forest_binding));
-  cp(out->saddles, h.saddles.data(), h.saddles.size() * sizeof(ehgp_forest_saddle));
-  cp(out->groups, h.groups.data(), h.groups.size() * sizeof(ehgp_forest_group));
-  cp(out->batches, h.fbatches.data(), h.fbatches.size() * sizeof(ehgp_forest_batch));
-  cp(out->roots, h.roots.data(), h.roots.size() * sizeof(ehgp_forest_root));
-  cp(out->vertical, h.vertical.data(), h.vertical.size() * sizeof(ehgp_vertical_assignment));
+  if (h.off.empty()) return EHGP_OK;
+  // Each order's arenas go to their global offsets with local indices shifted, in chunks
+  // spread over the host cores.
+  using ehgp::HierOff;
+  const uint32_t keff = (uint32_t)h.off.size() - 2;
+  std::vector<std::function<void()>> tasks;
+  constexpr uint64_t kChunk = 1u << 18;
+  auto shift = [](uint32_t v, uint32_t d) { return v == ehgp::kInvalid32 ? v : v + d; };
+  auto add = [&](void* dst_base, uint64_t count, auto&& one) {
+    if (!dst_base) return;
+    for (uint64_t lo = 0; lo < count; lo += kChunk) {
+      const uint64_t hi = std::min(count, lo + kChunk);
+      tasks.emplace_back([=] {
+        for (uint64_t i = lo; i < hi; ++i) one(i);
+      });
+    }
+  };
+  for (uint32_t k = 1; k <= keff; ++k) {
+    const ehgp::HierOrderOut& o = h.outs[k];
+    const HierOff f = h.off[k];
+    add(out->journal_batches, o.jb.size(), [&o, f, out](uint64_t i) {
+      ehgp_journal_batch x = o.jb[i];
+      x.role_offset += f.role;
+      out->journal_batches[f.jb + i] = x;
+    });
+    add(out->batches, o.fb.size(), [&o, f, out](uint64_t i) {
+      ehgp_forest_batch y = o.fb[i];
+      y.birth_offset += f.birth;
+      y.saddle_offset += f.sad;
+      y.group_offset += f.grp;
+      out->batches[f.jb + i] = y;
+    });
+    add(out->roles, o.roles.size(), [&o, f, out](uint64_t i) {
+      ehgp_role_record x = o.roles[i];
+      x.batch += f.jb;
+      out->roles[f.role + i] = x;
+    });
+    add(out->families, o.fam.size(), [&o, f, out](uint64_t i) {
+      ehgp_family_record x = o.fam[i];
+      x.role_record += f.role;
+      x.batch += f.jb;
+      out->families[f.fam + i] = x;
+    });
+    add(out->nodes, o.nodes.size(), [&o, f, out, shift](uint64_t i) {
+      ehgp_forest_node x = o.nodes[i];
+      x.child_offset += f.child;
+      x.atomic_group = shift(x.atomic_group, f.grp);
+      out->nodes[f.node + i] = x;
+    });
+    add(out->children, o.children.size(), [&o, f, out](uint64_t i) { out->children[f.child + i] = o.children[i] + f.node; });
+    add(out->births, o.births.size(), [&o, f, out, shift](uint64_t i) {
+      ehgp_forest_birth x = o.births[i];
+      x.batch += f.jb;
+      x.order_one_node = shift(x.order_one_node, f.node);
+      out->births[f.birth + i] = x;
+    });
+    add(out->bindings, o.bindings.size(), [&o, f, out, shift](uint64_t i) {
+      ehgp_forest_binding x = o.bindings[i];
+      x.family += f.fam;
+      x.prior_root = shift(x.prior_root, f.node);
+      out->bindings[f.bind + i] = x;
+    });
+    add(out->saddles, o.saddles.size(), [&o, f, out](uint64_t i) {
+      ehgp_forest_saddle x = o.saddles[i];
+      x.family += f.fam;
+      x.batch += f.jb;
+      x.arm_offset += f.bind;
+      x.group += f.grp;
+      out->saddles[f.sad + i] = x;
+    });
+    add(out->groups, o.groups.size(), [&o, f, out, shift](uint64_t i) {
+      ehgp_forest_group x = o.groups[i];
+      x.batch += f.jb;
+      x.saddle_offset += f.sad;
+      x.child_offset += f.child;
+      x.created_node = shift(x.created_node, f.node);
+      x.result_node = shift(x.result_node, f.node);
+      out->groups[f.grp + i] = x;
+    });
+    add(out->roots, o.roots.size(), [&o, f, out](uint64_t i) {
+      ehgp_forest_root x = o.roots[i];
+      x.node += f.node;
+      out->roots[f.root + i] = x;
+    });
+    if (k >= 2 && k < h.vert.size()) {
+      const std::vector<ehgp_vertical_assignment>& v = h.vert[k];
+      add(out->vertical, v.size(), [&v, f, out](uint64_t i) { out->vertical[f.vert + i] = v[i]; });
+    }
+  }
+  add(out->arm_removed, h.arm_seeds, [&h, out](uint64_t i) { out->arm_removed[i] = h.p_removed[i]; });
+  if (!tasks.empty()) {
+    const uint32_t hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const uint32_t nt = (uint32_t)std::min<uint64_t>(hw, tasks.size());
+    std::atomic<uint64_t> next{0};
+    auto work = [&] {
+      for (uint64_t t; (t = next.fetch_add(1)) < tasks.size();) tasks[t]();
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t i = 1; i < nt; ++i) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+  }
   return EHGP_OK;
 }
 
@@ -2122,6 +2166,8 @@ int ehgp_hier_stats(const ehgp_ctx* ctx, double* ms, uint64_t* stats) {
     ms[1] = h.ms_descent;
     ms[2] = h.ms_forest;
     ms[3] = h.ms_orders;
+    for (int i = 0; i < 4; ++i) ms[4 + i] = h.ms_host[i];
+    for (uint32_t k = 1; k <= 16; ++k) ms[7 + k] = k < h.outs.size() ? h.outs[k].ms : 0.0;
   }
   if (stats) {
     stats[0] = h.arms;
