@@ -40,6 +40,7 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <memory>
 #include <numeric>
 #include <thread>
 #include <vector>
@@ -969,18 +970,48 @@ struct HierDsu {
   uint32_t parent, rroot, order;  // order 0: not yet born
 };
 
+// Growable storage of plain C records that keeps its capacity across calls and leaves new
+// storage uninitialised; n counts the records in use.  Writers stay within the capacity
+// reserved up front (fits() reports an overrun, which is never written).
+template <class T>
+struct Arena {
+  std::unique_ptr<T[]> p;
+  uint64_t cap = 0, n = 0;
+  void reset(uint64_t need) {
+    if (need > cap) {
+      p.reset(new T[need]);
+      cap = need;
+    }
+    n = 0;
+  }
+  uint64_t size() const { return n; }
+  bool fits() const { return n <= cap; }
+  T& operator[](uint64_t i) { return p[i]; }
+  const T& operator[](uint64_t i) const { return p[i]; }
+  T* begin() { return p.get(); }
+  T* end() { return p.get() + n; }
+  void push_back(const T& x) {
+    if (n < cap) p[n] = x;
+    ++n;
+  }
+  template <class It>
+  void append(It first, It last) {
+    for (; first != last; ++first) push_back(*first);
+  }
+};
+
 struct HierOrderOut {  // one order's journal and forest arenas, local indices
-  std::vector<ehgp_journal_batch> jb;
-  std::vector<ehgp_role_record> roles;
-  std::vector<ehgp_family_record> fam;
-  std::vector<ehgp_forest_node> nodes;
-  std::vector<uint32_t> children;
-  std::vector<ehgp_forest_birth> births;
-  std::vector<ehgp_forest_binding> bindings;
-  std::vector<ehgp_forest_saddle> saddles;
-  std::vector<ehgp_forest_group> groups;
-  std::vector<ehgp_forest_batch> fb;
-  std::vector<ehgp_forest_root> roots;
+  Arena<ehgp_journal_batch> jb;
+  Arena<ehgp_role_record> roles;
+  Arena<ehgp_family_record> fam;
+  Arena<ehgp_forest_node> nodes;
+  Arena<uint32_t> children;
+  Arena<ehgp_forest_birth> births;
+  Arena<ehgp_forest_binding> bindings;
+  Arena<ehgp_forest_saddle> saddles;
+  Arena<ehgp_forest_group> groups;
+  Arena<ehgp_forest_batch> fb;
+  Arena<ehgp_forest_root> roots;
   int status = EHGP_OK;
   const char* msg = "";
   double ms = 0;
@@ -1468,14 +1499,39 @@ int hier_run(Ctx& ctx, uint32_t K) {
   auto& outs = h.outs;
   for (uint32_t k = 1; k <= keff; ++k) {
     HierOrderOut& o = outs[k];
-    o.jb.clear(); o.roles.clear(); o.fam.clear(); o.nodes.clear(); o.children.clear(); o.births.clear();
-    o.bindings.clear(); o.saddles.clear(); o.groups.clear(); o.fb.clear(); o.roots.clear();
     o.status = EHGP_OK;
     o.msg = "";
   }
   const auto t_init = std::chrono::steady_clock::now();
-  auto run_order = [&](uint32_t k, HierOrderOut& o) {
+  // Each order runs a lean sequential core (union-find over its batches; it writes the arm
+  // bindings in place and handles multi-role batches whole) and publishes chunks of
+  // single-role batches with the running counters at their start; a shared pool of host
+  // threads rebuilds those batches' journal and forest records from the bindings while the
+  // cores go on.  Record positions and contents equal those of one sequential pass.
+  struct Cnt {
+    uint64_t bi, si;
+    uint32_t jb, role, birth, sad, grp, node, child, count;
+    uint64_t carriers, reduced;
+  };
+  constexpr uint32_t kChunkBatches = 1u << 14, kSnapBlock = 4096;
+  struct Progress {
+    std::vector<std::unique_ptr<Cnt[]>> blocks;  // published chunk starts, kSnapBlock per block
+    std::atomic<uint32_t> published{0}, claimed{0};
+    std::atomic<int> done{0}, bad{0};
+  };
+  std::vector<Progress> prog(keff + 1);
+  auto order_range = [&](uint32_t k, uint64_t& b_lo, uint64_t& b_hi, uint64_t& s_lo, uint64_t& s_hi,
+                         uint64_t& arm_lo, uint64_t& arm_hi) {
+    b_lo = k == 1 ? 0 : rb[k];
+    b_hi = k == 1 ? 0 : rb[k + 1];
+    s_lo = rb[k + 1];
+    s_hi = rb[k + 2 > 16 ? 16 : k + 2];
+    arm_lo = s_hi > s_lo ? arm_off[s_lo - fam_lo] : 0;
+    arm_hi = s_hi > s_lo ? arm_off[s_hi - fam_lo] : 0;
+  };
+  auto run_core = [&](uint32_t k, HierOrderOut& o) {
     const auto to0 = std::chrono::steady_clock::now();
+    Progress& pg = prog[k];
     auto fail_o = [&](const char* m) {
       o.status = EHGP_ERR_DEGENERATE;
       o.msg = m;
@@ -1487,21 +1543,39 @@ int hier_run(Ctx& ctx, uint32_t K) {
       }
       return x;
     };
-    uint64_t carriers = 0, reduced = 0;
-    const uint64_t b_lo = k == 1 ? 0 : rb[k], b_hi = k == 1 ? 0 : rb[k + 1];
-    const uint64_t s_lo = rb[k + 1], s_hi = rb[k + 2 > 16 ? 16 : k + 2];
-    const uint64_t arm_hi = s_hi > s_lo ? arm_off[s_hi - fam_lo] : 0;  // arms of this order end here
-    o.fam.reserve(s_hi - s_lo);
-    o.saddles.reserve(s_hi - s_lo);
-    o.groups.reserve(s_hi - s_lo);
-    o.births.reserve(k == 1 ? n : b_hi - b_lo);
-    {
-      const uint64_t nroles = (k == 1 ? n : b_hi - b_lo) + (s_hi - s_lo);
-      o.roles.reserve(nroles);
-      o.jb.reserve(nroles);
-      o.fb.reserve(nroles);
-      if (s_hi > s_lo) o.bindings.reserve(arm_off[s_hi - fam_lo] - arm_off[s_lo - fam_lo]);
-    }
+    uint64_t b_lo, b_hi, s_lo, s_hi, arm_lo, arm_hi;
+    order_range(k, b_lo, b_hi, s_lo, s_hi, arm_lo, arm_hi);
+    const uint64_t births_k = k == 1 ? n : b_hi - b_lo, fams_k = s_hi - s_lo, arms_k = arm_hi - arm_lo;
+    // capacities are upper bounds (one batch holds at least one role; a group at least one
+    // saddle; a multifusion's children are distinct prior roots of its arms' carriers)
+    o.jb.reset(births_k + fams_k);
+    o.fb.reset(births_k + fams_k);
+    o.roles.reset(births_k + fams_k);
+    o.fam.reset(fams_k);
+    o.saddles.reset(fams_k);
+    o.groups.reset(fams_k);
+    o.births.reset(births_k);
+    o.bindings.reset(arms_k);
+    o.nodes.reset((k == 1 ? n : 0) + fams_k);
+    o.children.reset(arms_k);
+    o.roots.reset(births_k);
+    pg.blocks.clear();
+    pg.blocks.resize((births_k + fams_k) / kSnapBlock + 2);  // chunks <= batches / kChunkBatches + multi-role batches + 1
+    Cnt c{b_lo, s_lo, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t nchunk = 0;
+    Cnt open = c;  // start of the chunk being filled
+    auto close_chunk = [&] {
+      if (open.count == 0) return;
+      const uint32_t blk = nchunk / kSnapBlock;
+      if (!pg.blocks[blk]) pg.blocks[blk].reset(new Cnt[kSnapBlock]);
+      pg.blocks[blk][nchunk % kSnapBlock] = open;
+      ++nchunk;
+      pg.published.store(nchunk, std::memory_order_release);
+    };
+    auto reopen = [&] {
+      open = c;
+      open.count = 0;
+    };
     struct Role {
       uint32_t proj, role, fi, pos;
     };
@@ -1517,48 +1591,143 @@ int hier_run(Ctx& ctx, uint32_t K) {
     std::vector<Arm> arms_b;
     std::vector<Plan> plans;
     std::vector<ehgp_forest_node> gnodes;
-    uint64_t bi = b_lo, si = s_lo;
+    uint64_t& bi = c.bi;
+    uint64_t& si = c.si;
+    uint64_t& carriers = c.carriers;
+    uint64_t& reduced = c.reduced;
     bool singles = k == 1;
-    while (singles || bi < b_hi || si < s_hi) {
-      uint32_t cls = kInvalid32, lev = kInvalid32;
-      if (!singles) {
-        const uint32_t cls_b = bi < b_hi ? cls_rp[bi] : kInvalid32;
-        const uint32_t cls_s = si < s_hi ? cls_rp[si] : kInvalid32;
-        cls = std::min(cls_b, cls_s);
-        lev = cls_b <= cls_s ? rank_order[bi] : rank_order[si];
-        // fast paths: the batch holds exactly one role (almost every batch off ties)
-        const bool one_b = cls_b == cls && !(bi + 1 < b_hi && cls_rp[bi + 1] == cls) && cls_s != cls;
-        const bool one_s = cls_s == cls && !(si + 1 < s_hi && cls_rp[si + 1] == cls) && cls_b != cls;
-        if (one_b) {
-          const uint32_t bidx = (uint32_t)o.jb.size();
-          const uint32_t pos = (uint32_t)(bi - rb[2]), fi = rank_order[bi];
-          const uint32_t handle = n + pos;
-          o.jb.push_back({k, lev, (uint32_t)o.roles.size(), 1, 1, 0});
-          o.roles.push_back({bidx, n + fi, 0});
-          ehgp_forest_batch fb{k, lev, (uint32_t)o.births.size(), 1, (uint32_t)o.saddles.size(), 0,
-                               (uint32_t)o.groups.size(), 0, (uint32_t)carriers, (uint32_t)reduced, 0, 0};
-          o.births.push_back({n + fi, bidx, k, handle, kInvalid32});
-          dsu[handle].order = k;
-          dsu[handle].rroot = kInvalid32;
-          ++carriers;
-          fb.post_carriers = (uint32_t)carriers;
-          fb.post_roots = (uint32_t)reduced;
-          o.fb.push_back(fb);
-          ++bi;
-          continue;
+    auto core = [&]() {
+      while (singles || bi < b_hi || si < s_hi) {
+        uint32_t cls = kInvalid32, lev = kInvalid32;
+        if (!singles) {
+          const uint32_t cls_b = bi < b_hi ? cls_rp[bi] : kInvalid32;
+          const uint32_t cls_s = si < s_hi ? cls_rp[si] : kInvalid32;
+          cls = std::min(cls_b, cls_s);
+          lev = cls_b <= cls_s ? rank_order[bi] : rank_order[si];
+          // single-role batches (almost every batch off ties): union-find only here
+          const bool one_b = cls_b == cls && !(bi + 1 < b_hi && cls_rp[bi + 1] == cls) && cls_s != cls;
+          const bool one_s = cls_s == cls && !(si + 1 < s_hi && cls_rp[si + 1] == cls) && cls_b != cls;
+          if (one_b) {
+            const uint32_t handle = n + (uint32_t)(bi - rb[2]);
+            dsu[handle].order = k;
+            dsu[handle].rroot = kInvalid32;
+            ++carriers;
+            ++c.jb; ++c.role; ++c.birth;
+            ++bi;
+            if (++open.count == kChunkBatches) { close_chunk(); reopen(); }
+            continue;
+          }
+          if (one_s) {
+            const uint32_t pos = (uint32_t)(si - fam_lo), fidx = (uint32_t)(si - s_lo);
+            const uint32_t a0 = arm_off[pos], a1 = arm_off[pos + 1];
+            uint32_t dc[4], pr[4];
+            int ndc = 0, np = 0;
+            for (uint32_t a = a0; a < a1; ++a) {
+              // two-stage prefetch: the arm's record 64 arms ahead, its parent's 32 ahead
+              if (a + 64 < arm_hi) __builtin_prefetch(&dsu[term[a + 64] < birth_count ? term[a + 64] : 0]);
+              if (a + 32 < arm_hi && term[a + 32] < birth_count) __builtin_prefetch(&dsu[dsu[term[a + 32]].parent]);
+              if (term[a] >= birth_count || !dsu[term[a]].order) {
+                fail_o("a strict arm descended to a minimum that is not yet born");
+                return;
+              }
+              const uint32_t c0 = find(term[a]);
+              const uint32_t p0 = dsu[c0].rroot;
+              o.bindings[a - arm_lo] = {a, fidx, c0, p0};
+              bool dup = false;
+              for (int t = 0; t < ndc; ++t) dup |= dc[t] == c0;
+              if (dup) continue;
+              int j = ndc++;
+              while (j > 0 && dc[j - 1] > c0) { dc[j] = dc[j - 1]; --j; }
+              dc[j] = c0;
+              if (p0 != kInvalid32) {
+                int q = np++;
+                while (q > 0 && pr[q - 1] > p0) { pr[q] = pr[q - 1]; --q; }
+                pr[q] = p0;
+                if ((q > 0 && pr[q - 1] == p0) || (q + 1 < np && pr[q + 1] == p0)) {
+                  fail_o("a frozen carrier class repeats a reduced root");
+                  return;
+                }
+              }
+            }
+            uint32_t result;
+            if (np == 1) {
+              result = pr[0];
+            } else {
+              if (np == 0 && k == 1) {
+                fail_o("an order-one group has no root");
+                return;
+              }
+              result = c.node++;
+              if (np >= 2) c.child += (uint32_t)np;
+            }
+            // commit: the distinct carriers are pre-batch roots; the least survives
+            for (int t = 1; t < ndc; ++t) dsu[dc[t]].parent = dc[0];
+            carriers -= (uint64_t)(ndc - 1);
+            dsu[dc[0]].rroot = result;
+            reduced = reduced - (uint64_t)np + 1;
+            ++c.jb; ++c.role; ++c.sad; ++c.grp;
+            ++si;
+            if (++open.count == kChunkBatches) { close_chunk(); reopen(); }
+            continue;
+          }
         }
-        if (one_s) {
-          const uint32_t bidx = (uint32_t)o.jb.size();
-          const uint32_t pos = (uint32_t)(si - fam_lo), fi = rank_order[si];
+        // a multi-role batch, whole: the arenas' counts follow the core's counters
+        close_chunk();
+        o.jb.n = c.jb; o.fb.n = c.jb; o.roles.n = c.role; o.fam.n = (uint32_t)(si - s_lo); o.births.n = c.birth;
+        o.bindings.n = si < s_hi ? arm_off[si - fam_lo] - arm_lo : arms_k;
+        o.saddles.n = c.sad; o.groups.n = c.grp; o.nodes.n = c.node; o.children.n = c.child;
+        const uint32_t bidx = (uint32_t)o.jb.size();
+        ehgp_journal_batch jb{k, lev, (uint32_t)o.roles.size(), 0, 0, 0};
+        ehgp_forest_batch fb{};
+        fb.order = k;
+        fb.level_event = lev;
+        fb.pre_carriers = (uint32_t)carriers;
+        fb.pre_roots = (uint32_t)reduced;
+        batch_roles.clear();
+        if (singles) {
+          for (uint32_t p = 0; p < n; ++p) batch_roles.push_back({p, 0, kInvalid32, p});
+        } else {
+          while (bi < b_hi && cls_rp[bi] == cls) {
+            batch_roles.push_back({n + rank_order[bi], 0, rank_order[bi], (uint32_t)(bi - rb[2])});
+            ++bi;
+          }
+          const size_t nbr = batch_roles.size();
+          while (si < s_hi && cls_rp[si] == cls) {
+            batch_roles.push_back({n + rank_order[si], 1, rank_order[si], (uint32_t)(si - fam_lo)});
+            ++si;
+          }
+          if (nbr && nbr < batch_roles.size())
+            std::inplace_merge(batch_roles.begin(), batch_roles.begin() + nbr, batch_roles.end(),
+                               [](const Role& x, const Role& y) { return x.proj < y.proj; });
+        }
+        singles = false;
+        // journal roles and saddle families
+        fam_pos.clear();
+        fam_local.clear();
+        for (size_t q = 0; q < batch_roles.size(); ++q) {
+          const Role& r = batch_roles[q];
           const uint32_t ridx = (uint32_t)o.roles.size();
-          o.jb.push_back({k, lev, ridx, 1, 0, 1});
-          o.roles.push_back({bidx, n + fi, 1});
-          const uint32_t a0 = arm_off[pos], a1 = arm_off[pos + 1];
-          const uint32_t fidx = (uint32_t)o.fam.size();
-          o.fam.push_back({fi, n + fi, ridx, bidx, k, a0, a1 - a0});
-          uint32_t car[4], dc[4];
-          int ndc = 0;
-          for (uint32_t a = a0; a < a1; ++a) {
+          o.roles.push_back({bidx, r.proj, r.role});
+          if (r.role == 0) {
+            ++jb.birth_roles;
+            continue;
+          }
+          ++jb.saddle_roles;
+          // arm seeds follow the rank partition: the family at position p owns seeds arm_off[p]..
+          fam_local.push_back((uint32_t)o.fam.size());
+          o.fam.push_back({r.fi, r.proj, ridx, bidx, k, arm_off[r.pos], arm_off[r.pos + 1] - arm_off[r.pos]});
+          fam_pos.push_back(r.pos);
+        }
+        jb.role_count = (uint32_t)batch_roles.size();
+        o.jb.push_back(jb);
+        // arms resolved against the pre-batch components
+        arms_b.clear();
+        arm_b_off.clear();
+        for (uint32_t q = 0; q < fam_pos.size(); ++q) {
+          const uint32_t fpos = fam_pos[q];
+          arm_b_off.push_back((uint32_t)arms_b.size());
+          for (uint64_t a = arm_off[fpos]; a < arm_off[fpos + 1]; ++a) {
+            // two-stage prefetch: the arm's record 64 arms ahead, its parent's 32 ahead
             if (a + 64 < arm_hi) __builtin_prefetch(&dsu[term[a + 64] < birth_count ? term[a + 64] : 0]);
             if (a + 32 < arm_hi && term[a + 32] < birth_count) __builtin_prefetch(&dsu[dsu[term[a + 32]].parent]);
             if (term[a] >= birth_count || !dsu[term[a]].order) {
@@ -1566,299 +1735,306 @@ int hier_run(Ctx& ctx, uint32_t K) {
               return;
             }
             const uint32_t c0 = find(term[a]);
-            car[a - a0] = c0;
-            int j = ndc;
-            bool dup = false;
-            for (int t = 0; t < ndc; ++t) dup |= dc[t] == c0;
-            if (!dup) {
-              while (j > 0 && dc[j - 1] > c0) { dc[j] = dc[j - 1]; --j; }
-              dc[j] = c0;
-              ++ndc;
+            arms_b.push_back({(uint32_t)a, c0, dsu[c0].rroot});
+          }
+        }
+        arm_b_off.push_back((uint32_t)arms_b.size());
+        // frozen-root quotient: transitive carrier classes, ordered by least carrier
+        plans.clear();
+        plan_car.clear();
+        plan_prior.clear();
+        plan_sad.clear();
+        if (!fam_pos.empty()) {
+          cars.clear();
+          for (const Arm& a : arms_b) cars.push_back(a.carrier);
+          std::sort(cars.begin(), cars.end());
+          cars.erase(std::unique(cars.begin(), cars.end()), cars.end());
+          const uint32_t nc = (uint32_t)cars.size();
+          auto qi = [&](uint32_t x) { return (uint32_t)(std::lower_bound(cars.begin(), cars.end(), x) - cars.begin()); };
+          qp.resize(nc);
+          std::iota(qp.begin(), qp.end(), 0u);
+          auto qf = [&](uint32_t x) {
+            while (qp[x] != x) x = qp[x] = qp[qp[x]];
+            return x;
+          };
+          for (uint32_t q = 0; q + 1 < arm_b_off.size(); ++q) {
+            const uint32_t a0 = qf(qi(arms_b[arm_b_off[q]].carrier));
+            for (uint32_t a = arm_b_off[q] + 1; a < arm_b_off[q + 1]; ++a) {
+              const uint32_t x = qf(a0), y = qf(qi(arms_b[a].carrier));
+              if (x != y) qp[std::max(x, y)] = std::min(x, y);
             }
           }
-          uint32_t pr[4];
-          int np = 0;
-          for (int t = 0; t < ndc; ++t)
-            if (dsu[dc[t]].rroot != kInvalid32) {
-              const uint32_t x = dsu[dc[t]].rroot;
-              int j = np++;
-              while (j > 0 && pr[j - 1] > x) { pr[j] = pr[j - 1]; --j; }
-              pr[j] = x;
+          plan_of.assign(nc, kInvalid32);
+          for (uint32_t i = 0; i < nc; ++i) {
+            const uint32_t r0 = qf(i);
+            if (plan_of[r0] == kInvalid32) {
+              plan_of[r0] = (uint32_t)plans.size();
+              plans.push_back({0, 0, 0, 0, 0, 0, 0, kInvalid32, 0});
             }
-          for (int t = 1; t < np; ++t)
-            if (pr[t] == pr[t - 1]) {
+          }
+          for (uint32_t i = 0; i < nc; ++i) {
+            Plan& p = plans[plan_of[qf(i)]];
+            ++p.c_cnt;
+            if (dsu[cars[i]].rroot != kInvalid32) ++p.p_cnt;
+          }
+          for (uint32_t q = 0; q + 1 < arm_b_off.size(); ++q) ++plans[plan_of[qf(qi(arms_b[arm_b_off[q]].carrier))]].s_cnt;
+          uint32_t co = 0, po = 0, so = 0;
+          for (Plan& p : plans) {
+            p.c_off = co; p.p_off = po; p.s_off = so;
+            co += p.c_cnt; po += p.p_cnt; so += p.s_cnt;
+            p.c_cnt = p.p_cnt = p.s_cnt = 0;
+          }
+          plan_car.resize(co);
+          plan_prior.resize(po);
+          plan_sad.resize(so);
+          for (uint32_t i = 0; i < nc; ++i) {
+            Plan& p = plans[plan_of[qf(i)]];
+            plan_car[p.c_off + p.c_cnt++] = cars[i];
+            if (dsu[cars[i]].rroot != kInvalid32) plan_prior[p.p_off + p.p_cnt++] = dsu[cars[i]].rroot;
+          }
+          for (uint32_t q = 0; q + 1 < arm_b_off.size(); ++q) {
+            Plan& p = plans[plan_of[qf(qi(arms_b[arm_b_off[q]].carrier))]];
+            plan_sad[p.s_off + p.s_cnt++] = q;
+          }
+          uint32_t pending = 0;
+          for (Plan& p : plans) {
+            uint32_t* pr = plan_prior.data() + p.p_off;
+            std::sort(pr, pr + p.p_cnt);
+            if (std::adjacent_find(pr, pr + p.p_cnt) != pr + p.p_cnt) {
               fail_o("a frozen carrier class repeats a reduced root");
               return;
             }
-          uint32_t kind, created = kInvalid32, result;
-          if (np == 1) {
-            kind = 1;
-            result = pr[0];
-          } else {
-            if (np == 0 && k == 1) {
-              fail_o("an order-one group has no root");
-              return;
+            if (p.p_cnt == 1) {
+              p.kind = 1;
+              p.created = kInvalid32;
+              p.result = pr[0];
+            } else {
+              if (p.p_cnt == 0 && k == 1) {
+                fail_o("an order-one group has no root");
+                return;
+              }
+              p.kind = p.p_cnt == 0 ? 0 : 2;
+              p.created = (uint32_t)o.nodes.size() + pending++;
+              p.result = p.created;
             }
-            kind = np == 0 ? 0 : 2;
-            created = (uint32_t)o.nodes.size();
-            result = created;
-          }
-          const uint32_t gidx = (uint32_t)o.groups.size(), sidx = (uint32_t)o.saddles.size();
-          const uint32_t bind0 = (uint32_t)o.bindings.size();
-          for (uint32_t a = a0; a < a1; ++a)
-            o.bindings.push_back({a, fidx, car[a - a0], dsu[car[a - a0]].rroot});
-          o.saddles.push_back({fidx, fi, bidx, bind0, a1 - a0, (uint32_t)ndc, (uint32_t)(ndc - np), (uint32_t)np, gidx});
-          const uint32_t ccnt = kind == 2 ? (uint32_t)np : 0u;
-          o.groups.push_back({bidx, sidx, 1, (uint32_t)ndc, (uint32_t)(ndc - np), (uint32_t)np,
-                              (uint32_t)o.children.size(), ccnt, created, result, kind});
-          if (kind != 1) o.nodes.push_back({k, lev, kind == 0 ? 1u : 2u, (uint32_t)o.children.size(), ccnt, kInvalid32, gidx});
-          if (kind == 2) o.children.insert(o.children.end(), pr, pr + np);
-          ehgp_forest_batch fb{k, lev, (uint32_t)o.births.size(), 0, sidx, 1, gidx, 1, (uint32_t)carriers,
-                               (uint32_t)reduced, 0, 0};
-          // commit: the distinct carriers are pre-batch roots; the least survives
-          for (int t = 1; t < ndc; ++t) dsu[dc[t]].parent = dc[0];
-          carriers -= (uint64_t)(ndc - 1);
-          dsu[dc[0]].rroot = result;
-          reduced = reduced - (uint64_t)np + 1;
-          fb.post_carriers = (uint32_t)carriers;
-          fb.post_roots = (uint32_t)reduced;
-          o.fb.push_back(fb);
-          ++si;
-          continue;
-        }
-      }
-      const uint32_t bidx = (uint32_t)o.jb.size();
-      ehgp_journal_batch jb{k, lev, (uint32_t)o.roles.size(), 0, 0, 0};
-      ehgp_forest_batch fb{};
-      fb.order = k;
-      fb.level_event = lev;
-      fb.pre_carriers = (uint32_t)carriers;
-      fb.pre_roots = (uint32_t)reduced;
-      batch_roles.clear();
-      if (singles) {
-        for (uint32_t p = 0; p < n; ++p) batch_roles.push_back({p, 0, kInvalid32, p});
-      } else {
-        while (bi < b_hi && cls_rp[bi] == cls) {
-          batch_roles.push_back({n + rank_order[bi], 0, rank_order[bi], (uint32_t)(bi - rb[2])});
-          ++bi;
-        }
-        const size_t nbr = batch_roles.size();
-        while (si < s_hi && cls_rp[si] == cls) {
-          batch_roles.push_back({n + rank_order[si], 1, rank_order[si], (uint32_t)(si - fam_lo)});
-          ++si;
-        }
-        if (nbr && nbr < batch_roles.size())
-          std::inplace_merge(batch_roles.begin(), batch_roles.begin() + nbr, batch_roles.end(),
-                             [](const Role& x, const Role& y) { return x.proj < y.proj; });
-      }
-      singles = false;
-      // journal roles and saddle families
-      fam_pos.clear();
-      fam_local.clear();
-      for (size_t q = 0; q < batch_roles.size(); ++q) {
-        const Role& r = batch_roles[q];
-        const uint32_t ridx = (uint32_t)o.roles.size();
-        o.roles.push_back({bidx, r.proj, r.role});
-        if (r.role == 0) {
-          ++jb.birth_roles;
-          continue;
-        }
-        ++jb.saddle_roles;
-        // arm seeds follow the rank partition: the family at position p owns seeds arm_off[p]..
-        fam_local.push_back((uint32_t)o.fam.size());
-        o.fam.push_back({r.fi, r.proj, ridx, bidx, k, arm_off[r.pos], arm_off[r.pos + 1] - arm_off[r.pos]});
-        fam_pos.push_back(r.pos);
-      }
-      jb.role_count = (uint32_t)batch_roles.size();
-      o.jb.push_back(jb);
-      // arms resolved against the pre-batch components
-      arms_b.clear();
-      arm_b_off.clear();
-      for (uint32_t q = 0; q < fam_pos.size(); ++q) {
-        const uint32_t fpos = fam_pos[q];
-        arm_b_off.push_back((uint32_t)arms_b.size());
-        for (uint64_t a = arm_off[fpos]; a < arm_off[fpos + 1]; ++a) {
-          // two-stage prefetch: the arm's record 64 arms ahead, its parent's 32 ahead
-          if (a + 64 < arm_hi) __builtin_prefetch(&dsu[term[a + 64] < birth_count ? term[a + 64] : 0]);
-          if (a + 32 < arm_hi && term[a + 32] < birth_count) __builtin_prefetch(&dsu[dsu[term[a + 32]].parent]);
-          if (term[a] >= birth_count || !dsu[term[a]].order) {
-            fail_o("a strict arm descended to a minimum that is not yet born");
-            return;
-          }
-          const uint32_t c0 = find(term[a]);
-          arms_b.push_back({(uint32_t)a, c0, dsu[c0].rroot});
-        }
-      }
-      arm_b_off.push_back((uint32_t)arms_b.size());
-      // frozen-root quotient: transitive carrier classes, ordered by least carrier
-      plans.clear();
-      plan_car.clear();
-      plan_prior.clear();
-      plan_sad.clear();
-      if (!fam_pos.empty()) {
-        cars.clear();
-        for (const Arm& a : arms_b) cars.push_back(a.carrier);
-        std::sort(cars.begin(), cars.end());
-        cars.erase(std::unique(cars.begin(), cars.end()), cars.end());
-        const uint32_t nc = (uint32_t)cars.size();
-        auto qi = [&](uint32_t x) { return (uint32_t)(std::lower_bound(cars.begin(), cars.end(), x) - cars.begin()); };
-        qp.resize(nc);
-        std::iota(qp.begin(), qp.end(), 0u);
-        auto qf = [&](uint32_t x) {
-          while (qp[x] != x) x = qp[x] = qp[qp[x]];
-          return x;
-        };
-        for (uint32_t q = 0; q + 1 < arm_b_off.size(); ++q) {
-          const uint32_t a0 = qf(qi(arms_b[arm_b_off[q]].carrier));
-          for (uint32_t a = arm_b_off[q] + 1; a < arm_b_off[q + 1]; ++a) {
-            const uint32_t x = qf(a0), y = qf(qi(arms_b[a].carrier));
-            if (x != y) qp[std::max(x, y)] = std::min(x, y);
           }
         }
-        plan_of.assign(nc, kInvalid32);
-        for (uint32_t i = 0; i < nc; ++i) {
-          const uint32_t r0 = qf(i);
-          if (plan_of[r0] == kInvalid32) {
-            plan_of[r0] = (uint32_t)plans.size();
-            plans.push_back({0, 0, 0, 0, 0, 0, 0, kInvalid32, 0});
-          }
-        }
-        for (uint32_t i = 0; i < nc; ++i) {
-          Plan& p = plans[plan_of[qf(i)]];
-          ++p.c_cnt;
-          if (dsu[cars[i]].rroot != kInvalid32) ++p.p_cnt;
-        }
-        for (uint32_t q = 0; q + 1 < arm_b_off.size(); ++q) ++plans[plan_of[qf(qi(arms_b[arm_b_off[q]].carrier))]].s_cnt;
-        uint32_t co = 0, po = 0, so = 0;
-        for (Plan& p : plans) {
-          p.c_off = co; p.p_off = po; p.s_off = so;
-          co += p.c_cnt; po += p.p_cnt; so += p.s_cnt;
-          p.c_cnt = p.p_cnt = p.s_cnt = 0;
-        }
-        plan_car.resize(co);
-        plan_prior.resize(po);
-        plan_sad.resize(so);
-        for (uint32_t i = 0; i < nc; ++i) {
-          Plan& p = plans[plan_of[qf(i)]];
-          plan_car[p.c_off + p.c_cnt++] = cars[i];
-          if (dsu[cars[i]].rroot != kInvalid32) plan_prior[p.p_off + p.p_cnt++] = dsu[cars[i]].rroot;
-        }
-        for (uint32_t q = 0; q + 1 < arm_b_off.size(); ++q) {
-          Plan& p = plans[plan_of[qf(qi(arms_b[arm_b_off[q]].carrier))]];
-          plan_sad[p.s_off + p.s_cnt++] = q;
-        }
-        uint32_t pending = 0;
-        for (Plan& p : plans) {
-          uint32_t* pr = plan_prior.data() + p.p_off;
-          std::sort(pr, pr + p.p_cnt);
-          if (std::adjacent_find(pr, pr + p.p_cnt) != pr + p.p_cnt) {
-            fail_o("a frozen carrier class repeats a reduced root");
-            return;
-          }
-          if (p.p_cnt == 1) {
-            p.kind = 1;
-            p.created = kInvalid32;
-            p.result = pr[0];
-          } else {
-            if (p.p_cnt == 0 && k == 1) {
-              fail_o("an order-one group has no root");
-              return;
+        fb.saddle_offset = (uint32_t)o.saddles.size();
+        fb.group_offset = (uint32_t)o.groups.size();
+        gnodes.clear();
+        for (const Plan& p : plans) {
+          const uint32_t g_soff = (uint32_t)o.saddles.size();
+          const uint32_t gidx = (uint32_t)o.groups.size();
+          for (uint32_t t = 0; t < p.s_cnt; ++t) {
+            const uint32_t q = plan_sad[p.s_off + t];
+            const uint32_t fidx = fam_local[q];
+            const uint32_t arm_o = (uint32_t)o.bindings.size();
+            tmp.clear();
+            uint32_t nprior = 0;
+            for (uint32_t a = arm_b_off[q]; a < arm_b_off[q + 1]; ++a) {
+              const Arm& am = arms_b[a];
+              o.bindings.push_back({am.seed, fidx, am.carrier, am.prior});
+              tmp.push_back(am.carrier);
             }
-            p.kind = p.p_cnt == 0 ? 0 : 2;
-            p.created = (uint32_t)o.nodes.size() + pending++;
-            p.result = p.created;
+            std::sort(tmp.begin(), tmp.end());
+            tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+            for (uint32_t c0 : tmp) nprior += dsu[c0].rroot != kInvalid32;  // carriers are pre-batch roots
+            o.saddles.push_back({fidx, o.fam[fidx].event, bidx, arm_o, arm_b_off[q + 1] - arm_b_off[q],
+                                 (uint32_t)tmp.size(), (uint32_t)tmp.size() - nprior, nprior, gidx});
           }
+          const uint32_t ccnt = p.kind == 2 ? p.p_cnt : 0u;
+          o.groups.push_back({bidx, g_soff, (uint32_t)o.saddles.size() - g_soff, p.c_cnt, p.c_cnt - p.p_cnt, p.p_cnt,
+                              (uint32_t)o.children.size(), ccnt, p.created, p.result, p.kind});
+          if (p.kind != 1)
+            gnodes.push_back({k, lev, p.kind == 0 ? 1u : 2u, (uint32_t)o.children.size(), ccnt, kInvalid32, gidx});
+          if (p.kind == 2)
+            o.children.append(plan_prior.begin() + p.p_off, plan_prior.begin() + p.p_off + p.p_cnt);
         }
-      }
-      fb.saddle_offset = (uint32_t)o.saddles.size();
-      fb.group_offset = (uint32_t)o.groups.size();
-      gnodes.clear();
-      for (const Plan& p : plans) {
-        const uint32_t g_soff = (uint32_t)o.saddles.size();
-        const uint32_t gidx = (uint32_t)o.groups.size();
-        for (uint32_t t = 0; t < p.s_cnt; ++t) {
-          const uint32_t q = plan_sad[p.s_off + t];
-          const uint32_t fidx = fam_local[q];
-          const uint32_t arm_o = (uint32_t)o.bindings.size();
-          tmp.clear();
-          uint32_t nprior = 0;
-          for (uint32_t a = arm_b_off[q]; a < arm_b_off[q + 1]; ++a) {
-            const Arm& am = arms_b[a];
-            o.bindings.push_back({am.seed, fidx, am.carrier, am.prior});
-            tmp.push_back(am.carrier);
+        o.nodes.append(gnodes.begin(), gnodes.end());
+        // births of this batch (hidden from this batch's arms); handles are global
+        fb.birth_offset = (uint32_t)o.births.size();
+        new_births.clear();
+        for (const Role& r : batch_roles) {
+          if (r.role != 0) continue;
+          const uint32_t handle = k == 1 ? r.proj : n + r.pos;
+          uint32_t node = kInvalid32;
+          if (k == 1) {
+            node = (uint32_t)o.nodes.size();
+            o.nodes.push_back({1, kInvalid32, 0, (uint32_t)o.children.size(), 0, handle, kInvalid32});
           }
-          std::sort(tmp.begin(), tmp.end());
-          tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
-          for (uint32_t c0 : tmp) nprior += dsu[c0].rroot != kInvalid32;  // carriers are pre-batch roots
-          o.saddles.push_back({fidx, o.fam[fidx].event, bidx, arm_o, arm_b_off[q + 1] - arm_b_off[q],
-                               (uint32_t)tmp.size(), (uint32_t)tmp.size() - nprior, nprior, gidx});
+          o.births.push_back({r.proj, bidx, k, handle, node});
+          new_births.push_back(handle);
         }
-        const uint32_t ccnt = p.kind == 2 ? p.p_cnt : 0u;
-        o.groups.push_back({bidx, g_soff, (uint32_t)o.saddles.size() - g_soff, p.c_cnt, p.c_cnt - p.p_cnt, p.p_cnt,
-                            (uint32_t)o.children.size(), ccnt, p.created, p.result, p.kind});
-        if (p.kind != 1)
-          gnodes.push_back({k, lev, p.kind == 0 ? 1u : 2u, (uint32_t)o.children.size(), ccnt, kInvalid32, gidx});
-        if (p.kind == 2)
-          o.children.insert(o.children.end(), plan_prior.begin() + p.p_off, plan_prior.begin() + p.p_off + p.p_cnt);
-      }
-      o.nodes.insert(o.nodes.end(), gnodes.begin(), gnodes.end());
-      // births of this batch (hidden from this batch's arms); handles are global
-      fb.birth_offset = (uint32_t)o.births.size();
-      new_births.clear();
-      for (const Role& r : batch_roles) {
-        if (r.role != 0) continue;
-        const uint32_t handle = k == 1 ? r.proj : n + r.pos;
-        uint32_t node = kInvalid32;
-        if (k == 1) {
-          node = (uint32_t)o.nodes.size();
-          o.nodes.push_back({1, kInvalid32, 0, (uint32_t)o.children.size(), 0, handle, kInvalid32});
+        // commit: unions (least handle survives), reduced roots, then births
+        for (const Plan& p : plans) {
+          uint32_t r0 = find(plan_car[p.c_off]);
+          uint32_t had_reduced = dsu[r0].rroot != kInvalid32;
+          for (uint32_t i = 1; i < p.c_cnt; ++i) {
+            const uint32_t r1 = find(plan_car[p.c_off + i]);
+            if (r1 == r0) continue;
+            had_reduced += dsu[r1].rroot != kInvalid32;
+            const uint32_t lo = std::min(r0, r1), hi = std::max(r0, r1);
+            dsu[hi].parent = lo;
+            r0 = lo;
+            --carriers;
+          }
+          dsu[r0].rroot = p.result;
+          reduced = reduced - had_reduced + 1;
         }
-        o.births.push_back({r.proj, bidx, k, handle, node});
-        new_births.push_back(handle);
-      }
-      // commit: unions (least handle survives), reduced roots, then births
-      for (const Plan& p : plans) {
-        uint32_t r0 = find(plan_car[p.c_off]);
-        uint32_t had_reduced = dsu[r0].rroot != kInvalid32;
-        for (uint32_t i = 1; i < p.c_cnt; ++i) {
-          const uint32_t r1 = find(plan_car[p.c_off + i]);
-          if (r1 == r0) continue;
-          had_reduced += dsu[r1].rroot != kInvalid32;
-          const uint32_t lo = std::min(r0, r1), hi = std::max(r0, r1);
-          dsu[hi].parent = lo;
-          r0 = lo;
-          --carriers;
+        for (size_t t = 0; t < new_births.size(); ++t) {
+          const uint32_t hnd = new_births[t];
+          dsu[hnd].order = k;
+          dsu[hnd].rroot = k == 1 ? o.births[fb.birth_offset + t].order_one_node : kInvalid32;
+          ++carriers;
+          if (k == 1) ++reduced;
         }
-        dsu[r0].rroot = p.result;
-        reduced = reduced - had_reduced + 1;
+        fb.birth_count = (uint32_t)new_births.size();
+        fb.saddle_count = (uint32_t)o.saddles.size() - fb.saddle_offset;
+        fb.group_count = (uint32_t)o.groups.size() - fb.group_offset;
+        fb.post_carriers = (uint32_t)carriers;
+        fb.post_roots = (uint32_t)reduced;
+        o.fb.push_back(fb);
+        c.jb = (uint32_t)o.jb.n; c.role = (uint32_t)o.roles.n; c.birth = (uint32_t)o.births.n;
+        c.sad = (uint32_t)o.saddles.n; c.grp = (uint32_t)o.groups.n; c.node = (uint32_t)o.nodes.n;
+        c.child = (uint32_t)o.children.n;
+        reopen();
       }
-      for (size_t t = 0; t < new_births.size(); ++t) {
-        const uint32_t hnd = new_births[t];
-        dsu[hnd].order = k;
-        dsu[hnd].rroot = k == 1 ? o.births[fb.birth_offset + t].order_one_node : kInvalid32;
-        ++carriers;
-        if (k == 1) ++reduced;
-      }
-      fb.birth_count = (uint32_t)new_births.size();
-      fb.saddle_count = (uint32_t)o.saddles.size() - fb.saddle_offset;
-      fb.group_count = (uint32_t)o.groups.size() - fb.group_offset;
-      fb.post_carriers = (uint32_t)carriers;
-      fb.post_roots = (uint32_t)reduced;
-      o.fb.push_back(fb);
+    };
+    core();
+    if (o.status == EHGP_OK) {
+      close_chunk();
+      o.jb.n = c.jb; o.fb.n = c.jb; o.roles.n = c.role; o.fam.n = fams_k; o.births.n = c.birth; o.bindings.n = arms_k;
+      o.saddles.n = c.sad; o.groups.n = c.grp; o.nodes.n = c.node; o.children.n = c.child;
+      if (!o.jb.fits() || !o.roles.fits() || !o.nodes.fits() || !o.children.fits() || !o.groups.fits() ||
+          !o.saddles.fits() || !o.births.fits() || !o.fb.fits() || !o.fam.fits() || !o.bindings.fits())
+        fail_o("internal: a forest arena bound was exceeded");
     }
-    // final roots of this order (local node ids)
-    const uint64_t h_lo = k == 1 ? 0 : n + (rb[k] - rb[2]), h_hi = k == 1 ? n : n + (rb[k + 1] - rb[2]);
-    for (uint64_t hnd = h_lo; hnd < h_hi; ++hnd)
-      if (dsu[hnd].order && dsu[hnd].parent == hnd && dsu[hnd].rroot != kInvalid32)
-        o.roots.push_back({k, (uint32_t)hnd, dsu[hnd].rroot});
-    std::sort(o.roots.begin(), o.roots.end(),
-              [](const ehgp_forest_root& x, const ehgp_forest_root& y) { return x.node < y.node; });
+    if (o.status == EHGP_OK) {
+      // final roots of this order (local node ids)
+      const uint64_t h_lo = k == 1 ? 0 : n + (rb[k] - rb[2]), h_hi = k == 1 ? n : n + (rb[k + 1] - rb[2]);
+      for (uint64_t hnd = h_lo; hnd < h_hi; ++hnd)
+        if (dsu[hnd].order && dsu[hnd].parent == hnd && dsu[hnd].rroot != kInvalid32)
+          o.roots.push_back({k, (uint32_t)hnd, dsu[hnd].rroot});
+      std::sort(o.roots.begin(), o.roots.end(),
+                [](const ehgp_forest_root& x, const ehgp_forest_root& y) { return x.node < y.node; });
+    }
     o.ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - to0).count();
+    pg.done.store(1, std::memory_order_release);
+  };
+  // Rebuilds the records of one published chunk of single-role batches.
+  auto replay = [&](uint32_t k, uint32_t j) {
+    HierOrderOut& o = outs[k];
+    Progress& pg = prog[k];
+    Cnt c = pg.blocks[j / kSnapBlock][j % kSnapBlock];
+    uint64_t b_lo, b_hi, s_lo, s_hi, arm_lo, arm_hi;
+    order_range(k, b_lo, b_hi, s_lo, s_hi, arm_lo, arm_hi);
+    (void)b_lo;
+    (void)arm_hi;
+    for (uint32_t t = 0; t < c.count; ++t) {
+      const uint32_t cls_b = c.bi < b_hi ? cls_rp[c.bi] : kInvalid32;
+      const uint32_t cls_s = c.si < s_hi ? cls_rp[c.si] : kInvalid32;
+      const uint32_t cls = std::min(cls_b, cls_s);
+      const uint32_t lev = cls_b <= cls_s ? rank_order[c.bi] : rank_order[c.si];
+      const bool one_b = cls_b == cls && !(c.bi + 1 < b_hi && cls_rp[c.bi + 1] == cls) && cls_s != cls;
+      const bool one_s = cls_s == cls && !(c.si + 1 < s_hi && cls_rp[c.si + 1] == cls) && cls_b != cls;
+      const uint32_t bidx = c.jb;
+      if (one_b) {
+        const uint32_t pos = (uint32_t)(c.bi - rb[2]), fi = rank_order[c.bi];
+        o.jb[bidx] = {k, lev, c.role, 1, 1, 0};
+        o.roles[c.role] = {bidx, n + fi, 0};
+        o.births[c.birth] = {n + fi, bidx, k, n + pos, kInvalid32};
+        o.fb[bidx] = {k, lev, c.birth, 1, c.sad, 0, c.grp, 0, (uint32_t)c.carriers, (uint32_t)c.reduced,
+                      (uint32_t)(c.carriers + 1), (uint32_t)c.reduced};
+        ++c.carriers;
+        ++c.jb; ++c.role; ++c.birth;
+        ++c.bi;
+        continue;
+      }
+      if (!one_s) {
+        pg.bad.store(1);
+        return;
+      }
+      const uint32_t pos = (uint32_t)(c.si - fam_lo), fi = rank_order[c.si], fidx = (uint32_t)(c.si - s_lo);
+      const uint32_t a0 = arm_off[pos], a1 = arm_off[pos + 1];
+      const uint32_t ridx = c.role;
+      o.jb[bidx] = {k, lev, ridx, 1, 0, 1};
+      o.roles[ridx] = {bidx, n + fi, 1};
+      o.fam[fidx] = {fi, n + fi, ridx, bidx, k, a0, a1 - a0};
+      uint32_t dc[4], pr[4];
+      int ndc = 0, np = 0;
+      for (uint32_t a = a0; a < a1; ++a) {
+        const ehgp_forest_binding& bd = o.bindings[a - arm_lo];
+        bool dup = false;
+        for (int q = 0; q < ndc; ++q) dup |= dc[q] == bd.carrier;
+        if (dup) continue;
+        dc[ndc++] = bd.carrier;
+        if (bd.prior_root != kInvalid32) {
+          int q = np++;
+          while (q > 0 && pr[q - 1] > bd.prior_root) { pr[q] = pr[q - 1]; --q; }
+          pr[q] = bd.prior_root;
+        }
+      }
+      const uint32_t kind = np == 1 ? 1u : np == 0 ? 0u : 2u;
+      const uint32_t created = kind == 1 ? kInvalid32 : c.node;
+      const uint32_t result = kind == 1 ? pr[0] : created;
+      const uint32_t ccnt = kind == 2 ? (uint32_t)np : 0u;
+      o.saddles[c.sad] = {fidx, fi, bidx, a0 - (uint32_t)arm_lo, a1 - a0, (uint32_t)ndc, (uint32_t)(ndc - np),
+                          (uint32_t)np, c.grp};
+      o.groups[c.grp] = {bidx, c.sad, 1, (uint32_t)ndc, (uint32_t)(ndc - np), (uint32_t)np, c.child, ccnt, created,
+                         result, kind};
+      if (kind != 1) o.nodes[c.node++] = {k, lev, kind == 0 ? 1u : 2u, c.child, ccnt, kInvalid32, c.grp};
+      for (uint32_t q = 0; q < ccnt; ++q) o.children[c.child + q] = pr[q];
+      c.child += ccnt;
+      o.fb[bidx] = {k, lev, c.birth, 0, c.sad, 1, c.grp, 1, (uint32_t)c.carriers, (uint32_t)c.reduced,
+                    (uint32_t)(c.carriers - (uint64_t)(ndc - 1)), (uint32_t)(c.reduced - (uint64_t)np + 1)};
+      c.carriers -= (uint64_t)(ndc - 1);
+      c.reduced = c.reduced - (uint64_t)np + 1;
+      ++c.jb; ++c.role; ++c.sad; ++c.grp;
+      ++c.si;
+    }
+  };
+  // claims and replays published chunks, highest order first, until every core is done
+  // and every chunk is claimed
+  auto work = [&] {
+    for (;;) {
+      bool did = false, all = true;
+      for (uint32_t k = keff; k >= 1; --k) {
+        Progress& pg = prog[k];
+        const int done = pg.done.load(std::memory_order_acquire);
+        const uint32_t pub = pg.published.load(std::memory_order_acquire);
+        uint32_t cl = pg.claimed.load(std::memory_order_relaxed);
+        while (cl < pub) {
+          if (pg.claimed.compare_exchange_weak(cl, cl + 1)) {
+            replay(k, cl);  // published chunks are complete even when the core stops later
+            did = true;
+            break;
+          }
+        }
+        if (!done || pg.claimed.load(std::memory_order_relaxed) < pg.published.load(std::memory_order_acquire))
+          all = false;
+        if (did) break;
+      }
+      if (did) continue;
+      if (all) return;
+      std::this_thread::yield();
+    }
   };
   {
+    const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint32_t extra = hw > keff ? std::min(hw - keff, 32u) : 0u;
     std::vector<std::thread> pool;
-    for (uint32_t k = 1; k <= keff; ++k) pool.emplace_back(run_order, k, std::ref(outs[k]));
+    for (uint32_t k = 1; k <= keff; ++k)
+      pool.emplace_back([&, k] {
+        run_core(k, outs[k]);
+        work();
+      });
+    for (uint32_t i = 0; i < extra; ++i) pool.emplace_back(work);
     for (auto& t : pool) t.join();
+    for (uint32_t k = 1; k <= keff; ++k)
+      if (outs[k].status == EHGP_OK && prog[k].bad.load()) {
+        outs[k].status = EHGP_ERR_DEGENERATE;
+        outs[k].msg = "internal: a forest chunk replay disagrees with its core";
+      }
   }
   const auto t_orders = std::chrono::steady_clock::now();
   for (uint32_t k = 1; k <= keff; ++k)
