@@ -1012,6 +1012,8 @@ struct HierOrderOut {  // one order's journal and forest arenas, local indices
   Arena<ehgp_forest_group> groups;
   Arena<ehgp_forest_batch> fb;
   Arena<ehgp_forest_root> roots;
+  Arena<uint32_t> node_cls;  // level class of each node (kInvalid32: an order-one birth node)
+  Arena<uint32_t> fam_res;   // resulting root of each family's atomic group (local node id)
   int status = EHGP_OK;
   const char* msg = "";
   double ms = 0;
@@ -1083,9 +1085,6 @@ struct HierState {
   std::vector<HierOff> off;
   uint64_t arm_seeds = 0;  // p_removed holds the removed point of each arm seed
   std::vector<std::vector<ehgp_vertical_assignment>> vert;  // per source order, global node ids
-  std::vector<uint32_t> evfam;                              // saddle event -> family (local to its order)
-  std::vector<std::vector<uint32_t>> sad_of_fam;            // per order: family -> saddle (local)
-  std::vector<uint32_t> h_class;  // level class by facade index
   uint32_t decision = EHGP_ERR_NOT_BUILT;
   double ms_device = 0, ms_forest = 0, ms_descent = 0, ms_orders = 0;
   double ms_host[4] = {0, 0, 0, 0};  // union-find init, order passes, concatenation, vertical maps
@@ -1491,8 +1490,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
   const auto t1 = std::chrono::steady_clock::now();
   const uint64_t birth_count = n + nb_higher;
   // union-find state packed per birth handle: one cache line touch per arm
-  h.dsu.resize(birth_count);
-  for (uint64_t i = 0; i < birth_count; ++i) h.dsu[i] = {(uint32_t)i, kInvalid32, 0};
+  h.dsu.resize(birth_count);  // each order initialises its own handle range
   HierDsu* dsu = h.dsu.data();
   // per-order arenas and union-find state persist across calls (no page faults when warm)
   if (h.outs.size() < keff + 1) h.outs.resize(keff + 1);
@@ -1546,6 +1544,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
     uint64_t b_lo, b_hi, s_lo, s_hi, arm_lo, arm_hi;
     order_range(k, b_lo, b_hi, s_lo, s_hi, arm_lo, arm_hi);
     const uint64_t births_k = k == 1 ? n : b_hi - b_lo, fams_k = s_hi - s_lo, arms_k = arm_hi - arm_lo;
+    const uint64_t h_lo = k == 1 ? 0 : n + (rb[k] - rb[2]), h_hi = h_lo + births_k;  // this order's handles
     // capacities are upper bounds (one batch holds at least one role; a group at least one
     // saddle; a multifusion's children are distinct prior roots of its arms' carriers)
     o.jb.reset(births_k + fams_k);
@@ -1559,6 +1558,10 @@ int hier_run(Ctx& ctx, uint32_t K) {
     o.nodes.reset((k == 1 ? n : 0) + fams_k);
     o.children.reset(arms_k);
     o.roots.reset(births_k);
+    o.node_cls.reset((k == 1 ? n : 0) + fams_k);
+    o.fam_res.reset(fams_k);
+    // this order's union-find handles
+    for (uint64_t i = h_lo; i < h_hi; ++i) dsu[i] = {(uint32_t)i, kInvalid32, 0};
     pg.blocks.clear();
     pg.blocks.resize((births_k + fams_k) / kSnapBlock + 2);  // chunks <= batches / kChunkBatches + multi-role batches + 1
     Cnt c{b_lo, s_lo, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -1625,8 +1628,8 @@ int hier_run(Ctx& ctx, uint32_t K) {
             for (uint32_t a = a0; a < a1; ++a) {
               // two-stage prefetch: the arm's record 64 arms ahead, its parent's 32 ahead
               if (a + 64 < arm_hi) __builtin_prefetch(&dsu[term[a + 64] < birth_count ? term[a + 64] : 0]);
-              if (a + 32 < arm_hi && term[a + 32] < birth_count) __builtin_prefetch(&dsu[dsu[term[a + 32]].parent]);
-              if (term[a] >= birth_count || !dsu[term[a]].order) {
+              if (a + 32 < arm_hi && term[a + 32] >= h_lo && term[a + 32] < h_hi) __builtin_prefetch(&dsu[dsu[term[a + 32]].parent]);
+              if (term[a] < h_lo || term[a] >= h_hi || !dsu[term[a]].order) {
                 fail_o("a strict arm descended to a minimum that is not yet born");
                 return;
               }
@@ -1729,8 +1732,8 @@ int hier_run(Ctx& ctx, uint32_t K) {
           for (uint64_t a = arm_off[fpos]; a < arm_off[fpos + 1]; ++a) {
             // two-stage prefetch: the arm's record 64 arms ahead, its parent's 32 ahead
             if (a + 64 < arm_hi) __builtin_prefetch(&dsu[term[a + 64] < birth_count ? term[a + 64] : 0]);
-            if (a + 32 < arm_hi && term[a + 32] < birth_count) __builtin_prefetch(&dsu[dsu[term[a + 32]].parent]);
-            if (term[a] >= birth_count || !dsu[term[a]].order) {
+            if (a + 32 < arm_hi && term[a + 32] >= h_lo && term[a + 32] < h_hi) __builtin_prefetch(&dsu[dsu[term[a + 32]].parent]);
+            if (term[a] < h_lo || term[a] >= h_hi || !dsu[term[a]].order) {
               fail_o("a strict arm descended to a minimum that is not yet born");
               return;
             }
@@ -1894,6 +1897,10 @@ int hier_run(Ctx& ctx, uint32_t K) {
         fb.post_carriers = (uint32_t)carriers;
         fb.post_roots = (uint32_t)reduced;
         o.fb.push_back(fb);
+        for (uint64_t i = c.node; i < o.nodes.n && i < o.nodes.cap; ++i)
+          o.node_cls[i] = o.nodes[i].level_event == kInvalid32 ? kInvalid32 : cls;
+        for (uint64_t sd = c.sad; sd < o.saddles.n && sd < o.saddles.cap; ++sd)
+          o.fam_res[o.saddles[sd].family] = o.groups[o.saddles[sd].group].result_node;
         c.jb = (uint32_t)o.jb.n; c.role = (uint32_t)o.roles.n; c.birth = (uint32_t)o.births.n;
         c.sad = (uint32_t)o.saddles.n; c.grp = (uint32_t)o.groups.n; c.node = (uint32_t)o.nodes.n;
         c.child = (uint32_t)o.children.n;
@@ -1911,7 +1918,6 @@ int hier_run(Ctx& ctx, uint32_t K) {
     }
     if (o.status == EHGP_OK) {
       // final roots of this order (local node ids)
-      const uint64_t h_lo = k == 1 ? 0 : n + (rb[k] - rb[2]), h_hi = k == 1 ? n : n + (rb[k + 1] - rb[2]);
       for (uint64_t hnd = h_lo; hnd < h_hi; ++hnd)
         if (dsu[hnd].order && dsu[hnd].parent == hnd && dsu[hnd].rroot != kInvalid32)
           o.roots.push_back({k, (uint32_t)hnd, dsu[hnd].rroot});
@@ -1982,7 +1988,11 @@ int hier_run(Ctx& ctx, uint32_t K) {
                           (uint32_t)np, c.grp};
       o.groups[c.grp] = {bidx, c.sad, 1, (uint32_t)ndc, (uint32_t)(ndc - np), (uint32_t)np, c.child, ccnt, created,
                          result, kind};
-      if (kind != 1) o.nodes[c.node++] = {k, lev, kind == 0 ? 1u : 2u, c.child, ccnt, kInvalid32, c.grp};
+      o.fam_res[fidx] = result;
+      if (kind != 1) {
+        o.node_cls[c.node] = cls;
+        o.nodes[c.node++] = {k, lev, kind == 0 ? 1u : 2u, c.child, ccnt, kInvalid32, c.grp};
+      }
       for (uint32_t q = 0; q < ccnt; ++q) o.children[c.child + q] = pr[q];
       c.child += ccnt;
       o.fb[bidx] = {k, lev, c.birth, 0, c.sad, 1, c.grp, 1, (uint32_t)c.carriers, (uint32_t)c.reduced,
@@ -2060,35 +2070,9 @@ int hier_run(Ctx& ctx, uint32_t K) {
   // group's resulting root (level <= a) is climbed through multifusion parents of level <= a
   // (the contract serializer's assignment, reference/morsehgp3d_oracle/serialization.py:1040-1099).
   {
-    h.h_class.resize(m);
-    if (m && (e = cudaMemcpyAsync(h.h_class.data(), h.lclass, (uint64_t)m * 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-      return abi_cuda_fail(&ctx, e, "level classes");
-    // event -> family and family -> saddle, local to each order (one host thread per order)
-    h.evfam.resize(m);
-    if (h.sad_of_fam.size() < keff + 1) h.sad_of_fam.resize(keff + 1);
-    {
-      std::vector<std::thread> pool;
-      const uint32_t nt = keff;
-      for (uint32_t k = 1; k <= keff; ++k)
-        pool.emplace_back([&, k] {
-          const uint64_t lo = (uint64_t)m * (k - 1) / nt, hi = (uint64_t)m * k / nt;
-          std::fill(h.evfam.begin() + lo, h.evfam.begin() + hi, kInvalid32);
-        });
-      for (auto& t : pool) t.join();
-      pool.clear();
-      for (uint32_t k = 1; k <= keff; ++k)
-        pool.emplace_back([&, k] {
-          const HierOrderOut& o = outs[k];
-          for (uint64_t f = 0; f < o.fam.size(); ++f) h.evfam[o.fam[f].event] = (uint32_t)f;
-          std::vector<uint32_t>& sof = h.sad_of_fam[k];
-          sof.assign(o.fam.size(), kInvalid32);
-          for (uint64_t sd = 0; sd < o.saddles.size(); ++sd) sof[o.saddles[sd].family] = (uint32_t)sd;
-        });
-      for (auto& t : pool) t.join();
-    }
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "level classes");
-    auto cls = [&](const ehgp_forest_node& nd) -> int64_t {
-      return nd.level_event == kInvalid32 ? -1 : (int64_t)h.h_class[nd.level_event];
+    auto cls = [](const HierOrderOut& o, uint32_t node) -> int64_t {
+      const uint32_t c = o.node_cls[node];
+      return c == kInvalid32 ? -1 : (int64_t)c;
     };
     if (h.vert.size() < keff + 1) h.vert.resize(keff + 1);
     std::vector<int> vstat(keff + 1, EHGP_OK);
@@ -2098,7 +2082,6 @@ int hier_run(Ctx& ctx, uint32_t K) {
     auto run_v = [&](uint32_t k) {
       const HierOrderOut& src = outs[k];
       const HierOrderOut& tgt = outs[k - 1];
-      const std::vector<uint32_t>& sof = h.sad_of_fam[k - 1];
       std::vector<ehgp_vertical_assignment>& vo = h.vert[k];
       vo.clear();
       const uint64_t h_lo = n + (rb[k] - rb[2]);  // first birth handle of order k
@@ -2117,23 +2100,20 @@ int hier_run(Ctx& ctx, uint32_t K) {
         const ehgp_forest_node& nd = src.nodes[i];
         const ehgp_forest_group& g = src.groups[nd.atomic_group];
         const uint64_t carrier = src.bindings[src.saddles[g.saddle_offset].arm_offset].carrier;
-        if (carrier < h_lo || carrier - h_lo >= src.births.size()) {
+        // the carrier's birth (rank k) and its saddle family of order k - 1 share the rank
+        // segment position, so both have the local index carrier - h_lo
+        const uint64_t f = carrier - h_lo;
+        if (carrier < h_lo || f >= tgt.fam.size()) {
           vstat[k] = EHGP_ERR_DEGENERATE;
           return;
         }
-        const uint32_t proj = src.births[carrier - h_lo].projection;
-        const uint32_t f = proj >= n && proj - n < m ? h.evfam[proj - n] : kInvalid32;
-        if (f == kInvalid32 || f >= tgt.fam.size() || tgt.fam[f].event != proj - n || sof[f] == kInvalid32) {
+        const uint32_t R = tgt.fam_res[f];
+        const int64_t lev = cls(src, (uint32_t)i);
+        if (R >= t_n || cls(tgt, R) > lev) {
           vstat[k] = EHGP_ERR_DEGENERATE;
           return;
         }
-        const uint32_t R = tgt.groups[tgt.saddles[sof[f]].group].result_node;
-        const int64_t lev = cls(nd);
-        if (R >= t_n || cls(tgt.nodes[R]) > lev) {
-          vstat[k] = EHGP_ERR_DEGENERATE;
-          return;
-        }
-        while (sweep < t_n && cls(tgt.nodes[sweep]) <= lev) {
+        while (sweep < t_n && cls(tgt, sweep) <= lev) {
           const ehgp_forest_node& p = tgt.nodes[sweep];
           if (p.kind == 2)
             for (uint32_t c = 0; c < p.child_count; ++c) up[find_up(tgt.children[p.child_offset + c])] = sweep;
