@@ -360,6 +360,26 @@ __global__ void k_uncertain(uint32_t m, const double* __restrict__ pre_hi, const
   if (at < cap) list[at] = p;
 }
 
+__global__ void k_iota(uint32_t m, uint32_t* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) out[i] = i;
+}
+
+// Gathers the facade records of the uncertain runs (host tie resolution) and scatters
+// them back with their exact-equality flags.
+__global__ void k_run_gather(uint32_t cnt, const uint32_t* __restrict__ idx, const EvRec* __restrict__ ev,
+                             EvRec* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < cnt) out[i] = ev[idx[i]];
+}
+__global__ void k_run_scatter(uint32_t cnt, const uint32_t* __restrict__ idx, const EvRec* __restrict__ in,
+                              const uint8_t* __restrict__ eq, EvRec* __restrict__ ev, uint8_t* __restrict__ eqprev) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= cnt) return;
+  ev[idx[i]] = in[i];
+  eqprev[idx[i]] = eq[i];
+}
+
 // ---- 2. level classes, rank partition, births -----------------------------------
 __global__ void k_level_class(uint32_t m, const uint8_t* __restrict__ eqprev, uint32_t* __restrict__ flag) {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -933,23 +953,27 @@ k_arm_step(DescentParams d, uint32_t m, const uint32_t* __restrict__ in_arm, con
     k += F[j] != kInvalid32;
   }
   const Cloud c{d.px, d.py, d.pz, d.S};
+  auto fail = [&](int why) {  // stats[3] counts failed arms
+    status[a] = (uint8_t)why;
+    atomicAdd(stats + 3, 1ull);
+  };
   Mini mb;
-  if (!facet_miniball(c, F, k, mb)) { status[a] = kArmInternal; return; }
+  if (!facet_miniball(c, F, k, mb)) { fail(kArmInternal); return; }
   uint32_t G[kMaxFacet];
   int cut_below = 0;
   const int s = topk_choice(d, c, mb, k, G, &cut_below);
-  if (s != kArmOk) { status[a] = (uint8_t)s; return; }
+  if (s != kArmOk) { fail(s); return; }
   bool same = true;
   for (int j = 0; j < k; ++j) same &= G[j] == F[j];
-  if (same) { status[a] = kArmUnresolved; return; }
+  if (same) { fail(kArmUnresolved); return; }
   if (!cut_below) {  // beta(G) <= cutoff = beta(F): the decrease must be strict
     slow(6);
     Mini mg;
-    if (!facet_miniball(c, G, k, mg)) { status[a] = kArmInternal; return; }
+    if (!facet_miniball(c, G, k, mg)) { fail(kArmInternal); return; }
     double glo, ghi, flo, fhi;
     if (!flevel(mg.fs, glo, ghi)) exact_level_fp(c, mg.T, mg.ts, glo, ghi);
     if (!flevel(mb.fs, flo, fhi)) exact_level_fp(c, mb.T, mb.ts, flo, fhi);
-    if (!(ghi < flo) && level_cmp_exact(c, mg.T, mg.ts, mb.T, mb.ts) >= 0) { status[a] = kArmPlateau; return; }
+    if (!(ghi < flo) && level_cmp_exact(c, mg.T, mg.ts, mb.T, mb.ts) >= 0) { fail(kArmPlateau); return; }
     atomicAdd(stats + 2, 1ull);
   }
   atomicAdd(stats, 1ull);
@@ -1071,7 +1095,6 @@ struct HierState {
   uint32_t* p_rank = nullptr;
   uint32_t* p_cls = nullptr;
   uint32_t* p_armoff = nullptr;
-  uint32_t* p_removed = nullptr;
   uint32_t* p_term = nullptr;
   uint8_t* p_stat = nullptr;
   uint32_t* d_cls_rp = nullptr;       // device views (event capacity)
@@ -1083,11 +1106,11 @@ struct HierState {
   // offsets of order k's records, off[keff + 1] the totals.  Records take their global
   // indices when they are copied out.  An empty `off` means no result.
   std::vector<HierOff> off;
-  uint64_t arm_seeds = 0;  // p_removed holds the removed point of each arm seed
+  uint64_t arm_seeds = 0;  // d_removed holds the removed point of each arm seed
   std::vector<std::vector<ehgp_vertical_assignment>> vert;  // per source order, global node ids
   uint32_t decision = EHGP_ERR_NOT_BUILT;
   double ms_device = 0, ms_forest = 0, ms_descent = 0, ms_orders = 0;
-  double ms_host[4] = {0, 0, 0, 0};  // union-find init, order passes, concatenation, vertical maps
+  double ms_host[4] = {0, 0, 0, 0};  // exact facade ties, order passes, (unused), vertical maps
   uint64_t descent_steps = 0, arms = 0, exact_boundaries = 0;
 };
 
@@ -1098,7 +1121,7 @@ void hier_free(Ctx& ctx) {
                   (void*)ctx.hier->q_fac[1]})
     if (p) cudaFree(p);
   for (void* p : {(void*)ctx.hier->p_rank, (void*)ctx.hier->p_cls, (void*)ctx.hier->p_armoff,
-                  (void*)ctx.hier->p_removed, (void*)ctx.hier->p_term, (void*)ctx.hier->p_stat})
+                  (void*)ctx.hier->p_term, (void*)ctx.hier->p_stat})
     if (p) cudaFreeHost(p);
   delete ctx.hier;
   ctx.hier = nullptr;
@@ -1259,12 +1282,8 @@ int hier_run(Ctx& ctx, uint32_t K) {
   // facade order by the FP64 level midpoints (diagnostics sort last)
   RadixScratch rs{h.radix_counts, ctx.radix.state, (uint32_t)((h.cap_events + kRadixTile - 1) / kRadixTile)};
   if (total) {
-    {
-      std::vector<uint32_t> iota(total);
-      std::iota(iota.begin(), iota.end(), 0u);
-      cudaMemcpyAsync(h.order0, iota.data(), total * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
-      cudaStreamSynchronize(st);
-    }
+    k_iota<<<nblk(total, kT), kT, 0, st>>>((uint32_t)total, h.order0);
+    ++launches;
     const IndirectKey stages[1] = {{h.key, 0}};
     const int bits[1] = {64};
     const int passes = radix_sort_indirect(st, (uint32_t)total, h.order0, h.order1, stages, bits, 1, rs, &launches);
@@ -1293,29 +1312,65 @@ int hier_run(Ctx& ctx, uint32_t K) {
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "hierarchy facade order");
   h.S = scale_h[0];
   if (unc > (1u << 20)) return abi_fail(&ctx, EHGP_ERR_CAPACITY, "too many uncertain level boundaries in the facade");
+  double ms_ties = 0;
   if (unc) {
+    const auto tt0 = std::chrono::steady_clock::now();
     std::vector<uint32_t> list(unc);
     cudaMemcpy(list.data(), h.uncertain, unc * sizeof(uint32_t), cudaMemcpyDeviceToHost);
     std::sort(list.begin(), list.end());
-    const Cloud hc_cloud{h.h_px.data(), h.h_py.data(), h.h_pz.data(), h.S};
-    HostCmp cmp{&hc_cloud};
-    std::vector<uint8_t> eq;
+    // maximal runs of positions whose order the FP64 intervals leave open: a run starts one
+    // before its first uncertain boundary (that boundary before it is certain)
+    struct Run {
+      uint32_t off, len;
+    };
+    std::vector<Run> runs;
+    std::vector<uint32_t> idx;
     for (size_t i = 0; i < list.size();) {
       const uint32_t s0 = list[i] - 1;
       uint32_t s1 = list[i];
       size_t j = i + 1;
       while (j < list.size() && list[j] == s1 + 1) s1 = list[j++];
-      const uint32_t len = s1 - s0 + 1;
-      std::vector<EvRec> run(len);
-      cudaMemcpy(run.data(), h.ev + s0, len * sizeof(EvRec), cudaMemcpyDeviceToHost);
-      std::sort(run.begin(), run.end(), [&](const EvRec& a, const EvRec& b2) { return cmp.less(a, b2, nullptr); });
-      eq.assign(len, 0);
-      for (uint32_t t = 1; t < len; ++t)
-        eq[t] = level_cmp_exact(hc_cloud, run[t - 1].ids, (int)run[t - 1].size, run[t].ids, (int)run[t].size) == 0;
-      cudaMemcpy(h.ev + s0, run.data(), len * sizeof(EvRec), cudaMemcpyHostToDevice);
-      cudaMemcpy(h.eqprev + s0, eq.data(), len, cudaMemcpyHostToDevice);
+      runs.push_back({(uint32_t)idx.size(), s1 - s0 + 1});
+      for (uint32_t t = s0; t <= s1; ++t) idx.push_back(t);
       i = j;
     }
+    // one gather, exact sorts of the runs on the host cores, one scatter (scratch: order0,
+    // order1 and ev_raw are free between the facade gather and the level classes)
+    const uint32_t cnt = (uint32_t)idx.size();
+    std::vector<EvRec> recs(cnt);
+    std::vector<uint8_t> eq(cnt, 0);
+    cudaMemcpyAsync(h.order1, idx.data(), (uint64_t)cnt * 4, cudaMemcpyHostToDevice, st);
+    k_run_gather<<<nblk(cnt, kT), kT, 0, st>>>(cnt, h.order1, h.ev, h.ev_raw);
+    cudaMemcpyAsync(recs.data(), h.ev_raw, (uint64_t)cnt * sizeof(EvRec), cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "facade tie runs");
+    const Cloud hc_cloud{h.h_px.data(), h.h_py.data(), h.h_pz.data(), h.S};
+    const HostCmp cmp{&hc_cloud};
+    std::atomic<size_t> next{0};
+    auto sort_runs = [&] {
+      for (size_t r; (r = next.fetch_add(1)) < runs.size();) {
+        EvRec* run = recs.data() + runs[r].off;
+        const uint32_t len = runs[r].len;
+        std::sort(run, run + len, [&](const EvRec& x, const EvRec& y) { return cmp.less(x, y, nullptr); });
+        for (uint32_t t = 1; t < len; ++t)
+          eq[runs[r].off + t] =
+              level_cmp_exact(hc_cloud, run[t - 1].ids, (int)run[t - 1].size, run[t].ids, (int)run[t].size) == 0;
+      }
+    };
+    {
+      const uint32_t hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+      const uint32_t nt = (uint32_t)std::min<size_t>(hw, runs.size());
+      std::vector<std::thread> pool;
+      for (uint32_t i = 1; i < nt; ++i) pool.emplace_back(sort_runs);
+      sort_runs();
+      for (auto& t : pool) t.join();
+    }
+    uint8_t* d_eq = reinterpret_cast<uint8_t*>(h.order0);
+    cudaMemcpyAsync(h.ev_raw, recs.data(), (uint64_t)cnt * sizeof(EvRec), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_eq, eq.data(), cnt, cudaMemcpyHostToDevice, st);
+    k_run_scatter<<<nblk(cnt, kT), kT, 0, st>>>(cnt, h.order1, h.ev_raw, d_eq, h.ev, h.eqprev);
+    launches += 2;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "facade tie runs");
+    ms_ties = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tt0).count();
   }
   // level classes
   if (m) {
@@ -1380,15 +1435,14 @@ int hier_run(Ctx& ctx, uint32_t K) {
   if (narms > h.cap_arms) return abi_fail(&ctx, EHGP_ERR_CAPACITY, "strict arms exceed the hierarchy buffers");
   // pinned host views
   if (h.pin_m < m + 1 || h.pin_arms < narms + 1) {
-    for (void* p : {(void*)h.p_rank, (void*)h.p_cls, (void*)h.p_armoff, (void*)h.p_removed, (void*)h.p_term,
-                    (void*)h.p_stat})
+    for (void* p : {(void*)h.p_rank, (void*)h.p_cls, (void*)h.p_armoff, (void*)h.p_term, (void*)h.p_stat})
       if (p) cudaFreeHost(p);
-    h.p_rank = h.p_cls = h.p_armoff = h.p_removed = h.p_term = nullptr;
+    h.p_rank = h.p_cls = h.p_armoff = h.p_term = nullptr;
     h.p_stat = nullptr;
     const uint64_t pm = (m + 1) + (m + 1) / 8, pa = (narms + 1) + (narms + 1) / 8;
     if (cudaMallocHost(&h.p_rank, pm * 4) != cudaSuccess || cudaMallocHost(&h.p_cls, pm * 4) != cudaSuccess ||
-        cudaMallocHost(&h.p_armoff, pm * 4) != cudaSuccess || cudaMallocHost(&h.p_removed, pa * 4) != cudaSuccess ||
-        cudaMallocHost(&h.p_term, pa * 4) != cudaSuccess || cudaMallocHost(&h.p_stat, pa) != cudaSuccess) {
+        cudaMallocHost(&h.p_armoff, pm * 4) != cudaSuccess || cudaMallocHost(&h.p_term, pa * 4) != cudaSuccess ||
+        cudaMallocHost(&h.p_stat, pa) != cudaSuccess) {
       h.pin_m = h.pin_arms = 0;
       return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "pinned host buffers for the hierarchy");
     }
@@ -1409,7 +1463,6 @@ int hier_run(Ctx& ctx, uint32_t K) {
     k_arm_expand<<<nblk(nfam, kT), kT, 0, st>>>((uint32_t)nfam, (uint32_t)fam_lo, h.rank_order, h.ev, h.d_armoff,
                                                h.arm_family, h.arm_local, h.d_removed);
     ++launches;
-    cudaMemcpyAsync(h.p_removed, h.d_removed, narms * 4, cudaMemcpyDeviceToHost, st);
     DescentParams dp{n, 2 * n - 2, g.tnodes, b.px, b.py, b.pz, h.S, h.slots, (uint32_t)(h.cap_slots - 1), h.bfac,
                      (uint32_t)nb_higher};
     cudaEventRecord(ctx.evk0, st);
@@ -1451,12 +1504,11 @@ int hier_run(Ctx& ctx, uint32_t K) {
     h.descent_rounds = rounds;
     cudaEventRecord(ctx.evk1, st);
     cudaMemcpyAsync(h.p_term, h.term, narms * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(h.p_stat, h.arm_status, narms, cudaMemcpyDeviceToHost, st);
   }
   uint32_t herr = 0;
-  unsigned long long dsteps = 0;
+  unsigned long long dst[4] = {0, 0, 0, 0};
   cudaMemcpyAsync(&herr, h.counters + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(&dsteps, h.dstats, sizeof(dsteps), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(dst, h.dstats, sizeof(dst), cudaMemcpyDeviceToHost, st);
   cudaMemcpyFromSymbolAsync(h.slow, g_descent_slow, sizeof(h.slow), 0, cudaMemcpyDeviceToHost, st);
   cudaEventRecord(ctx.ev1, st);
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "strict-arm descent");
@@ -1470,11 +1522,13 @@ int hier_run(Ctx& ctx, uint32_t K) {
       h.ms_descent = ms;
     }
   }
-  h.descent_steps = dsteps;
+  h.descent_steps = dst[0];
   h.arms = narms;
   h.exact_boundaries = unc;
   if (herr) return abi_fail(&ctx, EHGP_ERR_CAPACITY, "the birth facet table is full");
-  for (uint64_t a = 0; a < narms; ++a) {
+  if (dst[3] && (e = cudaMemcpy(h.p_stat, h.arm_status, narms, cudaMemcpyDeviceToHost)) != cudaSuccess)
+    return abi_cuda_fail(&ctx, e, "strict-arm status");
+  for (uint64_t a = 0; dst[3] && a < narms; ++a) {
     if (astat[a] == kArmOk) continue;
     static const char* msg[] = {"", "a strict arm descent is unresolved", "a strict arm descent met a plateau",
                                 "a strict arm descent exceeded its ball-query capacity",
@@ -2138,7 +2192,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
   h.ms_forest = std::chrono::duration<double, std::milli>(t2 - t1).count();
   {
     using msd = std::chrono::duration<double, std::milli>;
-    h.ms_host[0] = msd(t_init - t1).count();
+    h.ms_host[0] = ms_ties;
     h.ms_host[1] = msd(t_orders - t_init).count();
     h.ms_host[2] = msd(t_merge - t_orders).count();
     h.ms_host[3] = msd(t2 - t_merge).count();
@@ -2210,6 +2264,10 @@ int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out) {
     if (e != cudaSuccess) return ehgp::abi_cuda_fail(ctx, e, "facade copy");
   }
   if (h.off.empty()) return EHGP_OK;
+  if (out->arm_removed && h.arm_seeds) {
+    const cudaError_t e = cudaMemcpy(out->arm_removed, h.d_removed, h.arm_seeds * 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return ehgp::abi_cuda_fail(ctx, e, "arm seed copy");
+  }
   // Each order's arenas go to their global offsets with local indices shifted, in chunks
   // spread over the host cores.
   using ehgp::HierOff;
@@ -2298,7 +2356,6 @@ int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out) {
       add(out->vertical, v.size(), [&v, f, out](uint64_t i) { out->vertical[f.vert + i] = v[i]; });
     }
   }
-  add(out->arm_removed, h.arm_seeds, [&h, out](uint64_t i) { out->arm_removed[i] = h.p_removed[i]; });
   if (!tasks.empty()) {
     const uint32_t hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
     const uint32_t nt = (uint32_t)std::min<uint64_t>(hw, tasks.size());

@@ -436,7 +436,7 @@ class Context:
         st = np.zeros(13, np.uint64)
         self._check(self.lib.ehgp_hier_stats(self._h, _ptr(ms), _ptr(st)))
         return {"device_ms": ms[0], "descent_ms": ms[1], "forest_ms": ms[2], "slowest_order_ms": ms[3],
-                "host_init_ms": ms[4], "host_orders_ms": ms[5], "host_concat_ms": ms[6], "host_vertical_ms": ms[7],
+                "facade_ties_ms": ms[4], "host_orders_ms": ms[5], "host_offsets_ms": ms[6], "host_vertical_ms": ms[7],
                 "order_ms": [float(x) for x in ms[8:] if x > 0],
                 "arms": int(st[0]),
                 "descent_steps": int(st[1]), "exact_boundaries": int(st[2]), "events": int(st[3]),

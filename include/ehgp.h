@@ -395,9 +395,10 @@ int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out);
 
 /* Timing of the last ehgp_hierarchy call: ms[0] device stages (CUDA events),
  * ms[1] the strict-arm descent kernels, ms[2] the host forest pass, ms[3] its
- * slowest order (orders run on parallel host threads), ms[4..7] the host pass
- * split into union-find set-up, the order passes, concatenation of the order
- * arenas and the vertical maps, ms[8 + k - 1] the pass of order k (k <= 16,
+ * slowest order (orders run on parallel host threads), ms[4] the host's exact
+ * ordering of uncertain facade boundaries, ms[5..7] the host forest pass split
+ * into the order passes, the record offsets and the vertical maps,
+ * ms[8 + k - 1] the union-find core of order k (k <= 16,
  * zero above the last order); ms holds 24 doubles;
  * stats[0] strict arms, [1] descent steps, [2] facade boundaries settled
  * exactly on the host, [3] facade events, [4] arms that are not themselves a
