@@ -918,12 +918,14 @@ __device__ __forceinline__ int arm_facet(const EvRec& e, uint32_t removed, uint3
 
 // First probe of every arm: most arms are themselves a birth facet of their order.
 // Misses are queued with their facet for the descent steps.
-__global__ void k_arm_probe(DescentParams d, uint32_t narms, const uint32_t* __restrict__ fam_event /* rank_order + fam_lo */,
+__global__ void k_arm_probe(DescentParams d, uint32_t a0, uint32_t narms,
+                            const uint32_t* __restrict__ fam_event /* rank_order + fam_lo */,
                             const uint32_t* __restrict__ arm_family, const uint8_t* __restrict__ arm_local,
                             const EvRec* __restrict__ ev, uint32_t* __restrict__ term, uint8_t* __restrict__ status,
                             uint32_t* __restrict__ q_arm, uint32_t* __restrict__ q_fac, uint32_t* __restrict__ q_count) {
-  const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= narms) return;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= narms) return;
+  const uint32_t a = a0 + i;
   const EvRec e = ev[fam_event[arm_family[a]]];
   uint32_t F[kMaxFacet + 1];
   const int k = arm_facet(e, e.ids[arm_local[a]], F);
@@ -1463,13 +1465,16 @@ int hier_run(Ctx& ctx, uint32_t K) {
     k_arm_expand<<<nblk(nfam, kT), kT, 0, st>>>((uint32_t)nfam, (uint32_t)fam_lo, h.rank_order, h.ev, h.d_armoff,
                                                h.arm_family, h.arm_local, h.d_removed);
     ++launches;
-    DescentParams dp{n, 2 * n - 2, g.tnodes, b.px, b.py, b.pz, h.S, h.slots, (uint32_t)(h.cap_slots - 1), h.bfac,
-                     (uint32_t)nb_higher};
-    cudaEventRecord(ctx.evk0, st);
-    // first probe; misses queue for descent steps (queue buffers sized by the misses)
+  }
+  // the facade, rank partition, births and arm seeds are complete: the descent runs order
+  // by order below, overlapped with the host forest pass
+  uint32_t herr = 0;
+  cudaMemcpyAsync(&herr, h.counters + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "strict-arm seeds");
+  if (herr) return abi_fail(&ctx, EHGP_ERR_CAPACITY, "the birth facet table is full");
+  if (narms) {
     if (!h.qcount && (e = halloc(h, &h.qcount, 4)) != cudaSuccess)
       return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "descent queue");
-    cudaMemsetAsync(h.qcount, 0, 4 * sizeof(uint32_t), st);
     if (h.q_cap < narms) {  // worst case: every arm misses
       for (void* p : {(void*)h.q_arm[0], (void*)h.q_arm[1], (void*)h.q_fac[0], (void*)h.q_fac[1]})
         if (p) cudaFree(p);
@@ -1481,66 +1486,13 @@ int hier_run(Ctx& ctx, uint32_t K) {
         return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "descent queue buffers do not fit the device");
       h.q_cap = qc;
     }
-    k_arm_probe<<<nblk(narms, kT), kT, 0, st>>>(dp, (uint32_t)narms, h.rank_order + fam_lo, h.arm_family, h.arm_local, h.ev,
-                                                h.term, h.arm_status, h.q_arm[0], h.q_fac[0], h.qcount);
-    ++launches;
-    uint32_t pending = 0;
-    cudaMemcpyAsync(&pending, h.qcount, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "strict-arm probe");
-    h.first_misses = pending;
-    int cur = 0;
-    uint32_t rounds = 0;
-    while (pending) {
-      if (++rounds > (uint32_t)kDescentSteps) return abi_fail(&ctx, EHGP_ERR_DEGENERATE, "a strict arm descent exceeded its step budget");
-      uint32_t* oc = h.qcount + 1 + (1 - cur);
-      cudaMemsetAsync(oc, 0, sizeof(uint32_t), st);
-      k_arm_step<<<nblk(pending, 128), 128, 0, st>>>(dp, pending, h.q_arm[cur], h.q_fac[cur], h.q_arm[1 - cur],
-                                                     h.q_fac[1 - cur], oc, h.term, h.arm_status, h.dstats);
-      ++launches;
-      cudaMemcpyAsync(&pending, oc, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-      if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "strict-arm descent step");
-      cur = 1 - cur;
-    }
-    h.descent_rounds = rounds;
-    cudaEventRecord(ctx.evk1, st);
-    cudaMemcpyAsync(h.p_term, h.term, narms * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
   }
-  uint32_t herr = 0;
-  unsigned long long dst[4] = {0, 0, 0, 0};
-  cudaMemcpyAsync(&herr, h.counters + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(dst, h.dstats, sizeof(dst), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyFromSymbolAsync(h.slow, g_descent_slow, sizeof(h.slow), 0, cudaMemcpyDeviceToHost, st);
-  cudaEventRecord(ctx.ev1, st);
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "strict-arm descent");
-  {
-    float ms = 0;
-    cudaEventElapsedTime(&ms, ctx.ev0, ctx.ev1);
-    h.ms_device = ms;
-    if (narms) {
-      cudaEventElapsedTime(&ms, ctx.evk0, ctx.evk1);
-      ctx.kernel_ms = ms;
-      h.ms_descent = ms;
-    }
-  }
-  h.descent_steps = dst[0];
   h.arms = narms;
   h.exact_boundaries = unc;
-  if (herr) return abi_fail(&ctx, EHGP_ERR_CAPACITY, "the birth facet table is full");
-  if (dst[3] && (e = cudaMemcpy(h.p_stat, h.arm_status, narms, cudaMemcpyDeviceToHost)) != cudaSuccess)
-    return abi_cuda_fail(&ctx, e, "strict-arm status");
-  for (uint64_t a = 0; dst[3] && a < narms; ++a) {
-    if (astat[a] == kArmOk) continue;
-    static const char* msg[] = {"", "a strict arm descent is unresolved", "a strict arm descent met a plateau",
-                                "a strict arm descent exceeded its ball-query capacity",
-                                "a strict arm descent exceeded its step budget",
-                                "a strict arm descent found no consistent exact miniball or top-k"};
-    h.decision = astat[a] == kArmCapacity ? EHGP_ERR_CAPACITY : EHGP_ERR_DEGENERATE;
-    return abi_fail(&ctx, (int)h.decision, msg[astat[a] < 6 ? astat[a] : 5]);
-  }
   // ---- host: journal, seeds and the forest journal ------------------------------------
   // Orders are independent (their handles, components and nodes never meet), so each
-  // order runs on its own host thread with local indices; the arenas are then
-  // concatenated in order with the offsets the reference's single pass would give.
+  // order runs on its own host thread with local indices; records take the global offsets
+  // the reference's single pass would give when they are copied out.
   const auto t1 = std::chrono::steady_clock::now();
   const uint64_t birth_count = n + nb_higher;
   // union-find state packed per birth handle: one cache line touch per arm
@@ -2083,22 +2035,129 @@ int hier_run(Ctx& ctx, uint32_t K) {
       std::this_thread::yield();
     }
   };
+  // The strict-arm descent runs order by order, highest first, on this thread; an order's
+  // union-find core starts as soon as its terminal handles are on the host, while the
+  // device descends the lower orders.  ready[k]: 0 waiting, 1 go, 2 stopped.
+  std::unique_ptr<std::atomic<int>[]> ready(new std::atomic<int>[keff + 1]);
+  for (uint32_t k = 0; k <= keff; ++k) ready[k].store(0);
+  int dstatus = EHGP_OK;
+  const char* dmsg = "";
+  cudaError_t dcuda = cudaSuccess;
   {
     const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
     const uint32_t extra = hw > keff ? std::min(hw - keff, 32u) : 0u;
     std::vector<std::thread> pool;
     for (uint32_t k = 1; k <= keff; ++k)
       pool.emplace_back([&, k] {
-        run_core(k, outs[k]);
+        int r;
+        while ((r = ready[k].load(std::memory_order_acquire)) == 0) std::this_thread::sleep_for(std::chrono::microseconds(20));
+        if (r == 1) {
+          run_core(k, outs[k]);
+        } else {
+          outs[k].status = EHGP_ERR_DEGENERATE;
+          outs[k].msg = "the strict-arm descent stopped";
+          prog[k].done.store(1, std::memory_order_release);
+        }
         work();
       });
     for (uint32_t i = 0; i < extra; ++i) pool.emplace_back(work);
-    for (auto& t : pool) t.join();
-    for (uint32_t k = 1; k <= keff; ++k)
-      if (outs[k].status == EHGP_OK && prog[k].bad.load()) {
-        outs[k].status = EHGP_ERR_DEGENERATE;
-        outs[k].msg = "internal: a forest chunk replay disagrees with its core";
+    // descent, order by order
+    const DescentParams dp{n, 2 * n - 2, g.tnodes, b.px, b.py, b.pz, h.S, h.slots, (uint32_t)(h.cap_slots - 1), h.bfac,
+                           (uint32_t)nb_higher};
+    uint32_t misses = 0, max_rounds = 0;
+    unsigned long long failed_before = 0;
+    h.descent_steps = 0;
+    cudaEventRecord(ctx.evk0, st);
+    uint32_t k = keff;
+    auto stop = [&](int status, const char* msg) {
+      dstatus = status;
+      dmsg = msg;
+    };
+    for (; k >= 1 && dstatus == EHGP_OK; --k) {
+      const uint64_t s_lo = rb[k + 1], s_hi = rb[k + 2 > 16 ? 16 : k + 2];
+      const uint32_t a_lo = s_hi > s_lo ? arm_off[s_lo - fam_lo] : 0, a_hi = s_hi > s_lo ? arm_off[s_hi - fam_lo] : 0;
+      if (a_hi > a_lo) {
+        const uint32_t na = a_hi - a_lo;
+        cudaMemsetAsync(h.qcount, 0, 4 * sizeof(uint32_t), st);
+        k_arm_probe<<<nblk(na, kT), kT, 0, st>>>(dp, a_lo, na, h.rank_order + fam_lo, h.arm_family, h.arm_local, h.ev,
+                                                 h.term, h.arm_status, h.q_arm[0], h.q_fac[0], h.qcount);
+        ++launches;
+        uint32_t pending = 0;
+        cudaMemcpyAsync(&pending, h.qcount, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if ((dcuda = cudaStreamSynchronize(st)) != cudaSuccess) break;
+        misses += pending;
+        int cur = 0;
+        uint32_t rounds = 0;
+        while (pending) {
+          if (++rounds > (uint32_t)kDescentSteps) {
+            stop(EHGP_ERR_DEGENERATE, "a strict arm descent exceeded its step budget");
+            break;
+          }
+          uint32_t* oc = h.qcount + 1 + (1 - cur);
+          cudaMemsetAsync(oc, 0, sizeof(uint32_t), st);
+          k_arm_step<<<nblk(pending, 128), 128, 0, st>>>(dp, pending, h.q_arm[cur], h.q_fac[cur], h.q_arm[1 - cur],
+                                                         h.q_fac[1 - cur], oc, h.term, h.arm_status, h.dstats);
+          ++launches;
+          cudaMemcpyAsync(&pending, oc, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+          if ((dcuda = cudaStreamSynchronize(st)) != cudaSuccess) break;
+          cur = 1 - cur;
+        }
+        if (dcuda != cudaSuccess || dstatus != EHGP_OK) break;
+        max_rounds = std::max(max_rounds, rounds);
+        unsigned long long dst[4] = {0, 0, 0, 0};
+        cudaMemcpyAsync(h.p_term + a_lo, h.term + a_lo, (uint64_t)na * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(dst, h.dstats, sizeof(dst), cudaMemcpyDeviceToHost, st);
+        if ((dcuda = cudaStreamSynchronize(st)) != cudaSuccess) break;
+        h.descent_steps = dst[0];
+        if (dst[3] > failed_before) {  // an arm of this order failed: report the first one
+          failed_before = dst[3];
+          if ((dcuda = cudaMemcpy(h.p_stat + a_lo, h.arm_status + a_lo, na, cudaMemcpyDeviceToHost)) != cudaSuccess) break;
+          static const char* msg[] = {"", "a strict arm descent is unresolved", "a strict arm descent met a plateau",
+                                      "a strict arm descent exceeded its ball-query capacity",
+                                      "a strict arm descent exceeded its step budget",
+                                      "a strict arm descent found no consistent exact miniball or top-k"};
+          for (uint32_t a = a_lo; a < a_hi; ++a)
+            if (astat[a] != kArmOk) {
+              stop(astat[a] == kArmCapacity ? EHGP_ERR_CAPACITY : EHGP_ERR_DEGENERATE, msg[astat[a] < 6 ? astat[a] : 5]);
+              break;
+            }
+          if (dstatus != EHGP_OK) break;
+        }
       }
+      ready[k].store(1, std::memory_order_release);
+    }
+    // orders left waiting after a failure stop without running
+    for (uint32_t j = 1; j <= keff; ++j) {
+      int expect = 0;
+      ready[j].compare_exchange_strong(expect, 2);
+    }
+    cudaEventRecord(ctx.evk1, st);
+    cudaMemcpyFromSymbolAsync(h.slow, g_descent_slow, sizeof(h.slow), 0, cudaMemcpyDeviceToHost, st);
+    cudaEventRecord(ctx.ev1, st);
+    if (dcuda == cudaSuccess) dcuda = cudaStreamSynchronize(st);
+    h.first_misses = misses;
+    h.descent_rounds = max_rounds;
+    for (auto& t : pool) t.join();
+    for (uint32_t j = 1; j <= keff; ++j)
+      if (outs[j].status == EHGP_OK && prog[j].bad.load()) {
+        outs[j].status = EHGP_ERR_DEGENERATE;
+        outs[j].msg = "internal: a forest chunk replay disagrees with its core";
+      }
+  }
+  if (dcuda != cudaSuccess) return abi_cuda_fail(&ctx, dcuda, "strict-arm descent");
+  {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx.ev0, ctx.ev1);
+    h.ms_device = ms;
+    if (narms) {
+      cudaEventElapsedTime(&ms, ctx.evk0, ctx.evk1);
+      ctx.kernel_ms = ms;
+      h.ms_descent = ms;
+    }
+  }
+  if (dstatus != EHGP_OK) {
+    h.decision = (uint32_t)dstatus;
+    return abi_fail(&ctx, dstatus, dmsg);
   }
   const auto t_orders = std::chrono::steady_clock::now();
   for (uint32_t k = 1; k <= keff; ++k)
