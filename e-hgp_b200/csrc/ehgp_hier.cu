@@ -45,6 +45,8 @@
 #include <thread>
 #include <vector>
 
+#include <sys/mman.h>
+
 namespace ehgp {
 
 struct HierState;
@@ -992,8 +994,36 @@ k_arm_step(DescentParams d, uint32_t m, const uint32_t* __restrict__ in_arm, con
 }  // namespace
 
 // ---- host state ---------------------------------------------------------------------
+constexpr uint32_t kUnborn = 0xFFFFFFFEu;  // HierDsu::rroot of a handle not yet born
+
 struct HierDsu {
-  uint32_t parent, rroot, order;  // order 0: not yet born
+  uint32_t parent, rroot;  // rroot: the component's reduced root (at roots), kUnborn before the birth
+};
+
+// Anonymous mapping advised for transparent huge pages: the union-find array is read at
+// random, and 2 MB pages keep its translations in the TLB.  Capacity is kept across calls.
+struct HugeBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  HugeBuf() = default;
+  HugeBuf(const HugeBuf&) = delete;
+  HugeBuf& operator=(const HugeBuf&) = delete;
+  ~HugeBuf() {
+    if (p) munmap(p, bytes);
+  }
+  bool ensure(size_t need) {
+    if (need <= bytes) return true;
+    if (p) munmap(p, bytes);
+    p = nullptr;
+    bytes = 0;
+    const size_t align = size_t{2} << 20, b = (need + align - 1) / align * align;
+    void* q = mmap(nullptr, b, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+    if (q == MAP_FAILED) return false;
+    madvise(q, b, MADV_HUGEPAGE);
+    p = q;
+    bytes = b;
+    return true;
+  }
 };
 
 // Growable storage of plain C records that keeps its capacity across calls and leaves new
@@ -1092,7 +1122,7 @@ struct HierState {
   int S = 0;
   uint64_t events = 0, diagnostics = 0;
   std::vector<HierOrderOut> outs;     // per-order arenas (capacity kept across calls)
-  std::vector<HierDsu> dsu;
+  HugeBuf dsu;
   uint64_t pin_m = 0, pin_arms = 0;   // pinned host views of the last call
   uint32_t* p_rank = nullptr;
   uint32_t* p_cls = nullptr;
@@ -1496,8 +1526,9 @@ int hier_run(Ctx& ctx, uint32_t K) {
   const auto t1 = std::chrono::steady_clock::now();
   const uint64_t birth_count = n + nb_higher;
   // union-find state packed per birth handle: one cache line touch per arm
-  h.dsu.resize(birth_count);  // each order initialises its own handle range
-  HierDsu* dsu = h.dsu.data();
+  if (!h.dsu.ensure(birth_count * sizeof(HierDsu)))  // each order initialises its own handle range
+    return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "the union-find array does not fit host memory");
+  HierDsu* dsu = static_cast<HierDsu*>(h.dsu.p);
   // per-order arenas and union-find state persist across calls (no page faults when warm)
   if (h.outs.size() < keff + 1) h.outs.resize(keff + 1);
   auto& outs = h.outs;
@@ -1567,7 +1598,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
     o.node_cls.reset((k == 1 ? n : 0) + fams_k);
     o.fam_res.reset(fams_k);
     // this order's union-find handles
-    for (uint64_t i = h_lo; i < h_hi; ++i) dsu[i] = {(uint32_t)i, kInvalid32, 0};
+    for (uint64_t i = h_lo; i < h_hi; ++i) dsu[i] = {(uint32_t)i, kUnborn};
     pg.blocks.clear();
     pg.blocks.resize((births_k + fams_k) / kSnapBlock + 2);  // chunks <= batches / kChunkBatches + multi-role batches + 1
     Cnt c{b_lo, s_lo, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -1618,7 +1649,6 @@ int hier_run(Ctx& ctx, uint32_t K) {
           const bool one_s = cls_s == cls && !(si + 1 < s_hi && cls_rp[si + 1] == cls) && cls_b != cls;
           if (one_b) {
             const uint32_t handle = n + (uint32_t)(bi - rb[2]);
-            dsu[handle].order = k;
             dsu[handle].rroot = kInvalid32;
             ++carriers;
             ++c.jb; ++c.role; ++c.birth;
@@ -1635,7 +1665,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
               // two-stage prefetch: the arm's record 64 arms ahead, its parent's 32 ahead
               if (a + 64 < arm_hi) __builtin_prefetch(&dsu[term[a + 64] < birth_count ? term[a + 64] : 0]);
               if (a + 32 < arm_hi && term[a + 32] >= h_lo && term[a + 32] < h_hi) __builtin_prefetch(&dsu[dsu[term[a + 32]].parent]);
-              if (term[a] < h_lo || term[a] >= h_hi || !dsu[term[a]].order) {
+              if (term[a] < h_lo || term[a] >= h_hi || dsu[term[a]].rroot == kUnborn) {
                 fail_o("a strict arm descended to a minimum that is not yet born");
                 return;
               }
@@ -1739,7 +1769,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
             // two-stage prefetch: the arm's record 64 arms ahead, its parent's 32 ahead
             if (a + 64 < arm_hi) __builtin_prefetch(&dsu[term[a + 64] < birth_count ? term[a + 64] : 0]);
             if (a + 32 < arm_hi && term[a + 32] >= h_lo && term[a + 32] < h_hi) __builtin_prefetch(&dsu[dsu[term[a + 32]].parent]);
-            if (term[a] < h_lo || term[a] >= h_hi || !dsu[term[a]].order) {
+            if (term[a] < h_lo || term[a] >= h_hi || dsu[term[a]].rroot == kUnborn) {
               fail_o("a strict arm descended to a minimum that is not yet born");
               return;
             }
@@ -1892,7 +1922,6 @@ int hier_run(Ctx& ctx, uint32_t K) {
         }
         for (size_t t = 0; t < new_births.size(); ++t) {
           const uint32_t hnd = new_births[t];
-          dsu[hnd].order = k;
           dsu[hnd].rroot = k == 1 ? o.births[fb.birth_offset + t].order_one_node : kInvalid32;
           ++carriers;
           if (k == 1) ++reduced;
@@ -1925,7 +1954,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
     if (o.status == EHGP_OK) {
       // final roots of this order (local node ids)
       for (uint64_t hnd = h_lo; hnd < h_hi; ++hnd)
-        if (dsu[hnd].order && dsu[hnd].parent == hnd && dsu[hnd].rroot != kInvalid32)
+        if (dsu[hnd].parent == hnd && dsu[hnd].rroot != kInvalid32 && dsu[hnd].rroot != kUnborn)
           o.roots.push_back({k, (uint32_t)hnd, dsu[hnd].rroot});
       std::sort(o.roots.begin(), o.roots.end(),
                 [](const ehgp_forest_root& x, const ehgp_forest_root& y) { return x.node < y.node; });
