@@ -46,6 +46,9 @@
 #include <vector>
 
 #include <sys/mman.h>
+#if defined(__x86_64__)
+#include <immintrin.h>
+#endif
 
 namespace ehgp {
 
@@ -994,6 +997,26 @@ k_arm_step(DescentParams d, uint32_t m, const uint32_t* __restrict__ in_arm, con
 }  // namespace
 
 // ---- host state ---------------------------------------------------------------------
+// Streaming (non-temporal) store of one record of 4-byte words: the forest records are
+// written once and read at copy-out, so they bypass the caches that hold the union-find
+// arrays.  stream_fence() orders them before a release that publishes them.
+template <class T>
+inline void nt_store(T& dst, const T& v) {
+  static_assert(sizeof(T) % 4 == 0, "records of 4-byte words");
+#if defined(__x86_64__)
+  const int* s = reinterpret_cast<const int*>(&v);
+  int* d = reinterpret_cast<int*>(&dst);
+  for (size_t i = 0; i < sizeof(T) / 4; ++i) _mm_stream_si32(d + i, s[i]);
+#else
+  dst = v;
+#endif
+}
+inline void stream_fence() {
+#if defined(__x86_64__)
+  _mm_sfence();
+#endif
+}
+
 constexpr uint32_t kUnborn = 0xFFFFFFFEu;  // HierDsu::rroot of a handle not yet born
 
 struct HierDsu {
@@ -1070,6 +1093,8 @@ struct HierOrderOut {  // one order's journal and forest arenas, local indices
   Arena<ehgp_forest_root> roots;
   Arena<uint32_t> node_cls;  // level class of each node (kInvalid32: an order-one birth node)
   Arena<uint32_t> fam_res;   // resulting root of each family's atomic group (local node id)
+  Arena<uint32_t> v_res;     // vertical maps from this order: each node's carrier-saddle root one order down
+  Arena<uint32_t> v_cls;     // and its own level class
   int status = EHGP_OK;
   const char* msg = "";
   double ms = 0;
@@ -1551,8 +1576,11 @@ int hier_run(Ctx& ctx, uint32_t K) {
   constexpr uint32_t kChunkBatches = 1u << 14, kSnapBlock = 4096;
   struct Progress {
     std::vector<std::unique_ptr<Cnt[]>> blocks;  // published chunk starts, kSnapBlock per block
-    std::atomic<uint32_t> published{0}, claimed{0};
+    std::atomic<uint32_t> published{0}, claimed{0}, replayed{0};
     std::atomic<int> done{0}, bad{0};
+    // vertical maps from this order (k >= 2): parallel gathers, then one sweep
+    std::atomic<uint32_t> va_claimed{0}, va_done{0};
+    std::atomic<int> vb_claimed{0}, vb_done{0}, vstat{EHGP_OK};
   };
   std::vector<Progress> prog(keff + 1);
   auto order_range = [&](uint32_t k, uint64_t& b_lo, uint64_t& b_hi, uint64_t& s_lo, uint64_t& s_hi,
@@ -1610,6 +1638,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
       if (!pg.blocks[blk]) pg.blocks[blk].reset(new Cnt[kSnapBlock]);
       pg.blocks[blk][nchunk % kSnapBlock] = open;
       ++nchunk;
+      stream_fence();  // the chunk's bindings
       pg.published.store(nchunk, std::memory_order_release);
     };
     auto reopen = [&] {
@@ -1671,7 +1700,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
               }
               const uint32_t c0 = find(term[a]);
               const uint32_t p0 = dsu[c0].rroot;
-              o.bindings[a - arm_lo] = {a, fidx, c0, p0};
+              nt_store(o.bindings[a - arm_lo], ehgp_forest_binding{a, fidx, c0, p0});
               bool dup = false;
               for (int t = 0; t < ndc; ++t) dup |= dc[t] == c0;
               if (dup) continue;
@@ -1959,7 +1988,10 @@ int hier_run(Ctx& ctx, uint32_t K) {
       std::sort(o.roots.begin(), o.roots.end(),
                 [](const ehgp_forest_root& x, const ehgp_forest_root& y) { return x.node < y.node; });
     }
+    o.v_res.reset(o.nodes.n);
+    o.v_cls.reset(o.nodes.n);
     o.ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - to0).count();
+    stream_fence();
     pg.done.store(1, std::memory_order_release);
   };
   // Rebuilds the records of one published chunk of single-role batches.
@@ -1981,11 +2013,11 @@ int hier_run(Ctx& ctx, uint32_t K) {
       const uint32_t bidx = c.jb;
       if (one_b) {
         const uint32_t pos = (uint32_t)(c.bi - rb[2]), fi = rank_order[c.bi];
-        o.jb[bidx] = {k, lev, c.role, 1, 1, 0};
-        o.roles[c.role] = {bidx, n + fi, 0};
-        o.births[c.birth] = {n + fi, bidx, k, n + pos, kInvalid32};
-        o.fb[bidx] = {k, lev, c.birth, 1, c.sad, 0, c.grp, 0, (uint32_t)c.carriers, (uint32_t)c.reduced,
-                      (uint32_t)(c.carriers + 1), (uint32_t)c.reduced};
+        nt_store(o.jb[bidx], ehgp_journal_batch{k, lev, c.role, 1, 1, 0});
+        nt_store(o.roles[c.role], ehgp_role_record{bidx, n + fi, 0});
+        nt_store(o.births[c.birth], ehgp_forest_birth{n + fi, bidx, k, n + pos, kInvalid32});
+        nt_store(o.fb[bidx], ehgp_forest_batch{k, lev, c.birth, 1, c.sad, 0, c.grp, 0, (uint32_t)c.carriers,
+                                               (uint32_t)c.reduced, (uint32_t)(c.carriers + 1), (uint32_t)c.reduced});
         ++c.carriers;
         ++c.jb; ++c.role; ++c.birth;
         ++c.bi;
@@ -1998,9 +2030,9 @@ int hier_run(Ctx& ctx, uint32_t K) {
       const uint32_t pos = (uint32_t)(c.si - fam_lo), fi = rank_order[c.si], fidx = (uint32_t)(c.si - s_lo);
       const uint32_t a0 = arm_off[pos], a1 = arm_off[pos + 1];
       const uint32_t ridx = c.role;
-      o.jb[bidx] = {k, lev, ridx, 1, 0, 1};
-      o.roles[ridx] = {bidx, n + fi, 1};
-      o.fam[fidx] = {fi, n + fi, ridx, bidx, k, a0, a1 - a0};
+      nt_store(o.jb[bidx], ehgp_journal_batch{k, lev, ridx, 1, 0, 1});
+      nt_store(o.roles[ridx], ehgp_role_record{bidx, n + fi, 1});
+      nt_store(o.fam[fidx], ehgp_family_record{fi, n + fi, ridx, bidx, k, a0, a1 - a0});
       uint32_t dc[4], pr[4];
       int ndc = 0, np = 0;
       for (uint32_t a = a0; a < a1; ++a) {
@@ -2019,10 +2051,10 @@ int hier_run(Ctx& ctx, uint32_t K) {
       const uint32_t created = kind == 1 ? kInvalid32 : c.node;
       const uint32_t result = kind == 1 ? pr[0] : created;
       const uint32_t ccnt = kind == 2 ? (uint32_t)np : 0u;
-      o.saddles[c.sad] = {fidx, fi, bidx, a0 - (uint32_t)arm_lo, a1 - a0, (uint32_t)ndc, (uint32_t)(ndc - np),
-                          (uint32_t)np, c.grp};
-      o.groups[c.grp] = {bidx, c.sad, 1, (uint32_t)ndc, (uint32_t)(ndc - np), (uint32_t)np, c.child, ccnt, created,
-                         result, kind};
+      nt_store(o.saddles[c.sad], ehgp_forest_saddle{fidx, fi, bidx, a0 - (uint32_t)arm_lo, a1 - a0, (uint32_t)ndc,
+                                                    (uint32_t)(ndc - np), (uint32_t)np, c.grp});
+      nt_store(o.groups[c.grp], ehgp_forest_group{bidx, c.sad, 1, (uint32_t)ndc, (uint32_t)(ndc - np), (uint32_t)np,
+                                                  c.child, ccnt, created, result, kind});
       o.fam_res[fidx] = result;
       if (kind != 1) {
         o.node_cls[c.node] = cls;
@@ -2030,16 +2062,124 @@ int hier_run(Ctx& ctx, uint32_t K) {
       }
       for (uint32_t q = 0; q < ccnt; ++q) o.children[c.child + q] = pr[q];
       c.child += ccnt;
-      o.fb[bidx] = {k, lev, c.birth, 0, c.sad, 1, c.grp, 1, (uint32_t)c.carriers, (uint32_t)c.reduced,
-                    (uint32_t)(c.carriers - (uint64_t)(ndc - 1)), (uint32_t)(c.reduced - (uint64_t)np + 1)};
+      nt_store(o.fb[bidx], ehgp_forest_batch{k, lev, c.birth, 0, c.sad, 1, c.grp, 1, (uint32_t)c.carriers,
+                                             (uint32_t)c.reduced, (uint32_t)(c.carriers - (uint64_t)(ndc - 1)),
+                                             (uint32_t)(c.reduced - (uint64_t)np + 1)});
       c.carriers -= (uint64_t)(ndc - 1);
       c.reduced = c.reduced - (uint64_t)np + 1;
       ++c.jb; ++c.role; ++c.sad; ++c.grp;
       ++c.si;
     }
   };
-  // claims and replays published chunks, highest order first, until every core is done
-  // and every chunk is claimed
+  // ---- vertical maps: each reduced node of order k >= 2 at level a maps, on the closed
+  // cut at a, to the root of order k - 1 whose component contains it.  A carrier birth of
+  // the node's group is an event of rank k; that event is a saddle of order k - 1, whose
+  // group's resulting root (level <= a) is climbed through multifusion parents of level <= a
+  // (the contract serializer's assignment, reference/morsehgp3d_oracle/serialization.py:1040-1099).
+  // They run in the same pool as soon as orders k and k - 1 are complete: chunks of source
+  // nodes gather their targets in parallel, then one offline sweep per order climbs them
+  // (node ids grow with level in both forests, so the target forest's parent links are
+  // united in id order as the source levels rise; the image is one find with path compression).
+  constexpr uint32_t kVChunk = 1u << 15;
+  if (h.vert.size() < keff + 1) h.vert.resize(keff + 1);
+  auto vcls = [](const HierOrderOut& o, uint32_t node) -> int64_t {
+    const uint32_t c = o.node_cls[node];
+    return c == kInvalid32 ? -1 : (int64_t)c;
+  };
+  auto complete = [&](uint32_t k) {
+    Progress& pg = prog[k];
+    return pg.done.load(std::memory_order_acquire) &&
+           pg.replayed.load(std::memory_order_acquire) == pg.published.load(std::memory_order_acquire);
+  };
+  auto v_gather = [&](uint32_t k, uint32_t chunk) {
+    HierOrderOut& src = outs[k];
+    const HierOrderOut& tgt = outs[k - 1];
+    const uint64_t h_lo = n + (rb[k] - rb[2]);  // first birth handle of order k
+    const uint64_t i_hi = std::min<uint64_t>(src.nodes.size(), (uint64_t)(chunk + 1) * kVChunk);
+    for (uint64_t i = (uint64_t)chunk * kVChunk; i < i_hi; ++i) {
+      const ehgp_forest_node& nd = src.nodes[i];
+      const ehgp_forest_group& g = src.groups[nd.atomic_group];
+      const uint64_t carrier = src.bindings[src.saddles[g.saddle_offset].arm_offset].carrier;
+      // the carrier's birth (rank k) and its saddle family of order k - 1 share the rank
+      // segment position, so the family's local index is carrier - h_lo
+      const uint64_t f = carrier - h_lo;
+      if (carrier < h_lo || f >= tgt.fam.size()) {
+        prog[k].vstat.store(EHGP_ERR_DEGENERATE);
+        src.v_res[i] = kInvalid32;
+        continue;
+      }
+      src.v_res[i] = tgt.fam_res[f];
+      src.v_cls[i] = src.node_cls[i];
+    }
+  };
+  auto v_sweep = [&](uint32_t k) {
+    const HierOrderOut& src = outs[k];
+    const HierOrderOut& tgt = outs[k - 1];
+    std::vector<ehgp_vertical_assignment>& vo = h.vert[k];
+    vo.clear();
+    if (prog[k].vstat.load() != EHGP_OK) return;
+    const uint32_t t_n = (uint32_t)tgt.nodes.size();
+    std::vector<uint32_t> up(t_n);
+    std::iota(up.begin(), up.end(), 0u);
+    auto find_up = [&](uint32_t x) {
+      while (up[x] != x) {
+        up[x] = up[up[x]];
+        x = up[x];
+      }
+      return x;
+    };
+    uint32_t sweep = 0;  // next target node whose child links are not yet united
+    for (uint64_t i = 0; i < src.nodes.size(); ++i) {
+      const uint32_t R = src.v_res[i];
+      const int64_t lev = vcls(src, (uint32_t)i);
+      if (R >= t_n || vcls(tgt, R) > lev) {
+        prog[k].vstat.store(EHGP_ERR_DEGENERATE);
+        return;
+      }
+      while (sweep < t_n && vcls(tgt, sweep) <= lev) {
+        const ehgp_forest_node& p = tgt.nodes[sweep];
+        if (p.kind == 2)
+          for (uint32_t c = 0; c < p.child_count; ++c) up[find_up(tgt.children[p.child_offset + c])] = sweep;
+        ++sweep;
+      }
+      vo.push_back({(uint32_t)i, find_up(R), k, src.nodes[i].level_event});  // local ids; offsets at copy-out
+    }
+  };
+  // One step of vertical work (a gather chunk or a sweep) if one is ready; `pending` is
+  // cleared while some vertical map is unfinished.
+  auto vertical_step = [&](bool& pending) {
+    for (uint32_t k = keff; k >= 2; --k) {
+      Progress& pg = prog[k];
+      if (pg.vb_done.load(std::memory_order_acquire)) continue;
+      pending = false;
+      if (!complete(k) || !complete(k - 1)) continue;
+      if (outs[k].status != EHGP_OK || outs[k - 1].status != EHGP_OK || prog[k].bad.load() || prog[k - 1].bad.load()) {
+        int z = 0;
+        if (pg.vb_claimed.compare_exchange_strong(z, 1)) pg.vb_done.store(1, std::memory_order_release);
+        continue;
+      }
+      const uint32_t na = (uint32_t)((outs[k].nodes.size() + kVChunk - 1) / kVChunk);
+      uint32_t c = pg.va_claimed.load(std::memory_order_relaxed);
+      while (c < na) {
+        if (pg.va_claimed.compare_exchange_weak(c, c + 1)) {
+          v_gather(k, c);
+          pg.va_done.fetch_add(1, std::memory_order_acq_rel);
+          return true;
+        }
+      }
+      if (pg.va_done.load(std::memory_order_acquire) == na) {
+        int z = 0;
+        if (pg.vb_claimed.compare_exchange_strong(z, 1)) {
+          v_sweep(k);
+          pg.vb_done.store(1, std::memory_order_release);
+          return true;
+        }
+      }
+    }
+    return false;
+  };
+  // claims and replays published chunks, highest order first, then the vertical maps, until
+  // every core is done and every chunk and map is finished
   auto work = [&] {
     for (;;) {
       bool did = false, all = true;
@@ -2051,6 +2191,8 @@ int hier_run(Ctx& ctx, uint32_t K) {
         while (cl < pub) {
           if (pg.claimed.compare_exchange_weak(cl, cl + 1)) {
             replay(k, cl);  // published chunks are complete even when the core stops later
+            stream_fence();
+            pg.replayed.fetch_add(1, std::memory_order_acq_rel);
             did = true;
             break;
           }
@@ -2060,6 +2202,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
         if (did) break;
       }
       if (did) continue;
+      if (vertical_step(all)) continue;
       if (all) return;
       std::this_thread::yield();
     }
@@ -2206,71 +2349,11 @@ int hier_run(Ctx& ctx, uint32_t K) {
                   a.grp + (uint32_t)o.groups.size(),    a.root + (uint32_t)o.roots.size(), 0u};
   }
   const auto t_merge = std::chrono::steady_clock::now();
-  // ---- vertical maps: each reduced node of order k >= 2 at level a maps, on the closed
-  // cut at a, to the root of order k - 1 whose component contains it.  A carrier birth of
-  // the node's group is an event of rank k; that event is a saddle of order k - 1, whose
-  // group's resulting root (level <= a) is climbed through multifusion parents of level <= a
-  // (the contract serializer's assignment, reference/morsehgp3d_oracle/serialization.py:1040-1099).
   {
-    auto cls = [](const HierOrderOut& o, uint32_t node) -> int64_t {
-      const uint32_t c = o.node_cls[node];
-      return c == kInvalid32 ? -1 : (int64_t)c;
-    };
-    if (h.vert.size() < keff + 1) h.vert.resize(keff + 1);
-    std::vector<int> vstat(keff + 1, EHGP_OK);
-    // Offline sweep per source order: node ids grow with level in both forests, so the
-    // target forest's parent links are united in id (= level) order as the source levels
-    // rise; the image is then one find with path compression.
-    auto run_v = [&](uint32_t k) {
-      const HierOrderOut& src = outs[k];
-      const HierOrderOut& tgt = outs[k - 1];
-      std::vector<ehgp_vertical_assignment>& vo = h.vert[k];
-      vo.clear();
-      const uint64_t h_lo = n + (rb[k] - rb[2]);  // first birth handle of order k
-      const uint32_t t_n = (uint32_t)tgt.nodes.size();
-      std::vector<uint32_t> up(t_n);
-      std::iota(up.begin(), up.end(), 0u);
-      auto find_up = [&](uint32_t x) {
-        while (up[x] != x) {
-          up[x] = up[up[x]];
-          x = up[x];
-        }
-        return x;
-      };
-      uint32_t sweep = 0;  // next target node whose child links are not yet united
-      for (uint64_t i = 0; i < src.nodes.size(); ++i) {
-        const ehgp_forest_node& nd = src.nodes[i];
-        const ehgp_forest_group& g = src.groups[nd.atomic_group];
-        const uint64_t carrier = src.bindings[src.saddles[g.saddle_offset].arm_offset].carrier;
-        // the carrier's birth (rank k) and its saddle family of order k - 1 share the rank
-        // segment position, so both have the local index carrier - h_lo
-        const uint64_t f = carrier - h_lo;
-        if (carrier < h_lo || f >= tgt.fam.size()) {
-          vstat[k] = EHGP_ERR_DEGENERATE;
-          return;
-        }
-        const uint32_t R = tgt.fam_res[f];
-        const int64_t lev = cls(src, (uint32_t)i);
-        if (R >= t_n || cls(tgt, R) > lev) {
-          vstat[k] = EHGP_ERR_DEGENERATE;
-          return;
-        }
-        while (sweep < t_n && cls(tgt, sweep) <= lev) {
-          const ehgp_forest_node& p = tgt.nodes[sweep];
-          if (p.kind == 2)
-            for (uint32_t c = 0; c < p.child_count; ++c) up[find_up(tgt.children[p.child_offset + c])] = sweep;
-          ++sweep;
-        }
-        vo.push_back({(uint32_t)i + off[k].node, find_up(R) + off[k - 1].node, k, nd.level_event});
-      }
-    };
-    std::vector<std::thread> pool;
-    for (uint32_t k = 2; k <= keff; ++k) pool.emplace_back(run_v, k);
-    for (auto& t : pool) t.join();
     uint32_t vtot = 0;
     for (uint32_t k = 1; k <= keff; ++k) {
-      if (k >= 2 && vstat[k] != EHGP_OK)
-        return abi_fail(&ctx, vstat[k], "a reduced node has no lower-order image through its carrier saddle");
+      if (k >= 2 && prog[k].vstat.load() != EHGP_OK)
+        return abi_fail(&ctx, prog[k].vstat.load(), "a reduced node has no lower-order image through its carrier saddle");
       off[k].vert = vtot;
       if (k >= 2) vtot += (uint32_t)h.vert[k].size();
     }
@@ -2441,7 +2524,13 @@ int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out) {
     });
     if (k >= 2 && k < h.vert.size()) {
       const std::vector<ehgp_vertical_assignment>& v = h.vert[k];
-      add(out->vertical, v.size(), [&v, f, out](uint64_t i) { out->vertical[f.vert + i] = v[i]; });
+      const uint32_t tnode = h.off[k - 1].node;
+      add(out->vertical, v.size(), [&v, f, tnode, out](uint64_t i) {
+        ehgp_vertical_assignment x = v[i];
+        x.source_node += f.node;
+        x.target_node += tnode;
+        out->vertical[f.vert + i] = x;
+      });
     }
   }
   if (!tasks.empty()) {
