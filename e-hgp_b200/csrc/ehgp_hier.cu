@@ -1592,6 +1592,11 @@ int hier_run(Ctx& ctx, uint32_t K) {
     arm_lo = s_hi > s_lo ? arm_off[s_lo - fam_lo] : 0;
     arm_hi = s_hi > s_lo ? arm_off[s_hi - fam_lo] : 0;
   };
+  // fam_lim[k]: saddle positions below it have their terminal handles on the host (the
+  // descent of an order arrives in parts cut at batch boundaries); stop_all ends waits
+  std::unique_ptr<std::atomic<uint64_t>[]> fam_lim(new std::atomic<uint64_t>[keff + 1]);
+  for (uint32_t k = 0; k <= keff; ++k) fam_lim[k].store(0);
+  std::atomic<int> stop_all{0};
   auto run_core = [&](uint32_t k, HierOrderOut& o) {
     const auto to0 = std::chrono::steady_clock::now();
     Progress& pg = prog[k];
@@ -1665,12 +1670,22 @@ int hier_run(Ctx& ctx, uint32_t K) {
     uint64_t& carriers = c.carriers;
     uint64_t& reduced = c.reduced;
     bool singles = k == 1;
+    uint64_t lim = 0;  // saddle positions below lim have their terminal handles
     auto core = [&]() {
       while (singles || bi < b_hi || si < s_hi) {
         uint32_t cls = kInvalid32, lev = kInvalid32;
         if (!singles) {
           const uint32_t cls_b = bi < b_hi ? cls_rp[bi] : kInvalid32;
           const uint32_t cls_s = si < s_hi ? cls_rp[si] : kInvalid32;
+          if (cls_s <= cls_b && si >= lim) {  // the batch holds saddles: wait for their part of the descent
+            while ((lim = fam_lim[k].load(std::memory_order_acquire)) <= si) {
+              if (stop_all.load(std::memory_order_acquire)) {
+                fail_o("the strict-arm descent stopped");
+                return;
+              }
+              std::this_thread::sleep_for(std::chrono::microseconds(20));
+            }
+          }
           cls = std::min(cls_b, cls_s);
           lev = cls_b <= cls_s ? rank_order[bi] : rank_order[si];
           // single-role batches (almost every batch off ties): union-find only here
@@ -2245,59 +2260,83 @@ int hier_run(Ctx& ctx, uint32_t K) {
       dstatus = status;
       dmsg = msg;
     };
+    constexpr uint32_t kPartArms = 1u << 22;  // arms per part of an order's descent (about)
     for (; k >= 1 && dstatus == EHGP_OK; --k) {
       const uint64_t s_lo = rb[k + 1], s_hi = rb[k + 2 > 16 ? 16 : k + 2];
-      const uint32_t a_lo = s_hi > s_lo ? arm_off[s_lo - fam_lo] : 0, a_hi = s_hi > s_lo ? arm_off[s_hi - fam_lo] : 0;
-      if (a_hi > a_lo) {
-        const uint32_t na = a_hi - a_lo;
-        cudaMemsetAsync(h.qcount, 0, 4 * sizeof(uint32_t), st);
-        k_arm_probe<<<nblk(na, kT), kT, 0, st>>>(dp, a_lo, na, h.rank_order + fam_lo, h.arm_family, h.arm_local, h.ev,
-                                                 h.term, h.arm_status, h.q_arm[0], h.q_fac[0], h.qcount);
-        ++launches;
-        uint32_t pending = 0;
-        cudaMemcpyAsync(&pending, h.qcount, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-        if ((dcuda = cudaStreamSynchronize(st)) != cudaSuccess) break;
-        misses += pending;
-        int cur = 0;
-        uint32_t rounds = 0;
-        while (pending) {
-          if (++rounds > (uint32_t)kDescentSteps) {
-            stop(EHGP_ERR_DEGENERATE, "a strict arm descent exceeded its step budget");
-            break;
+      uint64_t p_lo = s_lo;
+      while (p_lo < s_hi && dstatus == EHGP_OK && dcuda == cudaSuccess) {
+        // the part ends at a batch boundary after about kPartArms arms
+        uint64_t p_hi = p_lo;
+        {
+          uint64_t lo = p_lo, hi = s_hi;  // first position whose arms reach the budget
+          const uint64_t goal = (uint64_t)arm_off[p_lo - fam_lo] + kPartArms;
+          while (lo < hi) {
+            const uint64_t mid = (lo + hi) / 2;
+            if ((uint64_t)arm_off[mid + 1 - fam_lo] >= goal) hi = mid; else lo = mid + 1;
           }
-          uint32_t* oc = h.qcount + 1 + (1 - cur);
-          cudaMemsetAsync(oc, 0, sizeof(uint32_t), st);
-          k_arm_step<<<nblk(pending, 128), 128, 0, st>>>(dp, pending, h.q_arm[cur], h.q_fac[cur], h.q_arm[1 - cur],
-                                                         h.q_fac[1 - cur], oc, h.term, h.arm_status, h.dstats);
-          ++launches;
-          cudaMemcpyAsync(&pending, oc, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-          if ((dcuda = cudaStreamSynchronize(st)) != cudaSuccess) break;
-          cur = 1 - cur;
+          p_hi = std::min<uint64_t>(lo + 1, s_hi);
+          while (p_hi < s_hi && cls_rp[p_hi] == cls_rp[p_hi - 1]) ++p_hi;
         }
-        if (dcuda != cudaSuccess || dstatus != EHGP_OK) break;
-        max_rounds = std::max(max_rounds, rounds);
-        unsigned long long dst[4] = {0, 0, 0, 0};
-        cudaMemcpyAsync(h.p_term + a_lo, h.term + a_lo, (uint64_t)na * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(dst, h.dstats, sizeof(dst), cudaMemcpyDeviceToHost, st);
-        if ((dcuda = cudaStreamSynchronize(st)) != cudaSuccess) break;
-        h.descent_steps = dst[0];
-        if (dst[3] > failed_before) {  // an arm of this order failed: report the first one
-          failed_before = dst[3];
-          if ((dcuda = cudaMemcpy(h.p_stat + a_lo, h.arm_status + a_lo, na, cudaMemcpyDeviceToHost)) != cudaSuccess) break;
-          static const char* msg[] = {"", "a strict arm descent is unresolved", "a strict arm descent met a plateau",
-                                      "a strict arm descent exceeded its ball-query capacity",
-                                      "a strict arm descent exceeded its step budget",
-                                      "a strict arm descent found no consistent exact miniball or top-k"};
-          for (uint32_t a = a_lo; a < a_hi; ++a)
-            if (astat[a] != kArmOk) {
-              stop(astat[a] == kArmCapacity ? EHGP_ERR_CAPACITY : EHGP_ERR_DEGENERATE, msg[astat[a] < 6 ? astat[a] : 5]);
+        const uint32_t a_lo = arm_off[p_lo - fam_lo], a_hi = arm_off[p_hi - fam_lo];
+        if (a_hi > a_lo) {
+          const uint32_t na = a_hi - a_lo;
+          cudaMemsetAsync(h.qcount, 0, 4 * sizeof(uint32_t), st);
+          k_arm_probe<<<nblk(na, kT), kT, 0, st>>>(dp, a_lo, na, h.rank_order + fam_lo, h.arm_family, h.arm_local,
+                                                   h.ev, h.term, h.arm_status, h.q_arm[0], h.q_fac[0], h.qcount);
+          ++launches;
+          uint32_t pending = 0;
+          cudaMemcpyAsync(&pending, h.qcount, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+          if ((dcuda = cudaStreamSynchronize(st)) != cudaSuccess) break;
+          misses += pending;
+          int cur = 0;
+          uint32_t rounds = 0;
+          while (pending) {
+            if (++rounds > (uint32_t)kDescentSteps) {
+              stop(EHGP_ERR_DEGENERATE, "a strict arm descent exceeded its step budget");
               break;
             }
-          if (dstatus != EHGP_OK) break;
+            uint32_t* oc = h.qcount + 1 + (1 - cur);
+            cudaMemsetAsync(oc, 0, sizeof(uint32_t), st);
+            k_arm_step<<<nblk(pending, 128), 128, 0, st>>>(dp, pending, h.q_arm[cur], h.q_fac[cur], h.q_arm[1 - cur],
+                                                           h.q_fac[1 - cur], oc, h.term, h.arm_status, h.dstats);
+            ++launches;
+            cudaMemcpyAsync(&pending, oc, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+            if ((dcuda = cudaStreamSynchronize(st)) != cudaSuccess) break;
+            cur = 1 - cur;
+          }
+          if (dcuda != cudaSuccess || dstatus != EHGP_OK) break;
+          max_rounds = std::max(max_rounds, rounds);
+          unsigned long long dst[4] = {0, 0, 0, 0};
+          cudaMemcpyAsync(h.p_term + a_lo, h.term + a_lo, (uint64_t)na * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+          cudaMemcpyAsync(dst, h.dstats, sizeof(dst), cudaMemcpyDeviceToHost, st);
+          if ((dcuda = cudaStreamSynchronize(st)) != cudaSuccess) break;
+          h.descent_steps = dst[0];
+          if (dst[3] > failed_before) {  // an arm of this part failed: report the first one
+            failed_before = dst[3];
+            if ((dcuda = cudaMemcpy(h.p_stat + a_lo, h.arm_status + a_lo, na, cudaMemcpyDeviceToHost)) != cudaSuccess)
+              break;
+            static const char* msg[] = {"", "a strict arm descent is unresolved", "a strict arm descent met a plateau",
+                                        "a strict arm descent exceeded its ball-query capacity",
+                                        "a strict arm descent exceeded its step budget",
+                                        "a strict arm descent found no consistent exact miniball or top-k"};
+            for (uint32_t a = a_lo; a < a_hi; ++a)
+              if (astat[a] != kArmOk) {
+                stop(astat[a] == kArmCapacity ? EHGP_ERR_CAPACITY : EHGP_ERR_DEGENERATE,
+                     msg[astat[a] < 6 ? astat[a] : 5]);
+                break;
+              }
+            if (dstatus != EHGP_OK) break;
+          }
         }
+        fam_lim[k].store(p_hi, std::memory_order_release);
+        ready[k].store(1, std::memory_order_release);
+        p_lo = p_hi;
       }
+      if (dcuda != cudaSuccess || dstatus != EHGP_OK) break;
+      fam_lim[k].store(s_hi, std::memory_order_release);
       ready[k].store(1, std::memory_order_release);
     }
+    if (dcuda != cudaSuccess || dstatus != EHGP_OK) stop_all.store(1, std::memory_order_release);
     // orders left waiting after a failure stop without running
     for (uint32_t j = 1; j <= keff; ++j) {
       int expect = 0;
