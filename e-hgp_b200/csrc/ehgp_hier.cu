@@ -1004,6 +1004,15 @@ template <class T>
 inline void nt_store(T& dst, const T& v) {
   static_assert(sizeof(T) % 4 == 0, "records of 4-byte words");
 #if defined(__x86_64__)
+  if (sizeof(T) % 16 == 0 && (reinterpret_cast<uintptr_t>(&dst) & 15) == 0) {  // whole 16-byte stores
+    __m128i* d = reinterpret_cast<__m128i*>(&dst);
+    for (size_t i = 0; i < sizeof(T) / 16; ++i) {
+      __m128i w;
+      std::memcpy(&w, reinterpret_cast<const char*>(&v) + 16 * i, 16);
+      _mm_stream_si128(d + i, w);
+    }
+    return;
+  }
   const int* s = reinterpret_cast<const int*>(&v);
   int* d = reinterpret_cast<int*>(&dst);
   for (size_t i = 0; i < sizeof(T) / 4; ++i) _mm_stream_si32(d + i, s[i]);
