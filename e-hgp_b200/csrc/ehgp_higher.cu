@@ -99,7 +99,8 @@ __device__ __forceinline__ double ptmax(const SetPt& p) { return fmax(fabs(p.x),
 struct QEntry {
   double A, Nx, Ny, Nz, bnd;
   uint32_t ids[4];  // ids[0] = owner a; ids[3] = kInvalid32 for a triangle
-  int size, sgn;
+  int16_t size, sgn;
+  float cut;  // candidates (sorted by distance from a) with |p - a|^2 above cut lie outside
 };
 static_assert(sizeof(QEntry) == 64, "queue entries are 64 bytes");
 
@@ -557,7 +558,8 @@ struct Ctl {
   uint32_t cap;  // record capacity
 };
 
-constexpr int kHWarps = 2;      // warps per block in k_higher (shared memory per warp ~22 KB)
+constexpr int kHOwnerWarps = 4;  // warps per owner block in k_higher (they share its staged candidate set)
+constexpr int kHBlocksPerSM = 4; // register budget: 65536 / (128 threads x 4 blocks) = 128 per thread
 constexpr int kCube = 32;       // cube-map cells per face edge for centre directions
 constexpr int kCellDirs = 8;    // direction slots per cell (0xffff = unused)
 
@@ -568,12 +570,15 @@ struct HigherTables {
   double cos_lim;          // cos(delta) raised by a margin: inside the cone for sure
 };
 
-struct WarpSmem {
+struct OwnerSmem {  // one owner's staged candidate set, shared by the block's warps
   uint32_t sid[kMaxCand];
   SetPt spt[kMaxCand];
   uint16_t supi[kMaxCand];
   uint32_t adm[kMaxCand][kMaxCand / 32];  // adm[j] bit k (j < k): face (a, j, k) within the bound
   float rho[kDirs];
+};
+
+struct WarpQueue {  // one warp's queued supports
   uint32_t iids[kMaxInteriorH];
   QEntry q[32];
 };
@@ -615,15 +620,27 @@ __device__ bool cone_rejects(const QEntry& E, double eA, double eN, const float*
   return r_lo > bound * (1.0 + 1e-9);
 }
 
+// Every point of the closed ball lies within its diameter of a: |p - a|^2 <= 4 r^2 = |N|^2 / A^2.
+// The cut adds 2e-5 for the FP64 values of A and N (relative errors below 1e-7 when the cut
+// is used at all) and for the binary32 distances that order C(a); otherwise no cut.
+__device__ float sphere_cut(const QEntry& E, double eA, double eN) {
+  const double nn2 = E.Nx * E.Nx + E.Ny * E.Ny + E.Nz * E.Nz;
+  if (!(eA <= 1e-7 * fabs(E.A)) || !(3.0 * eN * eN <= 1e-14 * nn2)) return INFINITY;
+  return __double2float_ru(nn2 / (E.A * E.A) * (1.0 + 2e-5));
+}
+
 // Classifies the queued supports against C(a) with the whole warp and emits the relevant ones.
-__device__ void classify_queue(WarpSmem& S, uint32_t qn, uint32_t m, const Cloud& c, uint32_t smax, HigherRec* out,
-                               uint32_t cap, uint32_t* counter, uint32_t lane, unsigned long long& emitted) {
+__device__ void classify_queue(const OwnerSmem& S, WarpQueue& Q, uint32_t qn, uint32_t m, const Cloud& c,
+                               uint32_t smax, HigherRec* out, uint32_t cap, uint32_t* counter, uint32_t lane,
+                               unsigned long long& emitted) {
   for (uint32_t e = 0; e < qn; ++e) {
-    const QEntry E = S.q[e];
+    const QEntry E = Q.q[e];
     const uint32_t icap = smax - (uint32_t)E.size;
     uint32_t interior = 0, shell = (uint32_t)E.size, wit = kInvalid32;
     bool reject = false;
     for (uint32_t base = 0; base < m; base += 32) {
+      // C(a) is sorted by distance from a: the rest of it lies beyond the sphere's diameter
+      if (S.spt[base].q > (double)E.cut) break;
       const uint32_t i = base + lane;
       int sd = 1;
       uint32_t w = kInvalid32;
@@ -640,7 +657,7 @@ __device__ void classify_queue(WarpSmem& S, uint32_t qn, uint32_t m, const Cloud
       const uint32_t bi = __ballot_sync(0xffffffffu, sd < 0), bs = __ballot_sync(0xffffffffu, sd == 0);
       if (sd < 0) {
         const uint32_t at = interior + __popc(bi & lanemask_lt());
-        if (at < icap) S.iids[at] = w;
+        if (at < icap) Q.iids[at] = w;
       }
       interior += __popc(bi);
       if (interior > icap) {
@@ -666,7 +683,7 @@ __device__ void classify_queue(WarpSmem& S, uint32_t qn, uint32_t m, const Cloud
       r.interior = interior;
       r.shell = shell;
       r.witness = wit;
-      for (uint32_t i = 0; i < (uint32_t)kMaxInteriorH; ++i) r.iids[i] = i < interior ? S.iids[i] : kInvalid32;
+      for (uint32_t i = 0; i < (uint32_t)kMaxInteriorH; ++i) r.iids[i] = i < interior ? Q.iids[i] : kInvalid32;
       for (uint32_t i = 1; i < interior; ++i) {  // interior ids ascending
         const uint32_t x = r.iids[i];
         uint32_t j = i;
@@ -703,24 +720,30 @@ __device__ __forceinline__ uint32_t select_bit(uint32_t x, uint32_t r) {
   return pos;
 }
 
-__global__ void __launch_bounds__(32 * kHWarps)
+__global__ void __launch_bounds__(32 * kHOwnerWarps, kHBlocksPerSM)
 k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf_pid, const uint32_t* __restrict__ cand,
          const uint32_t* __restrict__ candc, const double* __restrict__ px, const double* __restrict__ py,
          const double* __restrict__ pz, const int* __restrict__ cloud_scale, HigherRec* __restrict__ out,
          uint32_t* __restrict__ counter, unsigned long long* __restrict__ stats) {
-  __shared__ WarpSmem smem[kHWarps];
+  __shared__ OwnerSmem S;
+  __shared__ WarpQueue wq[kHOwnerWarps];
+  __shared__ double s_Mp;
+  __shared__ uint32_t s_mc;
+  __shared__ float s_rmax[kHOwnerWarps];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t pos = blockIdx.x * kHWarps + warp;
+  const uint32_t pos = blockIdx.x;
   if (pos >= n) return;
-  WarpSmem& S = smem[warp];
+  WarpQueue& Q = wq[warp];
   const uint32_t a = leaf_pid[pos];
   const Cloud c{px, py, pz, cloud_scale[0]};
   const uint32_t m = candc[a];
   if (m > (uint32_t)kMaxCand) return;  // reported by the host
   const double ax = px[a], ay = py[a], az = pz[a];
+  // warp 0 stages C(a) (and the support candidates, ids above a); the block clears the
+  // face mask and loads the cone bounds
   uint32_t mc = 0;
   double Mp = 0.0;
-  for (uint32_t base = 0; base < m; base += 32) {
+  for (uint32_t base = 0; warp == 0 && base < m; base += 32) {
     const uint32_t i = base + lane;
     const uint32_t p = i < m ? cand[(uint64_t)a * kMaxCand + i] : kInvalid32;
     if (i < m) {
@@ -739,23 +762,32 @@ k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf
     mc += __popc(b);
   }
   float rmax = 0.f;
-  for (uint32_t d = lane; d < (uint32_t)kDirs; d += 32) {
+  for (uint32_t d = threadIdx.x; d < (uint32_t)kDirs; d += 32 * kHOwnerWarps) {
     const float r = tb.rho[(uint64_t)a * kDirs + d];
     S.rho[d] = r;
     rmax = fmaxf(rmax, r);
   }
-  for (uint32_t i = lane; i < mc * (kMaxCand / 32); i += 32) S.adm[i / (kMaxCand / 32)][i % (kMaxCand / 32)] = 0u;
+  for (uint32_t i = threadIdx.x; i < (uint32_t)kMaxCand * (kMaxCand / 32); i += 32 * kHOwnerWarps)
+    S.adm[i / (kMaxCand / 32)][i % (kMaxCand / 32)] = 0u;
   for (int off = 16; off > 0; off >>= 1) {
     Mp = fmax(Mp, __shfl_xor_sync(0xffffffffu, Mp, off));
     rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, off));
   }
-  Mp *= (1.0 + 1e-15);
+  if (lane == 0) s_rmax[warp] = rmax;
+  if (threadIdx.x == 0) {
+    s_Mp = Mp * (1.0 + 1e-15);
+    s_mc = mc;
+  }
+  __syncthreads();
+  Mp = s_Mp;
+  mc = s_mc;
+  rmax = s_rmax[0];
+  for (int w = 1; w < kHOwnerWarps; ++w) rmax = fmaxf(rmax, s_rmax[w]);
   const double rmax2 = (double)rmax * (double)rmax * (1.0 + 1e-12);
-  __syncwarp();
   unsigned long long tested = 0, minimal = 0, pruned = 0, classified = 0, emitted = 0, admitted = 0;
   const uint64_t P2 = (uint64_t)mc * (mc - 1) / 2;
   // --- triangles (a, j, k); also the face bound adm(j, k) for the tetrahedra
-  for (uint64_t t0 = 0; t0 < P2; t0 += 32) {
+  for (uint64_t t0 = 32 * warp; t0 < P2; t0 += 32 * kHOwnerWarps) {
     const uint64_t t = t0 + lane;
     bool push = false;
     QEntry E;
@@ -778,20 +810,23 @@ k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf
       if (st == 0 && ctl.smax >= 3) {
         ++minimal;
         if (cone_rejects(E, eA, eN, S.rho, tb)) ++pruned;
-        else push = true;
+        else {
+          push = true;
+          E.cut = sphere_cut(E, eA, eN);
+        }
       }
     }
     const uint32_t b = __ballot_sync(0xffffffffu, push);
-    if (push) S.q[__popc(b & lanemask_lt())] = E;
+    if (push) Q.q[__popc(b & lanemask_lt())] = E;
     __syncwarp();
     classified += __popc(b);
-    classify_queue(S, __popc(b), m, c, ctl.smax, out, ctl.cap, counter, lane, emitted);
+    classify_queue(S, Q, __popc(b), m, c, ctl.smax, out, ctl.cap, counter, lane, emitted);
   }
-  __syncwarp();
+  __syncthreads();  // the face mask is complete
   // --- tetrahedra (a, j, k, l), j < k < l with adm(j,k), adm(j,l), adm(k,l)
   if (ctl.smax >= 4) {
     constexpr uint32_t kWords = kMaxCand / 32;
-    for (uint64_t t0 = 0; t0 < P2; t0 += 32) {
+    for (uint64_t t0 = 32 * warp; t0 < P2; t0 += 32 * kHOwnerWarps) {
       const uint64_t t = t0 + lane;
       uint32_t j = 0, k = 0, cnt = 0;
       if (t < P2) {
@@ -846,14 +881,17 @@ k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf
           if (quad_eval(c, S.spt[ij], S.spt[ik], S.spt[il], E.ids, Mp, E, eA, eN) == 0) {
             ++minimal;
             if (cone_rejects(E, eA, eN, S.rho, tb)) ++pruned;
-            else push = true;
+            else {
+              push = true;
+              E.cut = sphere_cut(E, eA, eN);
+            }
           }
         }
         const uint32_t b = __ballot_sync(0xffffffffu, push);
-        if (push) S.q[__popc(b & lanemask_lt())] = E;
+        if (push) Q.q[__popc(b & lanemask_lt())] = E;
         __syncwarp();
         classified += __popc(b);
-        classify_queue(S, __popc(b), m, c, ctl.smax, out, ctl.cap, counter, lane, emitted);
+        classify_queue(S, Q, __popc(b), m, c, ctl.smax, out, ctl.cap, counter, lane, emitted);
       }
     }
   }
@@ -867,8 +905,10 @@ k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf
     atomicAdd(stats + 0, tested);
     atomicAdd(stats + 1, classified);
     atomicAdd(stats + 2, emitted);
-    atomicAdd(stats + 3, (unsigned long long)m);
-    atomicAdd(stats + 4, (unsigned long long)mc);
+    if (warp == 0) {
+      atomicAdd(stats + 3, (unsigned long long)m);
+      atomicAdd(stats + 4, (unsigned long long)mc);
+    }
     atomicAdd(stats + 5, minimal);
     atomicAdd(stats + 6, pruned);
     atomicAdd(stats + 7, admitted);
@@ -1132,7 +1172,7 @@ int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   Ctl ctl{smax, h.capacity};
   cudaEventRecord(ctx.evk0, st);
   const HigherTables tb{h.dirs, h.cells, h.rho, h.cos_lim};
-  k_higher<<<nblocks(n, kHWarps), 32 * kHWarps, 0, st>>>(n, ctl, tb, b.leaf_pid, h.cand, h.candc, b.px, b.py, b.pz,
+  k_higher<<<n, 32 * kHOwnerWarps, 0, st>>>(n, ctl, tb, b.leaf_pid, h.cand, h.candc, b.px, b.py, b.pz,
                                                          g.scale, (HigherRec*)h.raw, h.counters, h.stats);
   cudaEventRecord(ctx.evk1, st);
   ++launches;
