@@ -946,7 +946,13 @@ __global__ void k_arm_probe(DescentParams d, uint32_t a0, uint32_t narms,
 // One strict descent step for every queued arm: exact miniball of F, exact canonical
 // top-k choice G at its centre, certified beta(G) < beta(F); G is probed and either
 // binds the arm or is queued for the next step.
-__global__ void __launch_bounds__(128)
+// Blocks per SM the descent step's register budget is sized for: 8 x 128 threads gives 64
+// registers and 32 warps per SM; the spills cost less than the latency they hide (measured at
+// 50k: 3 blocks 246 ms, 4 222, 6 188, 8 172, 10 168, 12 176).
+#ifndef EHGP_STEP_BLOCKS_PER_SM
+#define EHGP_STEP_BLOCKS_PER_SM 8
+#endif
+__global__ void __launch_bounds__(128, EHGP_STEP_BLOCKS_PER_SM)
 k_arm_step(DescentParams d, uint32_t m, const uint32_t* __restrict__ in_arm, const uint32_t* __restrict__ in_fac,
            uint32_t* __restrict__ out_arm, uint32_t* __restrict__ out_fac, uint32_t* __restrict__ out_count,
            uint32_t* __restrict__ term, uint8_t* __restrict__ status, unsigned long long* __restrict__ stats) {
