@@ -427,14 +427,22 @@ __global__ void k_sum_apply(uint32_t m, uint32_t* __restrict__ out, const uint32
   if (j < m) out[j] = out[j] + bsum[j / 1024u] - (minus1 ? 1u : 0u);
 }
 
+// Rank keys for the stable partition; the rank histogram is summed per block in shared
+// memory (16 bins) before one global add per bin.
 __global__ void k_rank_key(uint32_t m, const EvRec* __restrict__ ev, uint64_t* __restrict__ key,
                            uint32_t* __restrict__ iota, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t bins[16];
+  if (threadIdx.x < 16) bins[threadIdx.x] = 0;
+  __syncthreads();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
-  const uint32_t r = ev[i].rank;
-  key[i] = r;
-  iota[i] = i;
-  atomicAdd(&hist[r < 15 ? r : 15], 1u);
+  if (i < m) {
+    const uint32_t r = ev[i].rank;
+    key[i] = r;
+    iota[i] = i;
+    atomicAdd(&bins[r < 15 ? r : 15], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < 16 && bins[threadIdx.x]) atomicAdd(&hist[threadIdx.x], bins[threadIdx.x]);
 }
 
 __global__ void k_rank_gather(uint32_t m, const uint32_t* __restrict__ v0, const uint32_t* __restrict__ v1,

@@ -351,7 +351,12 @@ __device__ __forceinline__ float warp_top_merge(float top, float v, uint32_t lan
   return x;
 }
 
-__global__ void __launch_bounds__(kDirThreads)
+// register budget of the direction table: 10 blocks of 128 threads per SM (51 registers; its
+// shared list is 20.6 KB per block); measured higher-stage wall at 50k 113.6 ms at 7, 111.7 at 10
+#ifndef EHGP_DIRTABLE_BLOCKS_PER_SM
+#define EHGP_DIRTABLE_BLOCKS_PER_SM 10
+#endif
+__global__ void __launch_bounds__(kDirThreads, EHGP_DIRTABLE_BLOCKS_PER_SM)
 k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uint32_t* __restrict__ nb,
            const uint32_t* __restrict__ nbc, const double* __restrict__ px, const double* __restrict__ py,
            const double* __restrict__ pz, const double* __restrict__ gather_r2, uint8_t* __restrict__ todo,
