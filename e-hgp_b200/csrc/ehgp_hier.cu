@@ -1163,6 +1163,7 @@ struct HierState {
   uint32_t* q_arm[2] = {nullptr, nullptr};
   uint32_t* q_fac[2] = {nullptr, nullptr};
   uint64_t q_cap = 0;
+  cudaEvent_t ev_block = nullptr;  // blocking-sync event: the descent loop waits without spinning a core
   uint32_t first_misses = 0, descent_rounds = 0;
   unsigned long long slow[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   // host results
@@ -1203,6 +1204,7 @@ void hier_free(Ctx& ctx) {
   for (void* p : {(void*)ctx.hier->p_rank, (void*)ctx.hier->p_cls, (void*)ctx.hier->p_armoff,
                   (void*)ctx.hier->p_term, (void*)ctx.hier->p_stat})
     if (p) cudaFreeHost(p);
+  if (ctx.hier->ev_block) cudaEventDestroy(ctx.hier->ev_block);
   delete ctx.hier;
   ctx.hier = nullptr;
 }
@@ -2255,7 +2257,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
   cudaError_t dcuda = cudaSuccess;
   {
     const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
-    const uint32_t extra = hw > keff ? std::min(hw - keff, 32u) : 0u;
+    const uint32_t extra = hw > keff + 1 ? std::min(hw - keff - 1, 32u) : 0u;  // one CPU for this thread
     std::vector<std::thread> pool;
     for (uint32_t k = 1; k <= keff; ++k)
       pool.emplace_back([&, k] {
@@ -2271,7 +2273,14 @@ int hier_run(Ctx& ctx, uint32_t K) {
         work();
       });
     for (uint32_t i = 0; i < extra; ++i) pool.emplace_back(work);
-    // descent, order by order
+    // descent, order by order; the host thread sleeps in its waits (the cores need the CPUs)
+    if (!h.ev_block && cudaEventCreateWithFlags(&h.ev_block, cudaEventBlockingSync | cudaEventDisableTiming) != cudaSuccess)
+      h.ev_block = nullptr;
+    auto wait_stream = [&]() -> cudaError_t {
+      if (!h.ev_block) return cudaStreamSynchronize(st);
+      cudaError_t r = cudaEventRecord(h.ev_block, st);
+      return r == cudaSuccess ? cudaEventSynchronize(h.ev_block) : r;
+    };
     const DescentParams dp{n, 2 * n - 2, g.tnodes, b.px, b.py, b.pz, h.S, h.slots, (uint32_t)(h.cap_slots - 1), h.bfac,
                            (uint32_t)nb_higher};
     uint32_t misses = 0, max_rounds = 0;
@@ -2309,7 +2318,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
           ++launches;
           uint32_t pending = 0;
           cudaMemcpyAsync(&pending, h.qcount, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-          if ((dcuda = cudaStreamSynchronize(st)) != cudaSuccess) break;
+          if ((dcuda = wait_stream()) != cudaSuccess) break;
           misses += pending;
           int cur = 0;
           uint32_t rounds = 0;
@@ -2324,7 +2333,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
                                                            h.q_fac[1 - cur], oc, h.term, h.arm_status, h.dstats);
             ++launches;
             cudaMemcpyAsync(&pending, oc, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-            if ((dcuda = cudaStreamSynchronize(st)) != cudaSuccess) break;
+            if ((dcuda = wait_stream()) != cudaSuccess) break;
             cur = 1 - cur;
           }
           if (dcuda != cudaSuccess || dstatus != EHGP_OK) break;
@@ -2332,7 +2341,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
           unsigned long long dst[4] = {0, 0, 0, 0};
           cudaMemcpyAsync(h.p_term + a_lo, h.term + a_lo, (uint64_t)na * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
           cudaMemcpyAsync(dst, h.dstats, sizeof(dst), cudaMemcpyDeviceToHost, st);
-          if ((dcuda = cudaStreamSynchronize(st)) != cudaSuccess) break;
+          if ((dcuda = wait_stream()) != cudaSuccess) break;
           h.descent_steps = dst[0];
           if (dst[3] > failed_before) {  // an arm of this part failed: report the first one
             failed_before = dst[3];
@@ -2523,44 +2532,44 @@ int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out) {
     add(out->journal_batches, o.jb.size(), [&o, f, out](uint64_t i) {
       ehgp_journal_batch x = o.jb[i];
       x.role_offset += f.role;
-      out->journal_batches[f.jb + i] = x;
+      ehgp::nt_store(out->journal_batches[f.jb + i], x);
     });
     add(out->batches, o.fb.size(), [&o, f, out](uint64_t i) {
       ehgp_forest_batch y = o.fb[i];
       y.birth_offset += f.birth;
       y.saddle_offset += f.sad;
       y.group_offset += f.grp;
-      out->batches[f.jb + i] = y;
+      ehgp::nt_store(out->batches[f.jb + i], y);
     });
     add(out->roles, o.roles.size(), [&o, f, out](uint64_t i) {
       ehgp_role_record x = o.roles[i];
       x.batch += f.jb;
-      out->roles[f.role + i] = x;
+      ehgp::nt_store(out->roles[f.role + i], x);
     });
     add(out->families, o.fam.size(), [&o, f, out](uint64_t i) {
       ehgp_family_record x = o.fam[i];
       x.role_record += f.role;
       x.batch += f.jb;
-      out->families[f.fam + i] = x;
+      ehgp::nt_store(out->families[f.fam + i], x);
     });
     add(out->nodes, o.nodes.size(), [&o, f, out, shift](uint64_t i) {
       ehgp_forest_node x = o.nodes[i];
       x.child_offset += f.child;
       x.atomic_group = shift(x.atomic_group, f.grp);
-      out->nodes[f.node + i] = x;
+      ehgp::nt_store(out->nodes[f.node + i], x);
     });
     add(out->children, o.children.size(), [&o, f, out](uint64_t i) { out->children[f.child + i] = o.children[i] + f.node; });
     add(out->births, o.births.size(), [&o, f, out, shift](uint64_t i) {
       ehgp_forest_birth x = o.births[i];
       x.batch += f.jb;
       x.order_one_node = shift(x.order_one_node, f.node);
-      out->births[f.birth + i] = x;
+      ehgp::nt_store(out->births[f.birth + i], x);
     });
     add(out->bindings, o.bindings.size(), [&o, f, out, shift](uint64_t i) {
       ehgp_forest_binding x = o.bindings[i];
       x.family += f.fam;
       x.prior_root = shift(x.prior_root, f.node);
-      out->bindings[f.bind + i] = x;
+      ehgp::nt_store(out->bindings[f.bind + i], x);
     });
     add(out->saddles, o.saddles.size(), [&o, f, out](uint64_t i) {
       ehgp_forest_saddle x = o.saddles[i];
@@ -2568,7 +2577,7 @@ int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out) {
       x.batch += f.jb;
       x.arm_offset += f.bind;
       x.group += f.grp;
-      out->saddles[f.sad + i] = x;
+      ehgp::nt_store(out->saddles[f.sad + i], x);
     });
     add(out->groups, o.groups.size(), [&o, f, out, shift](uint64_t i) {
       ehgp_forest_group x = o.groups[i];
@@ -2577,12 +2586,12 @@ int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out) {
       x.child_offset += f.child;
       x.created_node = shift(x.created_node, f.node);
       x.result_node = shift(x.result_node, f.node);
-      out->groups[f.grp + i] = x;
+      ehgp::nt_store(out->groups[f.grp + i], x);
     });
     add(out->roots, o.roots.size(), [&o, f, out](uint64_t i) {
       ehgp_forest_root x = o.roots[i];
       x.node += f.node;
-      out->roots[f.root + i] = x;
+      ehgp::nt_store(out->roots[f.root + i], x);
     });
     if (k >= 2 && k < h.vert.size()) {
       const std::vector<ehgp_vertical_assignment>& v = h.vert[k];
@@ -2591,7 +2600,7 @@ int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out) {
         ehgp_vertical_assignment x = v[i];
         x.source_node += f.node;
         x.target_node += tnode;
-        out->vertical[f.vert + i] = x;
+        ehgp::nt_store(out->vertical[f.vert + i], x);
       });
     }
   }
@@ -2601,6 +2610,7 @@ int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out) {
     std::atomic<uint64_t> next{0};
     auto work = [&] {
       for (uint64_t t; (t = next.fetch_add(1)) < tasks.size();) tasks[t]();
+      ehgp::stream_fence();  // the streaming stores are complete before the join
     };
     std::vector<std::thread> pool;
     for (uint32_t i = 1; i < nt; ++i) pool.emplace_back(work);
