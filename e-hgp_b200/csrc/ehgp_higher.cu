@@ -104,20 +104,47 @@ struct QEntry {
 };
 static_assert(sizeof(QEntry) == 64, "queue entries are 64 bytes");
 
+// The exact fallbacks take their ids by value and return the signs packed two bits each
+// (sign + 1), so that no array of the hot path needs an address (and local memory).
+__device__ __noinline__ uint32_t tri_signs_packed(Cloud c, uint32_t i0, uint32_t i1, uint32_t i2) {
+  const uint32_t id[3] = {i0, i1, i2};
+  int sg[4];
+  tri_signs_exact(c, id, sg);
+  uint32_t r = 0;
+  for (int k = 0; k < 4; ++k) r |= (uint32_t)(sg[k] + 1) << (2 * k);
+  return r;
+}
+__device__ __noinline__ uint32_t quad_signs_packed(Cloud c, uint32_t i0, uint32_t i1, uint32_t i2, uint32_t i3) {
+  const uint32_t id[4] = {i0, i1, i2, i3};
+  int sg[5];
+  quad_signs_exact(c, id, sg);
+  uint32_t r = 0;
+  for (int k = 0; k < 5; ++k) r |= (uint32_t)(sg[k] + 1) << (2 * k);
+  return r;
+}
+__device__ __forceinline__ int packed_sign(uint32_t p, int k) { return (int)((p >> (2 * k)) & 3u) - 1; }
+
 // Triangle (a, a + e1, a + e2): minimal iff its three angles are acute.
 // Returns 0 minimal (E filled), 1 boundary reduced, 2 obtuse, 3 collinear; *adm is
 // false when the circumradius certainly exceeds rmax (no relevant tetrahedron
 // has this face: its circumsphere contains the face's circumcircle).
-__device__ int tri_eval(const Cloud& c, const SetPt& e1, const SetPt& e2, const uint32_t* id, double Mp, double rmax2,
+__device__ int tri_eval(const Cloud& c, const SetPt& e1, const SetPt& e2, uint32_t i0, uint32_t i1, uint32_t i2,
+                        double Mp, double rmax2,
                         QEntry& E, double& eA, double& eN, bool& adm) {
   const double M = fmax(ptmax(e1), ptmax(e2)) * (1.0 + 1e-15), M2 = M * M;
   const double G11 = e1.q, G22 = e2.q, G12 = (e1.x * e2.x + e1.y * e2.y) + e1.z * e2.z;
   const double db = G11 - G12, dc = G22 - G12;
   const double detG = G11 * G22 - G12 * G12;
   const double bG = kFilt * 3.0 * M2 + kTiny, bD = kFilt * 6.0 * M2 + kTiny, b4 = kFilt * 18.0 * M2 * M2 + kTiny;
-  int sg[4] = {fsign(G12, bG), fsign(db, bD), fsign(dc, bD), fsign(detG, b4)};
-  if (sg[0] == 2 || sg[1] == 2 || sg[2] == 2 || sg[3] == 2) tri_signs_exact(c, id, sg);
-  if (sg[3] == 0) {
+  int sg0 = fsign(G12, bG), sg1 = fsign(db, bD), sg2 = fsign(dc, bD), sg3 = fsign(detG, b4);
+  if (sg0 == 2 || sg1 == 2 || sg2 == 2 || sg3 == 2) {
+    const uint32_t pk = tri_signs_packed(c, i0, i1, i2);
+    sg0 = packed_sign(pk, 0);
+    sg1 = packed_sign(pk, 1);
+    sg2 = packed_sign(pk, 2);
+    sg3 = packed_sign(pk, 3);
+  }
+  if (sg3 == 0) {
     adm = false;
     return 3;
   }
@@ -127,8 +154,8 @@ __device__ int tri_eval(const Cloud& c, const SetPt& e1, const SetPt& e2, const 
     const double den = 4.0 * (detG + b4);
     adm = !(num * (1.0 - 1e-12) > rmax2 * den * (1.0 + 1e-9));
   }
-  if (sg[0] < 0 || sg[1] < 0 || sg[2] < 0) return 2;
-  if (sg[0] == 0 || sg[1] == 0 || sg[2] == 0) return 1;
+  if (sg0 < 0 || sg1 < 0 || sg2 < 0) return 2;
+  if (sg0 == 0 || sg1 == 0 || sg2 == 0) return 1;
   const double f1 = G22 * db, f2 = G11 * dc;
   E.A = detG;
   E.Nx = f1 * e1.x + f2 * e2.x;
@@ -145,7 +172,8 @@ __device__ int tri_eval(const Cloud& c, const SetPt& e1, const SetPt& e2, const 
 
 // Tetrahedron (a, a + e1, a + e2, a + e3): minimal iff the four barycentric
 // coordinates l_i / (2 detE^2) of its circumcentre are positive.
-__device__ int quad_eval(const Cloud& c, const SetPt& e1, const SetPt& e2, const SetPt& e3, const uint32_t* id,
+__device__ int quad_eval(const Cloud& c, const SetPt& e1, const SetPt& e2, const SetPt& e3, uint32_t i0, uint32_t i1,
+                         uint32_t i2, uint32_t i3,
                          double Mp, QEntry& E, double& eA, double& eN) {
   const double M = fmax(fmax(ptmax(e1), ptmax(e2)), ptmax(e3)) * (1.0 + 1e-15), M2 = M * M, M3 = M2 * M;
   const double c23x = e2.y * e3.z - e2.z * e3.y, c23y = e2.z * e3.x - e2.x * e3.z, c23z = e2.x * e3.y - e2.y * e3.x;
@@ -161,18 +189,25 @@ __device__ int quad_eval(const Cloud& c, const SetPt& e1, const SetPt& e2, const
   const double l0 = (2.0 * detE) * detE - ((l1 + l2) + l3);
   const double M6 = M3 * M3;
   const double bE = kFilt * 6.0 * M3 + kTiny, bl = kFilt * 108.0 * M6 + kTiny, b0 = kFilt * 396.0 * M6 + kTiny;
-  int sg[5] = {fsign(detE, bE), fsign(l0, b0), fsign(l1, bl), fsign(l2, bl), fsign(l3, bl)};
-  if (sg[0] == 2 || sg[1] == 2 || sg[2] == 2 || sg[3] == 2 || sg[4] == 2) quad_signs_exact(c, id, sg);
-  if (sg[0] == 0) return 3;
-  if (sg[1] < 0 || sg[2] < 0 || sg[3] < 0 || sg[4] < 0) return 2;
-  if (sg[1] == 0 || sg[2] == 0 || sg[3] == 0 || sg[4] == 0) return 1;
+  int sg0 = fsign(detE, bE), sg1 = fsign(l0, b0), sg2 = fsign(l1, bl), sg3 = fsign(l2, bl), sg4 = fsign(l3, bl);
+  if (sg0 == 2 || sg1 == 2 || sg2 == 2 || sg3 == 2 || sg4 == 2) {
+    const uint32_t pk = quad_signs_packed(c, i0, i1, i2, i3);
+    sg0 = packed_sign(pk, 0);
+    sg1 = packed_sign(pk, 1);
+    sg2 = packed_sign(pk, 2);
+    sg3 = packed_sign(pk, 3);
+    sg4 = packed_sign(pk, 4);
+  }
+  if (sg0 == 0) return 3;
+  if (sg1 < 0 || sg2 < 0 || sg3 < 0 || sg4 < 0) return 2;
+  if (sg1 == 0 || sg2 == 0 || sg3 == 0 || sg4 == 0) return 1;
   const double Am = 6.0 * M3, Nm = 18.0 * M2 * M2;
   E.A = detE;
   E.Nx = Nx;
   E.Ny = Ny;
   E.Nz = Nz;
   E.bnd = kFilt * (Am * 3.0 * Mp * Mp + 3.0 * Mp * Nm) + kTiny;
-  E.sgn = sg[0];
+  E.sgn = sg0;
   E.size = 4;
   eA = kFilt * Am + kTiny;
   eN = kFilt * Nm + kTiny;
@@ -644,7 +679,7 @@ __device__ float sphere_cut(const QEntry& E, double eA, double eN) {
 }
 
 // Classifies the queued supports against C(a) with the whole warp and emits the relevant ones.
-__device__ void classify_queue(const OwnerSmem& S, WarpQueue& Q, uint32_t qn, uint32_t m, const Cloud& c,
+__device__ __forceinline__ void classify_queue(const OwnerSmem& S, WarpQueue& Q, uint32_t qn, uint32_t m, const Cloud& c,
                                uint32_t smax, HigherRec* out, uint32_t cap, uint32_t* counter, uint32_t lane,
                                unsigned long long& emitted) {
   for (uint32_t e = 0; e < qn; ++e) {
@@ -664,7 +699,7 @@ __device__ void classify_queue(const OwnerSmem& S, WarpQueue& Q, uint32_t qn, ui
           const SetPt p = S.spt[i];
           const double v = E.A * p.q - ((p.x * E.Nx + p.y * E.Ny) + p.z * E.Nz);
           sd = fsign(v, E.bnd);
-          if (sd == 2) sd = side_exact(c, E.ids, E.size, w);
+          if (sd == 2) sd = side_exact(c, Q.q[e].ids, E.size, w);  // the queue entry's ids (shared memory)
           sd *= E.sgn;
         }
       }
@@ -684,29 +719,49 @@ __device__ void classify_queue(const OwnerSmem& S, WarpQueue& Q, uint32_t qn, ui
       }
     }
     __syncwarp();
-    if (!reject && lane == 0) {
-      HigherRec r;
-      r.size = (uint32_t)E.size;
-      for (int i = 0; i < 4; ++i) r.ids[i] = i < E.size ? E.ids[i] : 0u;
-      for (int i = 1; i < E.size; ++i) {  // support ids ascending
-        const uint32_t x = r.ids[i];
-        int j = i;
-        while (j > 0 && r.ids[j - 1] > x) { r.ids[j] = r.ids[j - 1]; --j; }
-        r.ids[j] = x;
+    if (!reject) {  // warp-uniform: the record is written by 16 lanes, one word each
+      uint32_t slot = 0;
+      if (lane == 0) {
+        for (uint32_t i = 1; i < interior; ++i) {  // interior ids ascending, in place
+          const uint32_t x = Q.iids[i];
+          uint32_t j = i;
+          while (j > 0 && Q.iids[j - 1] > x) {
+            Q.iids[j] = Q.iids[j - 1];
+            --j;
+          }
+          Q.iids[j] = x;
+        }
+        slot = atomicAdd(counter, 1u);
+        ++emitted;
       }
-      r.interior = interior;
-      r.shell = shell;
-      r.witness = wit;
-      for (uint32_t i = 0; i < (uint32_t)kMaxInteriorH; ++i) r.iids[i] = i < interior ? Q.iids[i] : kInvalid32;
-      for (uint32_t i = 1; i < interior; ++i) {  // interior ids ascending
-        const uint32_t x = r.iids[i];
-        uint32_t j = i;
-        while (j > 0 && r.iids[j - 1] > x) { r.iids[j] = r.iids[j - 1]; --j; }
-        r.iids[j] = x;
+      slot = __shfl_sync(0xffffffffu, slot, 0);
+      __syncwarp();
+      // support ids ascending (a triangle's fourth slot sorts last and is written as 0)
+      uint32_t s0 = E.ids[0], s1 = E.ids[1], s2 = E.ids[2], s3 = E.size == 4 ? E.ids[3] : kInvalid32;
+      auto cswap = [](uint32_t& x, uint32_t& y) {
+        const uint32_t lo = min(x, y), hi = max(x, y);
+        x = lo;
+        y = hi;
+      };
+      cswap(s0, s1);
+      cswap(s2, s3);
+      cswap(s0, s2);
+      cswap(s1, s3);
+      cswap(s1, s2);
+      if (E.size != 4) s3 = 0u;
+      if (slot < cap && lane < 16) {
+        uint32_t v;
+        if (lane == 0) v = (uint32_t)E.size;
+        else if (lane == 1) v = s0;
+        else if (lane == 2) v = s1;
+        else if (lane == 3) v = s2;
+        else if (lane == 4) v = s3;
+        else if (lane == 5) v = interior;
+        else if (lane == 6) v = shell;
+        else if (lane == 7) v = wit;
+        else v = lane - 8 < interior ? Q.iids[lane - 8] : kInvalid32;
+        reinterpret_cast<uint32_t*>(out + slot)[lane] = v;
       }
-      const uint32_t slot = atomicAdd(counter, 1u);
-      if (slot < cap) out[slot] = r;
-      ++emitted;
     }
     __syncwarp();
   }
@@ -816,7 +871,7 @@ k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf
       double eA, eN;
       bool adm;
       ++tested;
-      const int st = tri_eval(c, S.spt[ij], S.spt[ik], E.ids, Mp, rmax2, E, eA, eN, adm);
+      const int st = tri_eval(c, S.spt[ij], S.spt[ik], E.ids[0], E.ids[1], E.ids[2], Mp, rmax2, E, eA, eN, adm);
       if (adm) {
         atomicOr(&S.adm[j][k >> 5], 1u << (k & 31));
         ++admitted;
@@ -892,7 +947,7 @@ k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf
           E.ids[3] = S.sid[il];
           double eA, eN;
           ++tested;
-          if (quad_eval(c, S.spt[ij], S.spt[ik], S.spt[il], E.ids, Mp, E, eA, eN) == 0) {
+          if (quad_eval(c, S.spt[ij], S.spt[ik], S.spt[il], E.ids[0], E.ids[1], E.ids[2], E.ids[3], Mp, E, eA, eN) == 0) {
             ++minimal;
             if (cone_rejects(E, eA, eN, S.rho, tb)) ++pruned;
             else {
