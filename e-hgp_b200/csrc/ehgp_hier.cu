@@ -2293,78 +2293,90 @@ int hier_run(Ctx& ctx, uint32_t K) {
       dmsg = msg;
     };
     constexpr uint32_t kPartArms = 1u << 22;  // arms per part of an order's descent (about)
-    for (; k >= 1 && dstatus == EHGP_OK; --k) {
-      const uint64_t s_lo = rb[k + 1], s_hi = rb[k + 2 > 16 ? 16 : k + 2];
-      uint64_t p_lo = s_lo;
-      while (p_lo < s_hi && dstatus == EHGP_OK && dcuda == cudaSuccess) {
-        // the part ends at a batch boundary after about kPartArms arms
-        uint64_t p_hi = p_lo;
-        {
-          uint64_t lo = p_lo, hi = s_hi;  // first position whose arms reach the budget
-          const uint64_t goal = (uint64_t)arm_off[p_lo - fam_lo] + kPartArms;
-          while (lo < hi) {
-            const uint64_t mid = (lo + hi) / 2;
-            if ((uint64_t)arm_off[mid + 1 - fam_lo] >= goal) hi = mid; else lo = mid + 1;
-          }
-          p_hi = std::min<uint64_t>(lo + 1, s_hi);
-          while (p_hi < s_hi && cls_rp[p_hi] == cls_rp[p_hi - 1]) ++p_hi;
+    std::vector<uint64_t> plo(keff + 1);
+    for (uint32_t j = 1; j <= keff; ++j) plo[j] = rb[j + 1];
+    // Descends the next part of order k (cut at a batch boundary after about kPartArms arms)
+    // and publishes it to the order's core; false on a failure.
+    auto part = [&](uint32_t k) -> bool {
+      const uint64_t s_hi = rb[k + 2 > 16 ? 16 : k + 2];
+      uint64_t& p_lo = plo[k];
+      // the part ends at a batch boundary after about kPartArms arms
+      uint64_t p_hi = p_lo;
+      {
+        uint64_t lo = p_lo, hi = s_hi;  // first position whose arms reach the budget
+        const uint64_t goal = (uint64_t)arm_off[p_lo - fam_lo] + kPartArms;
+        while (lo < hi) {
+          const uint64_t mid = (lo + hi) / 2;
+          if ((uint64_t)arm_off[mid + 1 - fam_lo] >= goal) hi = mid; else lo = mid + 1;
         }
-        const uint32_t a_lo = arm_off[p_lo - fam_lo], a_hi = arm_off[p_hi - fam_lo];
-        if (a_hi > a_lo) {
-          const uint32_t na = a_hi - a_lo;
-          cudaMemsetAsync(h.qcount, 0, 4 * sizeof(uint32_t), st);
-          k_arm_probe<<<nblk(na, kT), kT, 0, st>>>(dp, a_lo, na, h.rank_order + fam_lo, h.arm_family, h.arm_local,
-                                                   h.ev, h.term, h.arm_status, h.q_arm[0], h.q_fac[0], h.qcount);
+        p_hi = std::min<uint64_t>(lo + 1, s_hi);
+        while (p_hi < s_hi && cls_rp[p_hi] == cls_rp[p_hi - 1]) ++p_hi;
+      }
+      const uint32_t a_lo = arm_off[p_lo - fam_lo], a_hi = arm_off[p_hi - fam_lo];
+      if (a_hi > a_lo) {
+        const uint32_t na = a_hi - a_lo;
+        cudaMemsetAsync(h.qcount, 0, 4 * sizeof(uint32_t), st);
+        k_arm_probe<<<nblk(na, kT), kT, 0, st>>>(dp, a_lo, na, h.rank_order + fam_lo, h.arm_family, h.arm_local,
+                                                 h.ev, h.term, h.arm_status, h.q_arm[0], h.q_fac[0], h.qcount);
+        ++launches;
+        uint32_t pending = 0;
+        cudaMemcpyAsync(&pending, h.qcount, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if ((dcuda = wait_stream()) != cudaSuccess) return false;
+        misses += pending;
+        int cur = 0;
+        uint32_t rounds = 0;
+        while (pending) {
+          if (++rounds > (uint32_t)kDescentSteps) {
+            stop(EHGP_ERR_DEGENERATE, "a strict arm descent exceeded its step budget");
+            break;
+          }
+          uint32_t* oc = h.qcount + 1 + (1 - cur);
+          cudaMemsetAsync(oc, 0, sizeof(uint32_t), st);
+          k_arm_step<<<nblk(pending, 128), 128, 0, st>>>(dp, pending, h.q_arm[cur], h.q_fac[cur], h.q_arm[1 - cur],
+                                                         h.q_fac[1 - cur], oc, h.term, h.arm_status, h.dstats);
           ++launches;
-          uint32_t pending = 0;
-          cudaMemcpyAsync(&pending, h.qcount, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+          cudaMemcpyAsync(&pending, oc, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
           if ((dcuda = wait_stream()) != cudaSuccess) break;
-          misses += pending;
-          int cur = 0;
-          uint32_t rounds = 0;
-          while (pending) {
-            if (++rounds > (uint32_t)kDescentSteps) {
-              stop(EHGP_ERR_DEGENERATE, "a strict arm descent exceeded its step budget");
+          cur = 1 - cur;
+        }
+        if (dcuda != cudaSuccess || dstatus != EHGP_OK) return false;
+        max_rounds = std::max(max_rounds, rounds);
+        unsigned long long dst[4] = {0, 0, 0, 0};
+        cudaMemcpyAsync(h.p_term + a_lo, h.term + a_lo, (uint64_t)na * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(dst, h.dstats, sizeof(dst), cudaMemcpyDeviceToHost, st);
+        if ((dcuda = wait_stream()) != cudaSuccess) return false;
+        h.descent_steps = dst[0];
+        if (dst[3] > failed_before) {  // an arm of this part failed: report the first one
+          failed_before = dst[3];
+          if ((dcuda = cudaMemcpy(h.p_stat + a_lo, h.arm_status + a_lo, na, cudaMemcpyDeviceToHost)) != cudaSuccess)
+            return false;
+          static const char* msg[] = {"", "a strict arm descent is unresolved", "a strict arm descent met a plateau",
+                                      "a strict arm descent exceeded its ball-query capacity",
+                                      "a strict arm descent exceeded its step budget",
+                                      "a strict arm descent found no consistent exact miniball or top-k"};
+          for (uint32_t a = a_lo; a < a_hi; ++a)
+            if (astat[a] != kArmOk) {
+              stop(astat[a] == kArmCapacity ? EHGP_ERR_CAPACITY : EHGP_ERR_DEGENERATE,
+                   msg[astat[a] < 6 ? astat[a] : 5]);
               break;
             }
-            uint32_t* oc = h.qcount + 1 + (1 - cur);
-            cudaMemsetAsync(oc, 0, sizeof(uint32_t), st);
-            k_arm_step<<<nblk(pending, 128), 128, 0, st>>>(dp, pending, h.q_arm[cur], h.q_fac[cur], h.q_arm[1 - cur],
-                                                           h.q_fac[1 - cur], oc, h.term, h.arm_status, h.dstats);
-            ++launches;
-            cudaMemcpyAsync(&pending, oc, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-            if ((dcuda = wait_stream()) != cudaSuccess) break;
-            cur = 1 - cur;
-          }
-          if (dcuda != cudaSuccess || dstatus != EHGP_OK) break;
-          max_rounds = std::max(max_rounds, rounds);
-          unsigned long long dst[4] = {0, 0, 0, 0};
-          cudaMemcpyAsync(h.p_term + a_lo, h.term + a_lo, (uint64_t)na * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-          cudaMemcpyAsync(dst, h.dstats, sizeof(dst), cudaMemcpyDeviceToHost, st);
-          if ((dcuda = wait_stream()) != cudaSuccess) break;
-          h.descent_steps = dst[0];
-          if (dst[3] > failed_before) {  // an arm of this part failed: report the first one
-            failed_before = dst[3];
-            if ((dcuda = cudaMemcpy(h.p_stat + a_lo, h.arm_status + a_lo, na, cudaMemcpyDeviceToHost)) != cudaSuccess)
-              break;
-            static const char* msg[] = {"", "a strict arm descent is unresolved", "a strict arm descent met a plateau",
-                                        "a strict arm descent exceeded its ball-query capacity",
-                                        "a strict arm descent exceeded its step budget",
-                                        "a strict arm descent found no consistent exact miniball or top-k"};
-            for (uint32_t a = a_lo; a < a_hi; ++a)
-              if (astat[a] != kArmOk) {
-                stop(astat[a] == kArmCapacity ? EHGP_ERR_CAPACITY : EHGP_ERR_DEGENERATE,
-                     msg[astat[a] < 6 ? astat[a] : 5]);
-                break;
-              }
-            if (dstatus != EHGP_OK) break;
-          }
+          if (dstatus != EHGP_OK) return false;
         }
-        fam_lim[k].store(p_hi, std::memory_order_release);
-        ready[k].store(1, std::memory_order_release);
-        p_lo = p_hi;
       }
-      if (dcuda != cudaSuccess || dstatus != EHGP_OK) break;
+      fam_lim[k].store(p_hi, std::memory_order_release);
+      ready[k].store(1, std::memory_order_release);
+      p_lo = p_hi;
+      return true;
+    };
+    // The first parts of the four largest orders first, so that their cores start early; then
+    // each order's remaining parts, highest order first.
+    bool dok = true;
+    for (k = keff; dok && k >= 1 && k + 4 > keff; --k)
+      if (plo[k] < rb[k + 2 > 16 ? 16 : k + 2]) dok = part(k);
+    for (k = keff; dok && k >= 1; --k) {
+      const uint64_t s_hi = rb[k + 2 > 16 ? 16 : k + 2];
+      while (dok && plo[k] < s_hi) dok = part(k);
+      if (!dok) break;
       fam_lim[k].store(s_hi, std::memory_order_release);
       ready[k].store(1, std::memory_order_release);
     }
