@@ -1138,6 +1138,7 @@ struct HierState {
   double* lmid = nullptr;
   double* lerr = nullptr;
   uint64_t* key = nullptr;
+  uint64_t* key2 = nullptr;     // key-value sort scratch
   uint32_t* order0 = nullptr;
   uint32_t* order1 = nullptr;
   uint32_t* perm = nullptr;
@@ -1241,6 +1242,7 @@ cudaError_t ensure_events(HierState& h, uint64_t m) {
   HA(h.lmid, cap);
   HA(h.lerr, cap);
   HA(h.key, cap);
+  HA(h.key2, cap);
   HA(h.order0, cap);
   HA(h.order1, cap);
   HA(h.perm, cap);
@@ -1366,9 +1368,8 @@ int hier_run(Ctx& ctx, uint32_t K) {
   if (total) {
     k_iota<<<nblk(total, kT), kT, 0, st>>>((uint32_t)total, h.order0);
     ++launches;
-    const IndirectKey stages[1] = {{h.key, 0}};
-    const int bits[1] = {64};
-    const int passes = radix_sort_indirect(st, (uint32_t)total, h.order0, h.order1, stages, bits, 1, rs, &launches);
+    // facade order: the event keys (FP64 level midpoints, diagnostics last) move with the indices
+    const int passes = radix_sort_kv(st, (uint32_t)total, h.order0, h.order1, h.key, h.key2, 64, rs, &launches);
     k_ev_gather<<<nblk(total, kT), kT, 0, st>>>((uint32_t)total, h.order0, h.order1, ctx.radix.state, passes, h.ev_raw,
                                                  h.lmid_raw, h.lerr_raw, h.ev, h.lmid, h.lerr, h.perm);
     ++launches;

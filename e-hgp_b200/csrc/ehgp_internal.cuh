@@ -73,6 +73,12 @@ int radix_sort_indirect(cudaStream_t stream, uint32_t n, uint32_t* vals0, uint32
                         const IndirectKey* stages, const int* stage_bits, int stage_count,
                         RadixScratch& scratch, uint64_t* launches);
 
+// Stable LSD sort of (keys0[i], vals0[i]) pairs by the low `bits` bits of the 64-bit keys,
+// the keys moving with the indices (keys1 is scratch of the same size); result selection
+// as for radix_sort_indirect.
+int radix_sort_kv(cudaStream_t stream, uint32_t n, uint32_t* vals0, uint32_t* vals1, uint64_t* keys0,
+                  uint64_t* keys1, int bits, RadixScratch& scratch, uint64_t* launches);
+
 __device__ __forceinline__ const uint32_t* radix_result(const uint32_t* state, int passes,
                                                         const uint32_t* vals0, const uint32_t* vals1) {
   return state[2 * passes] ? vals1 : vals0;

@@ -147,6 +147,77 @@ k_radix_downsweep(uint32_t n, uint32_t* __restrict__ vals0, uint32_t* __restrict
   }
 }
 
+// Key-value variant: the 64-bit keys move with the indices (keys0/keys1 ping-pong with
+// vals0/vals1 under the same pass state), so every pass reads and writes both coalesced
+// instead of gathering the key of each index.
+__global__ void __launch_bounds__(kRadixThreads)
+k_radix_upsweep_kv(uint32_t n, const uint64_t* __restrict__ keys0, const uint64_t* __restrict__ keys1, int shift,
+                   const uint32_t* __restrict__ state, int pass, uint32_t* __restrict__ counts, uint32_t tiles) {
+  __shared__ uint32_t hist[256];
+  const uint32_t tile = blockIdx.x;
+  hist[threadIdx.x] = 0;
+  __syncthreads();
+  const uint64_t* in = state[2 * pass] ? keys1 : keys0;
+  const uint32_t base = tile * kRadixTile;
+#pragma unroll
+  for (int r = 0; r < kRadixItems; ++r) {
+    const uint32_t i = base + r * kRadixThreads + threadIdx.x;
+    if (i < n) atomicAdd(&hist[(uint32_t)(in[i] >> shift) & 0xffu], 1u);
+  }
+  __syncthreads();
+  counts[threadIdx.x * tiles + tile] = hist[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kRadixThreads)
+k_radix_downsweep_kv(uint32_t n, uint32_t* __restrict__ vals0, uint32_t* __restrict__ vals1,
+                     uint64_t* __restrict__ keys0, uint64_t* __restrict__ keys1, int shift,
+                     const uint32_t* __restrict__ state, int pass, const uint32_t* __restrict__ counts,
+                     uint32_t tiles) {
+  if (state[2 * pass + 1]) return;  // every key has the same digit: order unchanged
+  constexpr int kWarps = kRadixThreads / 32;
+  __shared__ uint32_t base[256];
+  __shared__ uint32_t warp_cnt[kWarps][256];
+  const uint32_t tile = blockIdx.x;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const bool flip = state[2 * pass] != 0;
+  const uint32_t* in = flip ? vals1 : vals0;
+  uint32_t* out = flip ? vals0 : vals1;
+  const uint64_t* kin = flip ? keys1 : keys0;
+  uint64_t* kout = flip ? keys0 : keys1;
+  base[tid] = counts[tid * tiles + tile] + state[2 * (kRadixMaxPasses + 1) + tid];
+  const uint32_t lanemask_lt = (1u << lane) - 1u;
+  for (int r = 0; r < kRadixItems; ++r) {
+    const uint32_t i = tile * kRadixTile + r * kRadixThreads + tid;
+    const bool valid = i < n;
+    const uint32_t v = valid ? in[i] : 0u;
+    const uint64_t key = valid ? kin[i] : 0u;
+    const uint32_t dig = valid ? (uint32_t)(key >> shift) & 0xffu : 256u;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) warp_cnt[w][tid] = 0;
+    __syncthreads();
+    const uint32_t peers = __match_any_sync(0xffffffffu, dig);
+    const uint32_t rank = __popc(peers & lanemask_lt);
+    if (valid && rank == 0) warp_cnt[warp][dig] = __popc(peers);
+    __syncthreads();
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t c = warp_cnt[w][tid];
+      warp_cnt[w][tid] = run;
+      run += c;
+    }
+    __syncthreads();
+    if (valid) {
+      const uint32_t at = base[dig] + warp_cnt[warp][dig] + rank;
+      out[at] = v;
+      kout[at] = key;
+    }
+    __syncthreads();
+    base[tid] += run;
+    __syncthreads();
+  }
+}
+
 __global__ void k_radix_init(uint32_t* state) {
   if (threadIdx.x == 0) state[0] = 0;
 }
@@ -171,6 +242,28 @@ int radix_sort_indirect(cudaStream_t stream, uint32_t n, uint32_t* vals0, uint32
       *launches += 4;
       ++pass;
     }
+  }
+  return pass;
+}
+
+// Stable LSD sort of (keys0[i], vals0[i]) pairs by the low `bits` bits of the keys; the
+// result is in the buffer that radix_result(state, passes, vals0, vals1) selects (the keys
+// end beside it, in keys0 or keys1 under the same selection).
+int radix_sort_kv(cudaStream_t stream, uint32_t n, uint32_t* vals0, uint32_t* vals1, uint64_t* keys0,
+                  uint64_t* keys1, int bits, RadixScratch& scratch, uint64_t* launches) {
+  const uint32_t tiles = (n + kRadixTile - 1) / kRadixTile;
+  k_radix_init<<<1, 32, 0, stream>>>(scratch.state);
+  *launches += 1;
+  int pass = 0;
+  for (int shift = 0; shift < bits; shift += 8) {
+    k_radix_upsweep_kv<<<tiles, kRadixThreads, 0, stream>>>(n, keys0, keys1, shift, scratch.state, pass,
+                                                            scratch.counts, tiles);
+    k_radix_rowscan<<<256, 256, 0, stream>>>(scratch.counts, tiles, scratch.state);
+    k_radix_digits<<<1, 256, 0, stream>>>(n, scratch.state, pass);
+    k_radix_downsweep_kv<<<tiles, kRadixThreads, 0, stream>>>(n, vals0, vals1, keys0, keys1, shift, scratch.state,
+                                                              pass, scratch.counts, tiles);
+    *launches += 4;
+    ++pass;
   }
   return pass;
 }
