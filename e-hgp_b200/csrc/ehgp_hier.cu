@@ -1623,6 +1623,12 @@ int hier_run(Ctx& ctx, uint32_t K) {
   std::unique_ptr<std::atomic<uint64_t>[]> fam_lim(new std::atomic<uint64_t>[keff + 1]);
   for (uint32_t k = 0; k <= keff; ++k) fam_lim[k].store(0);
   std::atomic<int> stop_all{0};
+  // This order's union-find handles: every one a root, not yet born (done by the order's
+  // thread while the device descends its first part).
+  auto init_dsu = [&](uint32_t k) {
+    const uint64_t h_lo = k == 1 ? 0 : n + (rb[k] - rb[2]), h_hi = k == 1 ? n : n + (rb[k + 1] - rb[2]);
+    for (uint64_t i = h_lo; i < h_hi; ++i) dsu[i] = {(uint32_t)i, kUnborn};
+  };
   auto run_core = [&](uint32_t k, HierOrderOut& o) {
     const auto to0 = std::chrono::steady_clock::now();
     Progress& pg = prog[k];
@@ -1657,7 +1663,6 @@ int hier_run(Ctx& ctx, uint32_t K) {
     o.node_cls.reset((k == 1 ? n : 0) + fams_k);
     o.fam_res.reset(fams_k);
     // this order's union-find handles
-    for (uint64_t i = h_lo; i < h_hi; ++i) dsu[i] = {(uint32_t)i, kUnborn};
     pg.blocks.clear();
     pg.blocks.resize((births_k + fams_k) / kSnapBlock + 2);  // chunks <= batches / kChunkBatches + multi-role batches + 1
     Cnt c{b_lo, s_lo, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -2262,6 +2267,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
     std::vector<std::thread> pool;
     for (uint32_t k = 1; k <= keff; ++k)
       pool.emplace_back([&, k] {
+        init_dsu(k);
         int r;
         while ((r = ready[k].load(std::memory_order_acquire)) == 0) std::this_thread::sleep_for(std::chrono::microseconds(20));
         if (r == 1) {
