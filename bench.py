@@ -359,11 +359,15 @@ def run_ours(args, world, rank, local):
         "gpu_launches": int(launches),
         "gpu_launches_per_step": int(launches_per_step),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "kernel": "k_higher (triple/quad support enumeration)",
+                     # DRAM bytes of one k_higher launch: ncu capture of the 24^3 lattice (66.0 MB read +
+                     # 1405.1 MB written per launch over 13,824 owners), scaled per owner to this cloud
+                     "traffic": (65981440 + 1405138432) * n / 13824,
+                     "traffic_source": "ncu dram__bytes_read/write.sum on the 13,824-point case, scaled per owner",
+                     "kernel": "k_higher (triple/quad support enumeration)",
                      "kernel_ms": kmean, "algorithmic_bytes": alg_bytes,
                      "work": {"status_tests": tested, "classified": classified, "records": emitted,
                               "candidate_set_entries": set_entries},
-                     "note": "FP64 predicate-bound, not byte-bound: see DESIGN.md",
+                     "note": "FP64 predicate-bound, not byte-bound; traffic is mostly local-memory spills",
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "clocks": clocks.summary(),
     }
