@@ -2227,6 +2227,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
   // claims and replays published chunks, highest order first, then the vertical maps, until
   // every core is done and every chunk and map is finished
   auto work = [&] {
+    uint32_t idle = 0;  // idle rounds: a short spin, then 50 us sleeps (the cores need the CPUs)
     for (;;) {
       bool did = false, all = true;
       for (uint32_t k = keff; k >= 1; --k) {
@@ -2247,10 +2248,14 @@ int hier_run(Ctx& ctx, uint32_t K) {
           all = false;
         if (did) break;
       }
-      if (did) continue;
-      if (vertical_step(all)) continue;
+      if (!did && vertical_step(all)) did = true;
+      if (did) {
+        idle = 0;
+        continue;
+      }
       if (all) return;
-      std::this_thread::yield();
+      if (++idle < 64) std::this_thread::yield();
+      else std::this_thread::sleep_for(std::chrono::microseconds(50));
     }
   };
   // The strict-arm descent runs order by order, highest first, on this thread; an order's
