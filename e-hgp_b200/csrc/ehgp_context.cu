@@ -20,6 +20,18 @@ cudaError_t ctx_alloc(Ctx& ctx, void** ptr, size_t bytes) {
   return e;
 }
 
+void ctx_free(Ctx& ctx, void* ptr, size_t bytes) {
+  if (!ptr) return;
+  for (size_t i = 0; i < ctx.allocations.size(); ++i)
+    if (ctx.allocations[i] == ptr) {
+      ctx.allocations[i] = ctx.allocations.back();
+      ctx.allocations.pop_back();
+      cudaFree(ptr);
+      ctx.device_bytes -= bytes ? bytes : 16;
+      return;
+    }
+}
+
 }  // namespace ehgp
 
 namespace {
@@ -194,6 +206,47 @@ const char* ehgp_status_string(int status) {
 }
 
 uint64_t ehgp_ctx_device_bytes(const ehgp_ctx* ctx) { return ctx ? ctx->device_bytes : 0; }
+
+int ehgp_ctx_reserve(ehgp_ctx* ctx, uint32_t stage, uint64_t records) {
+  if (!ctx || stage > 1 || records == 0 || records >= 0xffff0000ull) return EHGP_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  ctx->last_error.clear();
+  if (ctx->poisoned) return fail(ctx, EHGP_ERR_POISONED, "the context is poisoned by an earlier CUDA failure");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamSynchronize");
+  // the resident records (if any) are dropped with the buffers
+  if (stage == 0) {
+    ctx->pb.K = 0;
+    ctx->pb.count = 0;
+    ctx->pb.witness_ready = false;
+    e = ehgp::pairs_records_alloc(*ctx, records);
+  } else {
+    ctx->hb.K = 0;
+    ctx->hb.count = 0;
+    e = ehgp::higher_records_alloc(*ctx, records);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, EHGP_ERR_OUT_OF_MEMORY, "the reserved record buffers do not fit the device");
+  }
+  return EHGP_OK;
+}
+
+uint64_t ehgp_ctx_regrowths(const ehgp_ctx* ctx) { return ctx ? ctx->regrowths : 0; }
+
+int ehgp_tune(ehgp_ctx* ctx, uint32_t knob, uint64_t value) {
+  if (!ctx) return EHGP_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  switch (knob) {
+    case EHGP_TUNE_HIGHER_LIST:
+      if (value < 1 || value > 1024) return fail(ctx, EHGP_ERR_INVALID_ARGUMENT, "list capacity must be in [1, 1024]");
+      ctx->hb.list_cap = (uint32_t)value;
+      return EHGP_OK;
+    default:
+      return fail(ctx, EHGP_ERR_INVALID_ARGUMENT, "unknown tuning knob");
+  }
+}
 
 int ehgp_lbvh_build(ehgp_ctx* ctx, const double* xyz, uint64_t n, const ehgp_lbvh_out* out) {
   return lbvh_build_common(ctx, xyz, n, out, 0);

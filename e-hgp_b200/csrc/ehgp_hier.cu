@@ -1194,6 +1194,10 @@ struct HierState {
   double ms_device = 0, ms_forest = 0, ms_descent = 0, ms_orders = 0;
   double ms_host[4] = {0, 0, 0, 0};  // exact facade ties, order passes, (unused), vertical maps
   uint64_t descent_steps = 0, arms = 0, exact_boundaries = 0;
+  // Schedule of the host forest pass and of the descent parts (results never depend on it):
+  // single-role batches per published chunk, arms per descent part, host pool threads
+  // (0: every hardware thread).
+  uint32_t chunk_batches = 1u << 14, part_arms = 1u << 22, pool_threads = 0;
 };
 
 void hier_free(Ctx& ctx) {
@@ -1599,7 +1603,8 @@ int hier_run(Ctx& ctx, uint32_t K) {
     uint32_t jb, role, birth, sad, grp, node, child, count;
     uint64_t carriers, reduced;
   };
-  constexpr uint32_t kChunkBatches = 1u << 14, kSnapBlock = 4096;
+  const uint32_t kChunkBatches = h.chunk_batches;
+  constexpr uint32_t kSnapBlock = 4096;
   struct Progress {
     std::vector<std::unique_ptr<Cnt[]>> blocks;  // published chunk starts, kSnapBlock per block
     std::atomic<uint32_t> published{0}, claimed{0}, replayed{0};
@@ -1664,7 +1669,8 @@ int hier_run(Ctx& ctx, uint32_t K) {
     o.fam_res.reset(fams_k);
     // this order's union-find handles
     pg.blocks.clear();
-    pg.blocks.resize((births_k + fams_k) / kSnapBlock + 2);  // chunks <= batches / kChunkBatches + multi-role batches + 1
+    // chunks <= batches / kChunkBatches + multi-role batches + 1 <= batches + 1
+    pg.blocks.resize((births_k + fams_k + 1) / kSnapBlock + 2);
     Cnt c{b_lo, s_lo, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     uint32_t nchunk = 0;
     Cnt open = c;  // start of the chunk being filled
@@ -2267,7 +2273,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
   const char* dmsg = "";
   cudaError_t dcuda = cudaSuccess;
   {
-    const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint32_t hw = h.pool_threads ? h.pool_threads : std::max(1u, std::thread::hardware_concurrency());
     const uint32_t extra = hw > keff + 1 ? std::min(hw - keff - 1, 32u) : 0u;  // one CPU for this thread
     std::vector<std::thread> pool;
     for (uint32_t k = 1; k <= keff; ++k)
@@ -2304,7 +2310,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
       dstatus = status;
       dmsg = msg;
     };
-    constexpr uint32_t kPartArms = 1u << 22;  // arms per part of an order's descent (about)
+    const uint32_t kPartArms = h.part_arms;  // arms per part of an order's descent (about)
     std::vector<uint64_t> plo(keff + 1);
     for (uint32_t j = 1; j <= keff; ++j) plo[j] = rb[j + 1];
     // Descends the next part of order k (cut at a batch boundary after about kPartArms arms)
@@ -2518,6 +2524,17 @@ int ehgp_hierarchy(ehgp_ctx* ctx, uint32_t K, ehgp_hier_counts* counts) {
     counts->decision = (uint32_t)s;
   }
   return s;
+}
+
+int ehgp_hier_schedule(ehgp_ctx* ctx, uint32_t chunk_batches, uint32_t part_arms, uint32_t host_threads) {
+  if (!ctx) return EHGP_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  if (!ctx->hier) ctx->hier = new ehgp::HierState();
+  ehgp::HierState& h = *ctx->hier;
+  h.chunk_batches = chunk_batches ? chunk_batches : 1u << 14;
+  h.part_arms = part_arms ? part_arms : 1u << 22;
+  h.pool_threads = host_threads;
+  return EHGP_OK;
 }
 
 int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out) {

@@ -227,7 +227,7 @@ k_gather(uint32_t n, uint32_t root, const TNode* __restrict__ tn, const uint32_t
   const uint32_t pos = blockIdx.x * kWarps + warp;
   if (pos >= n) return;
   const uint32_t a = leaf_pid[pos];
-  if (!todo[a]) return;
+  if (todo[a] != 1) return;
   const double ax = px[a], ay = py[a], az = pz[a];
   const double R2 = gather_r2[a] * (1.0 + 32.0 * kU);
   uint32_t* out = nb + (uint64_t)a * kMaxNb;
@@ -332,6 +332,9 @@ k_gather(uint32_t n, uint32_t root, const TNode* __restrict__ tn, const uint32_t
 // certifies rho_s when rho_s <= L / 2: every unlisted point has rho >= L / 2.
 constexpr int kDirThreads = 128;  // one block per point: four warps share its sorted list
 constexpr int kMaxCand = 256;     // candidate-set capacity per point
+constexpr int kLargeCand = 1024;  // large sets: staged whole in shared memory with their face mask
+constexpr int kHugeCand = 4096;   // huge sets: staged in shared memory, face mask in global scratch
+constexpr int kMegaCand = 16384;  // larger sets: set and face mask in global scratch (one per block)
 constexpr int kMaxNeed = kMaxInteriorH + 1;  // s_max - 2 for K = 10
 
 struct CertParams {
@@ -392,7 +395,7 @@ __device__ __forceinline__ float warp_top_merge(float top, float v, uint32_t lan
 #define EHGP_DIRTABLE_BLOCKS_PER_SM 10
 #endif
 __global__ void __launch_bounds__(kDirThreads, EHGP_DIRTABLE_BLOCKS_PER_SM)
-k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uint32_t* __restrict__ nb,
+k_dirtable(uint32_t n, uint32_t list_cap, CertParams cp, const uint32_t* __restrict__ leaf_pid, uint32_t* __restrict__ nb,
            const uint32_t* __restrict__ nbc, const double* __restrict__ px, const double* __restrict__ py,
            const double* __restrict__ pz, const double* __restrict__ gather_r2, uint8_t* __restrict__ todo,
            uint32_t* __restrict__ cand, uint32_t* __restrict__ candc, double* __restrict__ need_r,
@@ -405,10 +408,10 @@ k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uin
   const uint32_t pos = blockIdx.x;
   if (pos >= n) return;
   const uint32_t a = leaf_pid[pos];
-  if (!todo[a]) return;
+  if (todo[a] != 1) return;
   const uint32_t m = nbc[a];
-  if (m > (uint32_t)kMaxNb) {
-    if (t == 0) need_r[a] = INFINITY;
+  if (m > list_cap) {  // more neighbours than a list holds: the large-neighbourhood path
+    if (t == 0) todo[a] = 3;
     return;
   }
   const double ax = px[a], ay = py[a], az = pz[a];
@@ -570,11 +573,383 @@ k_dirtable(uint32_t n, CertParams cp, const uint32_t* __restrict__ leaf_pid, uin
   if (lane == 0) {
     candc[a] = overflow ? (uint32_t)kMaxCand + 1 : c;
     need_r[a] = worst_needed;
-    todo[a] = overflow ? 2 : 0;  // 2: candidate set too large (reported)
+    todo[a] = overflow ? 4 : 0;  // 4: certified, candidate set above kMaxCand (k_cand_large)
   }
 }
 
 
+
+// ---- 2b. large neighbourhoods ------------------------------------------------------------
+// Owners whose gather radius holds more than kMaxNb points (edges of dense clusters whose
+// bounds reach into a sparse background, points near the hull) take this path, with the
+// same certificate: their neighbour lists are counted, allocated in one arena and written
+// (one thread per owner, depth first, whole subtrees inside the radius taken as ranges); a
+// block per owner then stages its list in chunks and keeps, per direction, the `need` largest
+// lower bounds of 1 / rho_shr with every neighbour seen (the list is not sorted, so there is
+// no early exit), marks the candidates and writes C(a) sorted by binary32 distance.
+constexpr int kBigStack = 128;    // traversal stack: the LBVH is at most 63 + log2(n) + 1 deep
+constexpr int kBigThreads = 256;  // one block of eight warps per large owner
+constexpr int kBigChunk = 2048;   // neighbours staged per step
+
+__global__ void __launch_bounds__(128)
+k_gather_big(uint32_t nbig, const uint32_t* __restrict__ big, uint32_t root, const TNode* __restrict__ tn,
+             const uint32_t* __restrict__ leaf_pid, const uint32_t* __restrict__ n_begin,
+             const uint32_t* __restrict__ n_end, const double* __restrict__ px, const double* __restrict__ py,
+             const double* __restrict__ pz, const double* __restrict__ gather_r2, const uint64_t* __restrict__ off,
+             uint32_t* __restrict__ arena, uint32_t* __restrict__ cnt, uint32_t* __restrict__ err) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nbig) return;
+  const uint32_t a = big[i];
+  const double ax = px[a], ay = py[a], az = pz[a];
+  const double R2 = gather_r2[a] * (1.0 + 32.0 * kU);
+  const uint64_t cap = arena ? off[i + 1] - off[i] : 0;
+  uint32_t* out = arena ? arena + off[i] : nullptr;
+  uint64_t c = 0;
+  uint32_t stack[kBigStack];
+  int top = 0;
+  stack[top++] = root;
+  while (top > 0) {
+    const uint32_t node = stack[--top];
+    const TNode t = load_node(tn, node);
+    if (t.left == kInvalid32) {
+      const uint32_t pid = t.right;
+      const double dx = px[pid] - ax, dy = py[pid] - ay, dz = pz[pid] - az;
+      if (pid != a && dx * dx + dy * dy + dz * dz <= R2) {
+        if (c < cap) out[c] = pid;
+        ++c;
+      }
+      continue;
+    }
+    const double lx = fmax(fmax((double)t.lo[0] - ax, ax - (double)t.hi[0]), 0.0);
+    const double ly = fmax(fmax((double)t.lo[1] - ay, ay - (double)t.hi[1]), 0.0);
+    const double lz = fmax(fmax((double)t.lo[2] - az, az - (double)t.hi[2]), 0.0);
+    if ((lx * lx + ly * ly + lz * lz) * (1.0 - 16.0 * kU) > R2) continue;
+    const double ux = fmax(fabs((double)t.lo[0] - ax), fabs((double)t.hi[0] - ax));
+    const double uy = fmax(fabs((double)t.lo[1] - ay), fabs((double)t.hi[1] - ay));
+    const double uz = fmax(fabs((double)t.lo[2] - az), fabs((double)t.hi[2] - az));
+    if ((ux * ux + uy * uy + uz * uz) * (1.0 + 16.0 * kU) < R2) {  // the whole subtree is inside
+      for (uint32_t q = n_begin[node]; q < n_end[node]; ++q) {
+        const uint32_t pid = leaf_pid[q];
+        if (pid == a) continue;
+        if (c < cap) out[c] = pid;
+        ++c;
+      }
+      continue;
+    }
+    if (top + 2 > kBigStack) {
+      atomicOr(err, kErrCapacity);
+      return;
+    }
+    stack[top++] = t.right;
+    stack[top++] = t.left;
+  }
+  if (!arena) cnt[i] = (uint32_t)c;
+  else if (c != cap) atomicOr(err, kErrInternal);
+}
+
+// Dynamic shared memory of k_dirtable_big.
+constexpr size_t kBigSmem = (size_t)kBigChunk * 16 + (size_t)kDirs * kMaxNeed * 4 + (size_t)kDirs * 4 + 16 +
+                            (size_t)kDirs * 8 + (size_t)kMaxCand * 8;
+
+__global__ void __launch_bounds__(kBigThreads)
+k_dirtable_big(uint32_t nbig, CertParams cp, const uint32_t* __restrict__ big, const uint64_t* __restrict__ off,
+               const uint32_t* __restrict__ arena, const double* __restrict__ px, const double* __restrict__ py,
+               const double* __restrict__ pz, const double* __restrict__ gather_r2, uint8_t* __restrict__ todo,
+               uint32_t* __restrict__ cand, uint32_t* __restrict__ candc, double* __restrict__ need_r,
+               float* __restrict__ rho_tab) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float4* rel = reinterpret_cast<float4*>(smem);               // [kBigChunk] unit direction, 1 / |p - a|
+  float* topt = reinterpret_cast<float*>(rel + kBigChunk);     // [kDirs][kMaxNeed] descending
+  float* rho = topt + kDirs * kMaxNeed;                        // [kDirs] certified per-cone bounds
+  double* ext = reinterpret_cast<double*>(reinterpret_cast<uintptr_t>(rho + kDirs + 3) & ~uintptr_t(7));  // [kDirs]
+  uint32_t* cid = reinterpret_cast<uint32_t*>(ext + kDirs);    // [kMaxCand]
+  float* cds = reinterpret_cast<float*>(cid + kMaxCand);       // [kMaxCand] binary32 |p - a|
+  __shared__ double s_worst[kBigThreads / 32];
+  __shared__ float s_rmax[kBigThreads / 32];
+  __shared__ uint32_t s_c;
+  const uint32_t t = threadIdx.x, warp = t >> 5, lane = t & 31u;
+  if (blockIdx.x >= nbig) return;
+  const uint32_t a = big[blockIdx.x];
+  const uint64_t m = off[blockIdx.x + 1] - off[blockIdx.x];
+  const uint32_t* list = arena + off[blockIdx.x];
+  const double ax = px[a], ay = py[a], az = pz[a];
+  const double L2 = sqrt(gather_r2[a]) * (1.0 - 1e-9);  // the list covers |p - a| <= L
+  const double half_L = 0.5 * L2;
+  const double cd = cos(cp.delta), sdl = sin(cp.delta);
+  const float cdf = (float)cd, sdlf = (float)sdl;
+  const uint32_t need = cp.need;
+  for (uint32_t d = t; d < (uint32_t)kDirs; d += kBigThreads) {
+    const double s0 = cp.dirs[3 * d], s1 = cp.dirs[3 * d + 1], s2 = cp.dirs[3 * d + 2];
+    const double e = cone_ext(cp, s0, ax, 0) + cone_ext(cp, s1, ay, 1) + cone_ext(cp, s2, az, 2);
+    const double exit_r = fmin(fmin(cone_exit(cp, s0, ax, 0), cone_exit(cp, s1, ay, 1)), cone_exit(cp, s2, az, 2));
+    ext[d] = fmin(e * (1.0 + 1e-12), exit_r);
+    for (uint32_t j = 0; j < (uint32_t)kMaxNeed; ++j) topt[d * kMaxNeed + j] = 0.0f;
+  }
+  if (t == 0) s_c = 0;
+  __syncthreads();
+  // 1. per cone, the `need` largest lower bounds of 1 / rho_shr over the whole list
+  for (uint64_t base = 0; base < m; base += kBigChunk) {
+    const uint32_t cnt = (uint32_t)min((uint64_t)kBigChunk, m - base);
+    for (uint32_t j = t; j < cnt; j += kBigThreads) {
+      const uint32_t p = list[base + j];
+      const double x = px[p] - ax, y = py[p] - ay, z = pz[p] - az;
+      const double dd = sqrt(x * x + y * y + z * z);
+      const double inv = dd > 0.0 ? 1.0 / dd : 0.0;
+      const float df = (float)dd;
+      rel[j] = make_float4((float)(x * inv), (float)(y * inv), (float)(z * inv), 1.0f / df);
+    }
+    __syncthreads();
+    for (uint32_t d = warp; d < (uint32_t)kDirs; d += kBigThreads / 32) {
+      const float u0 = cp.dirs[3 * d], u1 = cp.dirs[3 * d + 1], u2 = cp.dirs[3 * d + 2];
+      const float inv_ext = 1.0f / __double2float_ru(ext[d]);
+      float top = lane < need ? topt[d * kMaxNeed + lane] : 0.0f;
+      float thr = __shfl_sync(0xffffffffu, top, need - 1);
+      for (uint32_t sb = 0; sb < cnt; sb += 32) {
+        const uint32_t j = sb + lane;
+        const float lim = 0.5f * (1.0f - 1e-5f) * fmaxf(thr, inv_ext);
+        const float4 r = j < cnt ? rel[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        float inv = 0.0f;
+        if (j < cnt && !(lim > r.w)) {
+          const float c = u0 * r.x + u1 * r.y + u2 * r.z;
+          const float cs = fmaxf(-1.0f, c - 1e-5f);
+          const float sn = sqrtf(fmaxf(0.0f, (1.0f - cs) * (1.0f + cs)));
+          const float cshr = cs * cdf - sn * sdlf - 1e-6f;
+          if (cshr > 1e-6f) inv = 2.0f * cshr * r.w * (1.0f - 1e-5f);
+        }
+        if (__any_sync(0xffffffffu, inv > thr)) {
+          top = warp_top_merge(top, inv, lane);
+          thr = __shfl_sync(0xffffffffu, top, need - 1);
+        }
+      }
+      if (lane < need) topt[d * kMaxNeed + lane] = top;
+    }
+    __syncthreads();
+  }
+  // certified per-cone bounds (same rule as the list path)
+  double worst = 0.0;
+  float rmax = 0.0f;
+  bool ok = true;
+  for (uint32_t d = t; d < (uint32_t)kDirs; d += kBigThreads) {
+    const float thr = topt[d * kMaxNeed + need - 1];
+    const double kth = thr > 0.0f ? (1.0 / (double)thr) * (1.0 + 1e-12) : INFINITY;
+    const double rho_s = fmin(kth, ext[d]);
+    const float rho_sf = __double2float_ru(rho_s);
+    rho[d] = rho_sf;
+    rho_tab[(uint64_t)a * kDirs + d] = rho_sf;
+    if (!(rho_s <= half_L)) ok = false;
+    worst = fmax(worst, rho_s);
+    rmax = fmaxf(rmax, rho_sf);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    worst = fmax(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+    rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+  }
+  if (lane == 0) {
+    s_worst[warp] = worst;
+    s_rmax[warp] = rmax;
+  }
+  ok = __syncthreads_and(ok);
+  for (int w = 0; w < kBigThreads / 32; ++w) {
+    worst = fmax(worst, s_worst[w]);
+    rmax = fmaxf(rmax, s_rmax[w]);
+  }
+  if (!ok) {  // the list must grow to 2 rho_s (with room); the owner stays on this path
+    if (t == 0) need_r[a] = worst;
+    return;
+  }
+  // 2. candidates: rho_lo_p(s) <= rho_s for some cone s
+  for (uint64_t j = t; j < m; j += kBigThreads) {
+    const uint32_t p = list[j];
+    const double x = px[p] - ax, y = py[p] - ay, z = pz[p] - az;
+    const double dd = sqrt(x * x + y * y + z * z);
+    const double inv = dd > 0.0 ? 1.0 / dd : 0.0;
+    const float df = (float)dd;
+    const float rw = 1.0f / df;
+    if (0.5f * (1.0f - 1e-5f) > rmax * rw) continue;  // beyond 2 rho_s of every cone
+    const float r0 = (float)(x * inv), r1 = (float)(y * inv), r2 = (float)(z * inv);
+    bool f = false;
+    for (uint32_t d = 0; d < (uint32_t)kDirs && !f; ++d) {
+      const float rho_sf = rho[d];
+      if (0.5f * (1.0f - 1e-5f) > rho_sf * rw) continue;
+      const float c = cp.dirs[3 * d] * r0 + cp.dirs[3 * d + 1] * r1 + cp.dirs[3 * d + 2] * r2;
+      const float cs = fminf(1.0f, c + 1e-5f);
+      const float sn = sqrtf(fmaxf(0.0f, (1.0f - cs) * (1.0f + cs)));
+      const float clo = (cs >= cdf) ? 1.0f : cs * cdf + sn * sdlf + 1e-6f;
+      f = clo > 0.0f && 2.0f * clo * rho_sf * rw * (1.0f + 2e-5f) >= 1.0f;
+    }
+    if (f) {
+      const uint32_t at = atomicAdd(&s_c, 1u);
+      if (at < (uint32_t)kMaxCand) {
+        cid[at] = p;
+        cds[at] = df;
+      }
+    }
+  }
+  __syncthreads();
+  const uint32_t c = s_c;
+  if (c > (uint32_t)kMaxCand) {
+    if (t == 0) {
+      candc[a] = (uint32_t)kMaxCand + 1;
+      need_r[a] = worst;
+      todo[a] = 4;  // certified, candidate set above kMaxCand (k_cand_large)
+    }
+    return;
+  }
+  // 3. C(a) in binary32 distance order (bitonic over kMaxCand slots)
+  for (uint32_t j = c + t; j < (uint32_t)kMaxCand; j += kBigThreads) {
+    cds[j] = INFINITY;
+    cid[j] = kInvalid32;
+  }
+  __syncthreads();
+  for (uint32_t k = 2; k <= (uint32_t)kMaxCand; k <<= 1)
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t x = t; x < (uint32_t)kMaxCand; x += kBigThreads) {
+        const uint32_t y = x ^ j;
+        if (y > x) {
+          const bool up = (x & k) == 0;
+          const float dx = cds[x], dy = cds[y];
+          if ((dx > dy) == up) {
+            cds[x] = dy;
+            cds[y] = dx;
+            const uint32_t tmp = cid[x];
+            cid[x] = cid[y];
+            cid[y] = tmp;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  for (uint32_t j = t; j < c; j += kBigThreads) cand[(uint64_t)a * kMaxCand + j] = cid[j];
+  if (t == 0) {
+    candc[a] = c;
+    need_r[a] = worst;
+    todo[a] = 0;
+  }
+}
+
+// ---- 2c. large candidate sets -------------------------------------------------------------
+// Owners certified with more than kMaxCand candidates: their candidate sets are counted and
+// then written, sorted by binary32 distance, into an arena (count -> allocate -> write), from
+// the certified per-cone bounds rho_tab and the owner's neighbour list (the per-point list,
+// or the large-neighbourhood arena); the candidate rule is the one of the direction tables.
+constexpr int kCandThreads = 256;
+
+template <bool kFromArena>
+__global__ void __launch_bounds__(kCandThreads)
+k_cand_large(uint32_t nown, const uint32_t* __restrict__ owners, const uint32_t* __restrict__ nb,
+             const uint32_t* __restrict__ nbc, const uint64_t* __restrict__ loff, const uint32_t* __restrict__ larena,
+             CertParams cp, const double* __restrict__ px, const double* __restrict__ py,
+             const double* __restrict__ pz, const float* __restrict__ rho_tab, const uint64_t* __restrict__ coff,
+             uint32_t* __restrict__ carena, uint32_t* __restrict__ ccnt, float* __restrict__ dist_scratch) {
+  // counting pass: carena == nullptr, ccnt[i] receives the count; writing pass: the sorted
+  // set goes to carena + coff[i] when its count equals ccnt[i]
+  __shared__ float rho[kDirs];
+  __shared__ float s_rmax[kCandThreads / 32];
+  __shared__ uint32_t s_c;
+  __shared__ float s_cds[kHugeCand];
+  __shared__ uint32_t s_cid[kHugeCand];
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  const uint32_t i = blockIdx.x;
+  if (i >= nown) return;
+  const uint32_t a = owners[i];
+  // the set is gathered and sorted in shared memory up to kHugeCand entries, above that in
+  // its own slot of the arena (kMegaCand at most), with the distances in `dist_scratch`
+  const bool in_arena = carena != nullptr && ccnt[i] > (uint32_t)kHugeCand;
+  float* cds = in_arena ? dist_scratch + coff[i] : s_cds;
+  uint32_t* cid = in_arena ? carena + coff[i] : s_cid;
+  const uint32_t cap = in_arena ? (uint32_t)kMegaCand : (uint32_t)kHugeCand;
+  const uint32_t* list = kFromArena ? larena + loff[i] : nb + (uint64_t)a * kMaxNb;
+  const uint64_t m = kFromArena ? loff[i + 1] - loff[i] : nbc[a];
+  const double ax = px[a], ay = py[a], az = pz[a];
+  const float cdf = (float)cos(cp.delta), sdlf = (float)sin(cp.delta);
+  float rmax = 0.0f;
+  for (uint32_t d = t; d < (uint32_t)kDirs; d += kCandThreads) {
+    rho[d] = rho_tab[(uint64_t)a * kDirs + d];
+    rmax = fmaxf(rmax, rho[d]);
+  }
+  for (int o = 16; o > 0; o >>= 1) rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+  if (lane == 0) s_rmax[warp] = rmax;
+  if (t == 0) s_c = 0;
+  __syncthreads();
+  for (int w = 0; w < kCandThreads / 32; ++w) rmax = fmaxf(rmax, s_rmax[w]);
+  const bool write = carena != nullptr;
+  for (uint64_t j = t; j < m; j += kCandThreads) {
+    const uint32_t p = list[j];
+    const double x = px[p] - ax, y = py[p] - ay, z = pz[p] - az;
+    const double dd = sqrt(x * x + y * y + z * z);
+    const double inv = dd > 0.0 ? 1.0 / dd : 0.0;
+    const float df = (float)dd;
+    const float rw = 1.0f / df;
+    if (0.5f * (1.0f - 1e-5f) > rmax * rw) continue;
+    const float r0 = (float)(x * inv), r1 = (float)(y * inv), r2 = (float)(z * inv);
+    bool f = false;
+    for (uint32_t d = 0; d < (uint32_t)kDirs && !f; ++d) {
+      const float rho_sf = rho[d];
+      if (0.5f * (1.0f - 1e-5f) > rho_sf * rw) continue;
+      const float c = cp.dirs[3 * d] * r0 + cp.dirs[3 * d + 1] * r1 + cp.dirs[3 * d + 2] * r2;
+      const float cs = fminf(1.0f, c + 1e-5f);
+      const float sn = sqrtf(fmaxf(0.0f, (1.0f - cs) * (1.0f + cs)));
+      const float clo = (cs >= cdf) ? 1.0f : cs * cdf + sn * sdlf + 1e-6f;
+      f = clo > 0.0f && 2.0f * clo * rho_sf * rw * (1.0f + 2e-5f) >= 1.0f;
+    }
+    if (f) {
+      const uint32_t at = atomicAdd(&s_c, 1u);
+      if (write && at < cap && at < ccnt[i]) {
+        cid[at] = p;
+        cds[at] = df;
+      }
+    }
+  }
+  __syncthreads();
+  const uint32_t c = s_c;
+  if (!write) {
+    if (t == 0) ccnt[i] = c;
+    return;
+  }
+  if (c != ccnt[i] || c > cap) return;  // the counting pass gave the same count
+  if (in_arena) {  // sorted in place (odd-even transposition: the slot holds exactly c entries)
+    for (uint32_t r = 0; r < c; ++r) {
+      for (uint32_t x = 2 * t + (r & 1); x + 1 < c; x += 2 * kCandThreads) {
+        const float dx = cds[x], dy = cds[x + 1];
+        if (dx > dy) {
+          cds[x] = dy;
+          cds[x + 1] = dx;
+          const uint32_t tmp = cid[x];
+          cid[x] = cid[x + 1];
+          cid[x + 1] = tmp;
+        }
+      }
+      __syncthreads();
+    }
+    return;
+  }
+  uint32_t P = 32;
+  while (P < c) P <<= 1;
+  for (uint32_t j = c + t; j < P; j += kCandThreads) {
+    cds[j] = INFINITY;
+    cid[j] = kInvalid32;
+  }
+  __syncthreads();
+  for (uint32_t k = 2; k <= P; k <<= 1)
+    for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
+      for (uint32_t x = t; x < P; x += kCandThreads) {
+        const uint32_t y = x ^ jj;
+        if (y > x) {
+          const bool up = (x & k) == 0;
+          const float dx = cds[x], dy = cds[y];
+          if ((dx > dy) == up) {
+            cds[x] = dy;
+            cds[y] = dx;
+            const uint32_t tmp = cid[x];
+            cid[x] = cid[y];
+            cid[y] = tmp;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  for (uint32_t j = t; j < c; j += kCandThreads) carena[coff[i] + j] = cid[j];
+}
 
 // ---- 3. owner-local enumeration ---------------------------------------------------------
 // One warp per owner a.  C(a) is staged in shared memory as rounded differences
@@ -619,13 +994,15 @@ struct HigherTables {
   double cos_lim;          // cos(delta) raised by a margin: inside the cone for sure
 };
 
-struct OwnerSmem {  // one owner's staged candidate set, shared by the block's warps
-  uint32_t sid[kMaxCand];
-  SetPt spt[kMaxCand];
-  uint16_t supi[kMaxCand];
-  uint32_t adm[kMaxCand][kMaxCand / 32];  // adm[j] bit k (j < k): face (a, j, k) within the bound
+template <int KC>
+struct OwnerSmemT {  // one owner's staged candidate set (at most KC), shared by the block's warps
+  uint32_t sid[KC];
+  SetPt spt[KC];
+  uint16_t supi[KC];
   float rho[kDirs];
 };
+// The face mask sits beside it: adm[j * (KC / 32) + w] bit k (j < k): face (a, j, k) within the bound.
+using OwnerSmem = OwnerSmemT<kMaxCand>;
 
 struct WarpQueue {  // one warp's queued supports
   uint32_t iids[kMaxInteriorH];
@@ -679,7 +1056,8 @@ __device__ float sphere_cut(const QEntry& E, double eA, double eN) {
 }
 
 // Classifies the queued supports against C(a) with the whole warp and emits the relevant ones.
-__device__ __forceinline__ void classify_queue(const OwnerSmem& S, WarpQueue& Q, uint32_t qn, uint32_t m, const Cloud& c,
+template <int KC>
+__device__ __forceinline__ void classify_queue(const OwnerSmemT<KC>& S, WarpQueue& Q, uint32_t qn, uint32_t m, const Cloud& c,
                                uint32_t smax, HigherRec* out, uint32_t cap, uint32_t* counter, uint32_t lane,
                                unsigned long long& emitted) {
   for (uint32_t e = 0; e < qn; ++e) {
@@ -789,24 +1167,22 @@ __device__ __forceinline__ uint32_t select_bit(uint32_t x, uint32_t r) {
   return pos;
 }
 
-__global__ void __launch_bounds__(32 * kHOwnerWarps, kHBlocksPerSM)
-k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf_pid, const uint32_t* __restrict__ cand,
-         const uint32_t* __restrict__ candc, const double* __restrict__ px, const double* __restrict__ py,
-         const double* __restrict__ pz, const int* __restrict__ cloud_scale, HigherRec* __restrict__ out,
-         uint32_t* __restrict__ counter, unsigned long long* __restrict__ stats) {
-  __shared__ OwnerSmem S;
-  __shared__ WarpQueue wq[kHOwnerWarps];
+// Enumeration of owner a over its candidate set clist[0..m) (m <= KC, sorted by binary32
+// distance from a), by the whole block; adm holds KC * KC / 32 words (shared or global).
+template <int KC>
+__device__ __forceinline__ void higher_owner(uint32_t a, const uint32_t* __restrict__ clist, uint32_t m,
+                                             OwnerSmemT<KC>& S, uint32_t* adm, WarpQueue* wq, const Ctl& ctl,
+                                             const HigherTables& tb, const double* __restrict__ px,
+                                             const double* __restrict__ py, const double* __restrict__ pz,
+                                             const int* __restrict__ cloud_scale, HigherRec* __restrict__ out,
+                                             uint32_t* __restrict__ counter, unsigned long long* __restrict__ stats) {
+  constexpr uint32_t kWords = KC / 32;
   __shared__ double s_Mp;
   __shared__ uint32_t s_mc;
   __shared__ float s_rmax[kHOwnerWarps];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t pos = blockIdx.x;
-  if (pos >= n) return;
   WarpQueue& Q = wq[warp];
-  const uint32_t a = leaf_pid[pos];
   const Cloud c{px, py, pz, cloud_scale[0]};
-  const uint32_t m = candc[a];
-  if (m > (uint32_t)kMaxCand) return;  // reported by the host
   const double ax = px[a], ay = py[a], az = pz[a];
   // warp 0 stages C(a) (and the support candidates, ids above a); the block clears the
   // face mask and loads the cone bounds
@@ -814,7 +1190,7 @@ k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf
   double Mp = 0.0;
   for (uint32_t base = 0; warp == 0 && base < m; base += 32) {
     const uint32_t i = base + lane;
-    const uint32_t p = i < m ? cand[(uint64_t)a * kMaxCand + i] : kInvalid32;
+    const uint32_t p = i < m ? clist[i] : kInvalid32;
     if (i < m) {
       SetPt s;
       s.x = px[p] - ax;
@@ -836,8 +1212,7 @@ k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf
     S.rho[d] = r;
     rmax = fmaxf(rmax, r);
   }
-  for (uint32_t i = threadIdx.x; i < (uint32_t)kMaxCand * (kMaxCand / 32); i += 32 * kHOwnerWarps)
-    S.adm[i / (kMaxCand / 32)][i % (kMaxCand / 32)] = 0u;
+  for (uint32_t i = threadIdx.x; i < (uint32_t)KC * kWords; i += 32 * kHOwnerWarps) adm[i] = 0u;
   for (int off = 16; off > 0; off >>= 1) {
     Mp = fmax(Mp, __shfl_xor_sync(0xffffffffu, Mp, off));
     rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, off));
@@ -869,11 +1244,11 @@ k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf
       E.ids[2] = S.sid[ik];
       E.ids[3] = kInvalid32;
       double eA, eN;
-      bool adm;
+      bool face_ok;
       ++tested;
-      const int st = tri_eval(c, S.spt[ij], S.spt[ik], E.ids[0], E.ids[1], E.ids[2], Mp, rmax2, E, eA, eN, adm);
-      if (adm) {
-        atomicOr(&S.adm[j][k >> 5], 1u << (k & 31));
+      const int st = tri_eval(c, S.spt[ij], S.spt[ik], E.ids[0], E.ids[1], E.ids[2], Mp, rmax2, E, eA, eN, face_ok);
+      if (face_ok) {
+        atomicOr(&adm[j * kWords + (k >> 5)], 1u << (k & 31));
         ++admitted;
       }
       if (st == 0 && ctl.smax >= 3) {
@@ -894,16 +1269,15 @@ k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf
   __syncthreads();  // the face mask is complete
   // --- tetrahedra (a, j, k, l), j < k < l with adm(j,k), adm(j,l), adm(k,l)
   if (ctl.smax >= 4) {
-    constexpr uint32_t kWords = kMaxCand / 32;
     for (uint64_t t0 = 32 * warp; t0 < P2; t0 += 32 * kHOwnerWarps) {
       const uint64_t t = t0 + lane;
       uint32_t j = 0, k = 0, cnt = 0;
       if (t < P2) {
         decode_pair(t, j, k);
-        if ((S.adm[j][k >> 5] >> (k & 31)) & 1u) {
+        if ((adm[j * kWords + (k >> 5)] >> (k & 31)) & 1u) {
           const uint32_t w0 = (k + 1) >> 5;
           for (uint32_t w = w0; w < kWords; ++w) {
-            uint32_t bits = S.adm[j][w] & S.adm[k][w];
+            uint32_t bits = adm[j * kWords + w] & adm[k * kWords + w];
             if (w == w0) bits &= ((k + 1) & 31) ? (0xffffffffu << ((k + 1) & 31)) : 0xffffffffu;
             cnt += __popc(bits);
           }
@@ -931,7 +1305,7 @@ k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf
           uint32_t r = q - oe, l = 0;
           const uint32_t w0 = (ok + 1) >> 5;
           for (uint32_t w = w0; w < kWords; ++w) {
-            uint32_t bits = S.adm[oj][w] & S.adm[ok][w];
+            uint32_t bits = adm[oj * kWords + w] & adm[ok * kWords + w];
             if (w == w0) bits &= ((ok + 1) & 31) ? (0xffffffffu << ((ok + 1) & 31)) : 0xffffffffu;
             const uint32_t pc = __popc(bits);
             if (r < pc) {
@@ -984,6 +1358,68 @@ k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf
   }
 }
 
+__global__ void __launch_bounds__(32 * kHOwnerWarps, kHBlocksPerSM)
+k_higher(uint32_t n, Ctl ctl, HigherTables tb, const uint32_t* __restrict__ leaf_pid, const uint32_t* __restrict__ cand,
+         const uint32_t* __restrict__ candc, const double* __restrict__ px, const double* __restrict__ py,
+         const double* __restrict__ pz, const int* __restrict__ cloud_scale, HigherRec* __restrict__ out,
+         uint32_t* __restrict__ counter, unsigned long long* __restrict__ stats) {
+  __shared__ OwnerSmem S;
+  __shared__ uint32_t adm[kMaxCand * (kMaxCand / 32)];
+  __shared__ WarpQueue wq[kHOwnerWarps];
+  const uint32_t pos = blockIdx.x;
+  if (pos >= n) return;
+  const uint32_t a = leaf_pid[pos];
+  const uint32_t m = candc[a];
+  if (m > (uint32_t)kMaxCand) return;  // a large candidate set (k_higher_large)
+  higher_owner<kMaxCand>(a, cand + (uint64_t)a * kMaxCand, m, S, adm, wq, ctl, tb, px, py, pz, cloud_scale, out,
+                         counter, stats);
+}
+
+// Owners whose candidate set exceeds kMaxCand: the same enumeration with the set staged in
+// dynamic shared memory (at most KC candidates) and the face mask in shared memory (KC <= 1024)
+// or in a per-block global scratch; blocks loop over the owners.
+// Placement of a large owner's staged set and face mask: kMode 0 both in shared memory,
+// 1 the set in shared memory and the mask in global scratch, 2 both in global scratch.
+template <int KC>
+constexpr size_t large_set_bytes() {
+  return (sizeof(OwnerSmemT<KC>) + 15) / 16 * 16;
+}
+template <int KC>
+constexpr size_t large_adm_bytes() {
+  return (size_t)KC * (KC / 32) * 4;
+}
+template <int KC, int kMode>
+constexpr size_t large_smem() {
+  return sizeof(WarpQueue) * kHOwnerWarps + (kMode <= 1 ? large_set_bytes<KC>() : 0) +
+         (kMode == 0 ? large_adm_bytes<KC>() : 0);
+}
+template <int KC, int kMode>
+constexpr size_t large_scratch_bytes() {  // per block
+  return (kMode >= 1 ? large_adm_bytes<KC>() : 0) + (kMode == 2 ? large_set_bytes<KC>() : 0);
+}
+
+template <int KC, int kMode>
+__global__ void __launch_bounds__(32 * kHOwnerWarps, 1)
+k_higher_large(uint32_t nown, const uint32_t* __restrict__ owners, const uint64_t* __restrict__ coff,
+               const uint32_t* __restrict__ carena, Ctl ctl, HigherTables tb, const double* __restrict__ px,
+               const double* __restrict__ py, const double* __restrict__ pz, const int* __restrict__ cloud_scale,
+               HigherRec* __restrict__ out, uint32_t* __restrict__ counter, unsigned long long* __restrict__ stats,
+               unsigned char* __restrict__ scratch) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned char* mine = scratch + (uint64_t)blockIdx.x * large_scratch_bytes<KC, kMode>();
+  WarpQueue* wq = reinterpret_cast<WarpQueue*>(smem);
+  unsigned char* after_q = smem + sizeof(WarpQueue) * kHOwnerWarps;
+  OwnerSmemT<KC>& S = *reinterpret_cast<OwnerSmemT<KC>*>(kMode <= 1 ? after_q : mine + large_adm_bytes<KC>());
+  uint32_t* adm = reinterpret_cast<uint32_t*>(kMode == 0 ? after_q + large_set_bytes<KC>() : mine);
+  for (uint32_t i = blockIdx.x; i < nown; i += gridDim.x) {
+    const uint32_t m = (uint32_t)(coff[i + 1] - coff[i]);
+    if (m <= (uint32_t)KC)
+      higher_owner<KC>(owners[i], carena + coff[i], m, S, adm, wq, ctl, tb, px, py, pz, cloud_scale, out, counter,
+                       stats);
+    __syncthreads();  // the next owner restages the shared set
+  }
+}
+
 __global__ void k_higher_keys(uint32_t m, const HigherRec* __restrict__ recs, uint64_t* __restrict__ khi,
                               uint64_t* __restrict__ klo, uint32_t* __restrict__ order) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1014,7 +1450,7 @@ __global__ void k_gather_init(uint32_t n, const double* __restrict__ R2w, double
 __global__ void k_gather_grow(uint32_t n, double* __restrict__ gr2, const uint8_t* __restrict__ todo,
                               const double* __restrict__ need_r) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || todo[i] != 1) return;
+  if (i >= n || (todo[i] != 1 && todo[i] != 3)) return;
   const double want = 4.0 * need_r[i] * need_r[i] * 1.1;
   gr2[i] = fmax(gr2[i] * 1.44, isfinite(want) ? want : gr2[i] * 4.0);
 }
@@ -1120,11 +1556,50 @@ void cube_cells(const std::vector<float>& dirs, double delta, std::vector<uint16
 
 }  // namespace
 
+// Bytes of each record buffer for `c` records: raw, sorted, khi, klo, order0, order1, radix counts.
+static void higher_record_bytes(uint64_t c, uint64_t* b) {
+  b[0] = c * sizeof(HigherRec);
+  b[1] = c * sizeof(HigherRec);
+  b[2] = c * sizeof(uint64_t);
+  b[3] = c * sizeof(uint64_t);
+  b[4] = c * sizeof(uint32_t);
+  b[5] = c * sizeof(uint32_t);
+  b[6] = 256ull * ((c + kRadixTile - 1) / kRadixTile) * sizeof(uint32_t);
+}
+
+cudaError_t higher_records_alloc(Ctx& ctx, uint64_t capacity) {
+  HigherBuffers& h = ctx.hb;
+  void** bufs[7] = {&h.raw, &h.sorted, (void**)&h.khi, (void**)&h.klo, (void**)&h.order0, (void**)&h.order1,
+                    (void**)&h.radix_counts};
+  uint64_t old_b[7], new_b[7];
+  higher_record_bytes(h.capacity, old_b);
+  higher_record_bytes(capacity, new_b);
+  for (int i = 0; i < 7; ++i) {
+    ctx_free(ctx, *bufs[i], old_b[i]);
+    *bufs[i] = nullptr;
+  }
+  h.capacity = 0;
+  for (int i = 0; i < 7; ++i) {
+    const cudaError_t e = ctx_alloc(ctx, bufs[i], new_b[i]);
+    if (e != cudaSuccess) {
+      for (int j = 0; j < i; ++j) {
+        ctx_free(ctx, *bufs[j], new_b[j]);
+        *bufs[j] = nullptr;
+      }
+      return e;
+    }
+  }
+  h.capacity = (uint32_t)capacity;
+  return cudaSuccess;
+}
+
 cudaError_t higher_alloc(Ctx& ctx) {
   const uint64_t n = ctx.max_points;
   HigherBuffers& h = ctx.hb;
   cudaError_t e = cudaSuccess;
-  h.capacity = (uint32_t)(512 * n + 4096);  // ~225 supports per point in lattices, more with ties
+  // records: about 200 per point in uniform clouds and 450 in jittered lattices; the buffer
+  // starts below that and grows on demand (count -> allocate -> emit)
+  if ((e = higher_records_alloc(ctx, 128 * n + 4096)) != cudaSuccess) return e;
 #define EHGP_ALLOC(ptr, bytes) \
   if ((e = ctx_alloc(ctx, (void**)&(ptr), (bytes))) != cudaSuccess) return e
   EHGP_ALLOC(h.nb, n * kMaxNb * sizeof(uint32_t));
@@ -1134,15 +1609,8 @@ cudaError_t higher_alloc(Ctx& ctx) {
   EHGP_ALLOC(h.gather_r2, n * sizeof(double));
   EHGP_ALLOC(h.rcap, n * sizeof(double));
   EHGP_ALLOC(h.todo, n * sizeof(uint8_t));
-  EHGP_ALLOC(h.raw, (uint64_t)h.capacity * sizeof(HigherRec));
-  EHGP_ALLOC(h.sorted, (uint64_t)h.capacity * sizeof(HigherRec));
-  EHGP_ALLOC(h.khi, (uint64_t)h.capacity * sizeof(uint64_t));
-  EHGP_ALLOC(h.klo, (uint64_t)h.capacity * sizeof(uint64_t));
-  EHGP_ALLOC(h.order0, (uint64_t)h.capacity * sizeof(uint32_t));
-  EHGP_ALLOC(h.order1, (uint64_t)h.capacity * sizeof(uint32_t));
   EHGP_ALLOC(h.counters, 8 * sizeof(uint32_t));
   EHGP_ALLOC(h.stats, 8 * sizeof(unsigned long long));
-  EHGP_ALLOC(h.radix_counts, 256ull * ((h.capacity + kRadixTile - 1) / kRadixTile) * sizeof(uint32_t));
   std::vector<float> dirs;
   double delta = 0;
   icosphere(dirs, delta);
@@ -1158,6 +1626,182 @@ cudaError_t higher_alloc(Ctx& ctx) {
   if ((e = cudaMemcpy(h.cells, cells.data(), cells.size() * sizeof(uint16_t), cudaMemcpyHostToDevice)) != cudaSuccess)
     return e;
   return cudaMemcpy(h.dirs, dirs.data(), dirs.size() * sizeof(float), cudaMemcpyHostToDevice);
+}
+
+// Grows a device array of ctx to hold `need` elements of `elem` bytes (contents dropped).
+template <class T>
+cudaError_t grow_array(Ctx& ctx, T*& ptr, uint64_t& cap, uint64_t need, uint64_t elem) {
+  if (cap >= need && ptr) return cudaSuccess;
+  ctx_free(ctx, ptr, cap * elem);
+  ptr = nullptr;
+  cap = 0;
+  const uint64_t c = need + need / 4 + 256;
+  const cudaError_t e = ctx_alloc(ctx, (void**)&ptr, c * elem);
+  if (e == cudaSuccess) cap = c;
+  return e;
+}
+
+// Neighbour lists of the owners in `big` (their current gather radii) into the arena:
+// counted, the arena grown to fit, then written (count -> allocate -> write); off receives
+// the prefix offsets (also on the device in h.big_off).
+int gather_big_lists(Ctx& ctx, uint32_t root, const std::vector<uint32_t>& big, std::vector<uint64_t>& off,
+                     uint64_t* launches) {
+  HigherBuffers& h = ctx.hb;
+  LbvhBuffers& b = ctx.lb;
+  GeomBuffers& g = ctx.gb;
+  cudaStream_t st = ctx.stream;
+  const uint32_t nb = (uint32_t)big.size();
+  cudaError_t e = cudaSuccess;
+  if (h.big_cap < nb) {
+    uint64_t c1 = h.big_cap, c2 = h.big_cap, c3 = h.big_cap;
+    if ((e = grow_array(ctx, h.big_ids, c1, nb, 4)) != cudaSuccess ||
+        (e = grow_array(ctx, h.big_off, c2, nb + 1, 8)) != cudaSuccess ||
+        (e = grow_array(ctx, h.big_cnt, c3, nb, 4)) != cudaSuccess) {
+      cudaGetLastError();
+      h.big_cap = 0;
+      return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "the large-neighbourhood owners do not fit the device");
+    }
+    h.big_cap = std::min(c1, std::min(c2 - 1, c3));
+  }
+  cudaMemcpyAsync(h.big_ids, big.data(), (uint64_t)nb * 4, cudaMemcpyHostToDevice, st);
+  k_gather_big<<<nblocks(nb, 128), 128, 0, st>>>(nb, h.big_ids, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end, b.px,
+                                                 b.py, b.pz, h.gather_r2, nullptr, nullptr, h.big_cnt, ctx.d_err);
+  ++*launches;
+  std::vector<uint32_t> cnt(nb);
+  uint32_t err = 0;
+  cudaMemcpyAsync(cnt.data(), h.big_cnt, (uint64_t)nb * 4, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&err, ctx.d_err, 4, cudaMemcpyDeviceToHost, st);
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "large neighbourhoods");
+  if (err) return abi_device_status(&ctx, err);
+  off.assign(nb + 1, 0);
+  for (uint32_t i = 0; i < nb; ++i) off[i + 1] = off[i] + cnt[i];
+  if ((e = grow_array(ctx, h.big_arena, h.arena_cap, off[nb], 4)) != cudaSuccess) {
+    cudaGetLastError();
+    return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "the large neighbourhoods do not fit the device");
+  }
+  cudaMemcpyAsync(h.big_off, off.data(), (uint64_t)(nb + 1) * 8, cudaMemcpyHostToDevice, st);
+  k_gather_big<<<nblocks(nb, 128), 128, 0, st>>>(nb, h.big_ids, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end, b.px,
+                                                 b.py, b.pz, h.gather_r2, h.big_off, h.big_arena, h.big_cnt,
+                                                 ctx.d_err);
+  ++*launches;
+  return EHGP_OK;
+}
+
+// One round of the large-neighbourhood path for the owners in `big`: their lists, then the
+// certified direction tables and candidate sets.
+int higher_big_round(Ctx& ctx, const CertParams& cp, uint32_t root, const std::vector<uint32_t>& big,
+                     std::vector<uint64_t>& off, uint64_t* launches) {
+  HigherBuffers& h = ctx.hb;
+  LbvhBuffers& b = ctx.lb;
+  cudaStream_t st = ctx.stream;
+  const uint32_t nb = (uint32_t)big.size();
+  int s = gather_big_lists(ctx, root, big, off, launches);
+  if (s != EHGP_OK) return s;
+  // the attribute is per function and device: set on every round (cheap)
+  cudaError_t e = cudaFuncSetAttribute(k_dirtable_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBigSmem);
+  if (e != cudaSuccess) return abi_cuda_fail(&ctx, e, "large-neighbourhood shared memory");
+  k_dirtable_big<<<nb, kBigThreads, kBigSmem, st>>>(nb, cp, h.big_ids, h.big_off, h.big_arena, b.px, b.py, b.pz,
+                                                     h.gather_r2, h.todo, h.cand, h.candc, h.rcap, h.rho);
+  ++*launches;
+  uint32_t err = 0;
+  cudaMemcpyAsync(&err, ctx.d_err, 4, cudaMemcpyDeviceToHost, st);
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "large neighbourhoods");
+  if (err) return abi_device_status(&ctx, err);
+  h.big_owners += nb;
+  h.big_entries += off[nb];
+  return EHGP_OK;
+}
+
+// Candidate sets above kMaxCand (owners certified with todo = 4): counted and written, sorted,
+// into cand_arena; owners in arena order in large_ids (the n_large sets of at most kLargeCand
+// first, then the n_huge sets of at most kHugeCand), prefix offsets in large_off.  lsmall:
+// owners certified on their per-point list; lbig: owners certified on the large path (their
+// lists are gathered again at the same radius).
+int higher_large_candidates(Ctx& ctx, const CertParams& cp, uint32_t root, const std::vector<uint32_t>& lsmall,
+                            const std::vector<uint32_t>& lbig, uint64_t* launches) {
+  HigherBuffers& h = ctx.hb;
+  LbvhBuffers& b = ctx.lb;
+  cudaStream_t st = ctx.stream;
+  const uint32_t ns = (uint32_t)lsmall.size(), nb = (uint32_t)lbig.size(), nt = ns + nb;
+  cudaError_t e = cudaSuccess;
+  std::vector<uint64_t> boff;
+  if (nb) {
+    const int s = gather_big_lists(ctx, root, lbig, boff, launches);
+    if (s != EHGP_OK) return s;
+  }
+  if (h.large_cap < nt) {
+    uint64_t c1 = h.large_cap, c2 = h.large_cap, c3 = h.large_cap, c4 = h.large_cap;
+    if ((e = grow_array(ctx, h.large_ids, c1, nt, 4)) != cudaSuccess ||
+        (e = grow_array(ctx, h.large_off, c2, nt + 1, 8)) != cudaSuccess ||
+        (e = grow_array(ctx, h.large_cnt, c3, nt, 4)) != cudaSuccess ||
+        (e = grow_array(ctx, h.large_dst, c4, nt, 8)) != cudaSuccess) {
+      cudaGetLastError();
+      h.large_cap = 0;
+      return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "the large candidate sets do not fit the device");
+    }
+    h.large_cap = std::min(std::min(c1, c2 - 1), std::min(c3, c4));
+  }
+  // launch order: the per-point-list owners, then the large-path owners (as gathered)
+  std::vector<uint32_t> launch(lsmall);
+  launch.insert(launch.end(), lbig.begin(), lbig.end());
+  cudaMemcpyAsync(h.large_ids, launch.data(), (uint64_t)nt * 4, cudaMemcpyHostToDevice, st);
+  if (ns)
+    k_cand_large<false><<<ns, kCandThreads, 0, st>>>(ns, h.large_ids, h.nb, h.nbc, nullptr, nullptr, cp, b.px, b.py,
+                                                     b.pz, h.rho, nullptr, nullptr, h.large_cnt, nullptr);
+  if (nb)
+    k_cand_large<true><<<nb, kCandThreads, 0, st>>>(nb, h.large_ids + ns, h.nb, h.nbc, h.big_off, h.big_arena, cp,
+                                                    b.px, b.py, b.pz, h.rho, nullptr, nullptr, h.large_cnt + ns,
+                                                    nullptr);
+  *launches += (ns ? 1 : 0) + (nb ? 1 : 0);
+  std::vector<uint32_t> cnt(nt);
+  cudaMemcpyAsync(cnt.data(), h.large_cnt, (uint64_t)nt * 4, cudaMemcpyDeviceToHost, st);
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "large candidate sets");
+  // arena order: sets of at most kLargeCand, then kHugeCand, then kMegaCand
+  auto cls = [](uint32_t c) { return c <= (uint32_t)kLargeCand ? 0 : c <= (uint32_t)kHugeCand ? 1 : 2; };
+  std::vector<uint32_t> ord;
+  for (uint32_t j = 0; j < nt; ++j)
+    if (cnt[j] > (uint32_t)kMegaCand) {
+      char msg[200];
+      snprintf(msg, sizeof msg, "a certified candidate set holds %u points, above the %d this build stages (PointId %u)",
+               cnt[j], kMegaCand, launch[j]);
+      return abi_fail(&ctx, EHGP_ERR_CAPACITY, msg);
+    }
+  for (int pass = 0; pass < 3; ++pass)
+    for (uint32_t j = 0; j < nt; ++j)
+      if (cls(cnt[j]) == pass) ord.push_back(j);
+  std::vector<uint64_t> dst(nt), pre(nt + 1, 0);
+  std::vector<uint32_t> ids(nt);
+  uint32_t per[3] = {0, 0, 0};
+  for (uint32_t q = 0; q < nt; ++q) {
+    const uint32_t j = ord[q];
+    dst[j] = pre[q];
+    pre[q + 1] = pre[q] + cnt[j];
+    ids[q] = launch[j];
+    ++per[cls(cnt[j])];
+  }
+  if ((e = grow_array(ctx, h.cand_arena, h.carena_cap, pre[nt], 4)) != cudaSuccess ||
+      (per[2] && (e = grow_array(ctx, h.cand_dist, h.cdist_cap, pre[nt], 4)) != cudaSuccess)) {
+    cudaGetLastError();
+    return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "the large candidate sets do not fit the device");
+  }
+  cudaMemcpyAsync(h.large_dst, dst.data(), (uint64_t)nt * 8, cudaMemcpyHostToDevice, st);
+  if (ns)
+    k_cand_large<false><<<ns, kCandThreads, 0, st>>>(ns, h.large_ids, h.nb, h.nbc, nullptr, nullptr, cp, b.px, b.py,
+                                                     b.pz, h.rho, h.large_dst, h.cand_arena, h.large_cnt, h.cand_dist);
+  if (nb)
+    k_cand_large<true><<<nb, kCandThreads, 0, st>>>(nb, h.large_ids + ns, h.nb, h.nbc, h.big_off, h.big_arena, cp,
+                                                    b.px, b.py, b.pz, h.rho, h.large_dst + ns, h.cand_arena,
+                                                    h.large_cnt + ns, h.cand_dist);
+  *launches += (ns ? 1 : 0) + (nb ? 1 : 0);
+  // the enumeration reads owners in arena order
+  cudaMemcpyAsync(h.large_ids, ids.data(), (uint64_t)nt * 4, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(h.large_off, pre.data(), (uint64_t)(nt + 1) * 8, cudaMemcpyHostToDevice, st);
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "large candidate sets");
+  h.n_large = per[0];
+  h.n_huge = per[1];
+  h.n_mega = per[2];
+  h.large_entries = pre[nt];
+  return EHGP_OK;
 }
 
 int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
@@ -1198,19 +1842,41 @@ int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   cp.need = smax - 2;
   if (cp.need < 1 || cp.need > (uint32_t)kMaxNeed) return abi_fail(&ctx, EHGP_ERR_INVALID_ARGUMENT, "K above 10 is not supported");
   uint32_t pending = n, overflowed = 0;
+  cudaError_t e0 = cudaSuccess;
   std::vector<uint8_t> todo(n);
-  for (int round = 0; round < 6 && pending > 0; ++round) {
+  std::vector<uint32_t> big;
+  std::vector<uint64_t> big_off;
+  std::vector<uint8_t> was_big(n, 0);
+  h.big_owners = h.big_entries = 0;
+  h.n_large = h.n_huge = h.n_mega = 0;
+  h.large_entries = 0;
+  // todo: 0 certified, 1 pending on the list path, 2 candidate set too large, 3 pending on
+  // the large-neighbourhood path
+  for (int round = 0; round < 8 && pending > 0; ++round) {
     k_gather<<<nblocks(n, kWarps), kThreads, 0, st>>>(n, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end, b.px, b.py,
                                                       b.pz, h.gather_r2, h.todo, h.nb, h.nbc);
-    k_dirtable<<<n, kDirThreads, 0, st>>>(n, cp, b.leaf_pid, h.nb, h.nbc, b.px, b.py, b.pz, h.gather_r2, h.todo,
+    const uint32_t list_cap = h.list_cap < (uint32_t)kMaxNb ? h.list_cap : (uint32_t)kMaxNb;
+    k_dirtable<<<n, kDirThreads, 0, st>>>(n, list_cap, cp, b.leaf_pid, h.nb, h.nbc, b.px, b.py, b.pz, h.gather_r2, h.todo,
                                           h.cand, h.candc, h.rcap, h.rho);
     launches += 2;
     cudaMemcpyAsync(todo.data(), h.todo, n, cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return abi_cuda_fail(&ctx, e, "higher-support certificate");
+    big.clear();
+    for (uint32_t i = 0; i < n; ++i)
+      if (todo[i] == 3) {
+        big.push_back(i);
+        was_big[i] = 1;
+      }
+    if (!big.empty()) {
+      const int s = higher_big_round(ctx, cp, root, big, big_off, &launches);
+      if (s != EHGP_OK) return s;
+      cudaMemcpyAsync(todo.data(), h.todo, n, cudaMemcpyDeviceToHost, st);
+      if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "higher-support certificate");
+    }
     pending = overflowed = 0;
     for (uint32_t i = 0; i < n; ++i) {
-      pending += todo[i] == 1;
+      pending += todo[i] == 1 || todo[i] == 3;
       overflowed += todo[i] == 2;
     }
     if (overflowed) break;
@@ -1236,29 +1902,91 @@ int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
              i < n ? std::sqrt(gr[i]) : 0.0);
     return abi_fail(&ctx, EHGP_ERR_CAPACITY, msg);
   }
-  cudaMemsetAsync(h.counters, 0, 8 * sizeof(uint32_t), st);
-  cudaMemsetAsync(h.stats, 0, 8 * sizeof(unsigned long long), st);
-  Ctl ctl{smax, h.capacity};
-  cudaEventRecord(ctx.evk0, st);
-  const HigherTables tb{h.dirs, h.cells, h.rho, h.cos_lim};
-  k_higher<<<n, 32 * kHOwnerWarps, 0, st>>>(n, ctl, tb, b.leaf_pid, h.cand, h.candc, b.px, b.py, b.pz,
-                                                         g.scale, (HigherRec*)h.raw, h.counters, h.stats);
-  cudaEventRecord(ctx.evk1, st);
-  ++launches;
+  {  // candidate sets above kMaxCand
+    std::vector<uint32_t> lsmall, lbig;
+    for (uint32_t i = 0; i < n; ++i)
+      if (todo[i] == 4) (was_big[i] ? lbig : lsmall).push_back(i);
+    if (!lsmall.empty() || !lbig.empty()) {
+      const int s = higher_large_candidates(ctx, cp, root, lsmall, lbig, &launches);
+      if (s != EHGP_OK) return s;
+    }
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device);
+  if (h.n_huge || h.n_mega) {  // per-block scratch of the huge- and mega-set kernels
+    const uint64_t bh = std::min<uint64_t>(h.n_huge, (uint64_t)sms), bm = std::min<uint64_t>(h.n_mega, (uint64_t)sms);
+    const uint64_t need = std::max(bh * large_scratch_bytes<kHugeCand, 1>(), bm * large_scratch_bytes<kMegaCand, 2>());
+    if ((e0 = grow_array(ctx, h.adm_scratch, h.adm_words, (need + 3) / 4, 4)) != cudaSuccess) {
+      cudaGetLastError();
+      return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "the scratch of the huge candidate sets does not fit the device");
+    }
+  }
+  if (h.n_large || h.n_huge || h.n_mega) {
+    cudaError_t ea = cudaFuncSetAttribute(k_higher_large<kLargeCand, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)large_smem<kLargeCand, 0>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_higher_large<kHugeCand, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)large_smem<kHugeCand, 1>());
+    if (ea != cudaSuccess) return abi_cuda_fail(&ctx, ea, "large candidate sets shared memory");
+  }
   uint32_t hc[2];
-  unsigned long long hs[8];
-  cudaMemcpyAsync(hc, h.counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(hc + 1, ctx.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(hs, h.stats, sizeof(hs), cudaMemcpyDeviceToHost, st);
-  cudaError_t e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return abi_cuda_fail(&ctx, e, "higher-support enumeration");
-  if (hc[1]) return abi_device_status(&ctx, hc[1]);
-  if (hc[0] > h.capacity) return abi_fail(&ctx, EHGP_ERR_CAPACITY, "higher-support records exceed the buffer");
-  {
-    float kms = 0;
-    cudaEventElapsedTime(&kms, ctx.evk0, ctx.evk1);
-    h.kernel_ms = kms;
-    for (int i = 0; i < 8; ++i) h.stats_host[i] = hs[i];
+  cudaError_t e = cudaSuccess;
+  const HigherTables tb{h.dirs, h.cells, h.rho, h.cos_lim};
+  // count -> allocate -> emit: the enumeration counts every record and writes those that fit;
+  // when the count exceeds the buffer, the buffer grows to it and the enumeration runs again
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    cudaMemsetAsync(h.counters, 0, 8 * sizeof(uint32_t), st);
+    cudaMemsetAsync(h.stats, 0, 8 * sizeof(unsigned long long), st);
+    const Ctl ctl{smax, h.capacity};
+    cudaEventRecord(ctx.evk0, st);
+    k_higher<<<n, 32 * kHOwnerWarps, 0, st>>>(n, ctl, tb, b.leaf_pid, h.cand, h.candc, b.px, b.py, b.pz, g.scale,
+                                              (HigherRec*)h.raw, h.counters, h.stats);
+    ++launches;
+    if (h.n_large) {
+      k_higher_large<kLargeCand, 0><<<std::min<uint32_t>(h.n_large, (uint32_t)sms), 32 * kHOwnerWarps,
+                                      large_smem<kLargeCand, 0>(), st>>>(
+          h.n_large, h.large_ids, h.large_off, h.cand_arena, ctl, tb, b.px, b.py, b.pz, g.scale, (HigherRec*)h.raw,
+          h.counters, h.stats, nullptr);
+      ++launches;
+    }
+    if (h.n_huge) {
+      const uint32_t o = h.n_large;
+      k_higher_large<kHugeCand, 1><<<std::min<uint32_t>(h.n_huge, (uint32_t)sms), 32 * kHOwnerWarps,
+                                     large_smem<kHugeCand, 1>(), st>>>(
+          h.n_huge, h.large_ids + o, h.large_off + o, h.cand_arena, ctl, tb, b.px, b.py, b.pz, g.scale,
+          (HigherRec*)h.raw, h.counters, h.stats, (unsigned char*)h.adm_scratch);
+      ++launches;
+    }
+    if (h.n_mega) {
+      const uint32_t o = h.n_large + h.n_huge;
+      k_higher_large<kMegaCand, 2><<<std::min<uint32_t>(h.n_mega, (uint32_t)sms), 32 * kHOwnerWarps,
+                                     large_smem<kMegaCand, 2>(), st>>>(
+          h.n_mega, h.large_ids + o, h.large_off + o, h.cand_arena, ctl, tb, b.px, b.py, b.pz, g.scale,
+          (HigherRec*)h.raw, h.counters, h.stats, (unsigned char*)h.adm_scratch);
+      ++launches;
+    }
+    cudaEventRecord(ctx.evk1, st);
+    unsigned long long hs[8];
+    cudaMemcpyAsync(hc, h.counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hc + 1, ctx.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hs, h.stats, sizeof(hs), cudaMemcpyDeviceToHost, st);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return abi_cuda_fail(&ctx, e, "higher-support enumeration");
+    if (hc[1]) return abi_device_status(&ctx, hc[1]);
+    {
+      float kms = 0;
+      cudaEventElapsedTime(&kms, ctx.evk0, ctx.evk1);
+      h.kernel_ms = kms;
+      for (int i = 0; i < 8; ++i) h.stats_host[i] = hs[i];
+    }
+    if (hc[0] <= h.capacity) break;
+    if (attempt == 1 || (uint64_t)hc[0] >= 0xffff0000ull)
+      return abi_fail(&ctx, EHGP_ERR_CAPACITY, "higher-support records exceed 32-bit record indices");
+    if ((e = higher_records_alloc(ctx, grown_capacity(hc[0]))) != cudaSuccess) {
+      cudaGetLastError();
+      return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "the higher-support records do not fit the device");
+    }
+    ++ctx.regrowths;
   }
   const uint32_t m = hc[0];
   if (m) {
@@ -1318,6 +2046,9 @@ int ehgp_higher_stats(const ehgp_ctx* ctx, double* kernel_ms, uint64_t* stats, u
   if (!ctx) return EHGP_ERR_INVALID_ARGUMENT;
   if (kernel_ms) *kernel_ms = ctx->hb.kernel_ms;
   for (uint32_t i = 0; stats && i < count && i < 8; ++i) stats[i] = ctx->hb.stats_host[i];
+  // [4] owners certified on the large-neighbourhood path, [5] their neighbour-list entries
+  if (stats && count > 4) stats[4] = ctx->hb.big_owners;
+  if (stats && count > 5) stats[5] = ctx->hb.big_entries;
   return EHGP_OK;
 }
 

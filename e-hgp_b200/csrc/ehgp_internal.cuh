@@ -219,6 +219,26 @@ struct HigherBuffers {
   uint32_t K = 0;
   double kernel_ms = 0;
   uint64_t stats_host[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  // owners whose certified neighbourhood holds more than the per-point list capacity
+  uint32_t* big_ids = nullptr;      // [big_cap] owners on the large-neighbourhood path
+  uint64_t* big_off = nullptr;      // [big_cap + 1] their offsets in the arena
+  uint32_t* big_cnt = nullptr;      // [big_cap] neighbour counts
+  uint32_t* big_arena = nullptr;    // [arena_cap] their neighbour ids
+  uint64_t big_cap = 0, arena_cap = 0;
+  uint64_t big_owners = 0, big_entries = 0;  // of the last call
+  uint32_t list_cap = 1024;         // list entries before an owner takes the large path (<= the list capacity)
+  // owners certified with more candidates than the per-point set holds
+  uint32_t* large_ids = nullptr;    // [large_cap] owners in the order of their sets in cand_arena
+  uint64_t* large_off = nullptr;    // [large_cap + 1] prefix offsets in cand_arena
+  uint32_t* large_cnt = nullptr;    // [large_cap] candidate counts (launch order)
+  uint64_t* large_dst = nullptr;    // [large_cap] destination offsets (launch order)
+  uint32_t* cand_arena = nullptr;   // [carena_cap]
+  uint32_t* adm_scratch = nullptr;  // [adm_words] face masks of the huge sets, one per block
+  uint64_t large_cap = 0, carena_cap = 0, adm_words = 0;
+  float* cand_dist = nullptr;       // [cdist_cap] distances of the sets sorted in the arena
+  uint64_t cdist_cap = 0;
+  uint32_t n_large = 0, n_huge = 0, n_mega = 0;  // owners with <= 1024, 4096, 16384 candidates (last call)
+  uint64_t large_entries = 0;
 };
 
 struct Ctx {
@@ -232,6 +252,7 @@ struct Ctx {
   std::string last_error;
   double last_ms = 0.0;
   uint64_t last_launches = 0;
+  uint64_t regrowths = 0;          // record buffers grown and enumerations re-run
   uint32_t* d_err = nullptr;       // device error word
   uint32_t* h_status = nullptr;    // pinned: [err, stats...]
   RadixScratch radix;
@@ -259,8 +280,17 @@ struct Ctx {
 
 // Allocation helper: records the bytes on ctx.
 cudaError_t ctx_alloc(Ctx& ctx, void** ptr, size_t bytes);
+// Frees one allocation of ctx_alloc (bytes as allocated).
+void ctx_free(Ctx& ctx, void* ptr, size_t bytes);
 
 // LBVH stage (ehgp_lbvh.cu)
+// Launch constants of the build that also size its scratch, shared by the context
+// allocation (lbvh_alloc) and the allocation-free layout (ehgp_noalloc.cu).
+constexpr int kLbvhFrameBlocks = 128;   // blocks of the exact-frame reduction (partials per axis)
+constexpr int kLbvhScanThreads = 1024;  // elements per block of the collision-group scan
+__host__ __device__ constexpr uint64_t lbvh_scan_block_sums(uint64_t n) {
+  return (n + kLbvhScanThreads - 1) / kLbvhScanThreads + 1;
+}
 cudaError_t lbvh_alloc(Ctx& ctx);
 // Runs the full device build on ctx.lb.xyz_in (input_kind 0 = f64, 1 = f32).
 // Returns the number of kernel launches issued.
@@ -275,10 +305,20 @@ uint64_t geom_prepare(Ctx& ctx, uint32_t n);
 
 // Pair supports (ehgp_pairs.cu)
 cudaError_t pairs_alloc(Ctx& ctx);
+// (Re)allocates the pair record buffers for `capacity` records.
+cudaError_t pairs_records_alloc(Ctx& ctx, uint64_t capacity);
 int pairs_run(Ctx& ctx, uint32_t K, uint32_t* out_count);
 
 // Triple/quad supports (ehgp_higher.cu)
 cudaError_t higher_alloc(Ctx& ctx);
+// (Re)allocates the triple/quad record buffers for `capacity` records.
+cudaError_t higher_records_alloc(Ctx& ctx, uint64_t capacity);
+// Record capacity to allocate when a stage counted `needed` records: a margin above the
+// count, within the 32-bit record indices of the stages.
+inline uint64_t grown_capacity(uint64_t needed) {
+  const uint64_t c = needed + needed / 8 + 4096;
+  return c < 0xffff0000ull ? c : 0xffff0000ull;
+}
 int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count);
 
 // Direct Morse hierarchy (ehgp_hier.cu)

@@ -289,7 +289,7 @@ __device__ __forceinline__ bool upper_better(const KeyId& a, const KeyId& b) {
   return a.key > b.key || (a.key == b.key && a.id < b.id);
 }
 
-constexpr int kFrameBlocks = 128;
+constexpr int kFrameBlocks = kLbvhFrameBlocks;
 
 __global__ void __launch_bounds__(kThreads)
 k_frame(uint32_t n, const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz,
@@ -394,7 +394,7 @@ k_leaves(uint32_t n, const uint32_t* __restrict__ vals0, const uint32_t* __restr
 
 // Inclusive scan of u32 in three launches (block scan, scan of block sums,
 // add).  Blocks of 1024 elements.
-constexpr int kScanThreads = 1024;
+constexpr int kScanThreads = kLbvhScanThreads;
 
 __device__ __forceinline__ uint32_t block_inclusive_scan(uint32_t v, uint32_t* s_warp) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -732,7 +732,7 @@ cudaError_t lbvh_alloc(Ctx& ctx) {
   EHGP_ALLOC(b.leaf_pid, n * sizeof(uint32_t));
   EHGP_ALLOC(b.leaf_code, n * sizeof(uint64_t));
   EHGP_ALLOC(b.group_of, n * sizeof(uint32_t));
-  EHGP_ALLOC(b.block_sums, ((n + kScanThreads - 1) / kScanThreads + 1) * sizeof(uint32_t));
+  EHGP_ALLOC(b.block_sums, lbvh_scan_block_sums(n) * sizeof(uint32_t));
   EHGP_ALLOC(b.gstart, (n + 1) * sizeof(uint32_t));
   EHGP_ALLOC(b.gcode, n * sizeof(uint64_t));
   EHGP_ALLOC(b.top_left, n * sizeof(uint32_t));

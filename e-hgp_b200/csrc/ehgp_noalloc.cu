@@ -15,7 +15,13 @@
 //
 // Set-up: the first call on a device (with that device current) looks up the
 // device address of the array with cudaGetSymbolAddress and caches it for
-// that device.  Make that first call before any stream capture.
+// that device.
+//
+// Streams: every call copies its status words back and synchronises its
+// stream, which a capturing stream does not allow, so the entry point must
+// never be called on a stream that is being captured into a CUDA graph; it
+// checks cudaStreamIsCapturing and refuses such a stream with
+// EHGP_ERR_INVALID_ARGUMENT.
 //
 // Sharing: every call on a device uses the same array and it keeps the last
 // call's contents; everything that must start at zero is cleared by each
@@ -54,7 +60,7 @@ constexpr uint64_t scratch_bytes() {
   L.take(n * 4);                // leaf_pid
   L.take(n * 8);                // leaf_code
   L.take(n * 4);                // group_of
-  L.take((n / 1024 + 2) * 4);   // block_sums
+  L.take(ehgp::lbvh_scan_block_sums(n) * 4);  // block_sums
   L.take((n + 1) * 4);          // gstart
   L.take(n * 8);                // gcode
   for (int i = 0; i < 6; ++i) L.take(n * 4);   // top_left/right, parents, grp_root_idx, grp_depth
@@ -63,7 +69,7 @@ constexpr uint64_t scratch_bytes() {
   L.take(3 * 2 * n * 4); L.take(3 * 2 * n * 4);   // n_lo n_hi
   L.take(2 * n * 4);            // n_flag
   L.take(12 * 8);               // frame
-  L.take(12 * 128 * 8);         // frame_partial
+  L.take(12 * ehgp::kLbvhFrameBlocks * 8);  // frame_partial
   L.take(4);                    // frame_done
   L.take(8 * 4);                // stats
   L.take(2 * n * sizeof(ehgp_lbvh_node) + n * sizeof(ehgp_lbvh_leaf) + n * 8);  // export
@@ -74,6 +80,7 @@ constexpr uint64_t scratch_bytes() {
 }
 
 constexpr uint64_t kScratchBytes = scratch_bytes();
+static_assert(kScratchBytes <= (uint64_t{8} << 20), "the fixed scratch array stays below 8 MiB per GPU");
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
@@ -101,7 +108,7 @@ void carve(ehgp::Ctx& c, unsigned char* base) {
   b.leaf_pid = (uint32_t*)at(n * 4);
   b.leaf_code = (uint64_t*)at(n * 8);
   b.group_of = (uint32_t*)at(n * 4);
-  b.block_sums = (uint32_t*)at((n / 1024 + 2) * 4);
+  b.block_sums = (uint32_t*)at(ehgp::lbvh_scan_block_sums(n) * 4);
   b.gstart = (uint32_t*)at((n + 1) * 4);
   b.gcode = (uint64_t*)at(n * 8);
   b.top_left = (uint32_t*)at(n * 4);
@@ -123,7 +130,7 @@ void carve(ehgp::Ctx& c, unsigned char* base) {
   b.n_hi = (uint32_t*)at(3 * 2 * n * 4);
   b.n_flag = (uint32_t*)at(2 * n * 4);
   b.frame = (uint64_t*)at(12 * 8);
-  b.frame_partial = (unsigned long long*)at(12 * 128 * 8);
+  b.frame_partial = (unsigned long long*)at(12 * ehgp::kLbvhFrameBlocks * 8);
   b.frame_done = (uint32_t*)at(4);
   b.stats = (uint32_t*)at(8 * 4);
   b.export_bytes = 2 * n * sizeof(ehgp_lbvh_node) + n * sizeof(ehgp_lbvh_leaf) + n * 8;
@@ -133,6 +140,8 @@ void carve(ehgp::Ctx& c, unsigned char* base) {
   c.radix.state = (uint32_t*)at(ehgp::kRadixStateWords * 4);
   c.d_err = (uint32_t*)at(4);
   c.max_points = n;
+  // the carve takes exactly the blocks that scratch_bytes() sized
+  if (L.off != kScratchBytes) c.max_points = 0;
 }
 
 }  // namespace
@@ -147,6 +156,11 @@ int ehgp_lbvh_build_noalloc(const double* xyz, uint64_t n, const ehgp_lbvh_out* 
   if (!xyz || !out) return EHGP_ERR_INVALID_ARGUMENT;
   if (n == 0) return EHGP_ERR_INVALID_ARGUMENT;
   if (n > kNoAllocMaxPoints) return EHGP_ERR_CAPACITY;
+  {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing((cudaStream_t)stream, &cap) != cudaSuccess) return EHGP_ERR_CUDA;
+    if (cap != cudaStreamCaptureStatusNone) return EHGP_ERR_INVALID_ARGUMENT;
+  }
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices) return EHGP_ERR_CUDA;
@@ -161,6 +175,7 @@ int ehgp_lbvh_build_noalloc(const double* xyz, uint64_t n, const ehgp_lbvh_out* 
   c.device = device;
   c.stream = (cudaStream_t)stream;
   carve(c, g_scratch_addr[device]);
+  if (c.max_points != kNoAllocMaxPoints) return EHGP_ERR_CUDA;  // layout and carve disagree
   uint32_t status[64] = {0};  // pageable host words: a copy into them allocates nothing
   c.h_status = status;
   const uint32_t n32 = (uint32_t)n;
@@ -176,11 +191,8 @@ int ehgp_lbvh_build_noalloc(const double* xyz, uint64_t n, const ehgp_lbvh_out* 
           cudaSuccess ||
       cudaStreamSynchronize(c.stream) != cudaSuccess)
     return EHGP_ERR_CUDA;
-  const uint32_t err = status[0];
-  if (err & ehgp::kErrNonFinite) return EHGP_ERR_INVALID_ARGUMENT;
-  if (err & ehgp::kErrDuplicate) return EHGP_ERR_DUPLICATE_POINT;
-  if (err & ehgp::kErrNumericRange) return EHGP_ERR_NUMERIC_RANGE;
-  if (err) return EHGP_ERR_CUDA;
+  // same mapping of the device error word as the context path
+  if (status[0]) return ehgp::abi_device_status(nullptr, status[0]);
   if (ehgp::lbvh_export(c, n32, out) != cudaSuccess) return EHGP_ERR_CUDA;
   return EHGP_OK;
 }

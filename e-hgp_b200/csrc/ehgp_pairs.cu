@@ -453,26 +453,56 @@ k_pair_gather(uint32_t m, const uint32_t* __restrict__ vals0, const uint32_t* __
 
 }  // namespace
 
+// Bytes of each record buffer for `c` records: raw, sorted, key, order0, order1, levelD, radix counts.
+static void pair_record_bytes(uint64_t c, uint64_t* b) {
+  b[0] = c * sizeof(PairRec);
+  b[1] = c * sizeof(PairRec);
+  b[2] = c * sizeof(uint64_t);
+  b[3] = c * sizeof(uint32_t);
+  b[4] = c * sizeof(uint32_t);
+  b[5] = c * 4 * sizeof(uint64_t);
+  b[6] = 256ull * ((c + kRadixTile - 1) / kRadixTile) * sizeof(uint32_t);
+}
+
+cudaError_t pairs_records_alloc(Ctx& ctx, uint64_t capacity) {
+  PairBuffers& p = ctx.pb;
+  void** bufs[7] = {&p.raw, &p.sorted, (void**)&p.key, (void**)&p.order0, (void**)&p.order1, (void**)&p.levelD,
+                    (void**)&p.radix_counts};
+  uint64_t old_b[7], new_b[7];
+  pair_record_bytes(p.capacity, old_b);
+  pair_record_bytes(capacity, new_b);
+  for (int i = 0; i < 7; ++i) {
+    ctx_free(ctx, *bufs[i], old_b[i]);
+    *bufs[i] = nullptr;
+  }
+  p.capacity = 0;
+  for (int i = 0; i < 7; ++i) {
+    const cudaError_t e = ctx_alloc(ctx, bufs[i], new_b[i]);
+    if (e != cudaSuccess) {
+      for (int j = 0; j < i; ++j) {
+        ctx_free(ctx, *bufs[j], new_b[j]);
+        *bufs[j] = nullptr;
+      }
+      return e;
+    }
+  }
+  p.capacity = (uint32_t)capacity;
+  return cudaSuccess;
+}
+
 cudaError_t pairs_alloc(Ctx& ctx) {
   const uint64_t n = ctx.max_points;
   PairBuffers& p = ctx.pb;
   cudaError_t e = cudaSuccess;
-  p.capacity = (uint32_t)(64 * n + 1024);
 #define EHGP_ALLOC(ptr, bytes) \
   if ((e = ctx_alloc(ctx, (void**)&(ptr), (bytes))) != cudaSuccess) return e
   EHGP_ALLOC(p.W, n * kW * sizeof(uint32_t));
   EHGP_ALLOC(p.R2, n * sizeof(double));
-  EHGP_ALLOC(p.raw, (uint64_t)p.capacity * sizeof(PairRec));
-  EHGP_ALLOC(p.sorted, (uint64_t)p.capacity * sizeof(PairRec));
-  EHGP_ALLOC(p.key, (uint64_t)p.capacity * sizeof(uint64_t));
-  EHGP_ALLOC(p.order0, (uint64_t)p.capacity * sizeof(uint32_t));
-  EHGP_ALLOC(p.order1, (uint64_t)p.capacity * sizeof(uint32_t));
-  EHGP_ALLOC(p.levelD, (uint64_t)p.capacity * 4 * sizeof(uint64_t));
   EHGP_ALLOC(p.counters, 8 * sizeof(uint32_t));
   EHGP_ALLOC(p.stats, 8 * sizeof(unsigned long long));
-  EHGP_ALLOC(p.radix_counts, 256ull * ((p.capacity + kRadixTile - 1) / kRadixTile) * sizeof(uint32_t));
 #undef EHGP_ALLOC
-  return cudaSuccess;
+  // records: about 38 per point in lattices and uniform clouds; grown on demand
+  return pairs_records_alloc(ctx, 48 * n + 1024);
 }
 
 // Witness lists + pair enumeration + (u, v) sort.  Returns the record count
@@ -496,29 +526,42 @@ int pairs_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   cudaEventRecord(ctx.ev0, st);
   k_witness_knn<<<nblocks(n), kThreads, 0, st>>>(n, kw, root, g.tnodes, b.leaf_pid, b.px, b.py, b.pz, p.W, p.R2,
                                                   ctx.d_err);
-  cudaMemsetAsync(p.counters, 0, 8 * sizeof(uint32_t), st);
-  cudaMemsetAsync(p.stats, 0, 8 * sizeof(unsigned long long), st);
-  cudaEventRecord(ctx.evk0, st);
-  k_pairs<<<nblocks(n, kWarpsPerBlock), kThreads, 0, st>>>(n, cap, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end,
-                                                           b.px, b.py, b.pz, g.scale, p.W, p.R2, (PairRec*)p.raw,
-                                                           p.capacity, p.counters, p.stats, ctx.d_err);
-  cudaEventRecord(ctx.evk1, st);
-  launches += 2;
+  ++launches;
   uint32_t hc[2] = {0, 0};
-  unsigned long long hs[8];
-  cudaMemcpyAsync(hc, p.counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(hc + 1, ctx.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(hs, p.stats, sizeof(hs), cudaMemcpyDeviceToHost, st);
-  cudaError_t e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return abi_cuda_fail(&ctx, e, "pair enumeration");
-  {
-    float kms = 0.f;
-    cudaEventElapsedTime(&kms, ctx.evk0, ctx.evk1);
-    ctx.kernel_ms = kms;
-    for (int i = 0; i < 8; ++i) ctx.kernel_stats[i] = hs[i];
+  cudaError_t e = cudaSuccess;
+  // count -> allocate -> emit: the enumeration counts every record and writes those that fit;
+  // when the count exceeds the buffer, the buffer grows to it and the enumeration runs again
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    cudaMemsetAsync(p.counters, 0, 8 * sizeof(uint32_t), st);
+    cudaMemsetAsync(p.stats, 0, 8 * sizeof(unsigned long long), st);
+    cudaEventRecord(ctx.evk0, st);
+    k_pairs<<<nblocks(n, kWarpsPerBlock), kThreads, 0, st>>>(n, cap, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end,
+                                                             b.px, b.py, b.pz, g.scale, p.W, p.R2, (PairRec*)p.raw,
+                                                             p.capacity, p.counters, p.stats, ctx.d_err);
+    cudaEventRecord(ctx.evk1, st);
+    ++launches;
+    unsigned long long hs[8];
+    cudaMemcpyAsync(hc, p.counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hc + 1, ctx.d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hs, p.stats, sizeof(hs), cudaMemcpyDeviceToHost, st);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return abi_cuda_fail(&ctx, e, "pair enumeration");
+    {
+      float kms = 0.f;
+      cudaEventElapsedTime(&kms, ctx.evk0, ctx.evk1);
+      ctx.kernel_ms = kms;
+      for (int i = 0; i < 8; ++i) ctx.kernel_stats[i] = hs[i];
+    }
+    if (hc[1]) return abi_device_status(&ctx, hc[1]);
+    if (hc[0] <= p.capacity) break;
+    if (attempt == 1 || (uint64_t)hc[0] >= 0xffff0000ull)
+      return abi_fail(&ctx, EHGP_ERR_CAPACITY, "pair-support records exceed 32-bit record indices");
+    if ((e = pairs_records_alloc(ctx, grown_capacity(hc[0]))) != cudaSuccess) {
+      cudaGetLastError();
+      return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "the pair-support records do not fit the device");
+    }
+    ++ctx.regrowths;
   }
-  if (hc[1]) return abi_device_status(&ctx, hc[1]);
-  if (hc[0] > p.capacity) return abi_fail(&ctx, EHGP_ERR_CAPACITY, "pair-support records exceed the buffer");
   const uint32_t m = hc[0];
   if (m) {
     k_pair_keys<<<(m + 255) / 256, 256, 0, st>>>(m, (const PairRec*)p.raw, p.key, p.order0);

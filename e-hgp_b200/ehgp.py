@@ -201,6 +201,10 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "ehgp_hier_copy": (C.c_int, [P, C.POINTER(HierOut)]),
         "ehgp_event_level": (C.c_int, [P, C.c_uint64, P, P, C.POINTER(C.c_int32)]),
         "ehgp_hier_stats": (C.c_int, [P, P, P]),
+        "ehgp_hier_schedule": (C.c_int, [P, C.c_uint32, C.c_uint32, C.c_uint32]),
+        "ehgp_ctx_reserve": (C.c_int, [P, C.c_uint32, C.c_uint64]),
+        "ehgp_ctx_regrowths": (C.c_uint64, [P]),
+        "ehgp_tune": (C.c_int, [P, C.c_uint32, C.c_uint64]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -297,6 +301,20 @@ class Context:
     @property
     def device_bytes(self) -> int:
         return int(self.lib.ehgp_ctx_device_bytes(self._h))
+
+    def reserve(self, stage: int, records: int) -> None:
+        """ehgp_ctx_reserve: record capacity of the pair (0) or triple/quad (1) buffers."""
+        self._check(self.lib.ehgp_ctx_reserve(self._h, stage, records))
+
+    TUNE_HIGHER_LIST = 1
+
+    def tune(self, knob: int, value: int) -> None:
+        """ehgp_tune: a tuning knob of later calls (results never depend on it)."""
+        self._check(self.lib.ehgp_tune(self._h, knob, value))
+
+    def regrowths(self) -> int:
+        """Second enumeration passes after a record buffer grew (count -> allocate -> emit)."""
+        return int(self.lib.ehgp_ctx_regrowths(self._h))
 
     def step_begin(self) -> None:
         self._check(self.lib.ehgp_step_begin(self._h))
@@ -429,6 +447,11 @@ class Context:
             for name, _, cf in _HIER_FIELDS:
                 out[name] = bufs[name][:int(cnts[cf])]
         return out
+
+    def hier_schedule(self, chunk_batches: int = 0, part_arms: int = 0, host_threads: int = 0) -> None:
+        """ehgp_hier_schedule: chunk, descent-part and thread counts of later hierarchy calls
+        (0 = default); the result never depends on them."""
+        self._check(self.lib.ehgp_hier_schedule(self._h, chunk_batches, part_arms, host_threads))
 
     def hier_stats(self) -> dict:
         """Timing and work counters of the last hierarchy call."""

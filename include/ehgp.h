@@ -64,6 +64,27 @@ const char* ehgp_status_string(int status);
 /* Device bytes owned by the context (resident buffers). */
 uint64_t ehgp_ctx_device_bytes(const ehgp_ctx* ctx);
 
+/* Support records are produced count -> allocate -> emit, as the reference's
+ * stream contract asks (no truncation; the budgeted streams of
+ * include/morsehgp3d/hierarchy/pair_support_stream.hpp:421-470 resume instead of
+ * dropping records): an enumeration counts every record and writes the ones that
+ * fit; when the count is above the buffer, the buffer grows to it and the
+ * enumeration runs once more.  ehgp_ctx_reserve sets the record capacity of the
+ * pair (stage 0) or triple/quad (stage 1) buffers up front, so that a caller who
+ * knows its clouds avoids the second pass (the resident records of that stage
+ * are dropped); ehgp_ctx_regrowths counts the second passes so far.  No
+ * counterpart in the reference. */
+int ehgp_ctx_reserve(ehgp_ctx* ctx, uint32_t stage, uint64_t records);
+uint64_t ehgp_ctx_regrowths(const ehgp_ctx* ctx);
+
+/* Tuning knobs of later calls on ctx; results never depend on them (no
+ * counterpart in the reference).
+ *   EHGP_TUNE_HIGHER_LIST: neighbour-list entries (1..1024, default 1024) that a
+ *     triple/quad owner may hold before its certificate moves to the
+ *     large-neighbourhood path (arena lists of any length). */
+enum { EHGP_TUNE_HIGHER_LIST = 1 };
+int ehgp_tune(ehgp_ctx* ctx, uint32_t knob, uint64_t value);
+
 /* ---- LBVH snapshot records (reference layout) ---------------------------- */
 /* Same fields, order and sizes as spatial::MortonLbvhSnapshotLeaf,
  * MortonLbvhSnapshotNode and MortonLbvhSnapshotCounters
@@ -237,13 +258,14 @@ typedef struct ehgp_higher_out {
 /* Every relevant minimal triple and quad support of the resident cloud for
  * maximum order K <= 10.  Replaces hierarchy::build_exact_higher_support_stream
  * (include/morsehgp3d/hierarchy/higher_support_stream.hpp:544) run to
- * completion.  EHGP_ERR_CAPACITY when a certified neighbourhood exceeds 512
- * points.  records == NULL only counts. */
+ * completion.  records == NULL only counts. */
 int ehgp_higher(ehgp_ctx* ctx, uint32_t K, const ehgp_higher_out* out);
 
 /* CUDA-event time of the last triple/quad enumeration kernel and its work
  * counters: [0] candidate supports tested, [1] closed-ball classifications,
- * [2] records, [3] neighbour-list entries. */
+ * [2] records, [3] neighbour-list entries, [4] owners whose certified
+ * neighbourhood exceeded the 1024-entry list and took the large-neighbourhood
+ * path (count -> allocate -> write), [5] entries of their lists. */
 int ehgp_higher_stats(const ehgp_ctx* ctx, double* kernel_ms, uint64_t* stats, uint32_t count);
 
 /* Allocation-free LBVH build.  No counterpart in the reference: it exists for
@@ -256,9 +278,11 @@ int ehgp_higher_stats(const ehgp_ctx* ctx, double* kernel_ms, uint64_t* stats, u
  * __device__ array of ehgp_lbvh_noalloc_scratch_bytes() bytes that every GPU
  * loading this library holds until exit; n above
  * ehgp_lbvh_noalloc_max_points() (16384) returns EHGP_ERR_CAPACITY.  The
- * first call on a device looks the array up (cudaGetSymbolAddress) and must
- * come before any stream capture.  Calls share the array: calls whose GPU
- * work overlaps race and must not be issued. */
+ * first call on a device looks the array up (cudaGetSymbolAddress).  Every
+ * call synchronises `stream` and copies status words back, so it must never
+ * be called on a stream that is being captured into a CUDA graph; such a
+ * stream is refused with EHGP_ERR_INVALID_ARGUMENT.  Calls share the array:
+ * calls whose GPU work overlaps race and must not be issued. */
 int ehgp_lbvh_build_noalloc(const double* xyz, uint64_t n, const ehgp_lbvh_out* out, void* stream);
 uint64_t ehgp_lbvh_noalloc_max_points(void);
 uint64_t ehgp_lbvh_noalloc_scratch_bytes(void);
@@ -392,6 +416,14 @@ typedef struct ehgp_hier_out {
 } ehgp_hier_out;
 
 int ehgp_hier_copy(ehgp_ctx* ctx, const ehgp_hier_out* out);
+
+/* Schedule of later ehgp_hierarchy calls on ctx; results never depend on it.  No
+ * counterpart in the reference, whose forest journal is one sequential pass
+ * (src/cpu/hierarchy/direct_morse_forest_journal.cpp:1042-2150): single-role batches
+ * per chunk that the host pool rebuilds in parallel (0: 16384), strict arms per part
+ * of the descent that an order's union-find core consumes while the device descends
+ * the next (0: 4,194,304), and host threads (0: every hardware thread). */
+int ehgp_hier_schedule(ehgp_ctx* ctx, uint32_t chunk_batches, uint32_t part_arms, uint32_t host_threads);
 
 /* Timing of the last ehgp_hierarchy call: ms[0] device stages (CUDA events),
  * ms[1] the strict-arm descent kernels, ms[2] the host forest pass, ms[3] its

@@ -18,8 +18,10 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -614,6 +616,121 @@ void analyze_fp(const Cloud& c, SupportGeo& g) {
   }
 }
 
+// FP64-filtered status of a 3- or 4-point support with the same 64 u m bound: 0 minimal,
+// 1 not minimal (boundary, exterior centre or dependent; which one does not matter to the
+// enumeration), 2 undecided (the exact analysis settles it).  Only a cheaper route to
+// analyze()'s status: a decided FP64 sign equals the exact sign.
+int status_fp(const Cloud& c, const u64* ids, int size) {
+  if (size == 3) {
+    const FV e1 = fdiff(c, ids[1], ids[0]), e2 = fdiff(c, ids[2], ids[0]);
+    const Fm G11 = dot3(e1, e1), G12 = dot3(e1, e2), G22 = dot3(e2, e2);
+    const int sa = fm_sign(G12), sb = fm_sign(G11 - G12), sc = fm_sign(G22 - G12);
+    if (sa == -1 || sb == -1 || sc == -1) return 1;  // an obtuse angle: exterior centre or dependent
+    if (sa == 2 || sb == 2 || sc == 2) return 2;
+    const int sd = fm_sign(G11 * G22 - G12 * G12);
+    return sd == 1 ? 0 : 2;  // three acute angles: detG > 0 exactly
+  }
+  const FV e1 = fdiff(c, ids[1], ids[0]), e2 = fdiff(c, ids[2], ids[0]), e3 = fdiff(c, ids[3], ids[0]);
+  const FV c23 = cross3(e2, e3), c31 = cross3(e3, e1), c12 = cross3(e1, e2);
+  const Fm detE = dot3(e1, c23);
+  const int sd = fm_sign(detE);
+  if (sd == 2) return 2;
+  if (sd == 0) return 1;
+  const FV N = add3(add3(scale3(dot3(e1, e1), c23), scale3(dot3(e2, e2), c31)), scale3(dot3(e3, e3), c12));
+  const Fm l1 = dot3(N, c23), l2 = dot3(N, c31), l3 = dot3(N, c12);
+  const Fm two{2.0, 2.0};
+  const Fm l0 = two * detE * detE - (l1 + l2 + l3);
+  const int s[4] = {fm_sign(l0), fm_sign(l1), fm_sign(l2), fm_sign(l3)};
+  bool und = false;
+  for (int i = 0; i < 4; ++i) {
+    if (s[i] == -1 || s[i] == 0) return 1;
+    und |= s[i] == 2;
+  }
+  return und ? 2 : 0;
+}
+
+// Side of w against a support whose exact geometry may not be computed yet: the FP64
+// filter first; the exact integers (analyze) only when it does not decide.
+struct LazyGeo {
+  const Cloud& c;
+  const FixedCloud& f;
+  SupportGeo g;
+  bool exact = false;
+  LazyGeo(const Cloud& c_, const FixedCloud& f_, const u64* ids, int size) : c(c_), f(f_) {
+    g.size = size;
+    for (int i = 0; i < size; ++i) g.ids[i] = ids[i];
+    analyze_fp(c, g);
+    // sign of A in FP64 (A = det G > 0 for a minimal triangle; det E for a tetrahedron)
+    const int sa = fm_sign(g.fA);
+    if (size == 3) g.sgn = 1;
+    else if (sa == 1 || sa == -1) g.sgn = sa;
+    else make_exact();
+  }
+  void make_exact() {
+    if (exact) return;
+    g = [&] { SupportGeo e = analyze(c, f, g.ids, g.size); analyze_fp(c, e); return e; }();
+    exact = true;
+  }
+  int side(u64 w) {
+    const FV p = fdiff(c, w, g.ids[0]);
+    const int s = fm_sign(g.fA * dot3(p, p) - dot3(p, g.fN));
+    if (s != 2) return s * g.sgn;
+    make_exact();
+    const BV q = bdiff(f, w, g.ids[0]);
+    const Big val = g.A * dot3(q, q) - dot3(q, g.Nv);
+    return (val < 0 ? -1 : (val > 0 ? 1 : 0)) * g.sgn;
+  }
+};
+
+// Every minimal 3- and 4-point support with at most cap(size) strict interior points,
+// enumerated by brute force over all tuples in (size, ids) order; emit(tid, geo, interior,
+// shell, extra) runs for each on thread tid, its tuples' least id split over threads by
+// `first` in strides, so a caller that keeps one buffer per least id restores the order.
+template <class Emit>
+void enumerate_higher(const Cloud& c, const FixedCloud& f, u64 smax, Emit&& emit) {
+  const u64 n = c.bits.size();
+  const unsigned hw = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  auto run = [&](unsigned tid) {
+    std::vector<u64> interior;
+    auto visit = [&](const u64* ids, int size) {
+      if (smax < (u64)size) return;
+      const int st = status_fp(c, ids, size);
+      if (st == 1) return;
+      if (st == 2 && analyze(c, f, ids, size).status != 0) return;
+      LazyGeo lg(c, f, ids, size);
+      const u64 cap = smax - size;
+      interior.clear();
+      u64 shell = size, extra = ~u64{0};
+      for (u64 w = 0; w < n; ++w) {
+        bool sup = false;
+        for (int i = 0; i < size; ++i) sup |= (w == ids[i]);
+        if (sup) continue;
+        const int sd = lg.side(w);
+        if (sd < 0) {
+          interior.push_back(w);
+          if (interior.size() > cap) return;
+        } else if (sd == 0) {
+          ++shell;
+          extra = std::min(extra, w);
+        }
+      }
+      lg.make_exact();
+      emit(tid, lg.g, interior, shell, extra);
+    };
+    u64 ids[4];
+    for (ids[0] = tid; ids[0] < n; ids[0] += hw)
+      for (ids[1] = ids[0] + 1; ids[1] < n; ++ids[1])
+        for (ids[2] = ids[1] + 1; ids[2] < n; ++ids[2]) {
+          visit(ids, 3);
+          for (ids[3] = ids[2] + 1; ids[3] < n; ++ids[3]) visit(ids, 4);
+        }
+  };
+  for (unsigned t = 1; t < hw; ++t) pool.emplace_back(run, t);
+  run(0);
+  for (auto& t : pool) t.join();
+}
+
 int higher_side(const Cloud& c, const FixedCloud& f, const SupportGeo& g, u64 w) {
   const FV p = fdiff(c, w, g.ids[0]);
   const int s = fm_sign(g.fA * dot3(p, p) - dot3(p, g.fN));
@@ -674,52 +791,31 @@ std::string higher_text(const Cloud& c, u64 K) {
   const FixedCloud f = fixed_cloud(c);
   const u64 n = c.bits.size();
   const u64 keff = std::min(K, n), smax = std::min(keff + 1, n);
-  std::string ev[2], dg[2];
-  std::vector<u64> interior;
-  auto visit = [&](const u64* ids, int size) {
-    if (smax < (u64)size) return;
-    SupportGeo g = analyze(c, f, ids, size);
-    if (g.status != 0) return;
-    analyze_fp(c, g);
-    const u64 cap = smax - size;
-    interior.clear();
-    u64 shell = size, extra = ~u64{0};
-    for (u64 w = 0; w < n; ++w) {
-      bool sup = false;
-      for (int i = 0; i < size; ++i) sup |= (w == ids[i]);
-      if (sup) continue;
-      const int sd = higher_side(c, f, g, w);
-      if (sd < 0) {
-        interior.push_back(w);
-        if (interior.size() > cap) return;
-      } else if (sd == 0) {
-        ++shell;
-        extra = std::min(extra, w);
-      }
-    }
+  // one buffer per (least id, size, event/diagnostic): concatenated in (size, ids) order
+  std::vector<std::string> ev3(n), ev4(n), dg3(n), dg4(n);
+  enumerate_higher(c, f, smax, [&](unsigned, const SupportGeo& g, const std::vector<u64>& interior, u64 shell,
+                                   u64 extra) {
+    const int size = g.size;
     const u64 I = interior.size();
     std::string head = std::to_string(size);
-    for (int i = 0; i < size; ++i) head += " " + std::to_string(ids[i]);
+    for (int i = 0; i < size; ++i) head += " " + std::to_string(g.ids[i]);
     std::string idt;
     for (u64 w : interior) idt += " " + std::to_string(w);
     const std::string sph = sphere_text(f, g);
+    const u64 a = g.ids[0];
     if (shell == (u64)size)
-      ev[size - 3] += "H " + head + " " + std::to_string(I + size) + " " + std::to_string(n - I - size) + " " + sph +
-                      " |" + idt + "\n";
+      (size == 3 ? ev3 : ev4)[a] += "H " + head + " " + std::to_string(I + size) + " " + std::to_string(n - I - size) +
+                                    " " + sph + " |" + idt + "\n";
     else
-      dg[size - 3] += "G " + head + " " + std::to_string(shell) + " " + std::to_string(extra) + " " +
-                      std::to_string(I + size) + " " + std::to_string(I + shell) + " " + std::to_string(n - I - shell) +
-                      " " + sph + " |" + idt + "\n";
-  };
-  u64 ids[4];
-  for (ids[0] = 0; ids[0] < n; ++ids[0])
-    for (ids[1] = ids[0] + 1; ids[1] < n; ++ids[1])
-      for (ids[2] = ids[1] + 1; ids[2] < n; ++ids[2]) {
-        visit(ids, 3);
-        for (ids[3] = ids[2] + 1; ids[3] < n; ++ids[3]) visit(ids, 4);
-      }
+      (size == 3 ? dg3 : dg4)[a] += "G " + head + " " + std::to_string(shell) + " " + std::to_string(extra) + " " +
+                                    std::to_string(I + size) + " " + std::to_string(I + shell) + " " +
+                                    std::to_string(n - I - shell) + " " + sph + " |" + idt + "\n";
+  });
   // the stream orders records by (support size, ids): triples before quads
-  return ev[0] + ev[1] + dg[0] + dg[1] + "S complete\n";
+  std::string out;
+  for (const auto* v : {&ev3, &ev4, &dg3, &dg4})
+    for (const auto& x : *v) out += x;
+  return out + "S complete\n";
 }
 
 // ---- direct hierarchy: facade, Morse event journal, arm seeds, forest journal --------
@@ -884,43 +980,27 @@ std::string hierarchy_text(const Cloud& c, u64 K) {
       }
   }
   // triple and quad supports
-  auto visit = [&](const u64* ids, int size) {
-    if (smax < (u64)size) return;
-    SupportGeo g = analyze(c, f, ids, size);
-    if (g.status != 0) return;
-    analyze_fp(c, g);
-    HEvent e;
-    e.size = size;
-    for (int i = 0; i < size; ++i) e.ids[i] = ids[i];
-    u64 shell = size;
-    for (u64 w = 0; w < n; ++w) {
-      bool sup = false;
-      for (int i = 0; i < size; ++i) sup |= (w == ids[i]);
-      if (sup) continue;
-      const int sd = higher_side(c, f, g, w);
-      if (sd < 0) {
-        e.interior.push_back(w);
-        if (e.interior.size() > smax - size) return;
-      } else if (sd == 0) {
-        ++shell;
-      }
-    }
-    if (shell != (u64)size) {
-      ++diagnostics;
-      return;
-    }
-    bool minimal = false;
-    e.level = ball_of(c, f, ids, size, &minimal).level;
-    ev.push_back(std::move(e));
-  };
   {
-    u64 ids[4];
-    for (ids[0] = 0; ids[0] < n; ++ids[0])
-      for (ids[1] = ids[0] + 1; ids[1] < n; ++ids[1])
-        for (ids[2] = ids[1] + 1; ids[2] < n; ++ids[2]) {
-          visit(ids, 3);
-          for (ids[3] = ids[2] + 1; ids[3] < n; ++ids[3]) visit(ids, 4);
-        }
+    std::vector<std::vector<HEvent>> per(std::max(1u, std::min(64u, std::thread::hardware_concurrency())));
+    std::vector<u64> diag(per.size(), 0);
+    enumerate_higher(c, f, smax, [&](unsigned tid, const SupportGeo& g, const std::vector<u64>& interior, u64 shell,
+                                     u64) {
+      if (shell != (u64)g.size) {
+        ++diag[tid];
+        return;
+      }
+      HEvent e;
+      e.size = g.size;
+      for (int i = 0; i < g.size; ++i) e.ids[i] = g.ids[i];
+      e.interior = interior;
+      bool minimal = false;
+      e.level = ball_of(c, f, e.ids, g.size, &minimal).level;
+      per[tid].push_back(std::move(e));
+    });
+    for (size_t t = 0; t < per.size(); ++t) {
+      diagnostics += diag[t];
+      for (auto& e : per[t]) ev.push_back(std::move(e));
+    }
   }
   for (auto& e : ev) {
     e.rank = e.interior.size() + e.size;
@@ -1035,19 +1115,28 @@ std::string hierarchy_text(const Cloud& c, u64 K) {
     while (parent[h] != h) h = parent[h];
     return h;
   };
+  std::vector<std::vector<u64>> order_handles(keff + 2);  // born handles of each order
   auto count_roots = [&](u64 order, bool reduced) {
     u64 k = 0;
-    for (u64 h = 0; h < birth_count; ++h)
+    for (u64 h : order_handles[order])
       if (active[h] && parent[h] == h && border[h] == order && (!reduced || rroot[h] >= 0)) ++k;
     return k;
   };
   std::map<std::vector<u64>, u64> locator;  // bound facet -> birth handle
   std::string N, C = "C", B, A, S, G, T, R;
   u64 nodes = 0, children = 0, births = 0, bindings = 0, saddles = 0, groups = 0;
+  // The successor G of a facet F in a strict descent depends on the geometry alone, so it is
+  // computed once per facet; where a descent stops depends on the locator at the call.
+  std::map<std::vector<u64>, std::vector<u64>> successor;
   auto descend = [&](std::vector<u64> F) -> u64 {
     for (int guard = 0; guard < 100000; ++guard) {
       const auto hit = locator.find(F);
       if (hit != locator.end()) return hit->second;
+      const auto memo = successor.find(F);
+      if (memo != successor.end()) {
+        F = memo->second;
+        continue;
+      }
       const XBall bf = facet_miniball(c, f, F);
       const u64 k = F.size();
       std::vector<std::pair<Big, u64>> d(n);
@@ -1067,6 +1156,7 @@ std::string hierarchy_text(const Cloud& c, u64 K) {
       if (Gs == F) throw std::logic_error("a strict arm descent is unresolved");
       const XBall bg = facet_miniball(c, f, Gs);
       if (!rat_less(bg.level, bf.level)) throw std::logic_error("a strict arm descent met a plateau");
+      successor.emplace(F, Gs);
       F = Gs;
     }
     throw std::logic_error("a strict arm descent did not terminate");
@@ -1224,6 +1314,7 @@ std::string hierarchy_text(const Cloud& c, u64 K) {
     for (auto& b : nb) {
       active[b.handle] = 1;
       border[b.handle] = b.order;
+      order_handles[b.order].push_back(b.handle);
       rroot[b.handle] = b.node;
       locator[b.key] = b.handle;
     }
@@ -1241,6 +1332,58 @@ std::string hierarchy_text(const Cloud& c, u64 K) {
     R += "R " + std::to_string(i) + " " + std::to_string(fr[i][0]) + " " + std::to_string(fr[i][2]) + " " +
          std::to_string(fr[i][1]) + "\n";
   return s + N + C + "\n" + B + A + S + G + T + R + "D 5 5 13\n";
+}
+
+// Exact classification of given supports against every point of the cloud: the leaf rule
+// of the pair stream (classify_sparse_closed_ball, src/cpu/hierarchy/pair_support_stream.cpp:1781-1952)
+// and of the higher stream (classify_terminal_support, higher_support_stream.cpp:1992-2110),
+// without any bound or pruning.  Per support (size, ids[4]): status (0 minimal, 1 not),
+// strict interior count, complete shell count (support included), least extra shell
+// PointId (or all ones), the first 10 strict interior ids ascending (unused all ones).
+void classify_supports(const Cloud& c, const FixedCloud& f, const uint32_t* sup, u64 count, uint32_t* out) {
+  const u64 n = c.bits.size();
+  const unsigned hw = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+  auto run = [&](unsigned tid) {
+    for (u64 i = tid; i < count; i += hw) {
+      const uint32_t* r = sup + 5 * i;
+      uint32_t* o = out + 14 * i;
+      const int size = (int)r[0];
+      u64 ids[4] = {r[1], r[2], r[3], r[4]};
+      for (int j = 0; j < 14; ++j) o[j] = 0xffffffffu;
+      o[0] = 1;
+      if (size < 2 || size > 4) continue;
+      bool ok = true;
+      for (int j = 0; j < size; ++j) ok &= ids[j] < n;
+      if (!ok) continue;
+      std::unique_ptr<LazyGeo> lg;
+      if (size >= 3) {
+        if (analyze(c, f, ids, size).status != 0) continue;
+        lg.reset(new LazyGeo(c, f, ids, size));
+      }
+      u64 I = 0, shell = (u64)size, extra = ~u64{0};
+      for (u64 w = 0; w < n; ++w) {
+        bool on = false;
+        for (int j = 0; j < size; ++j) on |= w == ids[j];
+        if (on) continue;
+        const int sd = size == 2 ? diametral_side(c, f, w, ids[0], ids[1]) : lg->side(w);
+        if (sd < 0) {
+          if (I < 10) o[4 + I] = (uint32_t)w;
+          ++I;
+        } else if (sd == 0) {
+          ++shell;
+          extra = std::min(extra, w);
+        }
+      }
+      o[0] = 0;
+      o[1] = (uint32_t)I;
+      o[2] = (uint32_t)shell;
+      o[3] = extra == ~u64{0} ? 0xffffffffu : (uint32_t)extra;
+    }
+  };
+  std::vector<std::thread> pool;
+  for (unsigned t = 1; t < hw; ++t) pool.emplace_back(run, t);
+  run(0);
+  for (auto& t : pool) t.join();
 }
 
 u64 put_text(const std::string& s, char* buf, u64 cap) {
@@ -1341,6 +1484,17 @@ int oracle_emst_forest(const double* xyz, u64 n, char* out, u64 cap, u64* needed
   }
 }
 
+
+int oracle_classify(const double* xyz, u64 n, const uint32_t* supports, u64 count, uint32_t* out, char* err,
+                    u64 errlen) {
+  try {
+    const Cloud c = canonical_cloud(xyz, n);
+    classify_supports(c, fixed_cloud(c), supports, count, out);
+    return 0;
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 1);
+  }
+}
 
 int oracle_hierarchy(const double* xyz, u64 n, u64 K, char* out, u64 cap, u64* needed, char* err, u64 errlen) {
   try {

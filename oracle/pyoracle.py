@@ -23,6 +23,23 @@ RESTATEMENT = os.path.join(HERE, "lib", "libehgp_oracle.so")
 REFERENCE = os.path.join(HERE, "_ref", "libehgp_ref.so")
 
 _libs: dict[str, C.CDLL] = {}
+_ref_root: list[str | None] = []
+
+
+def reference_root() -> str | None:
+    """Root of the reference checkout (EHGP_REFERENCE_ROOT, else the default of this
+    directory's Makefile, the recipe that compiles it), or None when it is absent."""
+    if not _ref_root:
+        root = os.environ.get("EHGP_REFERENCE_ROOT")
+        if not root:
+            import subprocess
+            try:
+                root = subprocess.run(["make", "-s", "-C", HERE, "print-ref-root"], capture_output=True, text=True,
+                                      timeout=30).stdout.strip()
+            except Exception:
+                root = None
+        _ref_root.append(root if root and os.path.isdir(root) else None)
+    return _ref_root[0]
 
 
 class OracleError(ValueError):
@@ -123,6 +140,25 @@ def _text_call(fn_name: str, which: str, pts: np.ndarray, *extra) -> str:
             return buf.value.decode()
         cap = int(needed.value) + 16
     raise RuntimeError("oracle output did not fit")
+
+
+def classify(points_canonical: np.ndarray, supports: np.ndarray) -> np.ndarray:
+    """Exact classification of supports (rows: size, id0..id3; PointIds of the canonical
+    cloud) against every point: rows (status 0 minimal / 1 not, strict interior count,
+    complete shell count, least extra shell PointId or 0xffffffff, first 10 interior ids).
+    `points_canonical` must already be in PointId order."""
+    lib = _lib("restatement")
+    fn = lib.oracle_classify
+    fn.restype = C.c_int
+    pts = np.ascontiguousarray(points_canonical, dtype=np.float64)
+    sup = np.ascontiguousarray(supports, dtype=np.uint32)
+    out = np.zeros((len(sup), 14), np.uint32)
+    err = C.create_string_buffer(512)
+    rc = fn(C.c_void_p(_p(pts)), C.c_uint64(len(pts)), C.c_void_p(_p(sup)), C.c_uint64(len(sup)),
+            C.c_void_p(_p(out)), err, C.c_uint64(512))
+    if rc != 0:
+        raise OracleError(rc, err.value.decode())
+    return out
 
 
 def knn(points: np.ndarray, k: int, which: str = "restatement") -> list[tuple[list[int], list[int], Fraction]]:

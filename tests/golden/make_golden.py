@@ -8,6 +8,7 @@ project-written Boost shim).  Run here, where the reference tree exists:
     python tests/golden/make_golden.py --higher  # slow: the reference higher-support stream (n = 12)
     python tests/golden/make_golden.py --hierarchy  # slow: the reference direct chain up to the forest journal
     python tests/golden/make_golden.py --definition  # the Python exhaustive-Gamma hgp_reduced forests
+    python tests/golden/make_golden.py --scale  # restatement digests at n = 216-256 (about 10 min)
 """
 import os
 import sys
@@ -192,7 +193,8 @@ if __name__ == "__main__" and "--hierarchy" in sys.argv:
 
 
 # ---- the normative hgp_reduced definition (Python exhaustive-Gamma oracle) ------------
-REF_PY = "/root/reference/reference"  # morsehgp3d_oracle, stdlib only; run here, where the reference exists
+# morsehgp3d_oracle (stdlib only) inside the reference checkout; run where the reference exists
+REF_PY = os.path.join(pyoracle.reference_root() or "", "reference")
 
 
 def definition_cases():
@@ -248,3 +250,62 @@ def main_definition():
 
 if __name__ == "__main__" and "--definition" in sys.argv:
     main_definition()
+
+
+# ---- parity at scale: digests of the restatement's supports and hierarchy ----------------
+def scale_cases():
+    """cfg1 (256 i.i.d. uniform points, seeds 0-9), a 6^3 jittered lattice, and 256-point
+    samples of the clustered generator with and without the 2^-10 snapping, K = 10."""
+    for seed in range(10):
+        yield f"uniform256_s{seed}", workloads.uniform_cube(256, seed)
+    yield "lattice6_f32", workloads.jittered_lattice(6, 5).astype(np.float64)
+    for seed in range(3):
+        yield f"clustered256_snap_s{seed}", workloads.clustered(256, 100 + seed)
+    for seed in range(2):
+        yield f"clustered256_s{seed}", workloads.clustered(256, 200 + seed, snapped=0.0)
+
+
+def higher_digest(rec: dict) -> str:
+    """Digest of higher-support records in the parsed form (pyoracle.parse_higher and
+    tests/geomcheck.gpu_higher_records give the same tuples)."""
+    import hashlib
+    return hashlib.sha256(repr((rec["events"], rec["diagnostics"])).encode()).hexdigest()
+
+
+def text_digest(text: str) -> str:
+    import hashlib
+    return hashlib.sha256(text.encode()).hexdigest()
+
+
+def _scale_one(args):
+    name, pts, K = args
+    P = np.asarray(pts, np.float64)
+    snap = pyoracle.lbvh_build(P)
+    canon = P[snap["source_index"].astype(np.int64)]
+    hi = pyoracle.higher(canon, K)
+    txt = pyoracle.hierarchy(P, K)
+    lines = txt.splitlines()
+    return name, {"points": P.tolist(), "K": K, "higher_sha256": higher_digest(hi),
+                  "higher_events": len(hi["events"]), "higher_diagnostics": len(hi["diagnostics"]),
+                  "hierarchy_sha256": text_digest(txt), "hierarchy_lines": len(lines),
+                  "hierarchy_last": lines[-1], "refused": txt.rstrip().endswith("D 4 3 4"),
+                  "facade_events": sum(1 for l in lines if l.startswith("F ")),
+                  "diagnostics": next(int(l.split()[1]) for l in lines if l.startswith("X "))}
+
+
+def main_scale():
+    import json
+    import multiprocessing as mp
+    jobs = [(name, pts, 10) for name, pts in scale_cases()]
+    out = {}
+    with mp.get_context("spawn").Pool(4) as pool:
+        for name, d in pool.imap_unordered(_scale_one, jobs):
+            out[name] = d
+            print(name, d["higher_events"], d["higher_diagnostics"], d["hierarchy_lines"], d["hierarchy_last"],
+                  flush=True)
+    with open(os.path.join(HERE, "scale_digests.json"), "w") as fh:
+        json.dump({k: out[k] for k, _, _ in jobs}, fh, separators=(",", ":"))
+
+
+if __name__ == "__main__" and "--scale" in sys.argv:
+    main_scale()

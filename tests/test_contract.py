@@ -19,8 +19,9 @@ from geomcheck import hier_dict_from_text
 from oracle import pyoracle
 
 DEFINITION = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "definition_*.json")))
-SCHEMA = "/root/reference/morsehgp3d/schemas/morsehgp3d-contract-v2.schema.json"
-SCHEMA_ALT = "/root/reference/schemas/morsehgp3d-contract-v2.schema.json"
+_REF = pyoracle.reference_root() or ""  # the reference checkout holds the schema
+SCHEMA = os.path.join(_REF, "morsehgp3d", "schemas", "morsehgp3d-contract-v2.schema.json")
+SCHEMA_ALT = os.path.join(_REF, "schemas", "morsehgp3d-contract-v2.schema.json")
 
 
 def canonical_order(pts):

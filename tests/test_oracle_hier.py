@@ -76,3 +76,18 @@ def test_vertical_maps_from_journal_match_definition(path):
     d = json.load(open(path))
     got = vertical_from_hier_text(pyoracle.hierarchy(np.array(d["points"]), d["K"]))
     assert sorted(got) == sorted(d["vertical"])
+
+
+def test_scale_digest_fixture_is_complete():
+    """golden/scale_digests.json (make_golden.py --scale) holds every case of the
+    plain-workload parity set: cfg1 seeds 0-9, the 6^3 lattice, clustered samples."""
+    import json
+    import os
+    d = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "scale_digests.json")))
+    names = set(d)
+    assert {f"uniform256_s{s}" for s in range(10)} <= names
+    assert "lattice6_f32" in names
+    assert any(k.startswith("clustered256_snap") for k in names)
+    assert any(k.startswith("clustered256_s") and "snap" not in k for k in names)
+    for k, v in d.items():
+        assert len(v["points"]) >= 216 and len(v["higher_sha256"]) == 64 and len(v["hierarchy_sha256"]) == 64, k

@@ -37,3 +37,36 @@ def test_restatement_higher_matches_golden(path):
 
 def test_golden_higher_has_diagnostics():
     assert sum(len(load_golden_higher(p)[2]["diagnostics"]) for p in GOLDEN) > 0
+
+
+def test_oracle_classify_agrees_with_the_streams():
+    """oracle.classify (every point, no pruning) reproduces the interior ids, shell counts
+    and least extra-shell witnesses of the restatement's pair and higher streams."""
+    rng = np.random.Generator(np.random.PCG64(61))
+    p = rng.random((40, 3))
+    p[:20] = np.round(p[:20] * 3) / 3  # cospherical ties: extra shells
+    pts = np.unique(p, axis=0)
+    snap = pyoracle.lbvh_build(pts)
+    P = pts[snap["source_index"].astype(np.int64)]
+    hi = pyoracle.higher(P, 10)
+    pa = pyoracle.pairs(P, 10)
+    rows, want = [], []
+    for m, ids, rank, ext, lev, cen, inter in hi["events"]:
+        rows.append([m, *ids, *([0] * (4 - m))])
+        want.append((len(inter), m, 0xffffffff, inter))
+    for m, ids, shell, wit, mr, orr, ext, lev, cen, inter in hi["diagnostics"]:
+        rows.append([m, *ids, *([0] * (4 - m))])
+        want.append((len(inter), shell, wit, inter))
+    for u, v, rank, ext, lev, cen, inter in pa["events"]:
+        rows.append([2, u, v, 0, 0])
+        want.append((len(inter), 2, 0xffffffff, inter))
+    for u, v, shell, wit, mr, orr, ext, lev, cen, inter in pa["diagnostics"]:
+        rows.append([2, u, v, 0, 0])
+        want.append((len(inter), shell, wit, inter))
+    assert len(hi["diagnostics"]) + len(pa["diagnostics"]) > 0
+    cls = pyoracle.classify(P, np.array(rows, np.uint32))
+    for row, w in zip(cls, want):
+        I, shell, wit, inter = w
+        assert row[0] == 0
+        assert (row[1], row[2], row[3]) == (I, shell, wit)
+        assert tuple(int(x) for x in row[4:4 + I]) == tuple(inter)
