@@ -70,6 +70,10 @@ constexpr int kDescentSteps = 512;   // descent steps per arm
 // conversions, [4] exact band orders, [5] exact cutoff comparisons, [6] strictness
 // checks on a cutoff equal to the level.
 __device__ unsigned long long g_descent_slow[8];
+// LBVH nodes visited by the descent's ball queries, striped over 64 counters by block
+// (one atomic per step, spread to keep a single address from serialising them).
+constexpr int kVisitStripes = 64;
+__device__ unsigned long long g_descent_visits[kVisitStripes];
 __device__ __forceinline__ void slow(int i) { atomicAdd(&g_descent_slow[i], 1ull); }
 
 // Descent status per arm.
@@ -765,7 +769,7 @@ __device__ __noinline__ bool facet_miniball(const Cloud& c, const uint32_t* F, i
 // success G holds k ascending ids and *cut_below is 1 when the cutoff lies strictly
 // below beta(F), 0 when it equals it.
 __device__ __noinline__ int topk_choice(const DescentParams& d, const Cloud& c, const Mini& mb, int k, uint32_t* G,
-                                        int* cut_below) {
+                                        int* cut_below, uint32_t* visits) {
   const FSphere& fs = mb.fs;
   double llo, lhi;
   if (!flevel(fs, llo, lhi)) { slow(3); exact_level_fp(c, mb.T, mb.ts, llo, lhi); }
@@ -792,6 +796,7 @@ __device__ __noinline__ int topk_choice(const DescentParams& d, const Cloud& c, 
   while (top > 0) {
     const uint32_t node = stack[--top];
     const TNode t = load_node(d.tn, node);
+    ++*visits;
     if (t.left == kInvalid32) {
       const uint32_t q = t.right;
       const double dx = c.px[q] - cx, dy = c.py[q] - cy, dz = c.pz[q] - cz;
@@ -982,7 +987,9 @@ k_arm_step(DescentParams d, uint32_t m, const uint32_t* __restrict__ in_arm, con
   if (!facet_miniball(c, F, k, mb)) { fail(kArmInternal); return; }
   uint32_t G[kMaxFacet];
   int cut_below = 0;
-  const int s = topk_choice(d, c, mb, k, G, &cut_below);
+  uint32_t visits = 0;
+  const int s = topk_choice(d, c, mb, k, G, &cut_below, &visits);
+  atomicAdd(&g_descent_visits[blockIdx.x % kVisitStripes], (unsigned long long)visits);
   if (s != kArmOk) { fail(s); return; }
   bool same = true;
   for (int j = 0; j < k; ++j) same &= G[j] == F[j];
@@ -1167,6 +1174,7 @@ struct HierState {
   cudaEvent_t ev_block = nullptr;  // blocking-sync event: the descent loop waits without spinning a core
   uint32_t first_misses = 0, descent_rounds = 0;
   unsigned long long slow[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long visits[kVisitStripes] = {};  // ball-query node visits of the descent steps
   // host results
   uint32_t n = 0, K = 0, keff = 0;
   int S = 0;
@@ -1194,6 +1202,9 @@ struct HierState {
   double ms_device = 0, ms_forest = 0, ms_descent = 0, ms_orders = 0;
   double ms_host[4] = {0, 0, 0, 0};  // exact facade ties, order passes, (unused), vertical maps
   uint64_t descent_steps = 0, arms = 0, exact_boundaries = 0;
+  cudaEvent_t ev_step[2] = {nullptr, nullptr};  // around each descent-step launch
+  double ms_steps = 0;                          // summed k_arm_step launch times
+  uint64_t step_launches = 0;
   // Schedule of the host forest pass and of the descent parts (results never depend on it):
   // single-role batches per published chunk, arms per descent part, host pool threads
   // (0: every hardware thread).
@@ -1210,6 +1221,8 @@ void hier_free(Ctx& ctx) {
                   (void*)ctx.hier->p_term, (void*)ctx.hier->p_stat})
     if (p) cudaFreeHost(p);
   if (ctx.hier->ev_block) cudaEventDestroy(ctx.hier->ev_block);
+  for (cudaEvent_t ev : ctx.hier->ev_step)
+    if (ev) cudaEventDestroy(ev);
   delete ctx.hier;
   ctx.hier = nullptr;
 }
@@ -1355,6 +1368,8 @@ int hier_run(Ctx& ctx, uint32_t K) {
   {
     const unsigned long long zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     cudaMemcpyToSymbolAsync(g_descent_slow, zero, sizeof(zero), 0, cudaMemcpyHostToDevice, st);
+    static const unsigned long long zv[kVisitStripes] = {};
+    cudaMemcpyToSymbolAsync(g_descent_visits, zv, sizeof(zv), 0, cudaMemcpyHostToDevice, st);
   }
   if (total)
     k_ev_build<<<nblk(total, kT), kT, 0, st>>>(np, nh, (const PairRecD*)ctx.pb.sorted, (const HigherRecD*)ctx.hb.sorted,
@@ -2304,6 +2319,10 @@ int hier_run(Ctx& ctx, uint32_t K) {
     uint32_t misses = 0, max_rounds = 0;
     unsigned long long failed_before = 0;
     h.descent_steps = 0;
+    h.ms_steps = 0;
+    h.step_launches = 0;
+    for (cudaEvent_t& ev : h.ev_step)
+      if (!ev && cudaEventCreate(&ev) != cudaSuccess) ev = nullptr;
     cudaEventRecord(ctx.evk0, st);
     uint32_t k = keff;
     auto stop = [&](int status, const char* msg) {
@@ -2350,11 +2369,18 @@ int hier_run(Ctx& ctx, uint32_t K) {
           }
           uint32_t* oc = h.qcount + 1 + (1 - cur);
           cudaMemsetAsync(oc, 0, sizeof(uint32_t), st);
+          if (h.ev_step[0]) cudaEventRecord(h.ev_step[0], st);
           k_arm_step<<<nblk(pending, 128), 128, 0, st>>>(dp, pending, h.q_arm[cur], h.q_fac[cur], h.q_arm[1 - cur],
                                                          h.q_fac[1 - cur], oc, h.term, h.arm_status, h.dstats);
+          if (h.ev_step[1]) cudaEventRecord(h.ev_step[1], st);
           ++launches;
+          ++h.step_launches;
           cudaMemcpyAsync(&pending, oc, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
           if ((dcuda = wait_stream()) != cudaSuccess) break;
+          if (h.ev_step[0] && h.ev_step[1]) {
+            float sm = 0.f;
+            if (cudaEventElapsedTime(&sm, h.ev_step[0], h.ev_step[1]) == cudaSuccess) h.ms_steps += sm;
+          }
           cur = 1 - cur;
         }
         if (dcuda != cudaSuccess || dstatus != EHGP_OK) return false;
@@ -2406,6 +2432,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
     }
     cudaEventRecord(ctx.evk1, st);
     cudaMemcpyFromSymbolAsync(h.slow, g_descent_slow, sizeof(h.slow), 0, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyFromSymbolAsync(h.visits, g_descent_visits, sizeof(h.visits), 0, cudaMemcpyDeviceToHost, st);
     cudaEventRecord(ctx.ev1, st);
     if (dcuda == cudaSuccess) dcuda = cudaStreamSynchronize(st);
     h.first_misses = misses;
@@ -2680,7 +2707,12 @@ int ehgp_hier_stats(const ehgp_ctx* ctx, double* ms, uint64_t* stats) {
     stats[4] = h.first_misses;
     stats[5] = h.descent_rounds;
     for (int i = 0; i < 7; ++i) stats[6 + i] = h.slow[i];
+    uint64_t v = 0;
+    for (int i = 0; i < ehgp::kVisitStripes; ++i) v += h.visits[i];
+    stats[13] = v;
+    stats[14] = h.step_launches;
   }
+  if (ms) ms[24] = h.ms_steps;
   return EHGP_OK;
 }
 

@@ -2046,9 +2046,9 @@ int ehgp_higher_stats(const ehgp_ctx* ctx, double* kernel_ms, uint64_t* stats, u
   if (!ctx) return EHGP_ERR_INVALID_ARGUMENT;
   if (kernel_ms) *kernel_ms = ctx->hb.kernel_ms;
   for (uint32_t i = 0; stats && i < count && i < 8; ++i) stats[i] = ctx->hb.stats_host[i];
-  // [4] owners certified on the large-neighbourhood path, [5] their neighbour-list entries
-  if (stats && count > 4) stats[4] = ctx->hb.big_owners;
-  if (stats && count > 5) stats[5] = ctx->hb.big_entries;
+  const ehgp::HigherBuffers& h = ctx->hb;
+  const uint64_t more[6] = {h.big_owners, h.big_entries, h.n_large, h.n_huge, h.n_mega, h.large_entries};
+  for (uint32_t i = 8; stats && i < count && i < 14; ++i) stats[i] = more[i - 8];
   return EHGP_OK;
 }
 

@@ -422,9 +422,11 @@ class Context:
         return recs[:m]
 
     def higher_stats(self) -> tuple[float, np.ndarray]:
+        """Kernel time (ms) of the last triple/quad enumeration and its 14 work counters
+        (include/ehgp.h, ehgp_higher_stats)."""
         ms = C.c_double()
-        st = np.zeros(8, np.uint64)
-        self._check(self.lib.ehgp_higher_stats(self._h, C.byref(ms), _ptr(st), 8))
+        st = np.zeros(14, np.uint64)
+        self._check(self.lib.ehgp_higher_stats(self._h, C.byref(ms), _ptr(st), 14))
         return ms.value, st
 
     def hierarchy(self, K: int = 10, arrays: bool = True) -> dict:
@@ -455,12 +457,13 @@ class Context:
 
     def hier_stats(self) -> dict:
         """Timing and work counters of the last hierarchy call."""
-        ms = np.zeros(24)
-        st = np.zeros(13, np.uint64)
+        ms = np.zeros(25)
+        st = np.zeros(15, np.uint64)
         self._check(self.lib.ehgp_hier_stats(self._h, _ptr(ms), _ptr(st)))
         return {"device_ms": ms[0], "descent_ms": ms[1], "forest_ms": ms[2], "slowest_order_ms": ms[3],
                 "facade_ties_ms": ms[4], "host_orders_ms": ms[5], "host_offsets_ms": ms[6], "host_vertical_ms": ms[7],
-                "order_ms": [float(x) for x in ms[8:] if x > 0],
+                "order_ms": [float(x) for x in ms[8:24] if x > 0], "step_kernels_ms": float(ms[24]),
+                "step_node_visits": int(st[13]), "step_launches": int(st[14]),
                 "arms": int(st[0]),
                 "descent_steps": int(st[1]), "exact_boundaries": int(st[2]), "events": int(st[3]),
                 "first_misses": int(st[4]), "descent_rounds": int(st[5]),

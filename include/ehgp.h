@@ -261,11 +261,15 @@ typedef struct ehgp_higher_out {
  * completion.  records == NULL only counts. */
 int ehgp_higher(ehgp_ctx* ctx, uint32_t K, const ehgp_higher_out* out);
 
-/* CUDA-event time of the last triple/quad enumeration kernel and its work
+/* CUDA-event time of the last triple/quad enumeration kernels and their work
  * counters: [0] candidate supports tested, [1] closed-ball classifications,
- * [2] records, [3] neighbour-list entries, [4] owners whose certified
- * neighbourhood exceeded the 1024-entry list and took the large-neighbourhood
- * path (count -> allocate -> write), [5] entries of their lists. */
+ * [2] records, [3] candidate-set entries, [4] support candidates (ids above
+ * the owner), [5] minimal supports, [6] minimal supports dropped by the cone
+ * bounds, [7] faces admitted; [8] owners whose certified neighbourhood
+ * exceeded the 1024-entry list and took the large-neighbourhood path (count ->
+ * allocate -> write), [9] entries of their lists, [10]-[12] owners whose
+ * candidate set exceeded 256 and was staged as a large (<= 1024), huge
+ * (<= 4096) or mega (<= 16384) set, [13] entries of those sets.  count <= 14. */
 int ehgp_higher_stats(const ehgp_ctx* ctx, double* kernel_ms, uint64_t* stats, uint32_t count);
 
 /* Allocation-free LBVH build.  No counterpart in the reference: it exists for
@@ -431,13 +435,16 @@ int ehgp_hier_schedule(ehgp_ctx* ctx, uint32_t chunk_batches, uint32_t part_arms
  * ordering of uncertain facade boundaries, ms[5..7] the host forest pass split
  * into the order passes, the record offsets and the vertical maps,
  * ms[8 + k - 1] the union-find core of order k (k <= 16,
- * zero above the last order); ms holds 24 doubles;
+ * zero above the last order);
  * stats[0] strict arms, [1] descent steps, [2] facade boundaries settled
  * exactly on the host, [3] facade events, [4] arms that are not themselves a
  * birth facet, [5] descent rounds (longest chain), [6..12] slow-path counts of
  * the descent (exhaustive miniball enumerations, exact hull signs, exact
  * closed-ball sides, exact level conversions, exact band orders, exact cutoff
- * comparisons, strictness checks at an equal cutoff); stats holds 13 words. */
+ * comparisons, strictness checks at an equal cutoff), [13] LBVH nodes visited by
+ * the descent steps' ball queries, [14] descent-step launches; ms[24] the summed
+ * CUDA-event time of the descent-step launches; ms holds 25 doubles and stats 15
+ * words. */
 int ehgp_hier_stats(const ehgp_ctx* ctx, double* ms, uint64_t* stats);
 
 /* Exact level of facade event `event` as num / (den 2^(2 scale)), two's

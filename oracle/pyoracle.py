@@ -161,6 +161,25 @@ def classify(points_canonical: np.ndarray, supports: np.ndarray) -> np.ndarray:
     return out
 
 
+def ref_pairs_budget(points: np.ndarray, K: int, work_units: int) -> dict:
+    """The reference's own pair stream on the whole cloud under a work-unit budget
+    (oracle/ref_driver.cpp ref_pairs_budget): time to the budget and how far it got."""
+    lib = _lib("reference")
+    fn = lib.ref_pairs_budget
+    fn.restype = C.c_int
+    pts = np.ascontiguousarray(points, dtype=np.float64)
+    st = np.zeros(6, np.uint64)
+    sec = np.zeros(2)
+    err = C.create_string_buffer(512)
+    rc = fn(C.c_void_p(_p(pts)), C.c_uint64(len(pts)), C.c_uint64(K), C.c_uint64(work_units), C.c_void_p(_p(st)),
+            C.c_void_p(_p(sec)), err, C.c_uint64(512))
+    if rc != 0:
+        raise OracleError(rc, err.value.decode())
+    return {"complete": int(st[0]) == 0, "work_units": int(st[1]), "resolved_pairs": int(st[2]),
+            "total_pairs": int(st[3]), "events": int(st[4]), "diagnostics": int(st[5]),
+            "lbvh_s": float(sec[0]), "stream_s": float(sec[1])}
+
+
 def knn(points: np.ndarray, k: int, which: str = "restatement") -> list[tuple[list[int], list[int], Fraction]]:
     """Per PointId p: (strict ids in (d, id) order, shell ids, cutoff squared distance)."""
     name = "oracle_knn" if which == "restatement" else "ref_knn"

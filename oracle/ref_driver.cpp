@@ -324,6 +324,39 @@ int ref_pairs(const double* xyz, uint64_t n, uint64_t K, char* out, uint64_t cap
   }
 }
 
+// The budgeted protocol of the CPU baseline: canonical cloud + LBVH, then
+// build_exact_pair_support_stream (include/morsehgp3d/hierarchy/pair_support_stream.hpp:415)
+// with maximum_work_unit_count = work_units (the other limits unlimited).  stats[0] status
+// (0 complete, 1 budget exhausted), [1] work units used, [2] resolved pairs, [3] total
+// pairs, [4] events, [5] relevant extra-shell diagnostics; seconds[0] cloud + LBVH,
+// seconds[1] the stream.
+int ref_pairs_budget(const double* xyz, uint64_t n, uint64_t K, uint64_t work_units, uint64_t* stats,
+                     double* seconds, char* err, uint64_t errlen) {
+  try {
+    using namespace morsehgp3d;
+    const auto pts = points_from(xyz, n);
+    const auto t0 = std::chrono::steady_clock::now();
+    const CanonicalPointCloud cloud = CanonicalPointCloud::rejecting_duplicates(pts);
+    const MortonLbvhIndex index = MortonLbvhIndex::build(cloud);
+    const auto t1 = std::chrono::steady_clock::now();
+    auto budget = unlimited_pair_budget();
+    budget.maximum_work_unit_count = work_units;
+    const auto res = hierarchy::build_exact_pair_support_stream(index, cloud, K, budget);
+    const auto t2 = std::chrono::steady_clock::now();
+    seconds[0] = std::chrono::duration<double>(t1 - t0).count();
+    seconds[1] = std::chrono::duration<double>(t2 - t1).count();
+    stats[0] = res.status == hierarchy::ExactPairSupportStreamStatus::complete ? 0 : 1;
+    stats[1] = res.audit.work_unit_count;
+    stats[2] = res.audit.resolved_pair_count;
+    stats[3] = res.audit.total_pair_count;
+    stats[4] = res.events.size();
+    stats[5] = res.relevant_extra_shell_diagnostics.size();
+    return 0;
+  } catch (const std::exception& e) {
+    return report(e, err, errlen, 1);
+  }
+}
+
 // build_exact_lbvh_boruvka (include/morsehgp3d/hierarchy/boruvka.hpp:130) and
 // build_compact_k1_forest on its edges (include/morsehgp3d/hierarchy/k1_forest.hpp:108).
 // Lines: "E u v num den" (EMST, canonical order), "M round label source u v num den"
