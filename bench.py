@@ -246,6 +246,104 @@ def cpu_baseline_line(ours_on_sample_ms: float | None) -> dict:
             "host_cores_total": os.cpu_count()}
 
 
+# ---- batched uneven clouds and a serving stream (one GPU) -------------------------------
+BATCH_CLOUDS = 64          # clouds of the batched workload timed per run (of its 512)
+SERVE_REQUESTS = 48        # requests of each serving-stream rate
+SERVE_WORKERS = 8
+
+
+def _plain_payload(ctx, pts, K):
+    """One cloud through the public API, one call at a time: host points in, the served
+    payload (EMST edges, hierarchy arrays, node level supports) out."""
+    ctx.lbvh_build(pts, outputs=False)
+    return ctx.served_result(K)
+
+
+def served_section(local: int) -> dict:
+    """Batched uneven clouds (Gaussian mixtures of 1-6 components + 10 % noise, sizes
+    log-uniform in [1,000, 20,000], binary32, K_max = 10): clouds/s of one cloud per call on
+    one context against the serving engine with SERVE_WORKERS workers, all submitted at once.
+    Serving stream: Poisson arrivals of clouds from the same generator with sizes log-uniform
+    in [500, 20,000] and K_max uniform in {4, 10}, at rates relative to the served throughput;
+    p50/p95/p99 latency (submit to result in host memory) and achieved clouds/s per rate."""
+    import ehgp
+    import workloads
+    clouds = workloads.batched_uneven(BATCH_CLOUDS, seed=7)
+    out = {"batched": {"workload": f"{BATCH_CLOUDS} of 512 mixture clouds, n log-uniform in [1000, 20000], f32",
+                       "points": int(sum(len(c) for c in clouds))}}
+    maxn = max(len(c) for c in clouds)
+    with ehgp.Context(max_points=max(maxn, 20000), device=local) as ctx:
+        for c in clouds[:2]:
+            _plain_payload(ctx, c, K_MAX)  # warm-up
+        t0 = time.perf_counter()
+        for c in clouds:
+            _plain_payload(ctx, c, K_MAX)
+        plain_s = time.perf_counter() - t0
+    with ehgp.Server(workers=SERVE_WORKERS, max_points=20000, device=local) as srv:
+        for rid in [srv.submit(c, K_MAX) for c in clouds[:SERVE_WORKERS]]:  # warm-up: every worker once
+            srv.wait(rid)
+            srv.release(rid)
+        t0 = time.perf_counter()
+        ids = [srv.submit(c, K_MAX) for c in clouds]
+        bad = sum(srv.wait(r) != 0 for r in ids)
+        served_s = time.perf_counter() - t0
+        for r in ids:
+            srv.release(r)
+        out["batched"].update({"plain_clouds_per_s": len(clouds) / plain_s, "served_clouds_per_s": len(clouds) / served_s,
+                               "served_over_plain": plain_s / served_s, "workers": SERVE_WORKERS, "failed": bad})
+        # the same comparison on uniform clouds, whose step is dominated by the host forest
+        # pass (the engine overlaps one cloud's host pass with another's device work)
+        ucl = [workloads.uniform_cube(int(n), 500 + i) for i, n in
+               enumerate(np.exp(np.random.Generator(np.random.PCG64(5)).uniform(np.log(1000), np.log(20000), 32)))]
+        with ehgp.Context(max_points=20000, device=local) as ctx:
+            _plain_payload(ctx, ucl[0], K_MAX)
+            t0 = time.perf_counter()
+            for c in ucl:
+                _plain_payload(ctx, c, K_MAX)
+            uplain = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        uids = [srv.submit(c, K_MAX) for c in ucl]
+        ubad = sum(srv.wait(r) != 0 for r in uids)
+        userved = time.perf_counter() - t0
+        for r in uids:
+            srv.release(r)
+        out["batched_uniform"] = {"workload": "32 uniform clouds, n log-uniform in [1000, 20000], f64",
+                                  "plain_clouds_per_s": len(ucl) / uplain, "served_clouds_per_s": len(ucl) / userved,
+                                  "served_over_plain": uplain / userved, "workers": SERVE_WORKERS, "failed": ubad}
+        # serving stream at rates relative to the served throughput
+        rng = np.random.Generator(np.random.PCG64(11))
+        sizes = np.exp(rng.uniform(np.log(500), np.log(20000), SERVE_REQUESTS)).astype(int)
+        reqs = [(workloads.mixture_cloud(int(n), rng), int(rng.choice([4, 10]))) for n in sizes]
+        cap = len(clouds) / served_s
+        rates = []
+        for frac in (0.25, 0.5, 1.0):
+            lam = frac * cap
+            gaps = rng.exponential(1.0 / lam, SERVE_REQUESTS)
+            t0 = time.perf_counter()
+            ids = []
+            due = t0
+            for (pts, K), g in zip(reqs, gaps):
+                due += g
+                while time.perf_counter() < due:
+                    time.sleep(min(0.001, max(0.0, due - time.perf_counter())))
+                ids.append(srv.submit(pts, K))
+            fails = sum(srv.wait(r) != 0 for r in ids)
+            wall = time.perf_counter() - t0
+            lat = [srv.info(r)["latency_ms"] for r in ids]
+            for r in ids:
+                srv.release(r)
+            rates.append({"offered_clouds_per_s": lam, "achieved_clouds_per_s": SERVE_REQUESTS / wall,
+                          "latency_ms": spread(lat), "failed": fails})
+        ok = [r for r in rates if r["latency_ms"]["p99"] < 100.0 and not r["failed"]]
+        out["serving"] = {"workload": (f"{SERVE_REQUESTS} Poisson arrivals per rate, mixture clouds n log-uniform in "
+                                       "[500, 20000], K_max in {4, 10}, f32"),
+                          "workers": SERVE_WORKERS, "rates": rates,
+                          "clouds_per_s_at_p99_below_100ms": max((r["achieved_clouds_per_s"] for r in ok),
+                                                                   default=None),
+                          "server": srv.stats()}
+    return out
+
+
 # ---- our path ----------------------------------------------------------------------------
 def run_ours(args, world, rank, local):
     import ctypes as C
@@ -441,6 +539,11 @@ def run_ours(args, world, rank, local):
             "algorithmic_bytes": d_bytes, "work": {"descent_steps": steps, "node_visits": visits},
             "note": "FP64 miniball and exact top-k per thread; latency-bound, not byte-bound",
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    if world == 1 and not args.no_served:
+        try:
+            line.update(served_section(local))
+        except Exception as exc:  # the headline line is printed either way
+            line["served_error"] = f"{type(exc).__name__}: {exc}"
     if world == 1:
         # our own time on the reference's sample, for a like-for-like reading
         sample = reference_sample(0)
@@ -530,6 +633,7 @@ def main():
     ap.add_argument("--chain", default=None, metavar="WORKLOAD",
                     help="one pass of the chain on lattice:SIDE, uniform:N, clustered:N or mixture:N (stage times)")
     ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--no-served", action="store_true", help="skip the batched and serving measurements")
     ap.add_argument("--K", type=int, default=K_MAX)
     args = ap.parse_args()
     if args.chain:

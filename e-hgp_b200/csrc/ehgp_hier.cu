@@ -62,7 +62,7 @@ constexpr double kTiny = 1e-300;
 constexpr int kMaxFacet = 10;
 constexpr int kT = 256;              // threads per block of the elementwise kernels
 constexpr int kCandCap = 64;         // ball-query candidates per descent step
-constexpr int kDStack = 64;          // LBVH traversal stack per descent thread
+constexpr int kDStack = 96;          // LBVH traversal stack per descent thread (depth <= 63 + log2 n + 1)
 constexpr int kDescentSteps = 512;   // descent steps per arm
 
 // Slow-path counters of the descent (read back per call): [0] exhaustive miniball
@@ -387,6 +387,18 @@ __global__ void k_run_scatter(uint32_t cnt, const uint32_t* __restrict__ idx, co
   if (i >= cnt) return;
   ev[idx[i]] = in[i];
   eqprev[idx[i]] = eq[i];
+}
+
+// Support records of facade events: out[5i] = size, out[5i + 1..4] = ids (unused 0); an
+// index of kInvalid32 (level 0) or past the facade gives size 0.
+__global__ void k_event_supports(uint32_t m, const uint32_t* __restrict__ idx, const EvRec* __restrict__ ev,
+                                 uint32_t nev, uint32_t* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const uint32_t e = idx[i];
+  const bool ok = e < nev;
+  out[5ull * i] = ok ? ev[e].size : 0u;
+  for (int j = 0; j < 4; ++j) out[5ull * i + 1 + j] = ok && (uint32_t)j < ev[e].size ? ev[e].ids[j] : 0u;
 }
 
 // ---- 2. level classes, rank partition, births -----------------------------------
@@ -793,6 +805,12 @@ __device__ __noinline__ int topk_choice(const DescentParams& d, const Cloud& c, 
   uint32_t stack[kDStack];
   int top = 0;
   stack[top++] = d.root;
+  // The nearest kCandCap points within R, sorted by FP64 squared distance; a farther point
+  // is dropped when the list is full.  Only the points up to the band around the k-th
+  // distance matter, so the traversal is pruned at the current k-th distance + 2 ed (it
+  // can only decrease), and the dropped points are checked to lie beyond the band below.
+  double R2_eff = R2;
+  bool dropped = false;
   while (top > 0) {
     const uint32_t node = stack[--top];
     const TNode t = load_node(d.tn, node);
@@ -801,12 +819,17 @@ __device__ __noinline__ int topk_choice(const DescentParams& d, const Cloud& c, 
       const uint32_t q = t.right;
       const double dx = c.px[q] - cx, dy = c.py[q] - cy, dz = c.pz[q] - cz;
       const double dd = dx * dx + dy * dy + dz * dz;
-      if (dd > R2) continue;
-      if (cnt == kCandCap) return kArmCapacity;
+      if (dd > R2_eff) continue;
+      if (cnt == kCandCap) {
+        if (dd >= cd[kCandCap - 1]) { dropped = true; continue; }
+        --cnt;
+        dropped = true;
+      }
       int j = cnt++;
       while (j > 0 && cd[j - 1] > dd) { cd[j] = cd[j - 1]; cid[j] = cid[j - 1]; --j; }
       cd[j] = dd;
       cid[j] = q;
+      if (cnt >= k) R2_eff = fmin(R2, (cd[k - 1] + 2.0 * ed) * (1.0 + 1e-12));
       continue;
     }
     double lb = 0.0;
@@ -817,7 +840,7 @@ __device__ __noinline__ int topk_choice(const DescentParams& d, const Cloud& c, 
         lb += g * g;
       }
     }
-    if (lb * (1.0 - 1e-6) > R2) continue;
+    if (lb * (1.0 - 1e-6) > R2_eff) continue;
     if (top + 2 > kDStack) return kArmCapacity;
     stack[top++] = t.left;
     stack[top++] = t.right;
@@ -825,6 +848,8 @@ __device__ __noinline__ int topk_choice(const DescentParams& d, const Cloud& c, 
   if (cnt < k) return kArmInternal;
   // partition around the k-th approximate distance
   const double tk = cd[k - 1];
+  // every dropped point is at least as far as the last kept one: it must lie past the band
+  if (dropped && !(cd[cnt - 1] > tk + 2.0 * ed)) return kArmCapacity;
   int below = 0, band0 = -1, band1 = -1;
   for (int i = 0; i < cnt; ++i) {
     if (cd[i] < tk - 2.0 * ed) below = i + 1;
@@ -2713,6 +2738,27 @@ int ehgp_hier_stats(const ehgp_ctx* ctx, double* ms, uint64_t* stats) {
     stats[14] = h.step_launches;
   }
   if (ms) ms[24] = h.ms_steps;
+  return EHGP_OK;
+}
+
+int ehgp_event_supports(ehgp_ctx* ctx, const uint32_t* events, uint64_t count, uint32_t* out) {
+  if (!ctx || (count && (!events || !out))) return EHGP_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  if (!ctx->hier || ctx->hier->decision != EHGP_OK || !ctx->hier->order0 || !ctx->hier->ev_raw)
+    return ehgp::abi_fail(ctx, EHGP_ERR_NOT_BUILT, "ehgp_event_supports needs a hierarchy result");
+  ehgp::HierState& h = *ctx->hier;
+  cudaStream_t st = ctx->stream;
+  // chunks through the facade's scratch (index: order0, output: ev_raw), free after the call
+  const uint64_t chunk = std::min<uint64_t>(h.cap_events, (h.cap_events * sizeof(ehgp::EvRec)) / 20);
+  for (uint64_t b0 = 0; b0 < count; b0 += chunk) {
+    const uint32_t m = (uint32_t)std::min<uint64_t>(chunk, count - b0);
+    cudaMemcpyAsync(h.order0, events + b0, (uint64_t)m * 4, cudaMemcpyHostToDevice, st);
+    ehgp::k_event_supports<<<ehgp::nblk(m, ehgp::kT), ehgp::kT, 0, st>>>(m, h.order0, h.ev, (uint32_t)h.events,
+                                                                        (uint32_t*)h.ev_raw);
+    cudaMemcpyAsync(out + 5 * b0, h.ev_raw, (uint64_t)m * 20, cudaMemcpyDeviceToHost, st);
+    const cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return ehgp::abi_cuda_fail(ctx, e, "facade event supports");
+  }
   return EHGP_OK;
 }
 

@@ -154,6 +154,28 @@ class HierOut(C.Structure):
     _fields_ = [(name, C.c_void_p) for name, _, _ in _HIER_FIELDS]
 
 
+class ServerLimits(C.Structure):
+    _fields_ = [("workers", C.c_uint32), ("max_points", C.c_uint64), ("hbm_fraction", C.c_double)]
+
+
+class CloudDesc(C.Structure):
+    _fields_ = [("xyz", C.c_void_p), ("n", C.c_uint64), ("dtype", C.c_uint32), ("K", C.c_uint32)]
+
+
+class RequestStats(C.Structure):
+    _fields_ = [("state", C.c_int32), ("status", C.c_int32), ("points", C.c_uint64), ("K", C.c_uint32),
+                ("worker", C.c_uint32), ("queued_ms", C.c_double), ("service_ms", C.c_double),
+                ("latency_ms", C.c_double), ("device_ms", C.c_double), ("counts", HierCounts)]
+
+
+class ServedOut(C.Structure):
+    _fields_ = [(f, C.c_void_p) for f in ("nodes", "children", "batches", "roots", "vertical", "node_supports",
+                                          "emst_u", "emst_v")]
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
+
 def limbs_to_int(a: np.ndarray) -> int:
     """Little-endian 64-bit limbs -> Python int."""
     v = 0
@@ -205,6 +227,17 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "ehgp_ctx_reserve": (C.c_int, [P, C.c_uint32, C.c_uint64]),
         "ehgp_ctx_regrowths": (C.c_uint64, [P]),
         "ehgp_tune": (C.c_int, [P, C.c_uint32, C.c_uint64]),
+        "ehgp_event_supports": (C.c_int, [P, P, C.c_uint64, P]),
+        "ehgp_server_create": (C.c_int, [C.c_int, C.POINTER(ServerLimits), C.POINTER(P)]),
+        "ehgp_server_destroy": (C.c_int, [P]),
+        "ehgp_cloud_submit": (C.c_int, [P, C.POINTER(CloudDesc), C.POINTER(C.c_uint64)]),
+        "ehgp_poll": (C.c_int, [P, C.c_uint64, C.POINTER(C.c_int32)]),
+        "ehgp_wait": (C.c_int, [P, C.c_uint64, C.c_uint64, C.POINTER(C.c_int32)]),
+        "ehgp_request_info": (C.c_int, [P, C.c_uint64, C.POINTER(RequestStats)]),
+        "ehgp_request_error": (C.c_char_p, [P, C.c_uint64]),
+        "ehgp_result_copy": (C.c_int, [P, C.c_uint64, C.POINTER(ServedOut)]),
+        "ehgp_result_release": (C.c_int, [P, C.c_uint64]),
+        "ehgp_server_info": (C.c_int, [P, P, C.c_uint32]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -482,6 +515,35 @@ class Context:
             return v - (1 << (64 * 36)) if v >> (64 * 36 - 1) else v
         return Fraction(signed(num), signed(den) << (2 * S.value))
 
+    def event_supports(self, events: np.ndarray) -> np.ndarray:
+        """ehgp_event_supports: (size, ids[4]) of facade events of the last hierarchy."""
+        ev = np.ascontiguousarray(events, dtype=np.uint32)
+        out = np.zeros((max(len(ev), 1), 5), np.uint32)
+        self._check(self.lib.ehgp_event_supports(self._h, _ptr(ev), len(ev), _ptr(out)))
+        return out[:len(ev)]
+
+    def served_result(self, K: int = 10) -> dict:
+        """The payload a served request carries, computed on this context for the
+        resident cloud (EMST, hierarchy arrays, node level supports)."""
+        n = self.n
+        u = np.zeros(max(n - 1, 1), np.uint32)
+        v = np.zeros(max(n - 1, 1), np.uint32)
+        self._check(self.lib.ehgp_emst(self._h, C.byref(EmstOut(_ptr(u), _ptr(v), None, None, None, 0, None))))
+        r = self.hierarchy(K, arrays=False)
+        sizes = {"nodes": r["nodes"], "children": r["children"], "batches": r["journal_batches"],
+                 "roots": r["final_roots"], "vertical": r["vertical_assignments"]}
+        arr = {"nodes": np.zeros(max(sizes["nodes"], 1), FOREST_NODE),
+               "children": np.zeros(max(sizes["children"], 1), np.uint32),
+               "batches": np.zeros(max(sizes["batches"], 1), FOREST_BATCH),
+               "roots": np.zeros(max(sizes["roots"], 1), FOREST_ROOT),
+               "vertical": np.zeros(max(sizes["vertical"], 1), VERTICAL_ASSIGNMENT)}
+        ho = HierOut(*[_ptr(arr[name]) if name in arr else None for name, _, _ in _HIER_FIELDS])
+        self._check(self.lib.ehgp_hier_copy(self._h, C.byref(ho)))
+        out = {k: a[:sizes[k]] for k, a in arr.items()}
+        out["node_supports"] = self.event_supports(out["nodes"]["level_event"])
+        out["emst_u"], out["emst_v"] = u[:n - 1], v[:n - 1]
+        return out
+
     def k1_forest(self) -> dict:
         """ehgp_k1_forest on the last EMST: reference-layout compact forest arenas."""
         n = self.n
@@ -497,3 +559,102 @@ class Context:
         L, N, Ch, B = (int(x) for x in counts)
         return {"level_num": lv[:L], "nodes": nodes[:N], "children": child[:Ch], "batches": batches[:B],
                 "root": int(root[0])}
+
+
+class Server:
+    """Serving engine (include/ehgp.h ehgp_server_*): clouds are submitted asynchronously and
+    run `workers` at a time on contexts of their own, admitted by device memory."""
+
+    def __init__(self, workers: int = 4, max_points: int = 100_000, device: int = 0, hbm_fraction: float = 0.8):
+        self.lib = load()
+        h = C.c_void_p()
+        lim = ServerLimits(workers, max_points, hbm_fraction)
+        st = self.lib.ehgp_server_create(device, C.byref(lim), C.byref(h))
+        if st != 0:
+            raise _ERRORS.get(st, EhgpError)(st, "ehgp_server_create failed")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.lib.ehgp_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, points: np.ndarray, K: int = 10) -> int:
+        pts = np.ascontiguousarray(points)
+        dtype = 1 if pts.dtype == np.float32 else 0
+        if dtype == 0:
+            pts = np.ascontiguousarray(pts, dtype=np.float64)
+        rid = C.c_uint64()
+        st = self.lib.ehgp_cloud_submit(self._h, C.byref(CloudDesc(pts.ctypes.data, len(pts), dtype, K)),
+                                        C.byref(rid))
+        if st != 0:
+            raise _ERRORS.get(st, EhgpError)(st, "ehgp_cloud_submit refused the cloud")
+        return rid.value
+
+    def poll(self, rid: int) -> int:
+        state = C.c_int32()
+        st = self.lib.ehgp_poll(self._h, rid, C.byref(state))
+        if st != 0:
+            raise _ERRORS.get(st, EhgpError)(st, "ehgp_poll")
+        return state.value
+
+    def wait(self, rid: int, timeout_s: float = 600.0) -> int:
+        """Waits for a request; returns its status (0 = complete)."""
+        status = C.c_int32()
+        st = self.lib.ehgp_wait(self._h, rid, int(timeout_s * 1e9), C.byref(status))
+        if st != 0:
+            raise _ERRORS.get(st, EhgpError)(st, "ehgp_wait")
+        return status.value
+
+    def info(self, rid: int) -> dict:
+        s = RequestStats()
+        st = self.lib.ehgp_request_info(self._h, rid, C.byref(s))
+        if st != 0:
+            raise _ERRORS.get(st, EhgpError)(st, "ehgp_request_info")
+        out = {f: getattr(s, f) for f, _ in RequestStats._fields_ if f != "counts"}
+        out["counts"] = {f: getattr(s.counts, f) for f, _ in HierCounts._fields_}
+        out["error"] = self.lib.ehgp_request_error(self._h, rid).decode()
+        return out
+
+    def result(self, rid: int) -> dict:
+        """Host copy of a completed request's result arrays."""
+        inf = self.info(rid)
+        if inf["state"] != REQ_DONE:
+            raise _ERRORS.get(inf["status"], EhgpError)(inf["status"], inf["error"] or "request not complete")
+        c = inf["counts"]
+        n = int(inf["points"])
+        res = {"nodes": np.zeros(max(c["nodes"], 1), FOREST_NODE), "children": np.zeros(max(c["children"], 1), "<u4"),
+               "batches": np.zeros(max(c["journal_batches"], 1), FOREST_BATCH),
+               "roots": np.zeros(max(c["final_roots"], 1), FOREST_ROOT),
+               "vertical": np.zeros(max(c["vertical_assignments"], 1), VERTICAL_ASSIGNMENT),
+               "node_supports": np.zeros((max(c["nodes"], 1), 5), "<u4"),
+               "emst_u": np.zeros(max(n - 1, 1), "<u4"), "emst_v": np.zeros(max(n - 1, 1), "<u4")}
+        out = ServedOut(*[_ptr(res[k]) for k, _ in ServedOut._fields_])
+        st = self.lib.ehgp_result_copy(self._h, rid, C.byref(out))
+        if st != 0:
+            raise _ERRORS.get(st, EhgpError)(st, "ehgp_result_copy")
+        sizes = {"nodes": c["nodes"], "children": c["children"], "batches": c["journal_batches"],
+                 "roots": c["final_roots"], "vertical": c["vertical_assignments"], "node_supports": c["nodes"],
+                 "emst_u": n - 1, "emst_v": n - 1}
+        return {k: v[:sizes[k]] for k, v in res.items()}
+
+    def release(self, rid: int) -> None:
+        self.lib.ehgp_result_release(self._h, rid)
+
+    def stats(self) -> dict:
+        v = np.zeros(8, np.uint64)
+        self.lib.ehgp_server_info(self._h, _ptr(v), 8)
+        return dict(zip(("budget", "reserved", "held", "bytes_per_point", "queued", "running", "completed",
+                         "memory_waits"), (int(x) for x in v)))

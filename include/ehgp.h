@@ -452,6 +452,92 @@ int ehgp_hier_stats(const ehgp_ctx* ctx, double* ms, uint64_t* stats);
  * the circumsphere at the cloud scale; not reduced). */
 int ehgp_event_level(ehgp_ctx* ctx, uint64_t event, uint64_t* num, uint64_t* den, int32_t* scale);
 
+/* Supports of facade events of the last ehgp_hierarchy result, for `count`
+ * event indices (e.g. the level_event of forest nodes): out[5i] the support
+ * size, out[5i + 1..4] its PointIds (unused 0); UINT32_MAX (level 0) gives size
+ * 0.  A level is the squared circumradius of its support (the circumsphere of a
+ * triangle centred in its plane; half the segment for a pair), so the supports
+ * keep exact levels once the context moves on to another cloud.  Stands in for
+ * reading ExactDirectSupportEvent::support_ids through the facade
+ * (morsehgp3d/include/morsehgp3d/hierarchy/direct_support_terminal.hpp:59-74). */
+int ehgp_event_supports(ehgp_ctx* ctx, const uint32_t* events, uint64_t count, uint32_t* out);
+
+/* ---- serving: many clouds on one GPU, continuous batching -----------------
+ * The reference plans a request front end over its contexts
+ * (morsehgp3d/docs/GPU_G4_ARCHITECTURE.md:269-294: fit / result accessors; its
+ * memory plan at 80 % of the device, :117-136) and has no batching or serving
+ * code.  A server runs `workers` requests at a time, each on a context of its
+ * own (CUDA stream, device buffers, host thread); submitted clouds queue and are
+ * admitted in order as soon as a worker is idle and the device-memory
+ * reservations of the running requests, with this one, stay within
+ * hbm_fraction of the device's memory.  Every request runs the whole chain
+ * (canonical cloud + LBVH, EMST, pair and triple/quad supports, direct
+ * hierarchy with vertical maps) with its state on the device, and its result is
+ * copied to host memory the request owns when it completes; it equals the
+ * result of the same cloud run alone.  Calls are thread-safe. */
+typedef struct ehgp_server ehgp_server;
+typedef uint64_t ehgp_request_id;
+
+typedef struct ehgp_server_limits {
+  uint32_t workers;      /* requests on the device at a time (1..64)              */
+  uint64_t max_points;   /* largest cloud a request may hold                       */
+  double hbm_fraction;   /* admission ceiling as a fraction of device memory (0.8) */
+} ehgp_server_limits;
+
+enum { EHGP_DTYPE_F64 = 0, EHGP_DTYPE_F32 = 1 };
+typedef struct ehgp_cloud_desc {
+  const void* xyz;   /* host, n interleaved x,y,z values of `dtype`; copied at submit */
+  uint64_t n;
+  uint32_t dtype;    /* EHGP_DTYPE_F64 or EHGP_DTYPE_F32 (widened exactly)           */
+  uint32_t K;        /* K_max, 1..10                                                 */
+} ehgp_cloud_desc;
+
+enum { EHGP_REQ_QUEUED = 0, EHGP_REQ_RUNNING = 1, EHGP_REQ_DONE = 2, EHGP_REQ_FAILED = 3 };
+typedef struct ehgp_request_stats {
+  int32_t state, status;     /* EHGP_REQ_*; the chain's status once finished        */
+  uint64_t points;
+  uint32_t K, worker;
+  double queued_ms;          /* submit to admission                                  */
+  double service_ms;         /* admission to completion (result in host memory)      */
+  double latency_ms;         /* submit to completion                                 */
+  double device_ms;          /* device timeline of the chain on its stream           */
+  ehgp_hier_counts counts;   /* sizes of the result arrays                           */
+} ehgp_request_stats;
+
+/* Host copies of a completed request's result; sizes from ehgp_request_stats.counts
+ * (nodes, children, journal_batches, final_roots, vertical_assignments) and n - 1
+ * EMST edges; any pointer may be NULL.  node_supports holds 5 words per node:
+ * the support size and PointIds of the event at the node's level (size 0: level
+ * 0); level_event fields index the request's own facade. */
+typedef struct ehgp_served_out {
+  ehgp_forest_node* nodes;
+  uint32_t* children;
+  ehgp_forest_batch* batches;
+  ehgp_forest_root* roots;
+  ehgp_vertical_assignment* vertical;
+  uint32_t* node_supports;
+  uint32_t* emst_u;
+  uint32_t* emst_v;
+} ehgp_served_out;
+
+int ehgp_server_create(int device, const ehgp_server_limits* limits, ehgp_server** out);
+int ehgp_server_destroy(ehgp_server* server);
+/* Queues a cloud (asynchronous; the points are copied).  EHGP_ERR_CAPACITY above
+ * max_points; EHGP_ERR_OUT_OF_MEMORY when the cloud alone exceeds the budget. */
+int ehgp_cloud_submit(ehgp_server* server, const ehgp_cloud_desc* cloud, ehgp_request_id* id);
+int ehgp_poll(ehgp_server* server, ehgp_request_id id, int32_t* state);
+/* Waits until the request has finished or timeout_ns passed (EHGP_ERR_TIMEOUT). */
+int ehgp_wait(ehgp_server* server, ehgp_request_id id, uint64_t timeout_ns, int32_t* status);
+int ehgp_request_info(ehgp_server* server, ehgp_request_id id, ehgp_request_stats* info);
+const char* ehgp_request_error(ehgp_server* server, ehgp_request_id id);
+int ehgp_result_copy(ehgp_server* server, ehgp_request_id id, const ehgp_served_out* out);
+/* Drops a finished request and its result. */
+int ehgp_result_release(ehgp_server* server, ehgp_request_id id);
+/* [0] memory budget, [1] bytes reserved by running requests, [2] device bytes held
+ * by the workers' contexts, [3] admission estimate in bytes per point, [4] queued,
+ * [5] running, [6] completed requests, [7] admissions deferred for memory. */
+int ehgp_server_info(ehgp_server* server, uint64_t* info, uint32_t count);
+
 #ifdef __cplusplus
 }
 #endif
