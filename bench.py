@@ -15,11 +15,12 @@ value : p95 over the K timed steps of the step time on the device timeline
         (CUDA events on the library's stream around the whole step; inputs
         already resident in HBM; the host-side forest sweep is inside).
 e2e   : p95 over K steps of the same step through the public C ABI with host
-        buffers: pinned host input copied in, and the results (EMST edges and
-        exact lengths, k=1 forest arenas, pair- and higher-support records,
-        the hgp_reduced forest nodes, child arena, forest batches and final
-        roots of every order, and the vertical maps between adjacent orders)
-        copied back to host memory; wall clock.
+        buffers (the reference's warm_e2e protocol): pinned host input copied
+        in, and the hgp_reduced payload copied back to pinned host memory:
+        EMST edges and exact lengths, k=1 forest arenas, the forest nodes (with
+        the support of each node's level, which gives its exact level), child
+        arena, forest batches and final roots of every order, and the vertical
+        maps between adjacent orders; wall clock.
 L2 is flushed (a 512 MiB write) before every timed step.
 
 Multi-GPU: replicas only (one independent cloud per rank, different seeds),
@@ -400,13 +401,6 @@ def run_ours(args, world, rank, local):
     e_D = pinned_np(m * 4, np.uint64).reshape(m, 4)
     rounds = np.zeros(1, np.uint32)
     eout = ehgp.EmstOut(e_u.ctypes.data, e_v.ctypes.data, e_D.ctypes.data, rounds.ctypes.data, None, 0, None)
-    pair_cap = int(cnt[0]) + 1024
-    recs = pinned_np(pair_cap, ehgp.PAIR_RECORD)
-    plv = pinned_np(pair_cap * 4, np.uint64).reshape(pair_cap, 4)
-    pout = ehgp.PairsOut(recs.ctypes.data, plv.ctypes.data, pair_cap, cnt.ctypes.data)
-    higher_cap = int(hcnt[0]) + 1024
-    hrecs = pinned_np(higher_cap, ehgp.HIGHER_RECORD)
-    hout = ehgp.HigherOut(hrecs.ctypes.data, higher_cap, hcnt.ctypes.data)
     slack = 1.05
     f_nodes = pinned_np(int(counts["nodes"] * slack) + 64, ehgp.FOREST_NODE)
     f_child = pinned_np(int(counts["children"] * slack) + 64, np.uint32)
@@ -416,18 +410,25 @@ def run_ours(args, world, rank, local):
     hier_out = ehgp.HierOut(None, None, None, None, None, f_nodes.ctypes.data, f_child.ctypes.data, None, None,
                             None, None, f_batch.ctypes.data, f_root.ctypes.data, f_vert.ctypes.data)
 
+    f_sup = pinned_np(5 * (int(counts["nodes"] * slack) + 64), np.uint32)
+
     def e2e_step():
+        """The warm_e2e protocol: host points in; the hgp_reduced payload out into pinned host
+        memory: the forests of orders 1..10 (nodes, child arena, batches, final roots) with the
+        exact level of every node (the support of its level event), the vertical maps, and the
+        EMST edges with their exact squared lengths and the compact k = 1 forest arenas.  The
+        support records stay on the device (they are inputs of the hierarchy, not its payload)."""
         t0 = time.perf_counter()
         ctx.lbvh_build(host_pts, outputs=False)
         ctx._check(lib.ehgp_emst(ctx._h, C.byref(eout)))
         ctx._check(lib.ehgp_k1_forest(ctx._h, C.byref(fout)))
-        ctx._check(lib.ehgp_pairs(ctx._h, K_MAX, C.byref(pout)))
-        ctx._check(lib.ehgp_higher(ctx._h, K_MAX, C.byref(hout)))
         ctx._check(lib.ehgp_hierarchy(ctx._h, K_MAX, C.byref(hc)))
         if (hc.nodes > len(f_nodes) or hc.children > len(f_child) or hc.journal_batches > len(f_batch)
                 or hc.final_roots > len(f_root) or hc.vertical_assignments > len(f_vert)):
             raise RuntimeError("the hierarchy payload outgrew its host buffers")
         ctx._check(lib.ehgp_hier_copy(ctx._h, C.byref(hier_out)))
+        lev = np.ascontiguousarray(f_nodes["level_event"][:hc.nodes])
+        ctx._check(lib.ehgp_event_supports(ctx._h, lev.ctypes.data, hc.nodes, f_sup.ctypes.data))
         return 1e3 * (time.perf_counter() - t0)
 
     for _ in range(max(args.warmup, 3)):
@@ -494,8 +495,8 @@ def run_ours(args, world, rank, local):
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved = alg_bytes / (kmean * 1e-3) / 1e9
-    d2h = (e_u.nbytes + e_v.nbytes + e_D.nbytes + sum(forest[k].nbytes for k in forest) + int(cnt[0]) * (64 + 32)
-           + int(hcnt[0]) * 64 + int(hc.nodes) * f_nodes.itemsize + int(hc.children) * 4
+    d2h = (e_u.nbytes + e_v.nbytes + e_D.nbytes + sum(forest[k].nbytes for k in forest)
+           + int(hc.nodes) * (f_nodes.itemsize + 20) + int(hc.children) * 4
            + int(hc.journal_batches) * f_batch.itemsize + int(hc.final_roots) * f_root.itemsize
            + int(hc.vertical_assignments) * f_vert.itemsize)
     line = {
