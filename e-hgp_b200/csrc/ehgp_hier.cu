@@ -374,8 +374,79 @@ __global__ void k_iota(uint32_t m, uint32_t* __restrict__ out) {
   if (i < m) out[i] = i;
 }
 
-// Gathers the facade records of the uncertain runs (host tie resolution) and scatters
-// them back with their exact-equality flags.
+// ---- exact order inside the runs that the FP64 level intervals leave open ----------
+// A run is a maximal range [lo, hi] of facade positions whose intervals overlap.  Each member
+// gets its exact level key once (|N|^2 and A^2 of its circumsphere, 2304-bit integers; the
+// level is |N|^2 / (4 A^2)), then one thread per run merge-sorts the run's positions by
+// (exact level, closed rank, interior ids, support ids) and writes the records back in that
+// order with their equal-level flags.
+__global__ void k_tie_keys(uint32_t cnt, const uint32_t* __restrict__ pos, const EvRec* __restrict__ ev, Cloud c,
+                           WL* __restrict__ knum, WL* __restrict__ ka2) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= cnt) return;
+  const EvRec r = ev[pos[i]];
+  W A;
+  WV N;
+  exact_sphere(c, r.ids, (int)r.size, A, N);
+  const WL x = widen<36>(N.x), y = widen<36>(N.y), z = widen<36>(N.z), a = widen<36>(A);
+  knum[i] = wadd(wadd(wmul(x, x), wmul(y, y)), wmul(z, z));
+  ka2[i] = wmul(a, a);
+}
+
+__device__ int tie_level_cmp(const WL* knum, const WL* ka2, uint32_t i, uint32_t j) {
+  return wcmp(wmul(knum[i], ka2[j]), wmul(knum[j], ka2[i]));
+}
+
+__device__ bool tie_less(const WL* knum, const WL* ka2, const EvRec* rec, uint32_t i, uint32_t j) {
+  const int s = tie_level_cmp(knum, ka2, i, j);
+  if (s != 0) return s < 0;
+  const EvRec& a = rec[i];
+  const EvRec& b = rec[j];
+  if (a.rank != b.rank) return a.rank < b.rank;
+  const uint32_t m = min(a.nint, b.nint);
+  for (uint32_t t = 0; t < m; ++t)
+    if (a.iids[t] != b.iids[t]) return a.iids[t] < b.iids[t];
+  if (a.nint != b.nint) return a.nint < b.nint;
+  const uint32_t ms = min(a.size, b.size);
+  for (uint32_t t = 0; t < ms; ++t)
+    if (a.ids[t] != b.ids[t]) return a.ids[t] < b.ids[t];
+  return a.size < b.size;
+}
+
+// rec[i]: copy of the member's record (members of run r are run_off[r] .. run_off[r + 1] - 1,
+// at facade positions run_lo[r] ...); idx / tmp: scratch of the member count.
+__global__ void k_tie_sort(uint32_t nruns, const uint32_t* __restrict__ run_off, const uint32_t* __restrict__ run_lo,
+                           const WL* __restrict__ knum, const WL* __restrict__ ka2, const EvRec* __restrict__ rec,
+                           uint32_t* __restrict__ idx, uint32_t* __restrict__ tmp, EvRec* __restrict__ ev,
+                           uint8_t* __restrict__ eqprev) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nruns) return;
+  const uint32_t b = run_off[r], L = run_off[r + 1] - b;
+  for (uint32_t t = 0; t < L; ++t) idx[b + t] = b + t;
+  // bottom-up merge sort (stable) of the member indices
+  uint32_t* src = idx + b;
+  uint32_t* dst = tmp + b;
+  for (uint32_t w = 1; w < L; w <<= 1) {
+    for (uint32_t lo = 0; lo < L; lo += 2 * w) {
+      const uint32_t mid = min(lo + w, L), hi = min(lo + 2 * w, L);
+      uint32_t i = lo, j = mid, o = lo;
+      while (i < mid && j < hi) dst[o++] = tie_less(knum, ka2, rec, src[j], src[i]) ? src[j++] : src[i++];
+      while (i < mid) dst[o++] = src[i++];
+      while (j < hi) dst[o++] = src[j++];
+    }
+    uint32_t* t = src;
+    src = dst;
+    dst = t;
+  }
+  const uint32_t p0 = run_lo[r];
+  for (uint32_t t = 0; t < L; ++t) {
+    ev[p0 + t] = rec[src[t]];
+    if (t > 0) eqprev[p0 + t] = tie_level_cmp(knum, ka2, src[t - 1], src[t]) == 0 ? 1 : 0;
+  }
+}
+
+// Gathers the facade records of the uncertain runs and scatters them back with their
+// exact-equality flags (kept for the member copies of the tie sort).
 __global__ void k_run_gather(uint32_t cnt, const uint32_t* __restrict__ idx, const EvRec* __restrict__ ev,
                              EvRec* __restrict__ out) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1216,7 +1287,15 @@ struct HierState {
   uint32_t* d_size_rp = nullptr;
   uint32_t* d_armoff = nullptr;
   uint32_t* d_removed = nullptr;
-  std::vector<double> h_px, h_py, h_pz;
+  // exact order of the facade's tie runs on the device (capacities kept across calls)
+  WL* tie_num = nullptr;   // [tie_cap] |N|^2 of each run member
+  WL* tie_a2 = nullptr;    // [tie_cap] A^2
+  uint32_t* tie_idx = nullptr;
+  uint32_t* tie_tmp = nullptr;
+  uint32_t* tie_pos = nullptr;
+  uint32_t* run_off = nullptr;
+  uint32_t* run_lo = nullptr;
+  uint64_t tie_cap = 0, run_cap = 0;
   // The result stays in the per-order arenas (local indices); off[k] holds the global
   // offsets of order k's records, off[keff + 1] the totals.  Records take their global
   // indices when they are copied out.  An empty `off` means no result.
@@ -1246,6 +1325,10 @@ void hier_free(Ctx& ctx) {
                   (void*)ctx.hier->p_term, (void*)ctx.hier->p_stat})
     if (p) cudaFreeHost(p);
   if (ctx.hier->ev_block) cudaEventDestroy(ctx.hier->ev_block);
+  for (void* q : {(void*)ctx.hier->tie_num, (void*)ctx.hier->tie_a2, (void*)ctx.hier->tie_idx,
+                  (void*)ctx.hier->tie_tmp, (void*)ctx.hier->tie_pos, (void*)ctx.hier->run_off,
+                  (void*)ctx.hier->run_lo})
+    if (q) cudaFree(q);
   for (cudaEvent_t ev : ctx.hier->ev_step)
     if (ev) cudaEventDestroy(ev);
   delete ctx.hier;
@@ -1320,24 +1403,6 @@ cudaError_t ensure_events(HierState& h, uint64_t m) {
   return cudaSuccess;
 }
 
-// Exact facade order of events within an uncertain run: (level, rank, interior, support).
-struct HostCmp {
-  const Cloud* c;
-  bool less(const EvRec& a, const EvRec& b, int* lev) const {
-    const int s = level_cmp_exact(*c, a.ids, (int)a.size, b.ids, (int)b.size);
-    if (lev) *lev = s;
-    if (s != 0) return s < 0;
-    if (a.rank != b.rank) return a.rank < b.rank;
-    const uint32_t m = std::min(a.nint, b.nint);
-    for (uint32_t i = 0; i < m; ++i)
-      if (a.iids[i] != b.iids[i]) return a.iids[i] < b.iids[i];
-    if (a.nint != b.nint) return a.nint < b.nint;
-    const uint32_t ms = std::min(a.size, b.size);
-    for (uint32_t i = 0; i < ms; ++i)
-      if (a.ids[i] != b.ids[i]) return a.ids[i] < b.ids[i];
-    return a.size < b.size;
-  }
-};
 
 void scan_minmax(cudaStream_t st, uint32_t m, const double* mid, const double* err, double* out, double* bsum,
                  bool forward_max, uint64_t* launches) {
@@ -1418,13 +1483,6 @@ int hier_run(Ctx& ctx, uint32_t K) {
                                                  h.lmid_raw, h.lerr_raw, h.ev, h.lmid, h.lerr, h.perm);
     ++launches;
   }
-  // copy the cloud for host-side exact tie resolution
-  h.h_px.resize(n);
-  h.h_py.resize(n);
-  h.h_pz.resize(n);
-  cudaMemcpyAsync(h.h_px.data(), b.px, n * sizeof(double), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(h.h_py.data(), b.py, n * sizeof(double), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(h.h_pz.data(), b.pz, n * sizeof(double), cudaMemcpyDeviceToHost, st);
   int scale_h[4];
   cudaMemcpyAsync(scale_h, g.scale, sizeof(scale_h), cudaMemcpyDeviceToHost, st);
   cudaMemsetAsync(h.eqprev, 0, m + 1, st);
@@ -1447,55 +1505,49 @@ int hier_run(Ctx& ctx, uint32_t K) {
     std::sort(list.begin(), list.end());
     // maximal runs of positions whose order the FP64 intervals leave open: a run starts one
     // before its first uncertain boundary (that boundary before it is certain)
-    struct Run {
-      uint32_t off, len;
-    };
-    std::vector<Run> runs;
-    std::vector<uint32_t> idx;
+    std::vector<uint32_t> run_off, run_lo, idx;
     for (size_t i = 0; i < list.size();) {
       const uint32_t s0 = list[i] - 1;
       uint32_t s1 = list[i];
       size_t j = i + 1;
       while (j < list.size() && list[j] == s1 + 1) s1 = list[j++];
-      runs.push_back({(uint32_t)idx.size(), s1 - s0 + 1});
+      run_off.push_back((uint32_t)idx.size());
+      run_lo.push_back(s0);
       for (uint32_t t = s0; t <= s1; ++t) idx.push_back(t);
       i = j;
     }
-    // one gather, exact sorts of the runs on the host cores, one scatter (scratch: order0,
-    // order1 and ev_raw are free between the facade gather and the level classes)
-    const uint32_t cnt = (uint32_t)idx.size();
-    std::vector<EvRec> recs(cnt);
-    std::vector<uint8_t> eq(cnt, 0);
-    cudaMemcpyAsync(h.order1, idx.data(), (uint64_t)cnt * 4, cudaMemcpyHostToDevice, st);
-    k_run_gather<<<nblk(cnt, kT), kT, 0, st>>>(cnt, h.order1, h.ev, h.ev_raw);
-    cudaMemcpyAsync(recs.data(), h.ev_raw, (uint64_t)cnt * sizeof(EvRec), cudaMemcpyDeviceToHost, st);
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "facade tie runs");
-    const Cloud hc_cloud{h.h_px.data(), h.h_py.data(), h.h_pz.data(), h.S};
-    const HostCmp cmp{&hc_cloud};
-    std::atomic<size_t> next{0};
-    auto sort_runs = [&] {
-      for (size_t r; (r = next.fetch_add(1)) < runs.size();) {
-        EvRec* run = recs.data() + runs[r].off;
-        const uint32_t len = runs[r].len;
-        std::sort(run, run + len, [&](const EvRec& x, const EvRec& y) { return cmp.less(x, y, nullptr); });
-        for (uint32_t t = 1; t < len; ++t)
-          eq[runs[r].off + t] =
-              level_cmp_exact(hc_cloud, run[t - 1].ids, (int)run[t - 1].size, run[t].ids, (int)run[t].size) == 0;
+    run_off.push_back((uint32_t)idx.size());
+    const uint32_t cnt = (uint32_t)idx.size(), nruns = (uint32_t)run_lo.size();
+    // settled on the device: exact level keys per member, then a merge sort per run
+    if (h.tie_cap < cnt || h.run_cap < nruns + 1) {
+      for (void* q : {(void*)h.tie_num, (void*)h.tie_a2, (void*)h.tie_idx, (void*)h.tie_tmp, (void*)h.tie_pos,
+                      (void*)h.run_off, (void*)h.run_lo})
+        if (q) cudaFree(q);
+      h.tie_num = h.tie_a2 = nullptr;
+      h.tie_idx = h.tie_tmp = h.tie_pos = h.run_off = h.run_lo = nullptr;
+      h.tie_cap = h.run_cap = 0;
+      const uint64_t tc = cnt + cnt / 4 + 64, rc = nruns + nruns / 4 + 64;
+      if (cudaMalloc(&h.tie_num, tc * sizeof(WL)) != cudaSuccess || cudaMalloc(&h.tie_a2, tc * sizeof(WL)) != cudaSuccess ||
+          cudaMalloc(&h.tie_idx, tc * 4) != cudaSuccess || cudaMalloc(&h.tie_tmp, tc * 4) != cudaSuccess ||
+          cudaMalloc(&h.tie_pos, tc * 4) != cudaSuccess || cudaMalloc(&h.run_off, rc * 4) != cudaSuccess ||
+          cudaMalloc(&h.run_lo, rc * 4) != cudaSuccess) {
+        cudaGetLastError();
+        return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "the facade tie runs do not fit the device");
       }
-    };
-    {
-      const uint32_t hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-      const uint32_t nt = (uint32_t)std::min<size_t>(hw, runs.size());
-      std::vector<std::thread> pool;
-      for (uint32_t i = 1; i < nt; ++i) pool.emplace_back(sort_runs);
-      sort_runs();
-      for (auto& t : pool) t.join();
+      h.tie_cap = tc;
+      h.run_cap = rc;
     }
-    uint8_t* d_eq = reinterpret_cast<uint8_t*>(h.order0);
-    cudaMemcpyAsync(h.ev_raw, recs.data(), (uint64_t)cnt * sizeof(EvRec), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(d_eq, eq.data(), cnt, cudaMemcpyHostToDevice, st);
-    k_run_scatter<<<nblk(cnt, kT), kT, 0, st>>>(cnt, h.order1, h.ev_raw, d_eq, h.ev, h.eqprev);
-    launches += 2;
+    // members' records are copied (ev_raw is free between the facade gather and the level
+    // classes) so that the sort writes the facade in place
+    cudaMemcpyAsync(h.tie_pos, idx.data(), (uint64_t)cnt * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(h.run_off, run_off.data(), (uint64_t)(nruns + 1) * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(h.run_lo, run_lo.data(), (uint64_t)nruns * 4, cudaMemcpyHostToDevice, st);
+    k_run_gather<<<nblk(cnt, kT), kT, 0, st>>>(cnt, h.tie_pos, h.ev, h.ev_raw);
+    const Cloud dc{b.px, b.py, b.pz, h.S};
+    k_tie_keys<<<nblk(cnt, 128), 128, 0, st>>>(cnt, h.tie_pos, h.ev, dc, h.tie_num, h.tie_a2);
+    k_tie_sort<<<nblk(nruns, 64), 64, 0, st>>>(nruns, h.run_off, h.run_lo, h.tie_num, h.tie_a2, h.ev_raw, h.tie_idx,
+                                               h.tie_tmp, h.ev, h.eqprev);
+    launches += 3;
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "facade tie runs");
     ms_ties = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tt0).count();
   }
@@ -2769,12 +2821,23 @@ int ehgp_event_level(ehgp_ctx* ctx, uint64_t event, uint64_t* num, uint64_t* den
     return ehgp::abi_fail(ctx, EHGP_ERR_INVALID_ARGUMENT, "no such facade event");
   const ehgp::HierState& h = *ctx->hier;
   ehgp::EvRec r;
-  const cudaError_t ce = cudaMemcpy(&r, h.ev + event, sizeof r, cudaMemcpyDeviceToHost);
+  cudaError_t ce = cudaMemcpy(&r, h.ev + event, sizeof r, cudaMemcpyDeviceToHost);
   if (ce != cudaSuccess) return ehgp::abi_cuda_fail(ctx, ce, "facade event copy");
-  const ehgp::Cloud c{h.h_px.data(), h.h_py.data(), h.h_pz.data(), h.S};
+  if (r.size < 2 || r.size > 4) return ehgp::abi_fail(ctx, EHGP_ERR_INVALID_ARGUMENT, "no such facade event");
+  // the support's coordinates only (the cloud stays on the device)
+  double sx[4], sy[4], sz[4];
+  uint32_t local[4];
+  for (uint32_t j = 0; j < r.size; ++j) {
+    if ((ce = cudaMemcpy(sx + j, ctx->lb.px + r.ids[j], 8, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (ce = cudaMemcpy(sy + j, ctx->lb.py + r.ids[j], 8, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (ce = cudaMemcpy(sz + j, ctx->lb.pz + r.ids[j], 8, cudaMemcpyDeviceToHost)) != cudaSuccess)
+      return ehgp::abi_cuda_fail(ctx, ce, "support coordinates");
+    local[j] = j;
+  }
+  const ehgp::Cloud c{sx, sy, sz, h.S};
   ehgp::W A;
   ehgp::WV N;
-  ehgp::exact_sphere(c, r.ids, (int)r.size, A, N);
+  ehgp::exact_sphere(c, local, (int)r.size, A, N);
   using WL = ehgp::WL;
   const WL x = ehgp::widen<36>(N.x), y = ehgp::widen<36>(N.y), z = ehgp::widen<36>(N.z), a = ehgp::widen<36>(A);
   const WL nn = ehgp::wadd(ehgp::wadd(ehgp::wmul(x, x), ehgp::wmul(y, y)), ehgp::wmul(z, z));

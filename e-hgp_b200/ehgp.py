@@ -308,6 +308,7 @@ class Context:
         if st != 0:
             raise _ERRORS.get(st, EhgpError)(st, "context creation failed")
         self.max_points = max_points
+        self.device = device
 
     def close(self) -> None:
         if self._h:
@@ -393,6 +394,48 @@ class Context:
             pts = pts.astype(np.float64, copy=False)
             st = self.lib.ehgp_lbvh_build(self._h, _ptr(pts), n, C.byref(out))
         self._check(st)
+        self.n = n
+        if snap is not None:
+            snap.root = int(root[0])
+        return snap
+
+    def lbvh_build_dlpack(self, points, outputs: bool = False) -> LbvhSnapshot | None:
+        """Zero-copy device input (ehgp_lbvh_build_device): `points` is a DLPack producer or a
+        __cuda_array_interface__ object (a torch or CuPy CUDA array) of shape (n, 3) on this
+        context's device.  binary64 points are read in place; binary32 points are widened
+        exactly on the device first (one temporary).  Work pending on torch's current stream
+        (the producer's) is waited for before the library's stream reads the points."""
+        import torch
+        if isinstance(points, torch.Tensor):
+            t = points
+        elif hasattr(points, "__dlpack__") or type(points).__name__ == "PyCapsule":
+            t = torch.from_dlpack(points)  # a producer, or a raw DLPack capsule
+        elif hasattr(points, "__cuda_array_interface__"):
+            t = torch.as_tensor(points, device=f"cuda:{self.device}")
+        else:
+            raise InvalidArgument(1, "points must be a CUDA array (DLPack or __cuda_array_interface__)")
+        if not t.is_cuda or t.device.index != self.device:
+            raise InvalidArgument(1, f"points must be on cuda:{self.device}")
+        if t.ndim != 2 or t.shape[1] != 3:
+            raise InvalidArgument(1, "points must have shape (n, 3)")
+        if t.dtype == torch.float32:
+            t = t.to(torch.float64)
+        elif t.dtype != torch.float64:
+            raise InvalidArgument(1, "points must be binary32 or binary64")
+        t = t.contiguous()
+        torch.cuda.current_stream(t.device).synchronize()
+        n = int(t.shape[0])
+        if outputs:
+            snap = LbvhSnapshot(
+                np.empty(n, np.uint64), np.empty((n, 2), np.uint64),
+                np.empty((max(2 * n - 1, 0), 10), np.uint64), np.empty(5, np.uint64),
+                np.empty(6, np.uint64), 0)
+            root = np.zeros(1, np.uint64)
+            out = LbvhOut(_ptr(snap.source_index), _ptr(snap.leaves), _ptr(snap.nodes),
+                          _ptr(snap.counters), _ptr(snap.root_aabb), _ptr(root))
+        else:
+            snap, out = None, LbvhOut(None, None, None, None, None, None)
+        self._check(self.lib.ehgp_lbvh_build_device(self._h, C.c_void_p(t.data_ptr()), n, C.byref(out)))
         self.n = n
         if snap is not None:
             snap.root = int(root[0])
@@ -658,3 +701,103 @@ class Server:
         self.lib.ehgp_server_info(self._h, _ptr(v), 8)
         return dict(zip(("budget", "reserved", "held", "bytes_per_point", "queued", "running", "completed",
                          "memory_waits"), (int(x) for x in v)))
+
+
+def _is_device_array(points) -> bool:
+    if isinstance(points, np.ndarray):
+        return False
+    try:
+        import torch
+        if isinstance(points, torch.Tensor):
+            return points.is_cuda
+    except ImportError:
+        pass
+    return (hasattr(points, "__cuda_array_interface__") or hasattr(points, "__dlpack__")
+            or type(points).__name__ == "PyCapsule")
+
+
+def fit(points, K: int = 10, device: int = 0) -> dict:
+    """One call from points to the hgp_reduced hierarchy, mirroring the front end the
+    reference plans (morsehgp3d/docs/GPU_G4_ARCHITECTURE.md:269-294, `fit`): a host array, or a
+    CUDA array by DLPack / __cuda_array_interface__ (read in place).  Returns the EMST edges, the
+    forest nodes of orders 1..K with the supports of their levels, the child arena, forest
+    batches, final roots, vertical maps, the hierarchy counts and the canonical points (PointId
+    order, binary64) that the supports index."""
+    if _is_device_array(points):
+        import torch
+        t = points if isinstance(points, torch.Tensor) else torch.from_dlpack(points)
+        n = int(t.shape[0])
+    else:
+        points = np.ascontiguousarray(points)
+        n = int(points.shape[0])
+    with Context(max_points=max(n, 1), device=device) as ctx:
+        snap = ctx.lbvh_build_dlpack(points, outputs=True) if _is_device_array(points) else ctx.lbvh_build(points)
+        res = ctx.served_result(K)
+        res["counts"] = dict(ctx.last_hier_counts)
+        if _is_device_array(points):
+            import torch
+            t = points if isinstance(points, torch.Tensor) else torch.from_dlpack(points)
+            host = t.detach().to("cpu", torch.float64).numpy()
+        else:
+            host = np.asarray(points, dtype=np.float64)
+        res["points"] = host[snap.source_index.astype(np.int64)]
+        res["K"] = K
+        return HierarchyResult(res)
+
+
+class HierarchyResult(dict):
+    """Result of `fit` (a dict of arrays) with on-demand cuts."""
+
+    def node_levels(self, order: int):
+        """Exact squared levels (Fractions) of the nodes of one order, by node index."""
+        from fractions import Fraction
+        P = self["points"]
+        nodes = self["nodes"]
+        sup = self["node_supports"]
+        out = {}
+        for i in np.nonzero(nodes["order"] == order)[0]:
+            m = int(sup[i, 0])
+            if m == 0:
+                out[int(i)] = Fraction(0)
+                continue
+            pts = [[Fraction(float(x)) for x in P[int(j)]] for j in sup[i, 1:1 + m]]
+            out[int(i)] = _circumradius2(pts)
+        return out
+
+    def cut(self, order: int, level, closed: bool = True) -> list[int]:
+        """Components of the order-`order` merge forest at squared level `level` (a number
+        or Fraction): the nodes born at or below the level (strictly below when closed is
+        False) whose parent, if any, is born above it; sorted node indices.  The cut of the
+        reference's filtration (reference/morsehgp3d_oracle/gamma.py:213, GammaFiltration.cut;
+        planned as result.cut(k, a), docs/GPU_G4_ARCHITECTURE.md:288-289), on the reduced forest."""
+        from fractions import Fraction
+        a = Fraction(level)
+        lev = self.node_levels(order)
+        nodes, ch = self["nodes"], self["children"]
+        parent = {}
+        for i in lev:
+            if nodes["kind"][i] == 2:
+                for c in ch[nodes["child_offset"][i]:nodes["child_offset"][i] + nodes["child_count"][i]]:
+                    parent[int(c)] = i
+        inside = (lambda x: x <= a) if closed else (lambda x: x < a)
+        return sorted(i for i, x in lev.items() if inside(x) and (i not in parent or not inside(lev[parent[i]])))
+
+
+def _circumradius2(pts):
+    """Exact squared circumradius of 2-4 points (Fractions); a triangle's circle is centred in
+    its plane."""
+    a = pts[0]
+    e = [[p[k] - a[k] for k in range(3)] for p in pts[1:]]
+    dot = lambda u, v: sum(x * y for x, y in zip(u, v))
+    if len(pts) == 2:
+        return dot(e[0], e[0]) / 4
+    cross = lambda u, v: [u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]]
+    if len(pts) == 3:
+        G11, G12, G22 = dot(e[0], e[0]), dot(e[0], e[1]), dot(e[1], e[1])
+        A = G11 * G22 - G12 * G12
+        N = [G22 * (G11 - G12) * e[0][k] + G11 * (G22 - G12) * e[1][k] for k in range(3)]
+    else:
+        c23, c31, c12 = cross(e[1], e[2]), cross(e[2], e[0]), cross(e[0], e[1])
+        A = dot(e[0], c23)
+        N = [dot(e[0], e[0]) * c23[k] + dot(e[1], e[1]) * c31[k] + dot(e[2], e[2]) * c12[k] for k in range(3)]
+    return dot(N, N) / (4 * A * A)

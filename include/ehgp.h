@@ -431,13 +431,13 @@ int ehgp_hier_schedule(ehgp_ctx* ctx, uint32_t chunk_batches, uint32_t part_arms
 
 /* Timing of the last ehgp_hierarchy call: ms[0] device stages (CUDA events),
  * ms[1] the strict-arm descent kernels, ms[2] the host forest pass, ms[3] its
- * slowest order (orders run on parallel host threads), ms[4] the host's exact
- * ordering of uncertain facade boundaries, ms[5..7] the host forest pass split
+ * slowest order (orders run on parallel host threads), ms[4] the exact
+ * ordering of the facade runs that FP64 level intervals leave open (on the device), ms[5..7] the host forest pass split
  * into the order passes, the record offsets and the vertical maps,
  * ms[8 + k - 1] the union-find core of order k (k <= 16,
  * zero above the last order);
  * stats[0] strict arms, [1] descent steps, [2] facade boundaries settled
- * exactly on the host, [3] facade events, [4] arms that are not themselves a
+ * exactly (2304-bit level comparisons on the device), [3] facade events, [4] arms that are not themselves a
  * birth facet, [5] descent rounds (longest chain), [6..12] slow-path counts of
  * the descent (exhaustive miniball enumerations, exact hull signs, exact
  * closed-ball sides, exact level conversions, exact band orders, exact cutoff
