@@ -1420,6 +1420,79 @@ k_higher_large(uint32_t nown, const uint32_t* __restrict__ owners, const uint64_
   }
 }
 
+// ---- single predicate evaluations (the product kernels' own filters and exact paths) ------
+// For the reference's predicate fixtures: one device thread evaluates one predicate on
+// PointIds of the resident cloud with the helpers the enumeration uses (FP64 with the
+// uniform error bounds, then the fixed-width exact integers).  out[0] the result, out[1] 1 when
+// an FP64 filter decided it (0 when the exact path did).
+__device__ uint32_t g_pred_ids[16];
+__device__ int32_t g_pred_out[2];
+
+__global__ void k_predicate(uint32_t pred, uint32_t count, const double* __restrict__ px,
+                            const double* __restrict__ py, const double* __restrict__ pz,
+                            const int* __restrict__ cloud_scale) {
+  const Cloud c{px, py, pz, cloud_scale[0]};
+  uint32_t ids[16];
+  for (uint32_t i = 0; i < count && i < 16; ++i) ids[i] = g_pred_ids[i];
+  int32_t res = 0, fp = 0;
+  auto setpt = [&](uint32_t p, uint32_t a) {
+    SetPt s;
+    s.x = px[p] - px[a];
+    s.y = py[p] - py[a];
+    s.z = pz[p] - pz[a];
+    s.q = (s.x * s.x + s.y * s.y) + s.z * s.z;
+    return s;
+  };
+  auto status = [&](const uint32_t* sup, int size, QEntry& E, double& eA, double& eN) -> int {
+    if (size == 1) return 0;
+    if (size == 2) return sup[0] == sup[1] ? 3 : 0;
+    const SetPt e1 = setpt(sup[1], sup[0]), e2 = setpt(sup[2], sup[0]);
+    double Mp = fmax(ptmax(e1), ptmax(e2));
+    E.ids[0] = sup[0];
+    E.ids[1] = sup[1];
+    E.ids[2] = sup[2];
+    E.ids[3] = size == 4 ? sup[3] : kInvalid32;
+    if (size == 3) {
+      bool adm;
+      return tri_eval(c, e1, e2, sup[0], sup[1], sup[2], Mp * (1.0 + 1e-15), INFINITY, E, eA, eN, adm);
+    }
+    const SetPt e3 = setpt(sup[3], sup[0]);
+    Mp = fmax(Mp, ptmax(e3));
+    return quad_eval(c, e1, e2, e3, sup[0], sup[1], sup[2], sup[3], Mp * (1.0 + 1e-15), E, eA, eN);
+  };
+  if (pred == 1) {  // side of the last id against the support sphere of the others
+    const int size = (int)count - 1;
+    const uint32_t w = ids[size];
+    QEntry E;
+    double eA = 0, eN = 0;
+    const int st = size >= 3 ? status(ids, size, E, eA, eN) : -1;
+    if (st == 0) {  // a minimal support: the enumeration's classification
+      const SetPt p = setpt(w, ids[0]);
+      const double v = E.A * p.q - ((p.x * E.Nx + p.y * E.Ny) + p.z * E.Nz);
+      int sd = fsign(v, E.bnd);
+      fp = sd != 2;
+      if (sd == 2) sd = side_exact(c, ids, size, w);
+      res = sd * E.sgn;
+    } else {  // any other support sphere: exact (orientation of A from its exact sign)
+      W A;
+      WV N;
+      exact_sphere(c, ids, size, A, N);
+      res = A.sign() == 0 ? 2 : side_exact(c, ids, size, w) * (A.sign() < 0 ? -1 : 1);  // 2: no sphere
+    }
+  } else if (pred == 2) {  // status of a 1- to 4-point support: 0 minimal, 1 boundary, 2 exterior, 3 dependent
+    QEntry E;
+    double eA = 0, eN = 0;
+    res = status(ids, (int)count, E, eA, eN);
+  } else if (pred == 3) {  // sign of level(left) - level(right); ids: left size, left ids, right ids
+    const int s1 = (int)ids[0];
+    res = level_cmp_exact(c, ids + 1, s1, ids + 1 + s1, (int)count - 1 - s1);
+  } else if (pred == 4) {  // sign of |ids[1] - ids[0]|^2 - |ids[2] - ids[0]|^2
+    res = dist_cmp_exact(c, ids, 1, ids[1], ids[2]);
+  }
+  g_pred_out[0] = res;
+  g_pred_out[1] = fp;
+}
+
 __global__ void k_higher_keys(uint32_t m, const HigherRec* __restrict__ recs, uint64_t* __restrict__ khi,
                               uint64_t* __restrict__ klo, uint32_t* __restrict__ order) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2014,6 +2087,35 @@ int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
 }  // namespace ehgp
 
 extern "C" {
+
+int ehgp_predicate_eval(ehgp_ctx* ctx, uint32_t predicate, const uint32_t* ids, uint32_t count, int32_t* out) {
+  if (!ctx || !ids || !out || predicate < 1 || predicate > 4 || count == 0 || count > 16)
+    return EHGP_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  ctx->last_error.clear();
+  if (ctx->poisoned) return ehgp::abi_fail(ctx, EHGP_ERR_POISONED, "the context is poisoned by an earlier CUDA failure");
+  if (ctx->built_n == 0) return ehgp::abi_fail(ctx, EHGP_ERR_NOT_BUILT, "ehgp_predicate_eval needs a resident cloud");
+  for (uint32_t i = 0; i < count; ++i)
+    if (ids[i] >= ctx->built_n && !(predicate == 3 && i == 0)) return EHGP_ERR_INVALID_ARGUMENT;
+  const uint32_t need = predicate == 1 ? 2 : predicate == 2 ? 1 : predicate == 3 ? 3 : 3;
+  if (count < need || (predicate == 1 && count > 5) || (predicate == 2 && count > 4) || (predicate == 4 && count != 3) ||
+      (predicate == 3 && (ids[0] < 1 || ids[0] > 4 || count - 1 - ids[0] < 1 || count - 1 - ids[0] > 4)))
+    return EHGP_ERR_INVALID_ARGUMENT;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return ehgp::abi_cuda_fail(ctx, e, "cudaSetDevice");
+  if (!ctx->geom_ready) {
+    ehgp::geom_prepare(*ctx, (uint32_t)ctx->built_n);
+    if ((e = cudaGetLastError()) != cudaSuccess) return ehgp::abi_cuda_fail(ctx, e, "traversal preparation");
+  }
+  if (!ctx->scale_valid)
+    return ehgp::abi_fail(ctx, EHGP_ERR_NUMERIC_RANGE, "the cloud exceeds the exact fixed-point range");
+  cudaStream_t st = ctx->stream;
+  cudaMemcpyToSymbolAsync(ehgp::g_pred_ids, ids, count * sizeof(uint32_t), 0, cudaMemcpyHostToDevice, st);
+  ehgp::k_predicate<<<1, 1, 0, st>>>(predicate, count, ctx->lb.px, ctx->lb.py, ctx->lb.pz, ctx->gb.scale);
+  cudaMemcpyFromSymbolAsync(out, ehgp::g_pred_out, 2 * sizeof(int32_t), 0, cudaMemcpyDeviceToHost, st);
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return ehgp::abi_cuda_fail(ctx, e, "predicate evaluation");
+  return EHGP_OK;
+}
 
 int ehgp_higher(ehgp_ctx* ctx, uint32_t K, const ehgp_higher_out* out) {
   if (!ctx) return EHGP_ERR_INVALID_ARGUMENT;

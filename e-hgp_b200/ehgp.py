@@ -228,6 +228,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "ehgp_ctx_regrowths": (C.c_uint64, [P]),
         "ehgp_tune": (C.c_int, [P, C.c_uint32, C.c_uint64]),
         "ehgp_event_supports": (C.c_int, [P, P, C.c_uint64, P]),
+        "ehgp_predicate_eval": (C.c_int, [P, C.c_uint32, P, C.c_uint32, P]),
         "ehgp_server_create": (C.c_int, [C.c_int, C.POINTER(ServerLimits), C.POINTER(P)]),
         "ehgp_server_destroy": (C.c_int, [P]),
         "ehgp_cloud_submit": (C.c_int, [P, C.POINTER(CloudDesc), C.POINTER(C.c_uint64)]),
@@ -557,6 +558,15 @@ class Context:
             v = limbs_to_int(a)
             return v - (1 << (64 * 36)) if v >> (64 * 36 - 1) else v
         return Fraction(signed(num), signed(den) << (2 * S.value))
+
+    PRED_SUPPORT_SIDE, PRED_SUPPORT_STATUS, PRED_LEVEL_CMP, PRED_DISTANCE_CMP = 1, 2, 3, 4
+
+    def predicate(self, kind: int, ids) -> tuple[int, bool]:
+        """ehgp_predicate_eval: (result, decided by the FP64 filter)."""
+        a = np.ascontiguousarray(ids, dtype=np.uint32)
+        out = np.zeros(2, np.int32)
+        self._check(self.lib.ehgp_predicate_eval(self._h, kind, _ptr(a), len(a), _ptr(out)))
+        return int(out[0]), bool(out[1])
 
     def event_supports(self, events: np.ndarray) -> np.ndarray:
         """ehgp_event_supports: (size, ids[4]) of facade events of the last hierarchy."""

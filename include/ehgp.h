@@ -272,6 +272,26 @@ int ehgp_higher(ehgp_ctx* ctx, uint32_t K, const ehgp_higher_out* out);
  * (<= 4096) or mega (<= 16384) set, [13] entries of those sets.  count <= 14. */
 int ehgp_higher_stats(const ehgp_ctx* ctx, double* kernel_ms, uint64_t* stats, uint32_t count);
 
+/* One exact predicate on PointIds of the resident cloud, evaluated on the device by
+ * the enumeration's own helpers (FP64 with the uniform error bounds, then the
+ * fixed-width exact integers); out[0] the result, out[1] 1 when an FP64 filter
+ * decided it.  Stands in for the reference's predicate replay tool
+ * (morsehgp3d/src/tools/predicate_replay.cpp) on the predicates this path uses:
+ *   EHGP_PRED_SUPPORT_SIDE   ids = support (1-4) then the query: -1 strictly
+ *                            inside, 0 on, +1 outside its support sphere
+ *                            (support_sphere_side; a triangle's circle is
+ *                            centred in its plane);
+ *   EHGP_PRED_SUPPORT_STATUS ids = support (1-4): 0 minimal, 1 boundary reduced,
+ *                            2 exterior centre, 3 affinely dependent
+ *                            (circumcenter_support_analysis, support_status);
+ *   EHGP_PRED_LEVEL_CMP      ids = left size, left ids, right ids: sign of
+ *                            level(left) - level(right) (compare_support_levels);
+ *   EHGP_PRED_DISTANCE_CMP   ids = a, p, q: sign of |p - a|^2 - |q - a|^2
+ *                            (compare_squared_distances).
+ * EHGP_ERR_NUMERIC_RANGE when the cloud leaves the exact fixed-point range. */
+enum { EHGP_PRED_SUPPORT_SIDE = 1, EHGP_PRED_SUPPORT_STATUS = 2, EHGP_PRED_LEVEL_CMP = 3, EHGP_PRED_DISTANCE_CMP = 4 };
+int ehgp_predicate_eval(ehgp_ctx* ctx, uint32_t predicate, const uint32_t* ids, uint32_t count, int32_t* out);
+
 /* Allocation-free LBVH build.  No counterpart in the reference: it exists for
  * callers that may not call cudaMalloc (a host framework that owns all device
  * memory through its own pool, or a latency-critical caller that cannot

@@ -9,6 +9,7 @@ project-written Boost shim).  Run here, where the reference tree exists:
     python tests/golden/make_golden.py --hierarchy  # slow: the reference direct chain up to the forest journal
     python tests/golden/make_golden.py --definition  # the Python exhaustive-Gamma hgp_reduced forests
     python tests/golden/make_golden.py --scale  # restatement digests at n = 216-256 (about 10 min)
+    python tests/golden/make_golden.py --predicates  # the reference's predicate fixtures, answered by its replay tool
 """
 import os
 import sys
@@ -309,3 +310,50 @@ def main_scale():
 
 if __name__ == "__main__" and "--scale" in sys.argv:
     main_scale()
+
+
+# ---- the reference's predicate fixtures, answered by its own replay tool ---------------
+PRED_KINDS = ("support_sphere_side", "compare_support_levels", "circumcenter_support_analysis",
+              "binary64_circumcenter_support_analysis", "compare_squared_distances")
+
+
+def main_predicates():
+    """Every fixture of morsehgp3d/tests/fixtures/predicates/ whose predicate this path
+    evaluates, with the answer of the reference's own tool (oracle/_ref/replay_predicate,
+    morsehgp3d/src/tools/predicate_replay.cpp compiled unmodified)."""
+    import glob
+    import json
+    import subprocess
+    root = pyoracle.reference_root()
+    tool = os.path.join(ROOT, "oracle", "_ref", "replay_predicate")
+    out = []
+    for path in sorted(glob.glob(os.path.join(root, "morsehgp3d", "tests", "fixtures", "predicates", "*.json"))):
+        d = json.load(open(path))
+        kind = d.get("predicate")
+        if kind not in PRED_KINDS:
+            continue
+        if kind == "support_sphere_side":
+            groups = {"support": d["support"], "point": [d["point"]]}
+            args = [str(len(d["support"]))] + [w for p in d["support"] for w in p] + d["point"]
+        elif kind == "compare_support_levels":
+            groups = {"left": d["left_support"], "right": d["right_support"]}
+            args = ([str(len(d["left_support"]))] + [w for p in d["left_support"] for w in p] +
+                    [str(len(d["right_support"]))] + [w for p in d["right_support"] for w in p])
+        elif kind == "compare_squared_distances":
+            groups = {"points": d["points"]}
+            args = [w for p in d["points"] for w in p]
+        else:
+            groups = {"points": d["points"]}
+            args = [str(len(d["points"]))] + [w for p in d["points"] for w in p]
+        r = subprocess.run([tool, kind, *args], capture_output=True, text=True)
+        res = json.loads(r.stdout) if r.returncode == 0 and r.stdout.strip() else {"error": r.stderr.strip()}
+        keep = {k: res[k] for k in ("sign", "support_status", "support_kind", "classification", "ordering",
+                                    "certification_stage", "error") if k in res}
+        out.append({"fixture": os.path.basename(path), "predicate": kind, "groups": groups, "reference": keep})
+        print(os.path.basename(path), kind, keep, flush=True)
+    with open(os.path.join(HERE, "predicates_ref.json"), "w") as fh:
+        json.dump(out, fh, indent=0, sort_keys=True)
+
+
+if __name__ == "__main__" and "--predicates" in sys.argv:
+    main_predicates()

@@ -70,3 +70,40 @@ def test_oracle_classify_agrees_with_the_streams():
         assert row[0] == 0
         assert (row[1], row[2], row[3]) == (I, shell, wit)
         assert tuple(int(x) for x in row[4:4 + I]) == tuple(inter)
+
+
+def test_restatement_agrees_with_reference_predicate_tool():
+    """The restatement's exact classification (oracle.classify) gives the reference replay
+    tool's answers on its support-sphere and support-status fixtures (sizes 2-4, distinct
+    points; golden/predicates_ref.json)."""
+    import json
+    cases = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "predicates_ref.json")))
+    assert len(cases) >= 39
+    checked = 0
+    for case in cases:
+        kind = case["predicate"]
+        if kind not in ("support_sphere_side", "circumcenter_support_analysis", "binary64_circumcenter_support_analysis"):
+            continue
+        groups = case["groups"]
+        pts_hex = groups["support"] + groups["point"] if kind == "support_sphere_side" else groups["points"]
+        pts = np.array([np.array([int(h, 16) for h in p], np.uint64).view(np.float64) + 0.0 for p in pts_hex])
+        size = len(groups["support"]) if kind == "support_sphere_side" else len(pts)
+        if size < 2 or len(np.unique(pts, axis=0)) != len(pts):
+            continue
+        snap = pyoracle.lbvh_build(pts)
+        P = pts[snap["source_index"].astype(np.int64)]
+        pid = np.empty(len(pts), np.int64)
+        pid[snap["source_index"].astype(np.int64)] = np.arange(len(pts))
+        sup = [int(pid[i]) for i in range(size)]
+        row = np.array([[size, *sup, *([0] * (4 - size))]], np.uint32)
+        cls = pyoracle.classify(P, row)[0]
+        ref = case["reference"]
+        if kind == "support_sphere_side":
+            if cls[0] != 0:
+                continue  # the classification applies to minimal supports only
+            side = -1 if cls[1] == 1 else (0 if cls[2] > size else 1)
+            assert side == {"negative": -1, "zero": 0, "positive": 1}[ref["sign"]], case["fixture"]
+        else:
+            assert (cls[0] == 0) == (ref["support_status"] == "minimal"), case["fixture"]
+        checked += 1
+    assert checked >= 15
