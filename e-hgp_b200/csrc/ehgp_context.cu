@@ -94,6 +94,7 @@ int lbvh_build_common(Ctx* ctx, const void* src, uint64_t n, const ehgp_lbvh_out
   ctx->geom_ready = false;
   ctx->emst_ready = false;
   ctx->pb.witness_ready = false;
+  ctx->pb.resident = false;
   ctx->pb.K = 0;  // supports are resident for one cloud and one K
   ctx->hb.K = 0;
   if (where == 0) {
@@ -220,6 +221,7 @@ int ehgp_ctx_reserve(ehgp_ctx* ctx, uint32_t stage, uint64_t records) {
     ctx->pb.K = 0;
     ctx->pb.count = 0;
     ctx->pb.witness_ready = false;
+    ctx->pb.resident = false;
     e = ehgp::pairs_records_alloc(*ctx, records);
   } else {
     ctx->hb.K = 0;
@@ -234,6 +236,13 @@ int ehgp_ctx_reserve(ehgp_ctx* ctx, uint32_t stage, uint64_t records) {
 }
 
 uint64_t ehgp_ctx_regrowths(const ehgp_ctx* ctx) { return ctx ? ctx->regrowths : 0; }
+
+int ehgp_ctx_counters(const ehgp_ctx* ctx, uint64_t* out, uint32_t count) {
+  if (!ctx || !out) return EHGP_ERR_INVALID_ARGUMENT;
+  const uint64_t v[4] = {ctx->device_bytes, ctx->regrowths, ctx->pair_runs, ctx->higher_runs};
+  for (uint32_t i = 0; i < count && i < 4; ++i) out[i] = v[i];
+  return EHGP_OK;
+}
 
 int ehgp_tune(ehgp_ctx* ctx, uint32_t knob, uint64_t value) {
   if (!ctx) return EHGP_ERR_INVALID_ARGUMENT;

@@ -1438,7 +1438,7 @@ int hier_run(Ctx& ctx, uint32_t K) {
   if (K == 0 || K > 10) return abi_fail(&ctx, EHGP_ERR_INVALID_ARGUMENT, "K_max must be in [1, 10]");
   // supports for this K
   uint32_t np = 0, nh = 0;
-  if (!(ctx.pb.K == K && ctx.pb.witness_ready)) {  // pair supports of this cloud and K
+  if (!(ctx.pb.K == K && ctx.pb.resident)) {  // pair supports of this cloud and K
     const int s = pairs_run(ctx, K, &np);
     if (s != EHGP_OK) return s;
   }

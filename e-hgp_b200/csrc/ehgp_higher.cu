@@ -1888,7 +1888,11 @@ int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   const uint32_t smax = (keff + 1 < n) ? keff + 1 : n;
   *out_count = 0;
   h.count = 0;
-  if (smax < 3 || n < 3) return EHGP_OK;
+  ++ctx.higher_runs;
+  if (smax < 3 || n < 3) {
+    h.K = K;
+    return EHGP_OK;
+  }
   if (smax - 3 > (uint32_t)kMaxInteriorH) return abi_fail(&ctx, EHGP_ERR_INVALID_ARGUMENT, "K above 10 is not supported");
   if (!p.witness_ready) {  // the witness radii come from the pair stage
     uint32_t pc = 0;

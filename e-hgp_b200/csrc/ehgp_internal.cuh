@@ -189,6 +189,7 @@ struct PairBuffers {
   uint32_t count = 0;               // records of the last run
   uint32_t K = 0;
   bool witness_ready = false;       // W / R2 computed for the resident cloud
+  bool resident = false;            // records of the resident cloud for K are in `sorted`
 };
 
 // Buffers of the triple/quad-support stage.
@@ -253,6 +254,7 @@ struct Ctx {
   double last_ms = 0.0;
   uint64_t last_launches = 0;
   uint64_t regrowths = 0;          // record buffers grown and enumerations re-run
+  uint64_t pair_runs = 0, higher_runs = 0;  // support enumerations run on this context
   uint32_t* d_err = nullptr;       // device error word
   uint32_t* h_status = nullptr;    // pinned: [err, stats...]
   RadixScratch radix;

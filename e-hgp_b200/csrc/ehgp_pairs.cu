@@ -517,7 +517,13 @@ int pairs_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   const uint32_t smax = (keff + 1 < n) ? keff + 1 : n;
   *out_count = 0;
   p.count = 0;
-  if (smax < 2 || n < 2) return EHGP_OK;
+  p.resident = false;
+  ++ctx.pair_runs;
+  if (smax < 2 || n < 2) {
+    p.K = K;
+    p.resident = true;
+    return EHGP_OK;
+  }
   const uint32_t cap = smax - 2;
   if (cap > (uint32_t)kMaxInterior) return abi_fail(&ctx, EHGP_ERR_INVALID_ARGUMENT, "K above 10 is not supported");
   const uint32_t root = 2 * n - 2;
@@ -585,6 +591,7 @@ int pairs_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   p.count = m;
   p.K = K;
   p.witness_ready = true;
+  p.resident = true;
   *out_count = m;
   return EHGP_OK;
 }

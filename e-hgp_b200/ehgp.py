@@ -229,6 +229,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "ehgp_tune": (C.c_int, [P, C.c_uint32, C.c_uint64]),
         "ehgp_event_supports": (C.c_int, [P, P, C.c_uint64, P]),
         "ehgp_predicate_eval": (C.c_int, [P, C.c_uint32, P, C.c_uint32, P]),
+        "ehgp_ctx_counters": (C.c_int, [P, P, C.c_uint32]),
+        "ehgp_checkpoint_save": (C.c_int, [P, C.c_uint32, C.c_char_p]),
+        "ehgp_checkpoint_load": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_uint32)]),
         "ehgp_server_create": (C.c_int, [C.c_int, C.POINTER(ServerLimits), C.POINTER(P)]),
         "ehgp_server_destroy": (C.c_int, [P]),
         "ehgp_cloud_submit": (C.c_int, [P, C.POINTER(CloudDesc), C.POINTER(C.c_uint64)]),
@@ -346,6 +349,24 @@ class Context:
     def tune(self, knob: int, value: int) -> None:
         """ehgp_tune: a tuning knob of later calls (results never depend on it)."""
         self._check(self.lib.ehgp_tune(self._h, knob, value))
+
+    def counters(self) -> dict:
+        """ehgp_ctx_counters: device bytes, regrowths, pair and triple/quad enumerations run."""
+        v = np.zeros(4, np.uint64)
+        self._check(self.lib.ehgp_ctx_counters(self._h, _ptr(v), 4))
+        return dict(zip(("device_bytes", "regrowths", "pair_runs", "higher_runs"), (int(x) for x in v)))
+
+    def checkpoint_save(self, path: str, K: int = 10) -> None:
+        """ehgp_checkpoint_save: cloud, K and support records of the resident cloud to `path`."""
+        self._check(self.lib.ehgp_checkpoint_save(self._h, K, os.fsencode(path)))
+
+    def checkpoint_load(self, path: str) -> int:
+        """ehgp_checkpoint_load: the cloud and support records of a checkpoint; returns its K."""
+        K = C.c_uint32()
+        self._check(self.lib.ehgp_checkpoint_load(self._h, os.fsencode(path), C.byref(K)))
+        with open(path, "rb") as f:  # header: magic, version, K, point count
+            self.n = int(np.frombuffer(f.read(24)[16:24], np.uint64)[0])
+        return K.value
 
     def regrowths(self) -> int:
         """Second enumeration passes after a record buffer grew (count -> allocate -> emit)."""

@@ -77,6 +77,24 @@ uint64_t ehgp_ctx_device_bytes(const ehgp_ctx* ctx);
 int ehgp_ctx_reserve(ehgp_ctx* ctx, uint32_t stage, uint64_t records);
 uint64_t ehgp_ctx_regrowths(const ehgp_ctx* ctx);
 
+/* [0] device bytes, [1] record-buffer regrowths, [2] pair enumerations and [3]
+ * triple/quad enumerations run on this context so far.  No reference counterpart. */
+int ehgp_ctx_counters(const ehgp_ctx* ctx, uint64_t* out, uint32_t count);
+
+/* Checkpoint and resume of a request after its support stages, in place of the
+ * reference's chunk -> checkpoint -> commit support streams
+ * (include/morsehgp3d/hierarchy/pair_support_stream.hpp:421-470) and its planned
+ * preemption manifest (docs/GPU_G4_ARCHITECTURE.md:239-252).  save writes the
+ * resident cloud (binary64, PointId order), K and the pair and triple/quad records
+ * for K (enumerating them first when they are not resident) to `path` with a
+ * 64-byte header and an FNV-1a checksum; load checks the file, rebuilds the cloud
+ * on ctx (the same PointIds) and makes the records resident, so a following
+ * ehgp_hierarchy(ctx, K) resumes without enumerating the supports again.  A file
+ * that fails its checks is refused with EHGP_ERR_INVALID_ARGUMENT and leaves the
+ * context as it was. */
+int ehgp_checkpoint_save(ehgp_ctx* ctx, uint32_t K, const char* path);
+int ehgp_checkpoint_load(ehgp_ctx* ctx, const char* path, uint32_t* K);
+
 /* Tuning knobs of later calls on ctx; results never depend on them (no
  * counterpart in the reference).
  *   EHGP_TUNE_HIGHER_LIST: neighbour-list entries (1..1024, default 1024) that a
