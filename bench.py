@@ -633,7 +633,9 @@ def run_chain(spec: str, K: int, repeat: int) -> None:
                 out["decision"] = "refused: relevant extra-shell diagnostics"
             out["hierarchy_wall_ms"] = 1e3 * (time.perf_counter() - t)
             hs = ctx.hier_stats()
-            out["hierarchy"] = {k: hs[k] for k in ("device_ms", "descent_ms", "forest_ms", "arms", "events")}
+            out["hierarchy"] = {k: hs[k] for k in ("device_ms", "descent_ms", "forest_ms", "slowest_order_ms",
+                                                   "host_orders_ms", "host_offsets_ms", "host_vertical_ms",
+                                                   "order_ms", "arms", "events")}
             out["hierarchy_counts"] = ctx.last_hier_counts
             out["total_wall_ms"] = 1e3 * (time.perf_counter() - t0)
             print(json.dumps(out), flush=True)

@@ -445,19 +445,11 @@ __global__ void k_tie_sort(uint32_t nruns, const uint32_t* __restrict__ run_off,
   }
 }
 
-// Gathers the facade records of the uncertain runs and scatters them back with their
-// exact-equality flags (kept for the member copies of the tie sort).
+// Gathers the facade records of the uncertain runs (the member copies of the tie sort).
 __global__ void k_run_gather(uint32_t cnt, const uint32_t* __restrict__ idx, const EvRec* __restrict__ ev,
                              EvRec* __restrict__ out) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < cnt) out[i] = ev[idx[i]];
-}
-__global__ void k_run_scatter(uint32_t cnt, const uint32_t* __restrict__ idx, const EvRec* __restrict__ in,
-                              const uint8_t* __restrict__ eq, EvRec* __restrict__ ev, uint8_t* __restrict__ eqprev) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= cnt) return;
-  ev[idx[i]] = in[i];
-  eqprev[idx[i]] = eq[i];
 }
 
 // Support records of facade events: out[5i] = size, out[5i + 1..4] = ids (unused 0); an

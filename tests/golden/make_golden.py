@@ -10,6 +10,7 @@ project-written Boost shim).  Run here, where the reference tree exists:
     python tests/golden/make_golden.py --definition  # the Python exhaustive-Gamma hgp_reduced forests
     python tests/golden/make_golden.py --scale  # restatement digests at n = 216-256 (about 10 min)
     python tests/golden/make_golden.py --predicates  # the reference's predicate fixtures, answered by its replay tool
+    python tests/golden/make_golden.py --scale-higher  # restatement triple/quad digests at n = 1000 (about 1.5 h)
 """
 import os
 import sys
@@ -357,3 +358,27 @@ def main_predicates():
 
 if __name__ == "__main__" and "--predicates" in sys.argv:
     main_predicates()
+
+
+# ---- completeness beyond the plain workload's size (triple/quad records only) -----------
+def main_scale_higher():
+    """Digests of the restatement's complete triple/quad stream (brute force over every
+    tuple, FP64-filtered, exact where undecided) for 1,000-point clouds: i.i.d. uniform and a
+    10^3 jittered lattice.  About 45 minutes each on 8 host threads."""
+    import json
+    cases = [("uniform1000_s0", workloads.uniform_cube(1000, 0)),
+             ("lattice10_f32", workloads.jittered_lattice(10, 6).astype(np.float64))]
+    out = {}
+    for name, pts in cases:
+        snap = pyoracle.lbvh_build(pts)
+        canon = pts[snap["source_index"].astype(np.int64)]
+        hi = pyoracle.higher(canon, 10)
+        out[name] = {"points": pts.tolist(), "K": 10, "higher_sha256": higher_digest(hi),
+                     "higher_events": len(hi["events"]), "higher_diagnostics": len(hi["diagnostics"])}
+        print(name, out[name]["higher_events"], out[name]["higher_diagnostics"], flush=True)
+        with open(os.path.join(HERE, "scale_higher_digests.json"), "w") as fh:
+            json.dump(out, fh, separators=(",", ":"))
+
+
+if __name__ == "__main__" and "--scale-higher" in sys.argv:
+    main_scale_higher()
