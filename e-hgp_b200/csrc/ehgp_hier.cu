@@ -62,7 +62,8 @@ constexpr double kTiny = 1e-300;
 constexpr int kMaxFacet = 10;
 constexpr int kT = 256;              // threads per block of the elementwise kernels
 constexpr int kCandCap = 64;         // ball-query candidates per descent step
-constexpr int kDStack = 96;          // LBVH traversal stack per descent thread (depth <= 63 + log2 n + 1)
+constexpr int kDStack = 96;
+constexpr uint32_t kSortQueueMin = 1u << 15;  // descent queues at least this long are sorted spatially          // LBVH traversal stack per descent thread (depth <= 63 + log2 n + 1)
 constexpr int kDescentSteps = 512;   // descent steps per arm
 
 // Slow-path counters of the descent (read back per call): [0] exhaustive miniball
@@ -1053,12 +1054,27 @@ __global__ void k_arm_probe(DescentParams d, uint32_t a0, uint32_t narms,
 #ifndef EHGP_STEP_BLOCKS_PER_SM
 #define EHGP_STEP_BLOCKS_PER_SM 8
 #endif
-__global__ void __launch_bounds__(128, EHGP_STEP_BLOCKS_PER_SM)
-k_arm_step(DescentParams d, uint32_t m, const uint32_t* __restrict__ in_arm, const uint32_t* __restrict__ in_fac,
-           uint32_t* __restrict__ out_arm, uint32_t* __restrict__ out_fac, uint32_t* __restrict__ out_count,
-           uint32_t* __restrict__ term, uint8_t* __restrict__ status, unsigned long long* __restrict__ stats) {
+// Sort keys of a descent queue: the top 24 bits of the Morton code of each facet's least
+// point, so that a warp's threads descend from nearby facets (shared traversal paths,
+// less divergence).  The order of processing never changes a result.
+__global__ void k_queue_keys(uint32_t m, const uint32_t* __restrict__ in_fac, const uint64_t* __restrict__ code,
+                             uint64_t* __restrict__ key, uint32_t* __restrict__ val) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
+  key[i] = code[in_fac[(uint64_t)i * kMaxFacet]] >> 39;
+  val[i] = i;
+}
+
+__global__ void __launch_bounds__(128, EHGP_STEP_BLOCKS_PER_SM)
+k_arm_step(DescentParams d, uint32_t m, const uint32_t* __restrict__ in_arm, const uint32_t* __restrict__ in_fac,
+           const uint32_t* __restrict__ rstate, int passes, const uint32_t* __restrict__ v0,
+           const uint32_t* __restrict__ v1, uint32_t* __restrict__ out_arm, uint32_t* __restrict__ out_fac,
+           uint32_t* __restrict__ out_count, uint32_t* __restrict__ term, uint8_t* __restrict__ status,
+           unsigned long long* __restrict__ stats) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= m) return;
+  // queue entry: in Morton order of the facets when the queue was sorted (passes >= 0)
+  const uint32_t i = passes >= 0 ? radix_result(rstate, passes, v0, v1)[t] : t;
   const uint32_t a = in_arm[i];
   uint32_t F[kMaxFacet];
   int k = 0;
@@ -2439,7 +2455,14 @@ int hier_run(Ctx& ctx, uint32_t K) {
           uint32_t* oc = h.qcount + 1 + (1 - cur);
           cudaMemsetAsync(oc, 0, sizeof(uint32_t), st);
           if (h.ev_step[0]) cudaEventRecord(h.ev_step[0], st);
-          k_arm_step<<<nblk(pending, 128), 128, 0, st>>>(dp, pending, h.q_arm[cur], h.q_fac[cur], h.q_arm[1 - cur],
+          int spasses = -1;  // large queues run in Morton order of their facets
+          if (pending >= kSortQueueMin && pending <= h.cap_events) {
+            k_queue_keys<<<nblk(pending, kT), kT, 0, st>>>(pending, h.q_fac[cur], b.code, h.key, h.order0);
+            ++launches;
+            spasses = radix_sort_kv(st, pending, h.order0, h.order1, h.key, h.key2, 24, rs, &launches);
+          }
+          k_arm_step<<<nblk(pending, 128), 128, 0, st>>>(dp, pending, h.q_arm[cur], h.q_fac[cur], ctx.radix.state,
+                                                         spasses, h.order0, h.order1, h.q_arm[1 - cur],
                                                          h.q_fac[1 - cur], oc, h.term, h.arm_status, h.dstats);
           if (h.ev_step[1]) cudaEventRecord(h.ev_step[1], st);
           ++launches;
