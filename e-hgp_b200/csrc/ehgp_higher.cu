@@ -1167,15 +1167,23 @@ __device__ __forceinline__ uint32_t select_bit(uint32_t x, uint32_t r) {
   return pos;
 }
 
+// Parts of one owner's enumeration that a block runs (higher_owner's `phases`): the
+// triangles with the face mask, the tetrahedra, clearing the mask first, the owner's counters.
+constexpr uint32_t kPhTri = 1, kPhTet = 2, kPhClear = 4, kPhStats = 8, kPhAll = 15;
+
 // Enumeration of owner a over its candidate set clist[0..m) (m <= KC, sorted by binary32
 // distance from a), by the whole block; adm holds KC * KC / 32 words (shared or global).
+// The block runs the pairs [t_lo, t_hi) of the support candidates (the triangles (a, j, k) and
+// the tetrahedra whose first two candidates are the pair), so one owner can be split over
+// blocks: all triangles (which complete the face mask) before any tetrahedron.
 template <int KC>
 __device__ __forceinline__ void higher_owner(uint32_t a, const uint32_t* __restrict__ clist, uint32_t m,
                                              OwnerSmemT<KC>& S, uint32_t* adm, WarpQueue* wq, const Ctl& ctl,
                                              const HigherTables& tb, const double* __restrict__ px,
                                              const double* __restrict__ py, const double* __restrict__ pz,
                                              const int* __restrict__ cloud_scale, HigherRec* __restrict__ out,
-                                             uint32_t* __restrict__ counter, unsigned long long* __restrict__ stats) {
+                                             uint32_t* __restrict__ counter, unsigned long long* __restrict__ stats,
+                                             uint64_t t_lo = 0, uint64_t t_hi = ~0ull, uint32_t phases = kPhAll) {
   constexpr uint32_t kWords = KC / 32;
   __shared__ double s_Mp;
   __shared__ uint32_t s_mc;
@@ -1212,7 +1220,8 @@ __device__ __forceinline__ void higher_owner(uint32_t a, const uint32_t* __restr
     S.rho[d] = r;
     rmax = fmaxf(rmax, r);
   }
-  for (uint32_t i = threadIdx.x; i < (uint32_t)KC * kWords; i += 32 * kHOwnerWarps) adm[i] = 0u;
+  if (phases & kPhClear)
+    for (uint32_t i = threadIdx.x; i < (uint32_t)KC * kWords; i += 32 * kHOwnerWarps) adm[i] = 0u;
   for (int off = 16; off > 0; off >>= 1) {
     Mp = fmax(Mp, __shfl_xor_sync(0xffffffffu, Mp, off));
     rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, off));
@@ -1229,9 +1238,9 @@ __device__ __forceinline__ void higher_owner(uint32_t a, const uint32_t* __restr
   for (int w = 1; w < kHOwnerWarps; ++w) rmax = fmaxf(rmax, s_rmax[w]);
   const double rmax2 = (double)rmax * (double)rmax * (1.0 + 1e-12);
   unsigned long long tested = 0, minimal = 0, pruned = 0, classified = 0, emitted = 0, admitted = 0;
-  const uint64_t P2 = (uint64_t)mc * (mc - 1) / 2;
+  const uint64_t P2 = min((uint64_t)mc * (mc - 1) / 2, t_hi);
   // --- triangles (a, j, k); also the face bound adm(j, k) for the tetrahedra
-  for (uint64_t t0 = 32 * warp; t0 < P2; t0 += 32 * kHOwnerWarps) {
+  for (uint64_t t0 = t_lo + 32 * warp; (phases & kPhTri) && t0 < P2; t0 += 32 * kHOwnerWarps) {
     const uint64_t t = t0 + lane;
     bool push = false;
     QEntry E;
@@ -1266,10 +1275,10 @@ __device__ __forceinline__ void higher_owner(uint32_t a, const uint32_t* __restr
     classified += __popc(b);
     classify_queue(S, Q, __popc(b), m, c, ctl.smax, out, ctl.cap, counter, lane, emitted);
   }
-  __syncthreads();  // the face mask is complete
+  if ((phases & kPhTri) && (phases & kPhTet)) __syncthreads();  // the face mask is complete
   // --- tetrahedra (a, j, k, l), j < k < l with adm(j,k), adm(j,l), adm(k,l)
-  if (ctl.smax >= 4) {
-    for (uint64_t t0 = 32 * warp; t0 < P2; t0 += 32 * kHOwnerWarps) {
+  if (ctl.smax >= 4 && (phases & kPhTet)) {
+    for (uint64_t t0 = t_lo + 32 * warp; t0 < P2; t0 += 32 * kHOwnerWarps) {
       const uint64_t t = t0 + lane;
       uint32_t j = 0, k = 0, cnt = 0;
       if (t < P2) {
@@ -1348,7 +1357,7 @@ __device__ __forceinline__ void higher_owner(uint32_t a, const uint32_t* __restr
     atomicAdd(stats + 0, tested);
     atomicAdd(stats + 1, classified);
     atomicAdd(stats + 2, emitted);
-    if (warp == 0) {
+    if (warp == 0 && (phases & kPhStats)) {
       atomicAdd(stats + 3, (unsigned long long)m);
       atomicAdd(stats + 4, (unsigned long long)mc);
     }
@@ -1418,6 +1427,43 @@ k_higher_large(uint32_t nown, const uint32_t* __restrict__ owners, const uint64_
                        stats);
     __syncthreads();  // the next owner restages the shared set
   }
+}
+
+// Owners with up to KC candidates split over blocks: block w runs pair chunk
+// w - chunk_off[i] (kSplitPairs pairs) of owner i, the last i with chunk_off[i] <= w.  Phase
+// kPhTri (with kPhStats on each owner's first chunk) fills the owners' face masks in global
+// memory (adm_all, KC * KC / 32 words per owner, zero on entry); the next launch, kPhTet,
+// reads them complete.  An owner's work is its O(m^2) pairs and their tetrahedra, so the
+// large sets spread over every SM instead of one block each.
+constexpr uint32_t kSplitPairs = 8192;
+template <int KC>
+__global__ void __launch_bounds__(32 * kHOwnerWarps, 2)
+k_higher_split(uint32_t nown, const uint32_t* __restrict__ owners, const uint64_t* __restrict__ coff,
+               const uint32_t* __restrict__ carena, const uint32_t* __restrict__ chunk_off, uint32_t phase, Ctl ctl,
+               HigherTables tb, const double* __restrict__ px, const double* __restrict__ py,
+               const double* __restrict__ pz, const int* __restrict__ cloud_scale, HigherRec* __restrict__ out,
+               uint32_t* __restrict__ counter, unsigned long long* __restrict__ stats, uint32_t* __restrict__ adm_all) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  WarpQueue* wq = reinterpret_cast<WarpQueue*>(smem);
+  OwnerSmemT<KC>& S = *reinterpret_cast<OwnerSmemT<KC>*>(smem + sizeof(WarpQueue) * kHOwnerWarps);
+  const uint32_t w = blockIdx.x;
+  uint32_t lo = 0, hi = nown;  // the owner: last i with chunk_off[i] <= w
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) / 2;
+    if (chunk_off[mid] <= w) lo = mid;
+    else hi = mid;
+  }
+  const uint32_t i = lo, c = w - chunk_off[i];
+  const uint32_t m = (uint32_t)(coff[i + 1] - coff[i]);
+  if (m > (uint32_t)KC) return;
+  const uint32_t ph = phase == kPhTri ? (c == 0 ? kPhTri | kPhStats : kPhTri) : kPhTet;
+  higher_owner<KC>(owners[i], carena + coff[i], m, S, adm_all + (uint64_t)i * KC * (KC / 32), wq, ctl, tb, px, py,
+                   pz, cloud_scale, out, counter, stats, (uint64_t)c * kSplitPairs, (uint64_t)(c + 1) * kSplitPairs,
+                   ph);
+}
+template <int KC>
+constexpr size_t split_smem() {
+  return sizeof(WarpQueue) * kHOwnerWarps + large_set_bytes<KC>();
 }
 
 // ---- single predicate evaluations (the product kernels' own filters and exact paths) ------
@@ -1866,11 +1912,29 @@ int higher_large_candidates(Ctx& ctx, const CertParams& cp, uint32_t root, const
                                                     b.px, b.py, b.pz, h.rho, h.large_dst + ns, h.cand_arena,
                                                     h.large_cnt + ns, h.cand_dist);
   *launches += (ns ? 1 : 0) + (nb ? 1 : 0);
-  // the enumeration reads owners in arena order
+  // the enumeration reads owners in arena order; the sets of at most kLargeCand and of at
+  // most kHugeCand run split into chunks of their candidate pairs: chunk prefixes of the
+  // first tier in split_off[0 .. per[0]], of the second in split_off[per[0] + 1 ..]
+  std::vector<uint32_t> chunk_off((uint64_t)per[0] + per[1] + 2, 0);
+  for (int tier = 0; tier < 2; ++tier) {
+    const uint32_t q0 = tier ? per[0] : 0, cnt_t = per[tier];
+    uint32_t* co = chunk_off.data() + (tier ? per[0] + 1 : 0);
+    for (uint32_t q = 0; q < cnt_t; ++q) {
+      const uint64_t mq = pre[q0 + q + 1] - pre[q0 + q], pairs = mq * (mq > 0 ? mq - 1 : 0) / 2;
+      co[q + 1] = co[q] + (uint32_t)std::max<uint64_t>(1, (pairs + kSplitPairs - 1) / kSplitPairs);
+    }
+  }
+  if ((e = grow_array(ctx, h.split_off, h.split_cap, chunk_off.size(), 4)) != cudaSuccess) {
+    cudaGetLastError();
+    return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "the large candidate sets do not fit the device");
+  }
+  cudaMemcpyAsync(h.split_off, chunk_off.data(), chunk_off.size() * 4, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(h.large_ids, ids.data(), (uint64_t)nt * 4, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(h.large_off, pre.data(), (uint64_t)(nt + 1) * 8, cudaMemcpyHostToDevice, st);
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return abi_cuda_fail(&ctx, e, "large candidate sets");
   h.n_large = per[0];
+  h.split_chunks = chunk_off[per[0]];
+  h.split_chunks_huge = chunk_off[(uint64_t)per[0] + 1 + per[1]];
   h.n_huge = per[1];
   h.n_mega = per[2];
   h.large_entries = pre[nt];
@@ -1990,20 +2054,31 @@ int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   }
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device);
-  if (h.n_huge || h.n_mega) {  // per-block scratch of the huge- and mega-set kernels
-    const uint64_t bh = std::min<uint64_t>(h.n_huge, (uint64_t)sms), bm = std::min<uint64_t>(h.n_mega, (uint64_t)sms);
-    const uint64_t need = std::max(bh * large_scratch_bytes<kHugeCand, 1>(), bm * large_scratch_bytes<kMegaCand, 2>());
+  if (h.n_mega) {  // per-block scratch of the mega-set kernel (staged set and face mask)
+    const uint64_t bm = std::min<uint64_t>(h.n_mega, (uint64_t)sms);
+    const uint64_t need = bm * large_scratch_bytes<kMegaCand, 2>();
     if ((e0 = grow_array(ctx, h.adm_scratch, h.adm_words, (need + 3) / 4, 4)) != cudaSuccess) {
       cudaGetLastError();
       return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "the scratch of the huge candidate sets does not fit the device");
     }
   }
+  if ((h.n_large || h.n_huge) &&
+      (e0 = grow_array(ctx, h.split_adm, h.split_adm_words,
+                       std::max((uint64_t)h.n_large * kLargeCand * (kLargeCand / 32),
+                                (uint64_t)h.n_huge * kHugeCand * (kHugeCand / 32)),
+                       4)) != cudaSuccess) {
+    cudaGetLastError();
+    return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "the face masks of the large candidate sets do not fit the device");
+  }
   if (h.n_large || h.n_huge || h.n_mega) {
-    cudaError_t ea = cudaFuncSetAttribute(k_higher_large<kLargeCand, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)large_smem<kLargeCand, 0>());
+    cudaError_t ea = cudaFuncSetAttribute(k_higher_split<kLargeCand>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)split_smem<kLargeCand>());
     if (ea == cudaSuccess)
-      ea = cudaFuncSetAttribute(k_higher_large<kHugeCand, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)large_smem<kHugeCand, 1>());
+      ea = cudaFuncSetAttribute(k_higher_split<kHugeCand>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)split_smem<kHugeCand>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_higher_large<kMegaCand, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)large_smem<kMegaCand, 2>());
     if (ea != cudaSuccess) return abi_cuda_fail(&ctx, ea, "large candidate sets shared memory");
   }
   uint32_t hc[2];
@@ -2019,20 +2094,24 @@ int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
     k_higher<<<n, 32 * kHOwnerWarps, 0, st>>>(n, ctl, tb, b.leaf_pid, h.cand, h.candc, b.px, b.py, b.pz, g.scale,
                                               (HigherRec*)h.raw, h.counters, h.stats);
     ++launches;
-    if (h.n_large) {
-      k_higher_large<kLargeCand, 0><<<std::min<uint32_t>(h.n_large, (uint32_t)sms), 32 * kHOwnerWarps,
-                                      large_smem<kLargeCand, 0>(), st>>>(
-          h.n_large, h.large_ids, h.large_off, h.cand_arena, ctl, tb, b.px, b.py, b.pz, g.scale, (HigherRec*)h.raw,
-          h.counters, h.stats, nullptr);
-      ++launches;
+    if (h.n_large) {  // split over chunks of pairs: the triangles (face masks), then the tetrahedra
+      cudaMemsetAsync(h.split_adm, 0, (uint64_t)h.n_large * kLargeCand * (kLargeCand / 32) * 4, st);
+      for (const uint32_t phase : {kPhTri, kPhTet}) {
+        k_higher_split<kLargeCand><<<h.split_chunks, 32 * kHOwnerWarps, split_smem<kLargeCand>(), st>>>(
+            h.n_large, h.large_ids, h.large_off, h.cand_arena, h.split_off, phase, ctl, tb, b.px, b.py, b.pz, g.scale,
+            (HigherRec*)h.raw, h.counters, h.stats, h.split_adm);
+        ++launches;
+      }
     }
     if (h.n_huge) {
       const uint32_t o = h.n_large;
-      k_higher_large<kHugeCand, 1><<<std::min<uint32_t>(h.n_huge, (uint32_t)sms), 32 * kHOwnerWarps,
-                                     large_smem<kHugeCand, 1>(), st>>>(
-          h.n_huge, h.large_ids + o, h.large_off + o, h.cand_arena, ctl, tb, b.px, b.py, b.pz, g.scale,
-          (HigherRec*)h.raw, h.counters, h.stats, (unsigned char*)h.adm_scratch);
-      ++launches;
+      cudaMemsetAsync(h.split_adm, 0, (uint64_t)h.n_huge * kHugeCand * (kHugeCand / 32) * 4, st);
+      for (const uint32_t phase : {kPhTri, kPhTet}) {
+        k_higher_split<kHugeCand><<<h.split_chunks_huge, 32 * kHOwnerWarps, split_smem<kHugeCand>(), st>>>(
+            h.n_huge, h.large_ids + o, h.large_off + o, h.cand_arena, h.split_off + o + 1, phase, ctl, tb, b.px, b.py,
+            b.pz, g.scale, (HigherRec*)h.raw, h.counters, h.stats, h.split_adm);
+        ++launches;
+      }
     }
     if (h.n_mega) {
       const uint32_t o = h.n_large + h.n_huge;

@@ -239,6 +239,10 @@ struct HigherBuffers {
   float* cand_dist = nullptr;       // [cdist_cap] distances of the sets sorted in the arena
   uint64_t cdist_cap = 0;
   uint32_t n_large = 0, n_huge = 0, n_mega = 0;  // owners with <= 1024, 4096, 16384 candidates (last call)
+  uint32_t* split_off = nullptr;    // [split_cap] pair-chunk prefix of the owners with <= 1024 candidates
+  uint32_t* split_adm = nullptr;    // [split_adm_words] their face masks, 1024 * 32 words each
+  uint64_t split_cap = 0, split_adm_words = 0;
+  uint32_t split_chunks = 0, split_chunks_huge = 0;  // blocks of one split launch per tier (last call)
   uint64_t large_entries = 0;
 };
 
