@@ -8,6 +8,10 @@
   (golden/make_golden.py --scale); the hierarchy comparison is the complete text of facade,
   journal, seeds, forest nodes, children, births, bindings, saddles, groups, batches and
   roots with exact levels.
+* Completeness at 1,000 points (golden/scale_higher_digests.json, make_golden.py
+  --scale-higher): the device's triple/quad stream on a 1,000-point i.i.d. uniform cloud and a
+  10^3 jittered lattice equals the restatement's brute force over every tuple, an enumerator
+  that shares neither the direction tables nor the candidate sets of the device.
 * The hierarchy's host schedule (chunk size of the parallel record rebuild, descent parts,
   host threads) never changes its result (n = 4096, chunks of 7 batches, parts of 3000 arms).
 * Soundness at the regular volumetric workload's size (37^3 = 50,653 jittered lattice points):
@@ -38,6 +42,10 @@ SCALE_PATH = os.path.join(os.path.dirname(__file__), "golden", "scale_digests.js
 SCALE = json.load(open(SCALE_PATH)) if os.path.exists(SCALE_PATH) else {}
 
 
+SCALE_HIGHER_PATH = os.path.join(os.path.dirname(__file__), "golden", "scale_higher_digests.json")
+SCALE_HIGHER = json.load(open(SCALE_HIGHER_PATH)) if os.path.exists(SCALE_HIGHER_PATH) else {}
+
+
 def higher_digest(rec):
     return hashlib.sha256(repr((rec["events"], rec["diagnostics"])).encode()).hexdigest()
 
@@ -50,6 +58,15 @@ def canonical(ctx, pts):
 @pytest.mark.parametrize("name", list(SCALE))
 def test_gpu_higher_matches_restatement_at_scale(ctx, name):
     d = SCALE[name]
+    P = canonical(ctx, np.array(d["points"]))
+    rec = gpu_higher_records(ctx, d["K"], P)
+    assert (len(rec["events"]), len(rec["diagnostics"])) == (d["higher_events"], d["higher_diagnostics"])
+    assert higher_digest(rec) == d["higher_sha256"]
+
+
+@pytest.mark.parametrize("name", list(SCALE_HIGHER))
+def test_gpu_higher_complete_at_1000_points(ctx, name):
+    d = SCALE_HIGHER[name]
     P = canonical(ctx, np.array(d["points"]))
     rec = gpu_higher_records(ctx, d["K"], P)
     assert (len(rec["events"]), len(rec["diagnostics"])) == (d["higher_events"], d["higher_diagnostics"])

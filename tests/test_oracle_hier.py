@@ -91,3 +91,15 @@ def test_scale_digest_fixture_is_complete():
     assert any(k.startswith("clustered256_s") and "snap" not in k for k in names)
     for k, v in d.items():
         assert len(v["points"]) >= 216 and len(v["higher_sha256"]) == 64 and len(v["hierarchy_sha256"]) == 64, k
+
+
+def test_scale_higher_fixture_is_complete():
+    """golden/scale_higher_digests.json (make_golden.py --scale-higher) holds the restatement's
+    complete triple/quad streams of a 1,000-point uniform cloud and a 10^3 jittered lattice."""
+    import json
+    import os
+    d = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "scale_higher_digests.json")))
+    assert {"uniform1000_s0", "lattice10_f32"} <= set(d)
+    for k, v in d.items():
+        assert len(v["points"]) == 1000 and v["K"] == 10 and len(v["higher_sha256"]) == 64, k
+        assert v["higher_events"] > 100000, k
