@@ -445,9 +445,26 @@ def run_ours(args, world, rank, local):
         ctx._check(lib.ehgp_event_supports(ctx._h, lev.ctypes.data, hc.nodes, f_sup.ctypes.data))
         return 1e3 * (time.perf_counter() - t0)
 
+    def payload_checksum():
+        """64-bit checksums (xor and odd-weighted sum of the words) of the last e2e step's
+        payload and its counts: the result must not change from step to step."""
+        parts = [f_nodes[:hc.nodes], f_child[:hc.children], f_batch[:hc.journal_batches], f_root[:hc.final_roots],
+                 f_vert[:hc.vertical_assignments], f_sup[:5 * hc.nodes], e_u, e_v, e_D,
+                 np.array([getattr(hc, f) for f, _ in ehgp.HierCounts._fields_], np.uint64)]
+        x = np.uint64(0)
+        t = np.uint64(0)
+        for a in parts:
+            b = np.ascontiguousarray(a).reshape(-1).view(np.uint8)
+            b = np.concatenate([b, np.zeros((-len(b)) % 8, np.uint8)]).view(np.uint64)
+            x ^= np.bitwise_xor.reduce(b) if len(b) else np.uint64(0)
+            with np.errstate(over="ignore"):
+                t = t * np.uint64(0x9E3779B97F4A7C15) + (b * np.uint64(0xBF58476D1CE4E5B9)).sum(dtype=np.uint64)
+        return f"{int(x):016x}{int(t):016x}"
+
     for _ in range(max(args.warmup, 3)):
         resident_step()
         e2e_step()
+    check_first = payload_checksum()  # outside the timed steps
     barrier(world)
     dev_ms, e2e_ms, kern_ms = [], [], []
     hstats = None
@@ -461,6 +478,7 @@ def run_ours(args, world, rank, local):
             l2_flush()
             e2e_ms.append(e2e_step())
     barrier(world)
+    check_last = payload_checksum()
     value = max_over_ranks(p95(dev_ms), world)
     e2e = max_over_ranks(p95(e2e_ms), world)
     hs_last = ctx.hier_stats()
@@ -524,6 +542,7 @@ def run_ours(args, world, rank, local):
                                                        "final_roots")},
                    "stage_ms": stage_ms},
         "latency_ms": {"device": spread(dev_ms), "e2e": spread(e2e_ms)},  # p50/p95/p99/max/MAD
+        "payload_checksum": {"warmup": check_first, "last_step": check_last, "stable": check_first == check_last},
         "e2e": {"value": e2e, "unit": "ms", "h2d_bytes_per_step": int(pts.nbytes), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "gpu_launches_per_step": int(launches_per_step),

@@ -875,6 +875,21 @@ __device__ __noinline__ int topk_choice(const DescentParams& d, const Cloud& c, 
   // can only decrease), and the dropped points are checked to lie beyond the band below.
   double R2_eff = R2;
   bool dropped = false;
+  // The node prune runs in binary32 (the FP64 pipe is the step's tighter unit): qf is the
+  // binary32 rounding of the centre and dqf its distance from it, rounded up (exact in binary64).
+  // Each axis gap to a node box is lowered by the rounding of the subtraction (a relative
+  // 2^-22) and by dqf, clamped at 0; the sum of squares is lowered by a relative 2^-20 and
+  // compared with R2_eff rounded up.  The bound never exceeds the exact one, so the prune skips
+  // only boxes that hold no point within R2_eff (the FP64 prune skips at least those; the
+  // leaves decide membership in FP64 as before).  Far from the origin the FP64 prune stays.
+  const double qv[3] = {cx, cy, cz};
+  const bool f32 = fabs(cx) < 0x1p60 && fabs(cy) < 0x1p60 && fabs(cz) < 0x1p60 && R2 < 0x1p100;
+  float qf[3], dqf[3];
+  for (int a = 0; a < 3; ++a) {
+    qf[a] = (float)qv[a];
+    dqf[a] = __double2float_ru(fabs(qv[a] - (double)qf[a]));
+  }
+  float R2f = __double2float_ru(R2_eff);
   while (top > 0) {
     const uint32_t node = stack[--top];
     const TNode t = load_node(d.tn, node);
@@ -893,18 +908,28 @@ __device__ __noinline__ int topk_choice(const DescentParams& d, const Cloud& c, 
       while (j > 0 && cd[j - 1] > dd) { cd[j] = cd[j - 1]; cid[j] = cid[j - 1]; --j; }
       cd[j] = dd;
       cid[j] = q;
-      if (cnt >= k) R2_eff = fmin(R2, (cd[k - 1] + 2.0 * ed) * (1.0 + 1e-12));
+      if (cnt >= k) {
+        R2_eff = fmin(R2, (cd[k - 1] + 2.0 * ed) * (1.0 + 1e-12));
+        R2f = __double2float_ru(R2_eff);
+      }
       continue;
     }
-    double lb = 0.0;
-    {
-      const double qv[3] = {cx, cy, cz};
+    if (f32) {
+      float lbf = 0.f;
+      for (int a = 0; a < 3; ++a) {
+        const float g0 = fmaxf(fmaxf(t.lo[a] - qf[a], qf[a] - t.hi[a]), 0.f);
+        const float g = fmaxf(g0 * (1.f - 0x1p-22f) - dqf[a], 0.f);
+        lbf += g * g;
+      }
+      if (lbf * (1.f - 0x1p-20f) > R2f) continue;
+    } else {
+      double lb = 0.0;
       for (int a = 0; a < 3; ++a) {
         const double g = fmax(fmax((double)t.lo[a] - qv[a], qv[a] - (double)t.hi[a]), 0.0);
         lb += g * g;
       }
+      if (lb * (1.0 - 1e-6) > R2_eff) continue;
     }
-    if (lb * (1.0 - 1e-6) > R2_eff) continue;
     if (top + 2 > kDStack) return kArmCapacity;
     stack[top++] = t.left;
     stack[top++] = t.right;
