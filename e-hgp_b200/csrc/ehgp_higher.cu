@@ -30,6 +30,8 @@
 //  3. Exact predicates: FP64 with a tracked error bound, then 832-bit integers
 //     at the cloud scale inside the bound.
 #include "ehgp_internal.cuh"
+
+#include <type_traits>
 #include "ehgp_exact.cuh"
 #include "ehgp_sphere.cuh"
 
@@ -1056,10 +1058,10 @@ __device__ float sphere_cut(const QEntry& E, double eA, double eN) {
 }
 
 // Classifies the queued supports against C(a) with the whole warp and emits the relevant ones.
-template <int KC>
+template <int KC, typename Count>
 __device__ __forceinline__ void classify_queue(const OwnerSmemT<KC>& S, WarpQueue& Q, uint32_t qn, uint32_t m, const Cloud& c,
                                uint32_t smax, HigherRec* out, uint32_t cap, uint32_t* counter, uint32_t lane,
-                               unsigned long long& emitted) {
+                               Count& emitted) {
   for (uint32_t e = 0; e < qn; ++e) {
     const QEntry E = Q.q[e];
     const uint32_t icap = smax - (uint32_t)E.size;
@@ -1237,7 +1239,10 @@ __device__ __forceinline__ void higher_owner(uint32_t a, const uint32_t* __restr
   rmax = s_rmax[0];
   for (int w = 1; w < kHOwnerWarps; ++w) rmax = fmaxf(rmax, s_rmax[w]);
   const double rmax2 = (double)rmax * (double)rmax * (1.0 + 1e-12);
-  unsigned long long tested = 0, minimal = 0, pruned = 0, classified = 0, emitted = 0, admitted = 0;
+  // per-lane work counters: 32-bit where a block's share of an owner cannot reach 2^32 (sets of
+  // up to 1,024 candidates, or a chunk of pairs), else 64-bit (registers are the scarce unit)
+  using Count = typename std::conditional<(KC <= 1024), uint32_t, unsigned long long>::type;
+  Count tested = 0, minimal = 0, pruned = 0, classified = 0, emitted = 0, admitted = 0;
   const uint64_t P2 = min((uint64_t)mc * (mc - 1) / 2, t_hi);
   // --- triangles (a, j, k); also the face bound adm(j, k) for the tetrahedra
   for (uint64_t t0 = t_lo + 32 * warp; (phases & kPhTri) && t0 < P2; t0 += 32 * kHOwnerWarps) {
@@ -1354,16 +1359,16 @@ __device__ __forceinline__ void higher_owner(uint32_t a, const uint32_t* __restr
     admitted += __shfl_xor_sync(0xffffffffu, admitted, off);
   }
   if (lane == 0) {
-    atomicAdd(stats + 0, tested);
-    atomicAdd(stats + 1, classified);
-    atomicAdd(stats + 2, emitted);
+    atomicAdd(stats + 0, (unsigned long long)tested);
+    atomicAdd(stats + 1, (unsigned long long)classified);
+    atomicAdd(stats + 2, (unsigned long long)emitted);
     if (warp == 0 && (phases & kPhStats)) {
       atomicAdd(stats + 3, (unsigned long long)m);
       atomicAdd(stats + 4, (unsigned long long)mc);
     }
-    atomicAdd(stats + 5, minimal);
-    atomicAdd(stats + 6, pruned);
-    atomicAdd(stats + 7, admitted);
+    atomicAdd(stats + 5, (unsigned long long)minimal);
+    atomicAdd(stats + 6, (unsigned long long)pruned);
+    atomicAdd(stats + 7, (unsigned long long)admitted);
   }
 }
 
