@@ -979,11 +979,12 @@ struct Ctl {
 #define EHGP_HIGHER_OWNER_WARPS 8
 #endif
 #ifndef EHGP_HIGHER_BLOCKS_PER_SM
-#define EHGP_HIGHER_BLOCKS_PER_SM 3
+#define EHGP_HIGHER_BLOCKS_PER_SM 4
 #endif
 // warps per owner block in k_higher (they share its staged candidate set), and the blocks per
-// SM its register budget is sized for: 65536 / (256 threads x 3 blocks) = 85 per thread, 24 warps
-// per SM (measured at 50k: 4 x 4 blocks 83 ms, 4 x 5 82, 12 x 2 83, 8 x 3 77)
+// SM its register budget is sized for: 65536 / (256 threads x 4 blocks) = 64 per thread, 32 warps
+// per SM (measured at 50k: 8 x 4 blocks 60.1 ms, 8 x 3 63.5, 8 x 2 81.4; earlier builds 4 x 4
+// 83, 4 x 5 82, 12 x 2 83, 8 x 3 77)
 constexpr int kHOwnerWarps = EHGP_HIGHER_OWNER_WARPS;
 constexpr int kHBlocksPerSM = EHGP_HIGHER_BLOCKS_PER_SM;
 constexpr int kCube = 32;       // cube-map cells per face edge for centre directions
