@@ -547,9 +547,10 @@ def run_ours(args, world, rank, local):
         "gpu_launches": int(launches),
         "gpu_launches_per_step": int(launches_per_step),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     # DRAM bytes of one k_higher launch: ncu capture of the 24^3 lattice (58.1 MB read +
-                     # 996.5 MB written per launch over 13,824 owners), scaled per owner to this cloud
-                     "traffic": (58064640 + 996533760) * n / 13824,
+                     # DRAM bytes of one k_higher launch: ncu capture of the 24^3 lattice (102.9 MB read +
+                     # 1,755.9 MB written per launch over 13,824 owners at the 64-register budget),
+                     # scaled per owner to this cloud
+                     "traffic": (102938368 + 1755928576) * n / 13824,
                      "traffic_source": "ncu dram__bytes_read/write.sum on the 13,824-point case, scaled per owner",
                      "kernel": "k_higher (triple/quad support enumeration)",
                      "kernel_ms": kmean, "algorithmic_bytes": alg_bytes,
