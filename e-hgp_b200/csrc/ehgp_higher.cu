@@ -599,7 +599,10 @@ k_gather_big(uint32_t nbig, const uint32_t* __restrict__ big, uint32_t root, con
              const uint32_t* __restrict__ n_end, const double* __restrict__ px, const double* __restrict__ py,
              const double* __restrict__ pz, const double* __restrict__ gather_r2, const uint64_t* __restrict__ off,
              uint32_t* __restrict__ arena, uint32_t* __restrict__ cnt, uint32_t* __restrict__ err) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  // one warp per owner: every lane takes the same walk (warp-uniform branches, broadcast loads);
+  // lane 0 appends single leaves, and a whole subtree inside the radius is copied by the 32
+  // lanes; the list keeps the order of one thread's walk
+  const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
   if (i >= nbig) return;
   const uint32_t a = big[i];
   const double ax = px[a], ay = py[a], az = pz[a];
@@ -617,7 +620,7 @@ k_gather_big(uint32_t nbig, const uint32_t* __restrict__ big, uint32_t root, con
       const uint32_t pid = t.right;
       const double dx = px[pid] - ax, dy = py[pid] - ay, dz = pz[pid] - az;
       if (pid != a && dx * dx + dy * dy + dz * dz <= R2) {
-        if (c < cap) out[c] = pid;
+        if (lane == 0 && c < cap) out[c] = pid;
         ++c;
       }
       continue;
@@ -630,21 +633,26 @@ k_gather_big(uint32_t nbig, const uint32_t* __restrict__ big, uint32_t root, con
     const double uy = fmax(fabs((double)t.lo[1] - ay), fabs((double)t.hi[1] - ay));
     const double uz = fmax(fabs((double)t.lo[2] - az), fabs((double)t.hi[2] - az));
     if ((ux * ux + uy * uy + uz * uz) * (1.0 + 16.0 * kU) < R2) {  // the whole subtree is inside
-      for (uint32_t q = n_begin[node]; q < n_end[node]; ++q) {
-        const uint32_t pid = leaf_pid[q];
-        if (pid == a) continue;
-        if (c < cap) out[c] = pid;
-        ++c;
+      const uint32_t q_hi = n_end[node];
+      for (uint32_t q0 = n_begin[node]; q0 < q_hi; q0 += 32) {
+        const uint32_t q = q0 + lane;
+        const uint32_t pid = q < q_hi ? leaf_pid[q] : kInvalid32;
+        const bool keep = q < q_hi && pid != a;
+        const uint32_t bal = __ballot_sync(0xffffffffu, keep);
+        const uint64_t pos = c + __popc(bal & lanemask_lt());
+        if (keep && pos < cap) out[pos] = pid;
+        c += __popc(bal);
       }
       continue;
     }
     if (top + 2 > kBigStack) {
-      atomicOr(err, kErrCapacity);
+      if (lane == 0) atomicOr(err, kErrCapacity);
       return;
     }
     stack[top++] = t.right;
     stack[top++] = t.left;
   }
+  if (lane != 0) return;
   if (!arena) cnt[i] = (uint32_t)c;
   else if (c != cap) atomicOr(err, kErrInternal);
 }
@@ -1789,7 +1797,7 @@ int gather_big_lists(Ctx& ctx, uint32_t root, const std::vector<uint32_t>& big, 
     h.big_cap = std::min(c1, std::min(c2 - 1, c3));
   }
   cudaMemcpyAsync(h.big_ids, big.data(), (uint64_t)nb * 4, cudaMemcpyHostToDevice, st);
-  k_gather_big<<<nblocks(nb, 128), 128, 0, st>>>(nb, h.big_ids, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end, b.px,
+  k_gather_big<<<nblocks((uint64_t)nb * 32, 128), 128, 0, st>>>(nb, h.big_ids, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end, b.px,
                                                  b.py, b.pz, h.gather_r2, nullptr, nullptr, h.big_cnt, ctx.d_err);
   ++*launches;
   std::vector<uint32_t> cnt(nb);
@@ -1805,7 +1813,7 @@ int gather_big_lists(Ctx& ctx, uint32_t root, const std::vector<uint32_t>& big, 
     return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "the large neighbourhoods do not fit the device");
   }
   cudaMemcpyAsync(h.big_off, off.data(), (uint64_t)(nb + 1) * 8, cudaMemcpyHostToDevice, st);
-  k_gather_big<<<nblocks(nb, 128), 128, 0, st>>>(nb, h.big_ids, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end, b.px,
+  k_gather_big<<<nblocks((uint64_t)nb * 32, 128), 128, 0, st>>>(nb, h.big_ids, root, g.tnodes, b.leaf_pid, b.n_begin, b.n_end, b.px,
                                                  b.py, b.pz, h.gather_r2, h.big_off, h.big_arena, h.big_cnt,
                                                  ctx.d_err);
   ++*launches;
