@@ -62,8 +62,8 @@ constexpr double kTiny = 1e-300;
 constexpr int kMaxFacet = 10;
 constexpr int kT = 256;              // threads per block of the elementwise kernels
 constexpr int kCandCap = 64;         // ball-query candidates per descent step
-constexpr int kDStack = 96;
-constexpr uint32_t kSortQueueMin = 1u << 15;  // descent queues at least this long are sorted spatially          // LBVH traversal stack per descent thread (depth <= 63 + log2 n + 1)
+constexpr int kDStack = 96;          // LBVH traversal stack per descent thread (depth <= 63 + log2 n + 1)
+constexpr uint32_t kSortQueueMin = 1u << 15;  // descent queues at least this long are sorted spatially
 constexpr int kDescentSteps = 512;   // descent steps per arm
 
 // Slow-path counters of the descent (read back per call): [0] exhaustive miniball
