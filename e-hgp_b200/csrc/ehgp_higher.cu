@@ -1997,7 +1997,6 @@ int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   cp.need = smax - 2;
   if (cp.need < 1 || cp.need > (uint32_t)kMaxNeed) return abi_fail(&ctx, EHGP_ERR_INVALID_ARGUMENT, "K above 10 is not supported");
   uint32_t pending = n, overflowed = 0;
-  cudaError_t e0 = cudaSuccess;
   std::vector<uint8_t> todo(n);
   std::vector<uint32_t> big;
   std::vector<uint64_t> big_off;
@@ -2071,13 +2070,13 @@ int higher_run(Ctx& ctx, uint32_t K, uint32_t* out_count) {
   if (h.n_mega) {  // per-block scratch of the mega-set kernel (staged set and face mask)
     const uint64_t bm = std::min<uint64_t>(h.n_mega, (uint64_t)sms);
     const uint64_t need = bm * large_scratch_bytes<kMegaCand, 2>();
-    if ((e0 = grow_array(ctx, h.adm_scratch, h.adm_words, (need + 3) / 4, 4)) != cudaSuccess) {
+    if (grow_array(ctx, h.adm_scratch, h.adm_words, (need + 3) / 4, 4) != cudaSuccess) {
       cudaGetLastError();
       return abi_fail(&ctx, EHGP_ERR_OUT_OF_MEMORY, "the scratch of the huge candidate sets does not fit the device");
     }
   }
   if ((h.n_large || h.n_huge) &&
-      (e0 = grow_array(ctx, h.split_adm, h.split_adm_words,
+      (grow_array(ctx, h.split_adm, h.split_adm_words,
                        std::max((uint64_t)h.n_large * kLargeCand * (kLargeCand / 32),
                                 (uint64_t)h.n_huge * kHugeCand * (kHugeCand / 32)),
                        4)) != cudaSuccess) {
