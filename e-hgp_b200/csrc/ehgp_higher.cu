@@ -1449,7 +1449,10 @@ k_higher_large(uint32_t nown, const uint32_t* __restrict__ owners, const uint64_
 // memory (adm_all, KC * KC / 32 words per owner, zero on entry); the next launch, kPhTet,
 // reads them complete.  An owner's work is its O(m^2) pairs and their tetrahedra, so the
 // large sets spread over every SM instead of one block each.
-constexpr uint32_t kSplitPairs = 8192;
+// pairs per chunk: small chunks keep the tetrahedron launch balanced (its chunks differ widely
+// in admissible tetrahedra); measured on 3k/8k/20k mixtures and a 20k clustered cloud, k_higher
+// 46/116/67/153 ms at 8,192, 29/67/60/93 at 2,048, 28/61/59/90 at 1,024, 29/61/61/92 at 512
+constexpr uint32_t kSplitPairs = 1024;
 template <int KC>
 __global__ void __launch_bounds__(32 * kHOwnerWarps, 2)
 k_higher_split(uint32_t nown, const uint32_t* __restrict__ owners, const uint64_t* __restrict__ coff,
